@@ -1,0 +1,229 @@
+"""Python mirror of IChollet/defmm's ``IBFMM_Mat<3>`` over the C ABI of
+``libdefmm_b200.so`` (include/defmm_b200.h).
+
+Names, argument meaning and call order follow include/interface.hpp:46-224:
+
+    A = IBFMM_Mat()
+    A.addSourceParticlesINP("mesh.inp", n)   # or addSourceParticle(xyz)
+    A.addTargetParticlesINP("mesh.inp", n)
+    A.prcmpt(L, Ncrit, kappa)                 # lvMAX=-1: leaf size criterion
+    gemv(A, In, Out)                          # Out[:] = A @ In (complex128)
+    CheckFULL(A)                              # sampled FP64 direct-sum check
+
+Differences, by design: errors raise ``DefmmError`` (the reference prints and
+exits); every ``gemv`` is correct (the reference's is only on its first call);
+``CheckFULL`` samples targets (the reference sums all N x M pairs).
+There is no CPU fallback: without the built library or without a CUDA device
+the calls that need them raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libdefmm_b200.so")
+_lib = None
+
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
+
+_INFO = {
+    "n_sources": 0, "n_targets": 1, "nlvl": 2, "cpt": 3, "max_stage": 4, "cells_T": 5,
+    "cells_S": 6, "slots_S": 7, "slots_T": 8, "far_hf": 9, "far_lf": 10, "near": 11,
+    "i_near": 12, "tables": 13, "device_bytes": 14, "list_records": 15,
+}
+PHASES = ["p2m", "m2m", "m2f", "m2l", "f2l", "l2l", "l2p", "p2p", "scatter", "total"]
+
+
+class DefmmError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"defmm_b200 error {code}: {msg}")
+        self.code = code
+
+
+def lib():
+    """Load the in-tree CUDA library; raise if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            raise DefmmError(-4, f"{_LIB_PATH} is missing: run defmm_b200.build.build()")
+        L = ctypes.CDLL(_LIB_PATH)
+        vp, dp, ip, i64 = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int32), ctypes.c_int64
+        sig = {
+            "defmm_create": (vp, []),
+            "defmm_destroy": (None, [vp]),
+            "defmm_last_error": (ctypes.c_char_p, [vp]),
+            "defmm_add_source_particle": (ctypes.c_int, [vp, dp]),
+            "defmm_add_target_particle": (ctypes.c_int, [vp, dp]),
+            "defmm_add_sources": (ctypes.c_int, [vp, dp, i64]),
+            "defmm_add_targets": (ctypes.c_int, [vp, dp, i64]),
+            "defmm_load_inp": (ctypes.c_int, [vp, ctypes.c_char_p, i64, ctypes.c_int]),
+            "defmm_prcmpt": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int]),
+            "defmm_upload": (ctypes.c_int, [vp]),
+            "defmm_set_precision": (ctypes.c_int, [vp, ctypes.c_int]),
+            "defmm_gemv": (ctypes.c_int, [vp, dp, dp]),
+            "defmm_gemv_device": (ctypes.c_int, [vp, vp, vp, i64, vp]),
+            "defmm_gemv_batched": (ctypes.c_int, [vp, i64, dp, dp]),
+            "defmm_check_full": (ctypes.c_int, [vp, i64, ctypes.c_uint64, dp]),
+            "defmm_info": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(i64)]),
+            "defmm_phase_times": (ctypes.c_int, [vp, dp]),
+            "defmm_set_profiling": (ctypes.c_int, [vp, ctypes.c_int]),
+            "defmm_keep_lists": (ctypes.c_int, [vp, ctypes.c_int]),
+            "defmm_dump_tree": (ctypes.c_int, [vp, ctypes.c_int, ip, dp, ip, ctypes.POINTER(i64), ip]),
+            "defmm_dump_lists": (ctypes.c_int, [vp, ip, ip, ip, ctypes.POINTER(i64)]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _ip(a):
+    return None if a is None else a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+
+
+class IBFMM_Mat:
+    """FMM operator for exp(i kappa r)/(4 pi r) between source and target
+    point clouds (include/interface.hpp:46)."""
+
+    def __init__(self):
+        self._h = lib().defmm_create()
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib is not None:
+            _lib.defmm_destroy(h)
+            self._h = None
+
+    # -- errors
+    def _check(self, st):
+        if st != 0:
+            raise DefmmError(st, lib().defmm_last_error(self._h).decode())
+
+    # -- particles (interface.hpp:59-98)
+    def addSourceParticle(self, part):
+        a = np.ascontiguousarray(part, dtype=np.float64).reshape(3)
+        self._check(lib().defmm_add_source_particle(self._h, _dp(a)))
+
+    def addTargetParticle(self, part):
+        a = np.ascontiguousarray(part, dtype=np.float64).reshape(3)
+        self._check(lib().defmm_add_target_particle(self._h, _dp(a)))
+
+    def addSourceParticles(self, pts):
+        a = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+        self._check(lib().defmm_add_sources(self._h, _dp(a), a.shape[0]))
+
+    def addTargetParticles(self, pts):
+        a = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+        self._check(lib().defmm_add_targets(self._h, _dp(a), a.shape[0]))
+
+    def addSourceParticlesINP(self, name, nparts):
+        self._check(lib().defmm_load_inp(self._h, os.fsencode(name), int(nparts), 0))
+
+    def addTargetParticlesINP(self, name, nparts):
+        self._check(lib().defmm_load_inp(self._h, os.fsencode(name), int(nparts), 1))
+
+    # -- precomputation (interface.hpp:100-151)
+    def prcmpt(self, L, Ncrit, kappa, lvMAX=-1):
+        self._check(lib().defmm_prcmpt(self._h, int(L), int(Ncrit), float(kappa), int(lvMAX)))
+
+    def upload(self):
+        self._check(lib().defmm_upload(self._h))
+
+    def set_precision(self, mode):
+        if isinstance(mode, str):
+            mode = {"fp64": PRECISION_FP64, "mixed": PRECISION_MIXED}[mode]
+        self._check(lib().defmm_set_precision(self._h, int(mode)))
+
+    def set_profiling(self, on=True):
+        self._check(lib().defmm_set_profiling(self._h, int(bool(on))))
+
+    def keep_lists(self, on=True):
+        self._check(lib().defmm_keep_lists(self._h, int(bool(on))))
+
+    # -- apply
+    def matvec(self, q):
+        q = np.ascontiguousarray(q, dtype=np.complex128)
+        nrhs = 1 if q.ndim == 1 else q.shape[0]
+        out = np.empty((nrhs, self.info("n_targets")), dtype=np.complex128)
+        self._check(lib().defmm_gemv_batched(self._h, nrhs, _dp(q.view(np.float64)), _dp(out.view(np.float64))))
+        return out[0] if q.ndim == 1 else out
+
+    def matvec_device(self, d_in, d_out, nrhs=1, stream=0):
+        """Device pointers (ints, e.g. torch.Tensor.data_ptr()) of complex128
+        vectors in user order; enqueued on `stream` without synchronising."""
+        self._check(lib().defmm_gemv_device(self._h, ctypes.c_void_p(d_in), ctypes.c_void_p(d_out),
+                                            int(nrhs), ctypes.c_void_p(stream) if stream else None))
+
+    def check_full(self, nsamples=2000, seed=7):
+        err = np.zeros(3)
+        self._check(lib().defmm_check_full(self._h, int(nsamples), int(seed), _dp(err)))
+        return {"linf": err[0], "l1": err[1], "l2": err[2]}
+
+    # -- introspection
+    def info(self, what=None):
+        if what is None:
+            return {k: self.info(k) for k in _INFO}
+        v = ctypes.c_int64(0)
+        self._check(lib().defmm_info(self._h, _INFO[what], ctypes.byref(v)))
+        return int(v.value)
+
+    def phase_times(self):
+        ms = np.zeros(10)
+        self._check(lib().defmm_phase_times(self._h, _dp(ms)))
+        return dict(zip(PHASES, ms.tolist()))
+
+    def tree(self, which):
+        """(cells_int (n,8), cells_dbl (n,4), dirs, perm) in the reference's
+        cell-array layout (SourceRoot/TargetRoot, interface.hpp:174-175)."""
+        w = 0 if which == "T" else 1
+        n = self.info("cells_T" if w == 0 else "cells_S")
+        ci = np.zeros((n, 8), np.int32)
+        cd = np.zeros((n, 4), np.float64)
+        nd = ctypes.c_int64(0)
+        self._check(lib().defmm_dump_tree(self._h, w, None, None, None, ctypes.byref(nd), None))
+        dirs = np.zeros(nd.value, np.int32)
+        npart = self.info("n_targets" if w == 0 else "n_sources")
+        perm = np.zeros(npart, np.int32)
+        self._check(lib().defmm_dump_tree(self._h, w, _ip(ci), _dp(cd), _ip(dirs), ctypes.byref(nd), _ip(perm)))
+        return ci, cd, dirs, perm
+
+    def lists(self):
+        n = (ctypes.c_int64 * 3)()
+        self._check(lib().defmm_dump_lists(self._h, None, None, None, n))
+        fh = np.zeros((n[0], 6), np.int32)
+        fl = np.zeros((n[1], 5), np.int32)
+        nr = np.zeros((n[2], 2), np.int32)
+        self._check(lib().defmm_dump_lists(self._h, _ip(fh), _ip(fl), _ip(nr), n))
+        return nr, fh, fl
+
+
+def SourceRoot(A):
+    return A.tree("S")
+
+
+def TargetRoot(A):
+    return A.tree("T")
+
+
+def gemv(A, In, Out):
+    """friend gemv(IBFMM_Mat&, Vecc& In, Vecc& Out) (interface.hpp:153-170)."""
+    Out[...] = A.matvec(In)
+
+
+def CheckFULL(A, nsamples=2000, seed=7):
+    """friend CheckFULL(IBFMM_Mat&) (interface.hpp:178-221), sampled targets."""
+    e = A.check_full(nsamples, seed)
+    print(f"Relative L^oo norm: {e['linf']}")
+    print(f"Relative L^1  norm: {e['l1']}")
+    print(f"Relative L^2  norm: {e['l2']}")
+    return e

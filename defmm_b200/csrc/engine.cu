@@ -1,0 +1,730 @@
+// Operator handle: host plan -> device arrays, matvec orchestration, C ABI.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/defmm_b200.h"
+#include "fmm_kernels.h"
+#include "plan.hpp"
+
+using dfb::DevPlan;
+using dfb::Plan;
+
+namespace {
+
+enum Phase { PH_P2M = 0, PH_M2M, PH_M2F, PH_M2L, PH_F2L, PH_L2L, PH_L2P, PH_P2P, PH_SCATTER, PH_TOTAL, PH_N };
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace
+
+struct defmm_handle {
+  std::vector<double> src, trg;  // user-order coordinates
+  Plan plan;
+  bool built = false;
+  bool uploaded = false;
+  bool keep_lists = false;
+  int precision = DEFMM_PRECISION_FP64;
+  std::string err;
+  // device state
+  int device = -1;
+  cudaStream_t st = nullptr, st2 = nullptr;
+  std::vector<void*> plan_allocs;  // freed when the plan is rebuilt
+  DevPlan dp;
+  const dfb::OpTable* ops = nullptr;
+  int ops_prec = -1;
+  // precision-dependent arrays
+  DevBuf M, Lx, F, J, q, sig, sig2, tables;
+  int64_t fj_cap = 0;  // slots per F / J batch buffer
+  // FP64 vectors
+  DevBuf pnear, pfar, qin, out, chk;
+  const int32_t *d_p2m_leaf = nullptr, *d_l2p_leaf = nullptr;
+  const int32_t *d_tfirst = nullptr, *d_tn = nullptr, *d_sfirst = nullptr, *d_sn = nullptr;
+  const int64_t* d_p2p_ptr = nullptr;
+  int64_t nchunk = 0;
+  size_t dev_bytes = 0;
+  double phase_ms[PH_N] = {0};
+  cudaEvent_t ev[2 * PH_N] = {};
+  cudaEvent_t ev_ready = nullptr, ev_done = nullptr;  // cross-stream ordering
+  bool events = false;
+  bool has_out = false;
+
+  int fail(int code, const std::string& m) {
+    err = m;
+    return code;
+  }
+};
+
+namespace {
+
+#define CK(call)                                                                             \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess) {                                                                 \
+      return h->fail(e_ == cudaErrorMemoryAllocation ? DEFMM_ERR_MEMORY : DEFMM_ERR_CUDA,     \
+                     std::string(#call) + ": " + cudaGetErrorString(e_));                   \
+    }                                                                                        \
+  } while (0)
+
+void free_buf(DevBuf& b) {
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.bytes = 0;
+}
+
+int ensure(defmm_handle* h, DevBuf& b, size_t bytes) {
+  if (b.bytes >= bytes && b.p) return 0;
+  free_buf(b);
+  if (!bytes) return 0;
+  cudaError_t e = cudaMalloc(&b.p, bytes);
+  if (e != cudaSuccess) {
+    b.p = nullptr;
+    cudaGetLastError();
+    return h->fail(DEFMM_ERR_MEMORY, "cudaMalloc of " + std::to_string(bytes) + " bytes: " + cudaGetErrorString(e));
+  }
+  b.bytes = bytes;
+  return 0;
+}
+
+template <typename V>
+int upload(defmm_handle* h, const std::vector<V>& v, const V** out) {
+  *out = nullptr;
+  if (v.empty()) return 0;
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, v.size() * sizeof(V));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return h->fail(DEFMM_ERR_MEMORY, std::string("device allocation failed: ") + cudaGetErrorString(e));
+  }
+  h->plan_allocs.push_back(p);
+  h->dev_bytes += v.size() * sizeof(V);
+  e = cudaMemcpy(p, v.data(), v.size() * sizeof(V), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return h->fail(DEFMM_ERR_CUDA, cudaGetErrorString(e));
+  *out = static_cast<const V*>(p);
+  return 0;
+}
+
+template <typename V>
+std::vector<int32_t> to_i32(const std::vector<V>& v) {
+  return std::vector<int32_t>(v.begin(), v.end());
+}
+
+void free_plan_device(defmm_handle* h) {
+  for (void* p : h->plan_allocs) cudaFree(p);
+  h->plan_allocs.clear();
+  free_buf(h->M);
+  free_buf(h->Lx);
+  free_buf(h->F);
+  free_buf(h->J);
+  free_buf(h->q);
+  free_buf(h->sig);
+  free_buf(h->sig2);
+  free_buf(h->tables);
+  free_buf(h->pnear);
+  free_buf(h->pfar);
+  free_buf(h->qin);
+  free_buf(h->out);
+  free_buf(h->chk);
+  h->ops_prec = -1;
+  h->dev_bytes = 0;
+  h->has_out = false;
+}
+
+int upload_plan(defmm_handle* h) {
+  Plan& p = h->plan;
+  DevPlan& d = h->dp;
+  std::memset(&d, 0, sizeof(d));
+  int st;
+#define UP(vec, field)                         \
+  do {                                         \
+    if ((st = upload(h, (vec), &(field)))) return st; \
+  } while (0)
+  std::vector<double4> c4(p.S.ncell);
+  for (int64_t c = 0; c < p.S.ncell; c++)
+    c4[c] = make_double4(p.S.ctr[3 * c], p.S.ctr[3 * c + 1], p.S.ctr[3 * c + 2], p.S.rad[c]);
+  UP(c4, d.S_ctr);
+  c4.resize(p.T.ncell);
+  for (int64_t c = 0; c < p.T.ncell; c++)
+    c4[c] = make_double4(p.T.ctr[3 * c], p.T.ctr[3 * c + 1], p.T.ctr[3 * c + 2], p.T.rad[c]);
+  UP(c4, d.T_ctr);
+  std::vector<double4>().swap(c4);
+  UP(p.S.first, d.S_first);
+  UP(p.S.nprt, d.S_nprt);
+  UP(p.S.lvl, d.S_lvl);
+  UP(p.T.first, d.T_first);
+  UP(p.T.nprt, d.T_nprt);
+  UP(p.T.lvl, d.T_lvl);
+  UP(p.T.parent, d.T_parent);
+  UP(p.S.pos, d.S_pos);
+  UP(p.T.pos, d.T_pos);
+  UP(p.S.perm, d.S_perm);
+  UP(p.T.perm, d.T_perm);
+  UP(p.sS.cell, d.sS_cell);
+  UP(p.sS.dir, d.sS_dir);
+  UP(p.sT.cell, d.sT_cell);
+  UP(p.sT.dir, d.sT_dir);
+  UP(p.sS.cell_ptr, d.S_cptr);
+  UP(p.sT.cell_ptr, d.T_cptr);
+  UP(to_i32(p.sS.cell_slots), d.S_cslot);
+  UP(p.sS.cell_dirs, d.S_cdir);
+  UP(to_i32(p.sT.cell_slots), d.T_cslot);
+  UP(p.sT.cell_dirs, d.T_cdir);
+  UP(p.m2m_ptr, d.m2m_ptr);
+  UP(p.m2m_child, d.m2m_child);
+  UP(p.l2l_ptr, d.l2l_ptr);
+  UP(p.l2l_parent, d.l2l_parent);
+  UP(p.m2l_ptr, d.m2l_ptr);
+  UP(p.m2l_src, d.m2l_src);
+  UP(p.m2l_tab, d.m2l_tab);
+  UP(p.perm, d.perm);
+  std::vector<double> mats;
+  for (int k = 0; k < 2; k++) mats.insert(mats.end(), p.m2m[k].begin(), p.m2m[k].end());
+  for (int k = 0; k < 2; k++) mats.insert(mats.end(), p.l2l[k].begin(), p.l2l[k].end());
+  UP(mats, d.mats);
+  std::vector<double> dirs;
+  for (size_t e = 0; e < p.dirs.size() && e < 32; e++) {
+    d.dir_off[e] = (int64_t)(dirs.size() / 3);
+    dirs.insert(dirs.end(), p.dirs[e].begin(), p.dirs[e].end());
+  }
+  if (dirs.empty()) dirs.assign(3, 0.);
+  UP(dirs, d.dirs);
+  int64_t off = 0;
+  for (size_t e = 0; e < p.sig.size() && e < 32; e++) {
+    d.sig_off[e] = off;
+    off += (int64_t)p.sig[e].size();
+  }
+  for (int l = 0; l < p.lv.nlvl && l < 32; l++) {
+    d.ishf[l] = (int8_t)(p.lv.isHF[l] ? 1 : 0);
+    d.hfstage[l] = (int8_t)p.lv.HFStage[l];
+  }
+  d.kappa = p.kappa;
+  d.nlvl = p.lv.nlvl;
+  UP(p.p2m_leaf, h->d_p2m_leaf);
+  UP(p.l2p_leaf, h->d_l2p_leaf);
+  UP(p.p2p_tfirst, h->d_tfirst);
+  UP(p.p2p_tn, h->d_tn);
+  UP(p.p2p_ptr, h->d_p2p_ptr);
+  UP(p.p2p_sfirst, h->d_sfirst);
+  UP(p.p2p_sn, h->d_sn);
+  h->nchunk = (int64_t)p.p2p_tfirst.size();
+#undef UP
+  {
+    void* e = nullptr;
+    CK(cudaMalloc(&e, sizeof(int)));
+    h->plan_allocs.push_back(e);
+    CK(cudaMemset(e, 0, sizeof(int)));
+    d.err = static_cast<int*>(e);
+  }
+  int64_t nS = (int64_t)p.S.perm.size(), nT = (int64_t)p.T.perm.size();
+  if ((st = ensure(h, h->pnear, 16 * nT)) || (st = ensure(h, h->pfar, 16 * nT)) ||
+      (st = ensure(h, h->qin, 16 * nS)) || (st = ensure(h, h->out, 16 * nT)))
+    return st;
+  return 0;
+}
+
+// Allocate / convert the arrays whose element type follows the precision.
+int prepare_precision(defmm_handle* h) {
+  if (h->ops_prec == h->precision) return 0;
+  Plan& p = h->plan;
+  const bool fp64 = h->precision == DEFMM_PRECISION_FP64;
+  const size_t cs = fp64 ? 16 : 8;
+  free_buf(h->M);
+  free_buf(h->Lx);
+  free_buf(h->F);
+  free_buf(h->J);
+  free_buf(h->q);
+  free_buf(h->sig);
+  free_buf(h->sig2);
+  free_buf(h->tables);
+  h->ops = dfb::op_table(p.L, fp64);
+  if (!h->ops) return h->fail(DEFMM_ERR_ARG, "unsupported order");
+  CK(h->ops->setup());
+  auto put = [&](DevBuf& b, const dfb::cplx* src, size_t n) -> int {
+    int st = ensure(h, b, std::max<size_t>(1, n) * cs);
+    if (st) return st;
+    if (!n) return 0;
+    if (fp64) {
+      CK(cudaMemcpy(b.p, src, n * 16, cudaMemcpyHostToDevice));
+    } else {
+      std::vector<float> f(2 * n);
+      for (size_t i = 0; i < n; i++) {
+        f[2 * i] = (float)src[i].real();
+        f[2 * i + 1] = (float)src[i].imag();
+      }
+      CK(cudaMemcpy(b.p, f.data(), n * 8, cudaMemcpyHostToDevice));
+    }
+    return 0;
+  };
+  std::vector<dfb::cplx> s1, s2;
+  for (size_t e = 0; e < p.sig.size() && e < 32; e++) {
+    s1.insert(s1.end(), p.sig[e].begin(), p.sig[e].end());
+    s2.insert(s2.end(), p.sig2[e].begin(), p.sig2[e].end());
+  }
+  int st;
+  if ((st = put(h->sig, s1.data(), s1.size())) || (st = put(h->sig2, s2.data(), s2.size())) ||
+      (st = put(h->tables, p.tables.data(), p.tables.size())))
+    return st;
+  const int64_t nS = (int64_t)p.S.perm.size();
+  if ((st = ensure(h, h->M, std::max<int64_t>(1, p.sS.n) * p.LL * cs)) ||
+      (st = ensure(h, h->Lx, std::max<int64_t>(1, p.sT.n) * p.LL * cs)) || (st = ensure(h, h->q, nS * cs)))
+    return st;
+  // F / J batch buffers: at least the largest cone of any level, at most
+  // about half of the free memory
+  int64_t need = 1, want = 0;
+  for (int l = 0; l < p.lv.nlvl; l++) {
+    const auto& cS = p.sS.cone_begin[l];
+    const auto& cT = p.sT.cone_begin[l];
+    for (size_t c = 0; c + 1 < cS.size(); c++) need = std::max(need, cS[c + 1] - cS[c]);
+    for (size_t c = 0; c + 1 < cT.size(); c++) need = std::max(need, cT[c + 1] - cT[c]);
+    want = std::max(want, std::max(cS.back() - cS.front(), cT.back() - cT.front()));
+  }
+  size_t fr = 0, tot = 0;
+  CK(cudaMemGetInfo(&fr, &tot));
+  const size_t per = (size_t)p.PP * cs;
+  int64_t cap = (int64_t)((fr * 0.45) / (2 * per));
+  cap = std::min<int64_t>(cap, (int64_t)((size_t)48 << 30) / (int64_t)per);
+  cap = std::min(cap, std::max(want, need));
+  if (cap < need) return h->fail(DEFMM_ERR_MEMORY, "not enough device memory for one cone of spectra");
+  h->fj_cap = cap;
+  if ((st = ensure(h, h->F, cap * per)) || (st = ensure(h, h->J, cap * per))) return st;
+  h->ops_prec = h->precision;
+  return 0;
+}
+
+void rec(defmm_handle* h, int i) {
+  if (h->events) cudaEventRecord(h->ev[i], h->st);
+}
+
+// One matvec, everything on the device: qin (user order) -> out (user order).
+int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) {
+  Plan& p = h->plan;
+  const bool fp64 = h->precision == DEFMM_PRECISION_FP64;
+  const DevPlan& d = h->dp;
+  const dfb::OpTable* ops = h->ops;
+  const int64_t nS = (int64_t)p.S.perm.size(), nT = (int64_t)p.T.perm.size();
+  const int nl = p.lv.nlvl;
+  h->st = s;
+  rec(h, 2 * PH_TOTAL);
+  rec(h, 2 * PH_P2M);
+  dfb::launch_gather(fp64, qin, d.S_perm, h->q.p, nS, 0, 0, 1, s);
+  CK(cudaMemsetAsync(h->pfar.p, 0, 16 * nT, s));
+  CK(cudaMemsetAsync(h->pnear.p, 0, 16 * nT, s));
+  CK(cudaMemsetAsync(h->Lx.p, 0, h->Lx.bytes, s));
+  // near field on the second stream, overlapping the far field
+  cudaEvent_t ready = h->ev_ready;
+  CK(cudaEventRecord(ready, s));
+  CK(cudaStreamWaitEvent(h->st2, ready, 0));
+  if (h->events) cudaEventRecord(h->ev[2 * PH_P2P], h->st2);
+  if (fp64)
+    dfb::launch_p2p_fp64(d, h->nchunk, h->d_tfirst, h->d_tn, h->d_p2p_ptr, h->d_sfirst, h->d_sn,
+                         (const double2*)h->q.p, (double2*)h->pnear.p, h->st2);
+  else
+    return h->fail(DEFMM_ERR_ARG, "mixed precision P2P not available");
+  if (h->events) cudaEventRecord(h->ev[2 * PH_P2P + 1], h->st2);
+  // upward pass
+  ops->p2m(d, h->d_p2m_leaf, (int)p.p2m_leaf.size(), h->q.p, h->sig2.p, h->M.p, s);
+  rec(h, 2 * PH_P2M + 1);
+  rec(h, 2 * PH_M2M);
+  for (int l = nl - 2; l >= p.lv.max_stage; l--)
+    ops->m2m(d, p.sS.lvl_begin[l], p.sS.lvl_begin[l + 1], h->sig.p, h->sig2.p, h->M.p, s);
+  rec(h, 2 * PH_M2M + 1);
+  // far field per level and cone batch, then the downward transfer
+  float tm2f = 0, tm2l = 0, tf2l = 0, tl2l = 0;
+  const size_t cs = fp64 ? 16 : 8;
+  for (int l = p.lv.max_stage; l < nl; l++) {
+    const auto& cS = p.sS.cone_begin[l];
+    const auto& cT = p.sT.cone_begin[l];
+    const int nc = (int)cS.size() - 1;
+    int c0 = 0;
+    while (c0 < nc) {
+      int c1 = c0 + 1;
+      while (c1 < nc && cS[c1 + 1] - cS[c0] <= h->fj_cap && cT[c1 + 1] - cT[c0] <= h->fj_cap) c1++;
+      const int64_t fs0 = cS[c0], fs1 = cS[c1], ts0 = cT[c0], ts1 = cT[c1];
+      if (ts1 > ts0 && fs1 > fs0) {
+        rec(h, 2 * PH_M2F);
+        ops->m2f(fs1 - fs0, (const char*)h->M.p + fs0 * p.LL * cs, h->F.p, s);
+        rec(h, 2 * PH_M2F + 1);
+        rec(h, 2 * PH_M2L);
+        ops->m2l(d, ts0, ts1, fs0, fs1, h->F.p, h->tables.p, h->J.p, s);
+        rec(h, 2 * PH_M2L + 1);
+        rec(h, 2 * PH_F2L);
+        ops->f2l(ts1 - ts0, h->J.p, (char*)h->Lx.p + ts0 * p.LL * cs, s);
+        rec(h, 2 * PH_F2L + 1);
+        if (h->events) {
+          float a;
+          CK(cudaEventSynchronize(h->ev[2 * PH_F2L + 1]));
+          cudaEventElapsedTime(&a, h->ev[2 * PH_M2F], h->ev[2 * PH_M2F + 1]);
+          tm2f += a;
+          cudaEventElapsedTime(&a, h->ev[2 * PH_M2L], h->ev[2 * PH_M2L + 1]);
+          tm2l += a;
+          cudaEventElapsedTime(&a, h->ev[2 * PH_F2L], h->ev[2 * PH_F2L + 1]);
+          tf2l += a;
+        }
+      }
+      c0 = c1;
+    }
+    if (l + 1 < nl) {
+      rec(h, 2 * PH_L2L);
+      ops->l2l(d, p.sT.lvl_begin[l + 1], p.sT.lvl_begin[l + 2], h->sig.p, h->sig2.p, h->Lx.p, s);
+      rec(h, 2 * PH_L2L + 1);
+      if (h->events) {
+        float a;
+        CK(cudaEventSynchronize(h->ev[2 * PH_L2L + 1]));
+        cudaEventElapsedTime(&a, h->ev[2 * PH_L2L], h->ev[2 * PH_L2L + 1]);
+        tl2l += a;
+      }
+    }
+  }
+  rec(h, 2 * PH_L2P);
+  ops->l2p(d, h->d_l2p_leaf, (int)p.l2p_leaf.size(), h->sig2.p, h->Lx.p, (double2*)h->pfar.p, s);
+  rec(h, 2 * PH_L2P + 1);
+  cudaEvent_t done = h->ev_done;
+  CK(cudaEventRecord(done, h->st2));
+  CK(cudaStreamWaitEvent(s, done, 0));
+  rec(h, 2 * PH_SCATTER);
+  dfb::launch_scatter((const double2*)h->pnear.p, (const double2*)h->pfar.p, d.T_perm, out, nT, s);
+  rec(h, 2 * PH_SCATTER + 1);
+  rec(h, 2 * PH_TOTAL + 1);
+  CK(cudaGetLastError());
+  if (h->events) {
+    CK(cudaStreamSynchronize(s));
+    auto el = [&](int ph) {
+      float a = 0;
+      cudaEventElapsedTime(&a, h->ev[2 * ph], h->ev[2 * ph + 1]);
+      return (double)a;
+    };
+    for (int i = 0; i < PH_N; i++) h->phase_ms[i] = 0;
+    h->phase_ms[PH_P2M] = el(PH_P2M);
+    h->phase_ms[PH_M2M] = el(PH_M2M);
+    h->phase_ms[PH_M2F] = tm2f;
+    h->phase_ms[PH_M2L] = tm2l;
+    h->phase_ms[PH_F2L] = tf2l;
+    h->phase_ms[PH_L2L] = tl2l;
+    h->phase_ms[PH_L2P] = el(PH_L2P);
+    h->phase_ms[PH_P2P] = el(PH_P2P);
+    h->phase_ms[PH_SCATTER] = el(PH_SCATTER);
+    h->phase_ms[PH_TOTAL] = el(PH_TOTAL);
+  }
+  return 0;
+}
+
+int ensure_device(defmm_handle* h) {
+  if (h->device >= 0) return 0;
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return h->fail(DEFMM_ERR_CUDA, "no CUDA device available");
+  }
+  CK(cudaGetDevice(&h->device));
+  CK(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&h->st2, cudaStreamNonBlocking));
+  for (int i = 0; i < 2 * PH_N; i++) CK(cudaEventCreate(&h->ev[i]));
+  CK(cudaEventCreateWithFlags(&h->ev_ready, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&h->ev_done, cudaEventDisableTiming));
+  return 0;
+}
+
+uint64_t splitmix(uint64_t& s) {
+  uint64_t z = (s += 0x9e3779b97f4a7c15ULL);
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+  return z ^ (z >> 31);
+}
+
+}  // namespace
+
+// ==================================================================== C ABI
+extern "C" {
+
+defmm_handle* defmm_create(void) { return new defmm_handle(); }
+
+void defmm_destroy(defmm_handle* h) {
+  if (!h) return;
+  if (h->device >= 0) {
+    cudaSetDevice(h->device);
+    free_plan_device(h);
+    for (int i = 0; i < 2 * PH_N; i++)
+      if (h->ev[i]) cudaEventDestroy(h->ev[i]);
+    if (h->ev_ready) cudaEventDestroy(h->ev_ready);
+    if (h->ev_done) cudaEventDestroy(h->ev_done);
+    if (h->st) cudaStreamDestroy(h->st);
+    if (h->st2) cudaStreamDestroy(h->st2);
+  }
+  delete h;
+}
+
+const char* defmm_last_error(const defmm_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+int defmm_add_source_particle(defmm_handle* h, const double xyz[3]) {
+  if (!h || !xyz) return DEFMM_ERR_ARG;
+  h->src.insert(h->src.end(), xyz, xyz + 3);
+  return 0;
+}
+int defmm_add_target_particle(defmm_handle* h, const double xyz[3]) {
+  if (!h || !xyz) return DEFMM_ERR_ARG;
+  h->trg.insert(h->trg.end(), xyz, xyz + 3);
+  return 0;
+}
+int defmm_add_sources(defmm_handle* h, const double* xyz, int64_t n) {
+  if (!h || (n > 0 && !xyz) || n < 0) return DEFMM_ERR_ARG;
+  h->src.insert(h->src.end(), xyz, xyz + 3 * n);
+  return 0;
+}
+int defmm_add_targets(defmm_handle* h, const double* xyz, int64_t n) {
+  if (!h || (n > 0 && !xyz) || n < 0) return DEFMM_ERR_ARG;
+  h->trg.insert(h->trg.end(), xyz, xyz + 3 * n);
+  return 0;
+}
+
+int defmm_load_inp(defmm_handle* h, const char* path, int64_t nparts, int which) {
+  if (!h || !path || nparts < 0 || (which != 0 && which != 1)) return DEFMM_ERR_ARG;
+  FILE* f = std::fopen(path, "r");
+  if (!f) return h->fail(DEFMM_ERR_IO, std::string("cannot open ") + path);
+  std::vector<double> v(3 * nparts);
+  for (int64_t i = 0; i < 3 * nparts; i++)
+    if (std::fscanf(f, "%lf", &v[i]) != 1) {
+      std::fclose(f);
+      return h->fail(DEFMM_ERR_IO, std::string("short INP file ") + path);
+    }
+  std::fclose(f);
+  auto& dst = which == 0 ? h->src : h->trg;
+  dst.insert(dst.end(), v.begin(), v.end());
+  return 0;
+}
+
+int defmm_set_profiling(defmm_handle* h, int on) {
+  if (!h) return DEFMM_ERR_ARG;
+  h->events = on != 0;
+  return 0;
+}
+
+int defmm_keep_lists(defmm_handle* h, int on) {
+  if (!h) return DEFMM_ERR_ARG;
+  h->keep_lists = on != 0;
+  return 0;
+}
+
+int defmm_prcmpt(defmm_handle* h, int L, int Ncrit, double kappa, int lvMAX) {
+  if (!h) return DEFMM_ERR_ARG;
+  if (h->src.empty() || h->trg.empty()) return h->fail(DEFMM_ERR_ARG, "no source or no target particles");
+  if (!(kappa >= 0.) || !std::isfinite(kappa)) return h->fail(DEFMM_ERR_ARG, "wavenumber must be finite and >= 0");
+  if (h->device >= 0) {
+    CK(cudaSetDevice(h->device));
+    free_plan_device(h);
+  }
+  h->built = false;
+  h->uploaded = false;
+  h->plan = Plan();
+  h->plan.keep_lists = h->keep_lists;
+  std::string e;
+  int st = dfb::build_plan(h->plan, h->src.data(), (int64_t)h->src.size() / 3, h->trg.data(),
+                           (int64_t)h->trg.size() / 3, L, Ncrit, kappa, lvMAX, e);
+  if (st) return h->fail(st, e);
+  if (h->plan.lv.nlvl > 32) return h->fail(DEFMM_ERR_DEPTH, "more than 32 tree levels");
+  h->built = true;
+  return 0;
+}
+
+int defmm_upload(defmm_handle* h) {
+  if (!h) return DEFMM_ERR_ARG;
+  if (!h->built) return h->fail(DEFMM_ERR_ARG, "upload before prcmpt");
+  int st = ensure_device(h);
+  if (st) return st;
+  CK(cudaSetDevice(h->device));
+  if (h->uploaded) return 0;
+  st = upload_plan(h);
+  if (st) return st;
+  h->uploaded = true;
+  return 0;
+}
+
+int defmm_set_precision(defmm_handle* h, int mode) {
+  if (!h || (mode != DEFMM_PRECISION_FP64 && mode != DEFMM_PRECISION_MIXED)) return DEFMM_ERR_ARG;
+  h->precision = mode;
+  return 0;
+}
+
+int defmm_gemv_device(defmm_handle* h, const void* d_in, void* d_out, int64_t nrhs, void* stream) {
+  if (!h || !d_in || !d_out || nrhs < 1) return DEFMM_ERR_ARG;
+  if (!h->built) return h->fail(DEFMM_ERR_ARG, "gemv before prcmpt");
+  int st = defmm_upload(h);
+  if (st) return st;
+  st = prepare_precision(h);
+  if (st) return st;
+  cudaStream_t s = stream ? (cudaStream_t)stream : h->st;
+  const int64_t nS = (int64_t)h->plan.S.perm.size(), nT = (int64_t)h->plan.T.perm.size();
+  for (int64_t r = 0; r < nrhs; r++) {
+    st = run_gemv(h, (const double2*)d_in + r * nS, (double2*)d_out + r * nT, s);
+    if (st) return st;
+  }
+  return 0;
+}
+
+int defmm_gemv_batched(defmm_handle* h, int64_t nrhs, const double* in, double* out) {
+  if (!h || !in || !out || nrhs < 1) return DEFMM_ERR_ARG;
+  if (!h->built) return h->fail(DEFMM_ERR_ARG, "gemv before prcmpt");
+  int st = defmm_upload(h);
+  if (st) return st;
+  st = prepare_precision(h);
+  if (st) return st;
+  const int64_t nS = (int64_t)h->plan.S.perm.size(), nT = (int64_t)h->plan.T.perm.size();
+  for (int64_t r = 0; r < nrhs; r++) {
+    CK(cudaMemcpyAsync(h->qin.p, in + 2 * r * nS, 16 * nS, cudaMemcpyHostToDevice, h->st));
+    st = run_gemv(h, (const double2*)h->qin.p, (double2*)h->out.p, h->st);
+    if (st) return st;
+    CK(cudaMemcpyAsync(out + 2 * r * nT, h->out.p, 16 * nT, cudaMemcpyDeviceToHost, h->st));
+  }
+  CK(cudaStreamSynchronize(h->st));
+  int flag = 0;
+  CK(cudaMemcpy(&flag, h->dp.err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (flag) return h->fail(DEFMM_ERR_ARG, "inconsistent interaction list detected on the device");
+  h->has_out = true;
+  return 0;
+}
+
+int defmm_gemv(defmm_handle* h, const double* in, double* out) { return defmm_gemv_batched(h, 1, in, out); }
+
+int defmm_check_full(defmm_handle* h, int64_t nsamples, uint64_t seed, double err[3]) {
+  if (!h || !err || nsamples < 1) return DEFMM_ERR_ARG;
+  if (!h->built || !h->has_out) return h->fail(DEFMM_ERR_ARG, "check before a host gemv");
+  CK(cudaSetDevice(h->device));
+  const int64_t nS = (int64_t)h->plan.S.perm.size(), nT = (int64_t)h->plan.T.perm.size();
+  nsamples = std::min(nsamples, nT);
+  // seeded partial Fisher-Yates over target indices
+  std::vector<int64_t> idx(nT);
+  for (int64_t i = 0; i < nT; i++) idx[i] = i;
+  uint64_t s = seed;
+  for (int64_t i = 0; i < nsamples; i++) {
+    int64_t j = i + (int64_t)(splitmix(s) % (uint64_t)(nT - i));
+    std::swap(idx[i], idx[j]);
+  }
+  idx.resize(nsamples);
+  std::sort(idx.begin(), idx.end());
+  std::vector<double> tpos(3 * nsamples);
+  for (int64_t i = 0; i < nsamples; i++)
+    for (int k = 0; k < 3; k++) tpos[3 * i + k] = h->trg[3 * idx[i] + k];
+  int st = ensure(h, h->chk, (size_t)nsamples * 40);
+  if (st) return st;
+  double* d_tpos = (double*)h->chk.p;
+  double2* d_res = (double2*)((char*)h->chk.p + 24 * nsamples);
+  CK(cudaMemcpy(d_tpos, tpos.data(), 24 * nsamples, cudaMemcpyHostToDevice));
+  dfb::launch_direct(nS, h->dp.S_pos, h->dp.S_perm, (const double2*)h->qin.p, nsamples, d_tpos, h->plan.kappa,
+                     d_res, h->st);
+  CK(cudaGetLastError());
+  std::vector<double> ex(2 * nsamples), fm(2 * nT);
+  CK(cudaMemcpyAsync(ex.data(), d_res, 16 * nsamples, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaMemcpyAsync(fm.data(), h->out.p, 16 * nT, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  // gaia_vectors.hpp:119-172 norms
+  double ainf = 0, binf = 0, a1 = 0, b1 = 0, a2 = 0, b2 = 0;
+  for (int64_t i = 0; i < nsamples; i++) {
+    const double er = ex[2 * i] - fm[2 * idx[i]], ei = ex[2 * i + 1] - fm[2 * idx[i] + 1];
+    const double d = std::hypot(er, ei), m = std::hypot(ex[2 * i], ex[2 * i + 1]);
+    ainf = std::max(ainf, d);
+    binf = std::max(binf, m);
+    a1 += d;
+    b1 += m;
+    a2 += d * d;
+    b2 += m * m;
+  }
+  err[0] = ainf / binf;
+  err[1] = a1 / b1;
+  err[2] = std::sqrt(a2 / b2);
+  return 0;
+}
+
+int defmm_info(const defmm_handle* h, int what, int64_t* v) {
+  if (!h || !v) return DEFMM_ERR_ARG;
+  const Plan& p = h->plan;
+  switch (what) {
+    case DEFMM_INFO_N_SOURCES: *v = (int64_t)h->src.size() / 3; return 0;
+    case DEFMM_INFO_N_TARGETS: *v = (int64_t)h->trg.size() / 3; return 0;
+    default: break;
+  }
+  if (!h->built) return DEFMM_ERR_ARG;
+  switch (what) {
+    case DEFMM_INFO_NLVL: *v = p.lv.nlvl; break;
+    case DEFMM_INFO_CPT: *v = p.lv.cpt; break;
+    case DEFMM_INFO_MAX_STAGE: *v = p.lv.max_stage; break;
+    case DEFMM_INFO_CELLS_T: *v = p.T.ncell; break;
+    case DEFMM_INFO_CELLS_S: *v = p.S.ncell; break;
+    case DEFMM_INFO_SLOTS_S: *v = p.sS.n; break;
+    case DEFMM_INFO_SLOTS_T: *v = p.sT.n; break;
+    case DEFMM_INFO_FAR_HF: *v = p.n_far_hf; break;
+    case DEFMM_INFO_FAR_LF: *v = p.n_far_lf; break;
+    case DEFMM_INFO_NEAR: *v = p.n_near; break;
+    case DEFMM_INFO_I_NEAR: *v = p.i_near; break;
+    case DEFMM_INFO_TABLES: *v = (int64_t)p.tab_lvl.size(); break;
+    case DEFMM_INFO_DEVICE_BYTES:
+      *v = (int64_t)(h->dev_bytes + h->M.bytes + h->Lx.bytes + h->F.bytes + h->J.bytes + h->q.bytes +
+                     h->sig.bytes + h->sig2.bytes + h->tables.bytes + h->pnear.bytes + h->pfar.bytes +
+                     h->qin.bytes + h->out.bytes);
+      break;
+    case DEFMM_INFO_LIST_RECORDS: *v = p.keep_lists ? 1 : 0; break;
+    default: return DEFMM_ERR_ARG;
+  }
+  return 0;
+}
+
+int defmm_phase_times(const defmm_handle* h, double ms[10]) {
+  if (!h || !ms) return DEFMM_ERR_ARG;
+  for (int i = 0; i < PH_N; i++) ms[i] = h->phase_ms[i];
+  return 0;
+}
+
+int defmm_dump_tree(const defmm_handle* h, int which, int32_t* ci, double* cd, int32_t* dirs, int64_t* ndirs,
+                    int32_t* perm) {
+  if (!h || !h->built || (which != 0 && which != 1)) return DEFMM_ERR_ARG;
+  const dfb::Tree& t = which ? h->plan.S : h->plan.T;
+  const dfb::Slots& s = which ? h->plan.sS : h->plan.sT;
+  int64_t nd = 0;
+  for (int64_t c = 0; c < t.ncell; c++) {
+    if (ci) {
+      int32_t* r = ci + 8 * c;
+      r[0] = t.idx[3 * c];
+      r[1] = t.idx[3 * c + 1];
+      r[2] = t.idx[3 * c + 2];
+      r[3] = t.lvl[c];
+      r[4] = t.nprt[c];
+      r[5] = t.first[c];
+      r[6] = t.nson[c];
+      r[7] = (int32_t)(s.cell_ptr[c + 1] - s.cell_ptr[c]);
+    }
+    if (cd) {
+      cd[4 * c] = t.ctr[3 * c];
+      cd[4 * c + 1] = t.ctr[3 * c + 1];
+      cd[4 * c + 2] = t.ctr[3 * c + 2];
+      cd[4 * c + 3] = t.rad[c];
+    }
+    for (int64_t j = s.cell_ptr[c]; j < s.cell_ptr[c + 1]; j++)
+      if (s.cell_dirs[j] >= 0) {
+        if (dirs) dirs[nd] = s.cell_dirs[j];
+        nd++;
+      }
+  }
+  if (ndirs) *ndirs = nd;
+  if (perm) std::memcpy(perm, t.perm.data(), t.perm.size() * 4);
+  return 0;
+}
+
+int defmm_dump_lists(const defmm_handle* h, int32_t* far_hf, int32_t* far_lf, int32_t* near_, int64_t n[3]) {
+  if (!h || !h->built || !n) return DEFMM_ERR_ARG;
+  const Plan& p = h->plan;
+  n[0] = (int64_t)p.rec_far_hf.size() / 6;
+  n[1] = (int64_t)p.rec_far_lf.size() / 5;
+  n[2] = (int64_t)p.rec_near.size() / 2;
+  if (far_hf) std::memcpy(far_hf, p.rec_far_hf.data(), p.rec_far_hf.size() * 4);
+  if (far_lf) std::memcpy(far_lf, p.rec_far_lf.data(), p.rec_far_lf.size() * 4);
+  if (near_) std::memcpy(near_, p.rec_near.data(), p.rec_near.size() * 4);
+  return 0;
+}
+
+}  // extern "C"

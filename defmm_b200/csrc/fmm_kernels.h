@@ -1,0 +1,37 @@
+// Host-visible launchers of the matvec kernels (fmm_kernels.cu).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "kernels.cuh"
+
+namespace dfb {
+
+// Per-(precision, order) launchers of the expansion phases.  Complex arrays
+// are passed untyped; their element type is double2 (FP64) or float2.
+struct OpTable {
+  cudaError_t (*setup)();
+  void (*p2m)(const DevPlan&, const int32_t* leaves, int n, const void* q, const void* sig2, void* M, cudaStream_t);
+  void (*m2m)(const DevPlan&, int64_t s0, int64_t s1, const void* sig, const void* sig2, void* M, cudaStream_t);
+  void (*l2l)(const DevPlan&, int64_t s0, int64_t s1, const void* sig, const void* sig2, void* Lx, cudaStream_t);
+  void (*m2f)(int64_t n, const void* M, void* F, cudaStream_t);
+  void (*f2l)(int64_t n, const void* J, void* Lx, cudaStream_t);
+  void (*m2l)(const DevPlan&, int64_t t0, int64_t t1, int64_t f0, int64_t f1, const void* F, const void* tables,
+              void* J, cudaStream_t);
+  void (*l2p)(const DevPlan&, const int32_t* leaves, int n, const void* sig2, const void* Lx, double2* pfar,
+              cudaStream_t);
+};
+
+const OpTable* op_table(int L, bool fp64);
+
+void launch_gather(bool fp64, const double2* qin, const int32_t* perm, void* q, int64_t n, int64_t stride_in,
+                   int64_t stride_q, int nrhs, cudaStream_t s);
+void launch_scatter(const double2* pnear, const double2* pfar, const int32_t* perm, double2* out, int64_t n,
+                    cudaStream_t s);
+void launch_p2p_fp64(const DevPlan& dp, int64_t nchunk, const int32_t* tfirst, const int32_t* tn, const int64_t* ptr,
+                     const int32_t* sfirst, const int32_t* sn, const double2* q, double2* pnear, cudaStream_t s);
+void launch_direct(int64_t ns, const double* spos, const int32_t* sperm, const double2* qin, int64_t nt,
+                   const double* tpos, double kappa, double2* out, cudaStream_t s);
+
+}  // namespace dfb

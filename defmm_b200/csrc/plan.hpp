@@ -1,0 +1,118 @@
+// Host-side plan of one directional FMM operator: octrees, frequency regime,
+// direction (cone) tables, interaction lists, expansion slots and transfer
+// spectra, laid out for the device kernels.
+//
+// Everything here follows the semantics of IChollet/defmm's precomputation
+// (include/interface.hpp:100-151) bit-exactly where the result is discrete
+// (trees, admissibility, cones, effective directions); the construction itself
+// is level-wise and multi-threaded instead of the reference's recursions.
+#pragma once
+
+#include <complex>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace dfb {
+
+typedef std::complex<double> cplx;
+
+// One octree, cells in depth-first pre-order (the reference's cell array
+// order, sort.hpp:187-220), particles in tree order.
+struct Tree {
+  int64_t ncell = 0;
+  int nlvl = 0;
+  std::vector<int32_t> idx;        // 3 per cell: integer coordinates at its level
+  std::vector<int32_t> lvl, nprt, first, parent, nson;
+  std::vector<int64_t> son_ptr;    // CSR into sons (ncell + 1)
+  std::vector<int32_t> sons;
+  std::vector<int32_t> sub_end;    // one past the last cell of the subtree (DFS)
+  std::vector<double> ctr;         // 3 per cell
+  std::vector<double> rad;
+  std::vector<int32_t> perm;       // tree order position -> user index
+  std::vector<double> pos;         // 3 per particle, tree order
+  std::vector<int64_t> lvl_cells;  // cells per level
+  bool leaf(int64_t c) const { return nson[c] == 0; }
+};
+
+// Per-level frequency regime (frequency.hpp:44-184).
+struct Levels {
+  int nlvl = 0, cpt = 0, max_stage = 0;
+  bool noHF = true;
+  std::vector<int> isHF, HFStage, nDir, nCellMax;
+  std::vector<char> prec;
+};
+
+// Expansion slots of one tree: one per (cell, effective direction) at
+// precomputed HF levels, one per cell at precomputed LF levels.  Slots are
+// ordered level-major, then cone-major, then by cell (DFS order), so one cone
+// of one level is a contiguous slot range.
+struct Slots {
+  int64_t n = 0;
+  std::vector<int32_t> cell, dir;          // per slot (dir = -1 for LF)
+  std::vector<int64_t> lvl_begin;          // nlvl + 1
+  std::vector<std::vector<int64_t>> cone_begin;  // per level: nDir + 1 offsets
+  // per cell: effective directions in increasing order with their slots
+  std::vector<int64_t> cell_ptr;           // ncell + 1 into cell_dirs / cell_slots
+  std::vector<int32_t> cell_dirs;
+  std::vector<int64_t> cell_slots;
+  int64_t slot_of(int64_t c, int d) const;  // -1 when absent; d = -1 for LF
+};
+
+struct Plan {
+  // parameters
+  int L = 0, P = 0, LL = 0, PP = 0, ncrit = 0, lvmax = -1;
+  double kappa = 0.;
+  double box_ctr[3] = {0, 0, 0}, box_rad = 0.;
+  Tree S, T;
+  Levels lv;
+  // direction tables per HF stage: 6*4^e unit vectors (newdirections.hpp:76-171)
+  std::vector<std::vector<double>> dirs;  // [stage][3*i]
+  // plane-wave signature grids per HF stage (planewave.hpp:44-69): [stage][d*LL + k]
+  std::vector<std::vector<cplx>> sig, sig2;
+  // separable interpolation matrices (interpolation.hpp:184-242), L x L column-major
+  std::vector<double> m2m[2], l2l[2];
+  // circulant embedding (circulant.hpp:47-93) and spectrum permutations
+  // (permutations.hpp:128-150)
+  std::vector<int32_t> itilda;             // LL
+  std::vector<double> tabZ;                // 3*PP
+  std::vector<uint16_t> perm;              // 64*PP
+  Slots sS, sT;
+  // transfer spectra: one per distinct (level, fundamental index)
+  std::vector<int32_t> tab_lvl;
+  std::vector<int64_t> tab_iz;
+  std::vector<cplx> tables;                // ntab * PP
+  // M2L, grouped by target slot (CSR over target slots)
+  std::vector<int64_t> m2l_ptr;            // sT.n + 1
+  std::vector<int32_t> m2l_src;            // source slot
+  std::vector<uint32_t> m2l_tab;           // (table index << 6) | hash
+  // M2M children of each source slot, L2L parents of each target slot
+  std::vector<int64_t> m2m_ptr;            // sS.n + 1
+  std::vector<int32_t> m2m_child;          // child slot
+  std::vector<int64_t> l2l_ptr;            // sT.n + 1
+  std::vector<int32_t> l2l_parent;         // parent slot
+  // leaves at precomputed levels (P2M sources / L2P targets)
+  std::vector<int32_t> p2m_leaf, l2p_leaf;
+  // near field, grouped by target leaf chunk (<= 32 targets per chunk)
+  std::vector<int32_t> p2p_tfirst, p2p_tn;   // per chunk
+  std::vector<int64_t> p2p_ptr;              // chunks + 1
+  std::vector<int32_t> p2p_sfirst, p2p_sn;   // source particle ranges
+  // statistics
+  int64_t n_far_hf = 0, n_far_lf = 0, n_near = 0, i_near = 0;
+  // Optional record of the lists for parity checks: far (t, s, lvl, cone,
+  // iz, hash) and near (t, s) in the reference's HorizontalPass order.
+  bool keep_lists = false;
+  std::vector<int32_t> rec_far_hf, rec_far_lf, rec_near;
+  double t_tree = 0, t_lists = 0, t_tables = 0;
+};
+
+// Build the plan; returns 0 or a negative status with `err` set.
+//   -2: coincident points keep a cell above ncrit (the reference recurses
+//       without end, sort.hpp:98-162)
+//   -3: the tree is too shallow for any M2L level (frequency.hpp:114-120)
+//   -1: invalid arguments
+int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
+               int64_t nt, int L, int ncrit, double kappa, int lvmax,
+               std::string& err);
+
+}  // namespace dfb

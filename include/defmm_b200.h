@@ -1,0 +1,154 @@
+/*
+ * defmm_b200 -- C ABI of a B200 (sm_100a) implementation of defmm's
+ * directional equispaced-interpolation FMM matvec for the Helmholtz kernel
+ * G(x, y) = exp(i k |x - y|) / (4 pi |x - y|)  (pairs with |x - y|^2 < 1e-16
+ * contribute nothing, as in the reference's P2P.hpp:66).
+ *
+ * The entry points replace the public interface of IChollet/defmm's
+ * `defmm::IBFMM_Mat<3>` (include/interface.hpp:46-224); each declaration cites
+ * the member it replaces.  Differences from the reference, by design:
+ *   - errors are returned as negative status codes (the reference prints and
+ *     calls exit(1)); defmm_last_error() gives the message;
+ *   - every defmm_gemv is correct (the reference's gemv never clears its
+ *     non-leaf expansions, interface.hpp:159, so only its first call is);
+ *   - handles are independent (the reference keeps process-global state).
+ * Complex vectors are interleaved (re, im) doubles, indexed in the user's
+ * particle order, like the reference's Vecc (std::complex<double>).
+ * A handle is not thread-safe; different handles may be used concurrently.
+ */
+#ifndef DEFMM_B200_H
+#define DEFMM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct defmm_handle defmm_handle;
+
+/* Status codes. */
+#define DEFMM_OK 0
+#define DEFMM_ERR_ARG (-1)        /* invalid argument or call order          */
+#define DEFMM_ERR_DEPTH (-2)      /* coincident points: tree never terminates */
+#define DEFMM_ERR_SHALLOW (-3)    /* no level admits far-field (M2L) work     */
+#define DEFMM_ERR_CUDA (-4)       /* CUDA runtime error / no device           */
+#define DEFMM_ERR_MEMORY (-5)     /* device memory exhausted                  */
+#define DEFMM_ERR_IO (-6)         /* INP file unreadable or short             */
+
+/* Arithmetic of the matvec. */
+#define DEFMM_PRECISION_FP64 0   /* plain FP64, the drop-in for the reference  */
+#define DEFMM_PRECISION_MIXED 1  /* FP32 bulk arithmetic, FP64 phase reduction */
+
+/* IBFMM_Mat<3>::IBFMM_Mat() (interface.hpp:57). */
+defmm_handle* defmm_create(void);
+/* ~IBFMM_Mat: releases host and device memory. */
+void defmm_destroy(defmm_handle* h);
+/* Message of the last failing call on this handle ("" if none). */
+const char* defmm_last_error(const defmm_handle* h);
+
+/* IBFMM_Mat<3>::addSourceParticle(flt part[3]) (interface.hpp:59-67). */
+int defmm_add_source_particle(defmm_handle* h, const double xyz[3]);
+/* IBFMM_Mat<3>::addTargetParticle(flt part[3]) (interface.hpp:69-77). */
+int defmm_add_target_particle(defmm_handle* h, const double xyz[3]);
+/* Bulk forms of the two calls above: n points, xyz interleaved. */
+int defmm_add_sources(defmm_handle* h, const double* xyz, int64_t n);
+int defmm_add_targets(defmm_handle* h, const double* xyz, int64_t n);
+/* IBFMM_Mat<3>::addSourceParticlesINP / addTargetParticlesINP
+ * (interface.hpp:79-98): read `nparts` lines "x y z" from an INP file.
+ * which = 0: sources, 1: targets.  Unlike the reference, a short or missing
+ * file is an error (DEFMM_ERR_IO) instead of silently reading zeros. */
+int defmm_load_inp(defmm_handle* h, const char* path, int64_t nparts, int which);
+
+/* IBFMM_Mat<3>::prcmpt(int L, int Ncrit, flt kappa, int lvMAX = -1)
+ * (interface.hpp:100-151): build both octrees (leaf = fewer than Ncrit
+ * particles, or fixed depth lvMAX when lvMAX >= 0), the frequency regime,
+ * cones, interaction lists, expansion slots and transfer spectra on the host
+ * (multi-threaded).  2 <= L <= 8. */
+int defmm_prcmpt(defmm_handle* h, int L, int Ncrit, double kappa, int lvMAX);
+
+/* Copy the plan to the current CUDA device (done by the first gemv when not
+ * called explicitly; prcmpt itself runs on the host only, so the plan can be
+ * inspected without a GPU). */
+int defmm_upload(defmm_handle* h);
+
+/* Select the matvec arithmetic (DEFMM_PRECISION_*); default FP64.
+ * May be called before or after prcmpt. */
+int defmm_set_precision(defmm_handle* h, int mode);
+
+/* friend gemv(IBFMM_Mat&, Vecc& In, Vecc& Out) (interface.hpp:153-170):
+ * Out = A * In for host vectors; In has n_sources complex entries, Out
+ * n_targets, both in user order.  Blocks until Out is written. */
+int defmm_gemv(defmm_handle* h, const double* in, double* out);
+
+/* Device-resident form: d_in / d_out are device pointers to nrhs stacked
+ * complex vectors (rhs-major, each in user order).  Runs on `stream`
+ * (a cudaStream_t; NULL = the handle's own stream) without synchronising. */
+int defmm_gemv_device(defmm_handle* h, const void* d_in, void* d_out,
+                      int64_t nrhs, void* stream);
+
+/* Many right-hand sides at once (host vectors, rhs-major). */
+int defmm_gemv_batched(defmm_handle* h, int64_t nrhs, const double* in,
+                       double* out);
+
+/* friend CheckFULL(IBFMM_Mat&) (interface.hpp:178-221), sampled: FP64 direct
+ * sum on the GPU at `nsamples` seeded random targets against the last gemv;
+ * err = {rel. Linf, rel. L1, rel. L2} over the samples (the reference prints
+ * the same three norms over all targets). */
+int defmm_check_full(defmm_handle* h, int64_t nsamples, uint64_t seed,
+                     double err[3]);
+
+/* Sizes and statistics.  what: see DEFMM_INFO_* below. */
+#define DEFMM_INFO_N_SOURCES 0
+#define DEFMM_INFO_N_TARGETS 1
+#define DEFMM_INFO_NLVL 2
+#define DEFMM_INFO_CPT 3
+#define DEFMM_INFO_MAX_STAGE 4
+#define DEFMM_INFO_CELLS_T 5
+#define DEFMM_INFO_CELLS_S 6
+#define DEFMM_INFO_SLOTS_S 7
+#define DEFMM_INFO_SLOTS_T 8
+#define DEFMM_INFO_FAR_HF 9
+#define DEFMM_INFO_FAR_LF 10
+#define DEFMM_INFO_NEAR 11
+#define DEFMM_INFO_I_NEAR 12
+#define DEFMM_INFO_TABLES 13
+#define DEFMM_INFO_DEVICE_BYTES 14
+#define DEFMM_INFO_LIST_RECORDS 15 /* 1 if lists were recorded (parity) */
+int defmm_info(const defmm_handle* h, int what, int64_t* value);
+
+/* Per-phase device times (ms) of the last gemv, in this order:
+ * gather+P2M, M2M, M2F, M2L, F2L, L2L, L2P, P2P, scatter, total. */
+int defmm_phase_times(const defmm_handle* h, double ms[10]);
+
+/* Per-phase timing with CUDA events (adds synchronisation between phases;
+ * off by default).  on = 0 / 1. */
+int defmm_set_profiling(defmm_handle* h, int on);
+
+/* Record the interaction lists at the next prcmpt (costs host memory; for
+ * parity checks against the reference). */
+int defmm_keep_lists(defmm_handle* h, int on);
+
+/* Tree dump in the layout of the reference's cell array (SourceRoot /
+ * TargetRoot, interface.hpp:174-175; cells in depth-first pre-order):
+ * which = 0 targets, 1 sources.  cells_int: 8 int32 per cell (idx0, idx1,
+ * idx2, lvl, nprt, first particle, number of sons, number of expansions);
+ * cells_dbl: 4 doubles per cell (ctr0, ctr1, ctr2, rad); dirs: effective
+ * directions of every cell, concatenated in cell order (may be NULL to query
+ * the count, returned in *ndirs); perm: user index of each tree-order
+ * particle.  Any output pointer may be NULL. */
+int defmm_dump_tree(const defmm_handle* h, int which, int32_t* cells_int,
+                    double* cells_dbl, int32_t* dirs, int64_t* ndirs,
+                    int32_t* perm);
+
+/* Recorded lists (defmm_keep_lists): far HF records (t, s, lvl, cone, iz,
+ * hash), far LF records (t, s, lvl, iz, hash), near records (t, s); counts
+ * in n[3].  Pointers may be NULL to query the counts. */
+int defmm_dump_lists(const defmm_handle* h, int32_t* far_hf, int32_t* far_lf,
+                     int32_t* near_, int64_t n[3]);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DEFMM_B200_H */
