@@ -1,0 +1,327 @@
+#!/usr/bin/env python
+"""FMM matvec throughput on B200: points/s of the directional Helmholtz FMM
+(defmm's method) on the sphere workload: N = 2,000,000 points uniform on the
+unit sphere, k = 2 pi 64 (128 wavelengths across the diameter), order 5,
+leaf size 64; complex FP64 charges uniform in [-1, 1]^2 (seeded synthetic
+data, no dataset).
+
+One step = one matvec (P2M .. L2P + P2P) over that input.  Both arithmetic
+paths are timed: plain FP64 (the drop-in) and mixed precision; `value` is the
+mixed path's points/s when its relative L2 deviation from the FP64 result is
+<= 1e-6 (otherwise the FP64 path's).  Inputs are resident in HBM for `value`
+(CUDA events around K steps on the launching stream); `e2e` is the same
+metric through the host-buffer C-ABI call (host->device copy of the charges
+and device->host copy of the potentials inside the timed region).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (launched by torchrun) every rank runs an independent replica
+(its own seeded charges): the matvec does not shard; value = all ranks'
+points / max-over-ranks time.  --impl reference times the reference's own
+CPU implementation (oracle/_ref/defmm_ref_fast, built unmodified) on a
+bounded sample of the same workload, on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FMM matvec points/s on 1 B200 at rel L2 err <=1e-6: mixed/learned vs plain FP64"
+UNIT = "points/s"
+MIXED_TOL = 1e-6
+
+
+def workload(name, rank=0):
+    from defmm_b200 import workloads as W
+    if name == "sphere2m":
+        return W.sphere_surface(2_000_000, seed=0)
+    if name == "sphere100k":
+        return W.sphere_surface(100_000, seed=0, wavelengths=32)
+    if name == "cube20k":
+        return W.cube_surface(20_000, seed=0)
+    raise KeyError(name)
+
+
+def cpu_sample(name):
+    """Bounded CPU sample of the same workload: same geometry and points per
+    wavelength^2, N/64 points at 1/8 of the wavenumber."""
+    from defmm_b200 import workloads as W
+    if name == "sphere2m":
+        return W.sphere_surface(2_000_000 // 64, seed=0, wavelengths=128 / 8), "sphere N=31,250, 16 wavelengths, order 5, leaf 64"
+    if name == "sphere100k":
+        return W.sphere_surface(100_000 // 16, seed=0, wavelengths=8), "sphere N=6,250, 8 wavelengths, order 5, leaf 64"
+    return workload(name), "full workload"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev=0):
+        self.dev = dev
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p["hbm_gbs"], p.get("bf16_tflops"), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, 1590.0, "fallback"
+
+
+def run_reference(args, name):
+    """Reference arm: the reference's own CPU matvec on the bounded sample."""
+    from defmm_b200 import workloads as W
+    from oracle import refrun
+    w, desc = cpu_sample(name)
+    q = W.charges(w.n, 1)
+    if not refrun.available(fast=True):
+        return {"impl": "reference", "unavailable": "reference build oracle/_ref/defmm_ref_fast is missing"}
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = refrun.run(w.points, w.points, q, w.order, w.ncrit, w.kappa, lists=False, fast=True)
+        if i >= args.warmup:
+            vals.append(w.n / r.summary["gemv_s"])
+    v = float(statistics.mean(vals))
+    return {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": name, "sample": desc},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "reference", "sample": desc},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="sphere2m")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args, args.workload)), flush=True)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    from defmm_b200 import IBFMM_Mat, replicas, workloads as W
+
+    def max_over_ranks(x):
+        return replicas.max_over_ranks(x, dist, "cuda")
+
+    w = workload(args.workload, rank)
+    q = W.charges(w.n, replicas.replica_seed(rank))
+    A = IBFMM_Mat()
+    A.addSourceParticles(w.points)
+    A.addTargetParticles(w.points)
+    t0 = time.perf_counter()
+    A.prcmpt(w.order, w.ncrit, w.kappa)
+    setup_s = time.perf_counter() - t0
+    A.upload()
+    info = A.info()
+    # a dedicated stream: torch's default stream is the legacy NULL stream,
+    # which the library's non-blocking streams would not order against
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    dq = torch.from_numpy(q).to("cuda")
+    dp = torch.empty(w.n, dtype=torch.complex128, device="cuda")
+
+    res = {}
+    for prec in ["fp64", "mixed"]:
+        A.set_precision(prec)
+        for _ in range(args.warmup):
+            A.matvec_device(dq.data_ptr(), dp.data_ptr(), 1, stream.cuda_stream)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        launches = 0
+        barrier()
+        torch.cuda.synchronize()
+        with Clocks(local) as ck:
+            e0.record(stream)
+            for _ in range(args.steps):
+                A.matvec_device(dq.data_ptr(), dp.data_ptr(), 1, stream.cuda_stream)
+                launches += A.info("launches")
+            e1.record(stream)
+            torch.cuda.synchronize()
+        barrier()
+        ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+        res[prec] = {"ms": ms, "p": dp.cpu().numpy(), "launches": launches, "clocks": ck.summary()}
+
+    p64, p32 = res["fp64"]["p"], res["mixed"]["p"]
+    err_mixed = float(np.linalg.norm(p32 - p64) / np.linalg.norm(p64))
+    head = "mixed" if err_mixed <= MIXED_TOL else "fp64"
+    A.set_precision(head)
+    ms = res[head]["ms"]
+    value = replicas.job_throughput(w.n, world, ms * 1e-3)
+
+    # end to end through the host-buffer C-ABI call
+    A.matvec(q)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        A.matvec(q)
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps)
+    chk = A.check_full(2000, seed=7)  # FP64 direct sum at 2,000 seeded targets
+
+    # per-phase device times (separate profiled runs, not part of `value`)
+    phases = {}
+    for prec in ["fp64", "mixed"]:
+        A.set_precision(prec)
+        A.set_profiling(True)
+        A.matvec_device(dq.data_ptr(), dp.data_ptr(), 1, stream.cuda_stream)
+        torch.cuda.synchronize()
+        phases[prec] = A.phase_times()
+        A.set_profiling(False)
+    A.set_precision(head)
+
+    # roofline of the dominant HBM-bound kernel, M2L (with the inverse DFT
+    # fused), on the headline path.  Algorithmic bytes per matvec: every
+    # source spectrum once (e P^3 per source slot), every permuted transfer
+    # spectrum once, the local expansion of every target slot read and
+    # written (2 e L^3), 8 B per list entry.
+    hbm, bf16, src = measured_peaks()
+    e = 16 if head == "fp64" else 8
+    L = w.order
+    PP = (2 * L - 1) ** 3
+    n_far = info["far_hf"] + info["far_lf"]
+    m2l_bytes = (e * PP * info["slots_S"] + e * PP * info["permuted_spectra"]
+                 + 2 * e * L ** 3 * info["m2l_targets"] + 8 * n_far)
+    m2l_ms = phases[head]["m2l"]
+    achieved = m2l_bytes / (m2l_ms * 1e-3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "m2l_traffic.json")
+    if os.path.exists(tp):
+        try:
+            with open(tp) as f:
+                tr = json.load(f)
+            traffic = tr.get(head, {}).get("bytes_per_pair", None)
+            if traffic is not None:
+                traffic = traffic * n_far
+        except (OSError, ValueError):
+            traffic = None
+    roofline = {"bound": "hbm", "kernel": "k_m2l (M2L + inverse DFT, all cone batches)", "achieved": achieved,
+                "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_source": src,
+                "traffic": traffic, "algorithmic_bytes": m2l_bytes}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            from oracle import refrun
+            ws, desc = cpu_sample(args.workload)
+            if refrun.available(fast=True):
+                r = refrun.run(ws.points, ws.points, W.charges(ws.n, 1), ws.order, ws.ncrit, ws.kappa,
+                               lists=False, fast=True)
+                cpu = {"value": ws.n / r.summary["gemv_s"], "unit": UNIT, "cores": 1, "kind": "reference",
+                       "sample": desc, "gemv_s": r.summary["gemv_s"]}
+        except Exception as ex:  # the baseline must not sink the GPU result
+            cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"failed: {ex}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64" if head == "mixed" else "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "n_points": w.n, "kappa": w.kappa, "order": w.order,
+                       "leaf_size": w.ncrit, "precision": head, "parallelism": f"replicas{world}",
+                       "l2": "working set per step >> L2 (126 MB): expansions and spectra are GBs"},
+            "matvecs_per_s": world / (ms * 1e-3),
+            "fp64": {"ms_per_step": res["fp64"]["ms"], "points_per_s": world * w.n / (res["fp64"]["ms"] * 1e-3)},
+            "mixed": {"ms_per_step": res["mixed"]["ms"], "points_per_s": world * w.n / (res["mixed"]["ms"] * 1e-3),
+                      "rel_l2_vs_fp64": err_mixed},
+            "speedup_mixed_vs_fp64": res["fp64"]["ms"] / res["mixed"]["ms"],
+            "accuracy": {"direct_sum_2000_targets": chk, "precision": head},
+            "e2e": {"value": world * w.n / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 16 * w.n,
+                    "d2h_bytes_per_step": 16 * w.n},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "clocks": res[head]["clocks"],
+            "gpu_launches": res[head]["launches"],
+            "phases_ms": phases,
+            "setup_s": setup_s,
+            "plan": {k: info[k] for k in ["nlvl", "cpt", "slots_S", "slots_T", "far_hf", "far_lf", "near",
+                                          "i_near", "tables", "permuted_spectra", "device_bytes"]},
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -33,7 +33,8 @@ PRECISION_MIXED = 1
 _INFO = {
     "n_sources": 0, "n_targets": 1, "nlvl": 2, "cpt": 3, "max_stage": 4, "cells_T": 5,
     "cells_S": 6, "slots_S": 7, "slots_T": 8, "far_hf": 9, "far_lf": 10, "near": 11,
-    "i_near": 12, "tables": 13, "device_bytes": 14, "list_records": 15,
+    "i_near": 12, "tables": 13, "device_bytes": 14, "list_records": 15, "launches": 16,
+    "m2l_targets": 17, "leaf_slots_S": 18, "permuted_spectra": 19,
 }
 PHASES = ["p2m", "m2m", "m2f", "m2l", "f2l", "l2l", "l2p", "p2p", "scatter", "total"]
 
@@ -53,6 +54,7 @@ def lib():
         L = ctypes.CDLL(_LIB_PATH)
         vp, dp, ip, i64 = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int32), ctypes.c_int64
         sig = {
+            "defmm_device_count": (ctypes.c_int, []),
             "defmm_create": (vp, []),
             "defmm_destroy": (None, [vp]),
             "defmm_last_error": (ctypes.c_char_p, [vp]),
@@ -89,6 +91,10 @@ def _dp(a):
 
 def _ip(a):
     return None if a is None else a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+
+
+def device_count() -> int:
+    return int(lib().defmm_device_count())
 
 
 class IBFMM_Mat:

@@ -41,13 +41,17 @@ struct defmm_handle {
   const dfb::OpTable* ops = nullptr;
   int ops_prec = -1;
   // precision-dependent arrays
-  DevBuf M, Lx, F, J, q, sig, sig2, tables;
-  int64_t fj_cap = 0;  // slots per F / J batch buffer
+  DevBuf M, Lx, F, q, sig, sig2, ptab;
+  const uint32_t* d_ptab_key = nullptr;
+  int64_t f_cap = 0;  // source slots per F batch buffer
   // FP64 vectors
   DevBuf pnear, pfar, qin, out, chk;
   const int32_t *d_p2m_leaf = nullptr, *d_l2p_leaf = nullptr;
   const int32_t *d_tfirst = nullptr, *d_tn = nullptr, *d_sfirst = nullptr, *d_sn = nullptr;
   const int64_t* d_p2p_ptr = nullptr;
+  const int32_t* d_p2p_order = nullptr;
+  unsigned long long* d_queue = nullptr;
+  int nsm = 148;
   int64_t nchunk = 0;
   size_t dev_bytes = 0;
   double phase_ms[PH_N] = {0};
@@ -55,6 +59,7 @@ struct defmm_handle {
   cudaEvent_t ev_ready = nullptr, ev_done = nullptr;  // cross-stream ordering
   bool events = false;
   bool has_out = false;
+  int64_t launches = 0;  // kernels launched by the last gemv call
 
   int fail(int code, const std::string& m) {
     err = m;
@@ -122,11 +127,10 @@ void free_plan_device(defmm_handle* h) {
   free_buf(h->M);
   free_buf(h->Lx);
   free_buf(h->F);
-  free_buf(h->J);
   free_buf(h->q);
   free_buf(h->sig);
   free_buf(h->sig2);
-  free_buf(h->tables);
+  free_buf(h->ptab);
   free_buf(h->pnear);
   free_buf(h->pfar);
   free_buf(h->qin);
@@ -184,6 +188,7 @@ int upload_plan(defmm_handle* h) {
   UP(p.m2l_src, d.m2l_src);
   UP(p.m2l_tab, d.m2l_tab);
   UP(p.perm, d.perm);
+  UP(p.ptab_key, h->d_ptab_key);
   std::vector<double> mats;
   for (int k = 0; k < 2; k++) mats.insert(mats.end(), p.m2m[k].begin(), p.m2m[k].end());
   for (int k = 0; k < 2; k++) mats.insert(mats.end(), p.l2l[k].begin(), p.l2l[k].end());
@@ -213,6 +218,7 @@ int upload_plan(defmm_handle* h) {
   UP(p.p2p_ptr, h->d_p2p_ptr);
   UP(p.p2p_sfirst, h->d_sfirst);
   UP(p.p2p_sn, h->d_sn);
+  UP(p.p2p_order, h->d_p2p_order);
   h->nchunk = (int64_t)p.p2p_tfirst.size();
 #undef UP
   {
@@ -221,6 +227,13 @@ int upload_plan(defmm_handle* h) {
     h->plan_allocs.push_back(e);
     CK(cudaMemset(e, 0, sizeof(int)));
     d.err = static_cast<int*>(e);
+    void* qc = nullptr;
+    CK(cudaMalloc(&qc, sizeof(unsigned long long)));
+    h->plan_allocs.push_back(qc);
+    h->d_queue = static_cast<unsigned long long*>(qc);
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, dev));
   }
   int64_t nS = (int64_t)p.S.perm.size(), nT = (int64_t)p.T.perm.size();
   if ((st = ensure(h, h->pnear, 16 * nT)) || (st = ensure(h, h->pfar, 16 * nT)) ||
@@ -238,11 +251,10 @@ int prepare_precision(defmm_handle* h) {
   free_buf(h->M);
   free_buf(h->Lx);
   free_buf(h->F);
-  free_buf(h->J);
   free_buf(h->q);
   free_buf(h->sig);
   free_buf(h->sig2);
-  free_buf(h->tables);
+  free_buf(h->ptab);
   h->ops = dfb::op_table(p.L, fp64);
   if (!h->ops) return h->fail(DEFMM_ERR_ARG, "unsupported order");
   CK(h->ops->setup());
@@ -268,32 +280,41 @@ int prepare_precision(defmm_handle* h) {
     s2.insert(s2.end(), p.sig2[e].begin(), p.sig2[e].end());
   }
   int st;
-  if ((st = put(h->sig, s1.data(), s1.size())) || (st = put(h->sig2, s2.data(), s2.size())) ||
-      (st = put(h->tables, p.tables.data(), p.tables.size())))
-    return st;
+  if ((st = put(h->sig, s1.data(), s1.size())) || (st = put(h->sig2, s2.data(), s2.size()))) return st;
+  {
+    // permuted spectra used by M2L, gathered once on the device
+    DevBuf base;
+    if ((st = put(base, p.tables.data(), p.tables.size()))) return st;
+    const int64_t np = (int64_t)p.ptab_key.size();
+    if ((st = ensure(h, h->ptab, std::max<int64_t>(1, np) * p.PP * cs))) {
+      free_buf(base);
+      return st;
+    }
+    h->ops->permute(np, h->d_ptab_key, h->dp.perm, base.p, h->ptab.p, h->st);
+    CK(cudaStreamSynchronize(h->st));
+    free_buf(base);
+  }
   const int64_t nS = (int64_t)p.S.perm.size();
   if ((st = ensure(h, h->M, std::max<int64_t>(1, p.sS.n) * p.LL * cs)) ||
       (st = ensure(h, h->Lx, std::max<int64_t>(1, p.sT.n) * p.LL * cs)) || (st = ensure(h, h->q, nS * cs)))
     return st;
-  // F / J batch buffers: at least the largest cone of any level, at most
-  // about half of the free memory
+  // F batch buffer: at least the largest cone of any level, at most about
+  // half of the free memory
   int64_t need = 1, want = 0;
   for (int l = 0; l < p.lv.nlvl; l++) {
     const auto& cS = p.sS.cone_begin[l];
-    const auto& cT = p.sT.cone_begin[l];
     for (size_t c = 0; c + 1 < cS.size(); c++) need = std::max(need, cS[c + 1] - cS[c]);
-    for (size_t c = 0; c + 1 < cT.size(); c++) need = std::max(need, cT[c + 1] - cT[c]);
-    want = std::max(want, std::max(cS.back() - cS.front(), cT.back() - cT.front()));
+    want = std::max(want, cS.back() - cS.front());
   }
   size_t fr = 0, tot = 0;
   CK(cudaMemGetInfo(&fr, &tot));
   const size_t per = (size_t)p.PP * cs;
-  int64_t cap = (int64_t)((fr * 0.45) / (2 * per));
-  cap = std::min<int64_t>(cap, (int64_t)((size_t)48 << 30) / (int64_t)per);
+  int64_t cap = (int64_t)((fr * 0.5) / per);
+  cap = std::min<int64_t>(cap, (int64_t)((size_t)64 << 30) / (int64_t)per);
   cap = std::min(cap, std::max(want, need));
   if (cap < need) return h->fail(DEFMM_ERR_MEMORY, "not enough device memory for one cone of spectra");
-  h->fj_cap = cap;
-  if ((st = ensure(h, h->F, cap * per)) || (st = ensure(h, h->J, cap * per))) return st;
+  h->f_cap = cap;
+  if ((st = ensure(h, h->F, cap * per))) return st;
   h->ops_prec = h->precision;
   return 0;
 }
@@ -311,32 +332,35 @@ int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) 
   const int64_t nS = (int64_t)p.S.perm.size(), nT = (int64_t)p.T.perm.size();
   const int nl = p.lv.nlvl;
   h->st = s;
+  int64_t nl_ = 0;
   rec(h, 2 * PH_TOTAL);
-  rec(h, 2 * PH_P2M);
   dfb::launch_gather(fp64, qin, d.S_perm, h->q.p, nS, 0, 0, 1, s);
+  nl_ += 1 + (h->nchunk ? 1 : 0) + (p.p2m_leaf.empty() ? 0 : 1) + (p.l2p_leaf.empty() ? 0 : 1) + 1;
   CK(cudaMemsetAsync(h->pfar.p, 0, 16 * nT, s));
   CK(cudaMemsetAsync(h->pnear.p, 0, 16 * nT, s));
   CK(cudaMemsetAsync(h->Lx.p, 0, h->Lx.bytes, s));
   // near field on the second stream, overlapping the far field
+  // (profiling runs it on the main stream so that phase times do not overlap)
+  cudaStream_t sn = h->events ? s : h->st2;
   cudaEvent_t ready = h->ev_ready;
   CK(cudaEventRecord(ready, s));
-  CK(cudaStreamWaitEvent(h->st2, ready, 0));
-  if (h->events) cudaEventRecord(h->ev[2 * PH_P2P], h->st2);
-  if (fp64)
-    dfb::launch_p2p_fp64(d, h->nchunk, h->d_tfirst, h->d_tn, h->d_p2p_ptr, h->d_sfirst, h->d_sn,
-                         (const double2*)h->q.p, (double2*)h->pnear.p, h->st2);
-  else
-    return h->fail(DEFMM_ERR_ARG, "mixed precision P2P not available");
-  if (h->events) cudaEventRecord(h->ev[2 * PH_P2P + 1], h->st2);
+  CK(cudaStreamWaitEvent(sn, ready, 0));
+  if (h->events) cudaEventRecord(h->ev[2 * PH_P2P], sn);
+  dfb::launch_p2p(fp64, d, h->nchunk, h->d_p2p_order, h->d_tfirst, h->d_tn, h->d_p2p_ptr, h->d_sfirst, h->d_sn,
+                  h->q.p, (double2*)h->pnear.p, h->d_queue, h->nsm, sn);
+  if (h->events) cudaEventRecord(h->ev[2 * PH_P2P + 1], sn);
   // upward pass
+  rec(h, 2 * PH_P2M);
   ops->p2m(d, h->d_p2m_leaf, (int)p.p2m_leaf.size(), h->q.p, h->sig2.p, h->M.p, s);
   rec(h, 2 * PH_P2M + 1);
   rec(h, 2 * PH_M2M);
-  for (int l = nl - 2; l >= p.lv.max_stage; l--)
+  for (int l = nl - 2; l >= p.lv.max_stage; l--) {
     ops->m2m(d, p.sS.lvl_begin[l], p.sS.lvl_begin[l + 1], h->sig.p, h->sig2.p, h->M.p, s);
+    nl_ += p.sS.lvl_begin[l + 1] > p.sS.lvl_begin[l] ? 1 : 0;
+  }
   rec(h, 2 * PH_M2M + 1);
   // far field per level and cone batch, then the downward transfer
-  float tm2f = 0, tm2l = 0, tf2l = 0, tl2l = 0;
+  float tm2f = 0, tm2l = 0, tl2l = 0;
   const size_t cs = fp64 ? 16 : 8;
   for (int l = p.lv.max_stage; l < nl; l++) {
     const auto& cS = p.sS.cone_begin[l];
@@ -345,27 +369,23 @@ int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) 
     int c0 = 0;
     while (c0 < nc) {
       int c1 = c0 + 1;
-      while (c1 < nc && cS[c1 + 1] - cS[c0] <= h->fj_cap && cT[c1 + 1] - cT[c0] <= h->fj_cap) c1++;
+      while (c1 < nc && cS[c1 + 1] - cS[c0] <= h->f_cap) c1++;
       const int64_t fs0 = cS[c0], fs1 = cS[c1], ts0 = cT[c0], ts1 = cT[c1];
       if (ts1 > ts0 && fs1 > fs0) {
         rec(h, 2 * PH_M2F);
         ops->m2f(fs1 - fs0, (const char*)h->M.p + fs0 * p.LL * cs, h->F.p, s);
+        nl_ += 2;
         rec(h, 2 * PH_M2F + 1);
         rec(h, 2 * PH_M2L);
-        ops->m2l(d, ts0, ts1, fs0, fs1, h->F.p, h->tables.p, h->J.p, s);
+        ops->m2l(d, ts0, ts1, fs0, fs1, h->F.p, h->ptab.p, h->Lx.p, s);
         rec(h, 2 * PH_M2L + 1);
-        rec(h, 2 * PH_F2L);
-        ops->f2l(ts1 - ts0, h->J.p, (char*)h->Lx.p + ts0 * p.LL * cs, s);
-        rec(h, 2 * PH_F2L + 1);
         if (h->events) {
           float a;
-          CK(cudaEventSynchronize(h->ev[2 * PH_F2L + 1]));
+          CK(cudaEventSynchronize(h->ev[2 * PH_M2L + 1]));
           cudaEventElapsedTime(&a, h->ev[2 * PH_M2F], h->ev[2 * PH_M2F + 1]);
           tm2f += a;
           cudaEventElapsedTime(&a, h->ev[2 * PH_M2L], h->ev[2 * PH_M2L + 1]);
           tm2l += a;
-          cudaEventElapsedTime(&a, h->ev[2 * PH_F2L], h->ev[2 * PH_F2L + 1]);
-          tf2l += a;
         }
       }
       c0 = c1;
@@ -373,6 +393,7 @@ int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) 
     if (l + 1 < nl) {
       rec(h, 2 * PH_L2L);
       ops->l2l(d, p.sT.lvl_begin[l + 1], p.sT.lvl_begin[l + 2], h->sig.p, h->sig2.p, h->Lx.p, s);
+      nl_ += p.sT.lvl_begin[l + 2] > p.sT.lvl_begin[l + 1] ? 1 : 0;
       rec(h, 2 * PH_L2L + 1);
       if (h->events) {
         float a;
@@ -386,12 +407,13 @@ int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) 
   ops->l2p(d, h->d_l2p_leaf, (int)p.l2p_leaf.size(), h->sig2.p, h->Lx.p, (double2*)h->pfar.p, s);
   rec(h, 2 * PH_L2P + 1);
   cudaEvent_t done = h->ev_done;
-  CK(cudaEventRecord(done, h->st2));
+  CK(cudaEventRecord(done, sn));
   CK(cudaStreamWaitEvent(s, done, 0));
   rec(h, 2 * PH_SCATTER);
   dfb::launch_scatter((const double2*)h->pnear.p, (const double2*)h->pfar.p, d.T_perm, out, nT, s);
   rec(h, 2 * PH_SCATTER + 1);
   rec(h, 2 * PH_TOTAL + 1);
+  h->launches += nl_;
   CK(cudaGetLastError());
   if (h->events) {
     CK(cudaStreamSynchronize(s));
@@ -405,7 +427,7 @@ int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) 
     h->phase_ms[PH_M2M] = el(PH_M2M);
     h->phase_ms[PH_M2F] = tm2f;
     h->phase_ms[PH_M2L] = tm2l;
-    h->phase_ms[PH_F2L] = tf2l;
+    h->phase_ms[PH_F2L] = 0.;  // fused into M2L
     h->phase_ms[PH_L2L] = tl2l;
     h->phase_ms[PH_L2P] = el(PH_L2P);
     h->phase_ms[PH_P2P] = el(PH_P2P);
@@ -443,6 +465,15 @@ uint64_t splitmix(uint64_t& s) {
 
 // ==================================================================== C ABI
 extern "C" {
+
+int defmm_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
 
 defmm_handle* defmm_create(void) { return new defmm_handle(); }
 
@@ -560,6 +591,7 @@ int defmm_gemv_device(defmm_handle* h, const void* d_in, void* d_out, int64_t nr
   st = prepare_precision(h);
   if (st) return st;
   cudaStream_t s = stream ? (cudaStream_t)stream : h->st;
+  h->launches = 0;
   const int64_t nS = (int64_t)h->plan.S.perm.size(), nT = (int64_t)h->plan.T.perm.size();
   for (int64_t r = 0; r < nrhs; r++) {
     st = run_gemv(h, (const double2*)d_in + r * nS, (double2*)d_out + r * nT, s);
@@ -576,6 +608,7 @@ int defmm_gemv_batched(defmm_handle* h, int64_t nrhs, const double* in, double* 
   st = prepare_precision(h);
   if (st) return st;
   const int64_t nS = (int64_t)h->plan.S.perm.size(), nT = (int64_t)h->plan.T.perm.size();
+  h->launches = 0;
   for (int64_t r = 0; r < nrhs; r++) {
     CK(cudaMemcpyAsync(h->qin.p, in + 2 * r * nS, 16 * nS, cudaMemcpyHostToDevice, h->st));
     st = run_gemv(h, (const double2*)h->qin.p, (double2*)h->out.p, h->st);
@@ -664,11 +697,25 @@ int defmm_info(const defmm_handle* h, int what, int64_t* v) {
     case DEFMM_INFO_I_NEAR: *v = p.i_near; break;
     case DEFMM_INFO_TABLES: *v = (int64_t)p.tab_lvl.size(); break;
     case DEFMM_INFO_DEVICE_BYTES:
-      *v = (int64_t)(h->dev_bytes + h->M.bytes + h->Lx.bytes + h->F.bytes + h->J.bytes + h->q.bytes +
-                     h->sig.bytes + h->sig2.bytes + h->tables.bytes + h->pnear.bytes + h->pfar.bytes +
+      *v = (int64_t)(h->dev_bytes + h->M.bytes + h->Lx.bytes + h->F.bytes + h->q.bytes + h->sig.bytes +
+                     h->sig2.bytes + h->ptab.bytes + h->pnear.bytes + h->pfar.bytes +
                      h->qin.bytes + h->out.bytes);
       break;
     case DEFMM_INFO_LIST_RECORDS: *v = p.keep_lists ? 1 : 0; break;
+    case DEFMM_INFO_LAUNCHES: *v = h->launches; break;
+    case DEFMM_INFO_PERMUTED_SPECTRA: *v = (int64_t)p.ptab_key.size(); break;
+    case DEFMM_INFO_M2L_TARGETS: {
+      int64_t n = 0;
+      for (int64_t k = 0; k < p.sT.n; k++) n += p.m2l_ptr[k + 1] > p.m2l_ptr[k] ? 1 : 0;
+      *v = n;
+      break;
+    }
+    case DEFMM_INFO_LEAF_SLOTS_S: {
+      int64_t n = 0;
+      for (int32_t c : p.p2m_leaf) n += p.sS.cell_ptr[c + 1] - p.sS.cell_ptr[c];
+      *v = n;
+      break;
+    }
     default: return DEFMM_ERR_ARG;
   }
   return 0;

@@ -3,6 +3,9 @@
 #include "kernels.cuh"
 #include "fmm_kernels.h"
 
+#include <algorithm>
+#include <type_traits>
+
 namespace dfb {
 
 // ----------------------------------------------------------------- basics --
@@ -26,11 +29,41 @@ __device__ __forceinline__ void lagrange_all(T x, T rad, T* b) {
   }
 }
 
-// exp(i a) with a in FP64 (argument reduction and evaluation by CUDA's sincos)
+// FP64 sin and cos of x: Cody-Waite reduction by pi/2 in two FMA steps
+// (pi/2 split into its double and the remainder), then the Taylor series of
+// sin to degree 15 and of cos to degree 16 on [-pi/4, pi/4] (truncation
+// below 7e-17 relative), quadrant by n mod 4.
+__device__ __forceinline__ void sincos_cw(double x, double& s, double& c) {
+  const double n = rint(x * 0.6366197723675814);
+  double r = fma(-n, 1.5707963267948966, x);
+  r = fma(-n, 6.123233995736766e-17, r);
+  const double r2 = r * r;
+  double ps = fma(r2, -7.647163731819816e-13, 1.6059043836821613e-10);
+  ps = fma(r2, ps, -2.505210838544172e-08);
+  ps = fma(r2, ps, 2.7557319223985893e-06);
+  ps = fma(r2, ps, -1.984126984126984e-04);
+  ps = fma(r2, ps, 8.333333333333333e-03);
+  ps = fma(r2, ps, -1.6666666666666666e-01);
+  const double sr = fma(r * r2, ps, r);
+  double pc = fma(r2, 4.779477332387385e-14, -1.1470745597729725e-11);
+  pc = fma(r2, pc, 2.08767569878681e-09);
+  pc = fma(r2, pc, -2.755731922398589e-07);
+  pc = fma(r2, pc, 2.48015873015873e-05);
+  pc = fma(r2, pc, -1.388888888888889e-03);
+  pc = fma(r2, pc, 4.1666666666666664e-02);
+  pc = fma(r2, pc, -0.5);
+  const double cr = fma(r2, pc, 1.0);
+  const int q = __double2int_rn(n) & 3;
+  const double ss = (q & 1) ? cr : sr, cc = (q & 1) ? sr : cr;
+  s = (q & 2) ? -ss : ss;
+  c = ((q + 1) & 2) ? -cc : cc;
+}
+
+// exp(i a) with a in FP64
 template <typename C>
 __device__ __forceinline__ C expi64(double a) {
   double s, c;
-  sincos(a, &s, &c);
+  sincos_cw(a, s, c);
   C r;
   r.x = c;
   r.y = s;
@@ -146,60 +179,9 @@ __global__ void __launch_bounds__(128) k_p2m(DevPlan P, const int32_t* __restric
 // ------------------------------------------------ separable 3-D transfer --
 // out[a,b,c] = sum A_s0(a,a') A_s1(b,b') A_s2(c,c') in[a',b',c'] computed in
 // three axis passes (axis 2, 1, 0 as interpolation.hpp:311-361); A(k, p) is
-// stored column-major mat[k + p*L].  One warp, values l = lane + 32 m.
-template <typename T, int L>
-__device__ __forceinline__ void separable_warp(const T* mats, int sg0, int sg1, int sg2,
-                                               typename cpx_t<T>::type* buf,
-                                               typename cpx_t<T>::type* buf2,
-                                               typename cpx_t<T>::type* res, int lane) {
-  typedef typename cpx_t<T>::type C;
-  constexpr int LL = L * L * L, NL = (LL + 31) / 32;
-  const T* m2 = mats + sg2 * L * L;
-  const T* m1 = mats + sg1 * L * L;
-  const T* m0 = mats + sg0 * L * L;
-#pragma unroll
-  for (int m = 0; m < NL; m++) {
-    const int l = lane + 32 * m;
-    if (l < LL) {
-      const int a = l / (L * L), b = (l / L) % L, c = l % L;
-      C acc = czero<C>();
-#pragma unroll
-      for (int p = 0; p < L; p++) rfma(acc, m2[c + p * L], buf[(a * L + b) * L + p]);
-      buf2[l] = acc;
-    }
-  }
-  __syncwarp();
-#pragma unroll
-  for (int m = 0; m < NL; m++) {
-    const int l = lane + 32 * m;
-    if (l < LL) {
-      const int a = l / (L * L), b = (l / L) % L, c = l % L;
-      C acc = czero<C>();
-#pragma unroll
-      for (int p = 0; p < L; p++) rfma(acc, m1[b + p * L], buf2[(a * L + p) * L + c]);
-      buf[l] = acc;
-    }
-  }
-  __syncwarp();
-#pragma unroll
-  for (int m = 0; m < NL; m++) {
-    const int l = lane + 32 * m;
-    if (l < LL) {
-      const int a = l / (L * L), b = (l / L) % L, c = l % L;
-      C acc = czero<C>();
-#pragma unroll
-      for (int p = 0; p < L; p++) rfma(acc, m0[a + p * L], buf[(p * L + b) * L + c]);
-      res[m] = acc;
-    }
-  }
-  __syncwarp();
-}
-
-// -------------------------------------------------------------------- M2M --
-// One warp per parent slot with children (upwpass.hpp:49-60):
-//   HF parent, direction d (hfM2Mblock M2M.hpp:76-105 / lf2hfM2M :108-124):
-//     M_d = conj(sig2_d) o sum_c exp(-i k d.v_c) A_{v_c}(sig_d o M_c)
-//   LF parent (lfM2M :35-41): M = sum_c A_{v_c}(M_c);   v_c = ctr_c - ctr_parent
+// stored column-major mat[k + p*L].  One warp; in every pass a lane owns
+// whole lines (L inputs in registers -> L outputs).  After the last pass lane
+// ln holds the outputs (a, b, c) for a = 0..L-1 of its line(s) (b, c) = ln.
 template <typename T, int L>
 struct XferCfg {
   // warps per CTA so that 2 LL-vectors per warp fit in 40 KB of shared memory
@@ -207,12 +189,81 @@ struct XferCfg {
 };
 
 template <typename T, int L>
+struct Sep {
+  typedef typename cpx_t<T>::type C;
+  static constexpr int NLN = (L * L + 31) / 32;  // lines per lane
+  __device__ static __forceinline__ void run(const T* mats, int sg0, int sg1, int sg2, C* buf, C* buf2,
+                                             C (&res)[NLN][L], int lane) {
+    const T* m2 = mats + sg2 * L * L;
+    const T* m1 = mats + sg1 * L * L;
+    const T* m0 = mats + sg0 * L * L;
+#pragma unroll
+    for (int q = 0; q < NLN; q++) {  // axis 2: lines (a, b)
+      const int ln = lane + 32 * q;
+      if (ln < L * L) {
+        C v[L];
+#pragma unroll
+        for (int p = 0; p < L; p++) v[p] = buf[ln * L + p];
+#pragma unroll
+        for (int k = 0; k < L; k++) {
+          C acc = czero<C>();
+#pragma unroll
+          for (int p = 0; p < L; p++) rfma(acc, m2[k + p * L], v[p]);
+          buf2[ln * L + k] = acc;
+        }
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < NLN; q++) {  // axis 1: lines (a, c)
+      const int ln = lane + 32 * q;
+      if (ln < L * L) {
+        const int a = ln / L, c = ln % L;
+        C v[L];
+#pragma unroll
+        for (int p = 0; p < L; p++) v[p] = buf2[(a * L + p) * L + c];
+#pragma unroll
+        for (int k = 0; k < L; k++) {
+          C acc = czero<C>();
+#pragma unroll
+          for (int p = 0; p < L; p++) rfma(acc, m1[k + p * L], v[p]);
+          buf[(a * L + k) * L + c] = acc;
+        }
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < NLN; q++) {  // axis 0: lines (b, c)
+      const int ln = lane + 32 * q;
+      if (ln < L * L) {
+        C v[L];
+#pragma unroll
+        for (int p = 0; p < L; p++) v[p] = buf[p * L * L + ln];
+#pragma unroll
+        for (int k = 0; k < L; k++) {
+          C acc = czero<C>();
+#pragma unroll
+          for (int p = 0; p < L; p++) rfma(acc, m0[k + p * L], v[p]);
+          res[q][k] = acc;
+        }
+      }
+    }
+    __syncwarp();
+  }
+};
+
+// -------------------------------------------------------------------- M2M --
+// One warp per parent slot with children (upwpass.hpp:49-60):
+//   HF parent, direction d (hfM2Mblock M2M.hpp:76-105 / lf2hfM2M :108-124):
+//     M_d = conj(sig2_d) o sum_c exp(-i k d.v_c) A_{v_c}(sig_d o M_c)
+//   LF parent (lfM2M :35-41): M = sum_c A_{v_c}(M_c);   v_c = ctr_c - ctr_parent
+template <typename T, int L>
 __global__ void __launch_bounds__(128) k_m2m(DevPlan P, int64_t s0, int64_t s1,
                                              const typename cpx_t<T>::type* __restrict__ sig,
                                              const typename cpx_t<T>::type* __restrict__ sig2,
                                              typename cpx_t<T>::type* __restrict__ M) {
   typedef typename cpx_t<T>::type C;
-  constexpr int LL = L * L * L, NL = (LL + 31) / 32, NW = XferCfg<T, L>::NW;
+  constexpr int LL = L * L * L, NW = XferCfg<T, L>::NW, NLN = Sep<T, L>::NLN;
   __shared__ T mats[2 * L * L];
   __shared__ C sbuf[NW][2][LL];
   for (int i = threadIdx.x; i < 2 * L * L; i += blockDim.x) mats[i] = (T)P.mats[i];
@@ -231,36 +282,48 @@ __global__ void __launch_bounds__(128) k_m2m(DevPlan P, int64_t s0, int64_t s1,
     double dv[3] = {0., 0., 0.};
     if (hf)
       for (int k = 0; k < 3; k++) dv[k] = P.dirs[3 * (P.dir_off[h] + d) + k];
-    C acc[NL];
+    C acc[NLN][L];
 #pragma unroll
-    for (int m = 0; m < NL; m++) acc[m] = czero<C>();
+    for (int q = 0; q < NLN; q++)
+#pragma unroll
+      for (int k = 0; k < L; k++) acc[q][k] = czero<C>();
     for (int64_t e = eb; e < ee; e++) {
       const int cs = P.m2m_child[e];
       const int cc = P.sS_cell[cs];
       const double4 cct = P.S_ctr[cc];
       const double v[3] = {cct.x - pct.x, cct.y - pct.y, cct.z - pct.z};
       const C* Mc = M + (int64_t)cs * LL;
+      __syncwarp();
       for (int l = lane; l < LL; l += 32) sbuf[warp][0][l] = hf ? cmul(sg[l], Mc[l]) : Mc[l];
       __syncwarp();
-      C res[NL];
-      separable_warp<T, L>(mats, v[0] < 0. ? 0 : 1, v[1] < 0. ? 0 : 1, v[2] < 0. ? 0 : 1,
-                           sbuf[warp][0], sbuf[warp][1], res, lane);
+      C res[NLN][L];
+      Sep<T, L>::run(mats, v[0] < 0. ? 0 : 1, v[1] < 0. ? 0 : 1, v[2] < 0. ? 0 : 1, sbuf[warp][0],
+                     sbuf[warp][1], res, lane);
       if (hf) {
         const C ph = expi64<C>(-P.kappa * (dv[0] * v[0] + dv[1] * v[1] + dv[2] * v[2]));
 #pragma unroll
-        for (int m = 0; m < NL; m++) cfma(acc[m], ph, res[m]);
+        for (int q = 0; q < NLN; q++)
+#pragma unroll
+          for (int k = 0; k < L; k++) cfma(acc[q][k], ph, res[q][k]);
       } else {
 #pragma unroll
-        for (int m = 0; m < NL; m++) {
-          acc[m].x += res[m].x;
-          acc[m].y += res[m].y;
-        }
+        for (int q = 0; q < NLN; q++)
+#pragma unroll
+          for (int k = 0; k < L; k++) {
+            acc[q][k].x += res[q][k].x;
+            acc[q][k].y += res[q][k].y;
+          }
       }
     }
 #pragma unroll
-    for (int m = 0; m < NL; m++) {
-      const int l = lane + 32 * m;
-      if (l < LL) M[ps * LL + l] = hf ? cmulc(sg2[l], acc[m]) : acc[m];
+    for (int q = 0; q < NLN; q++) {
+      const int ln = lane + 32 * q;
+      if (ln < L * L)
+#pragma unroll
+        for (int k = 0; k < L; k++) {
+          const int l = k * L * L + ln;
+          M[ps * LL + l] = hf ? cmulc(sg2[l], acc[q][k]) : acc[q][k];
+        }
     }
   }
 }
@@ -276,7 +339,7 @@ __global__ void __launch_bounds__(128) k_l2l(DevPlan P, int64_t s0, int64_t s1,
                                              const typename cpx_t<T>::type* __restrict__ sig2,
                                              typename cpx_t<T>::type* __restrict__ Lx) {
   typedef typename cpx_t<T>::type C;
-  constexpr int LL = L * L * L, NL = (LL + 31) / 32, NW = XferCfg<T, L>::NW;
+  constexpr int LL = L * L * L, NW = XferCfg<T, L>::NW, NLN = Sep<T, L>::NLN;
   __shared__ T mats[2 * L * L];
   __shared__ C sbuf[NW][2][LL];
   for (int i = threadIdx.x; i < 2 * L * L; i += blockDim.x) mats[i] = (T)P.mats[2 * L * L + i];
@@ -293,44 +356,54 @@ __global__ void __launch_bounds__(128) k_l2l(DevPlan P, int64_t s0, int64_t s1,
     const double4 pct = P.T_ctr[pc], cct = P.T_ctr[cc];
     const double v[3] = {cct.x - pct.x, cct.y - pct.y, cct.z - pct.z};
     const int sg0 = v[0] < 0. ? 0 : 1, sg1 = v[1] < 0. ? 0 : 1, sg2i = v[2] < 0. ? 0 : 1;
-    C acc[NL];
+    C acc[NLN][L];
 #pragma unroll
-    for (int m = 0; m < NL; m++) acc[m] = czero<C>();
+    for (int q = 0; q < NLN; q++)
+#pragma unroll
+      for (int k = 0; k < L; k++) acc[q][k] = czero<C>();
     for (int64_t e = eb; e < ee; e++) {
       const int ps = P.l2l_parent[e];
       const int d = P.sT_dir[ps];
       const C* Lp = Lx + (int64_t)ps * LL;
       const C* sg = sig + P.sig_off[h] + (int64_t)(hf ? d : 0) * LL;
       const C* sgq = sig2 + P.sig_off[h] + (int64_t)(hf ? d : 0) * LL;
+      __syncwarp();
       for (int l = lane; l < LL; l += 32) sbuf[warp][0][l] = hf ? cmul(sgq[l], Lp[l]) : Lp[l];
       __syncwarp();
-      C res[NL];
-      separable_warp<T, L>(mats, sg0, sg1, sg2i, sbuf[warp][0], sbuf[warp][1], res, lane);
+      C res[NLN][L];
+      Sep<T, L>::run(mats, sg0, sg1, sg2i, sbuf[warp][0], sbuf[warp][1], res, lane);
       if (hf) {
         const double* dv = P.dirs + 3 * (P.dir_off[h] + d);
         const C ph = expi64<C>(P.kappa * (v[0] * dv[0] + v[1] * dv[1] + v[2] * dv[2]));
 #pragma unroll
-        for (int m = 0; m < NL; m++) {
-          const int l = lane + 32 * m;
-          if (l < LL) cfma(acc[m], ph, cmulc(sg[l], res[m]));
+        for (int q = 0; q < NLN; q++) {
+          const int ln = lane + 32 * q;
+          if (ln < L * L)
+#pragma unroll
+            for (int k = 0; k < L; k++) cfma(acc[q][k], ph, cmulc(sg[k * L * L + ln], res[q][k]));
         }
       } else {
 #pragma unroll
-        for (int m = 0; m < NL; m++) {
-          acc[m].x += res[m].x;
-          acc[m].y += res[m].y;
-        }
+        for (int q = 0; q < NLN; q++)
+#pragma unroll
+          for (int k = 0; k < L; k++) {
+            acc[q][k].x += res[q][k].x;
+            acc[q][k].y += res[q][k].y;
+          }
       }
     }
 #pragma unroll
-    for (int m = 0; m < NL; m++) {
-      const int l = lane + 32 * m;
-      if (l < LL) {
-        C o = Lx[cs * LL + l];
-        o.x += acc[m].x;
-        o.y += acc[m].y;
-        Lx[cs * LL + l] = o;
-      }
+    for (int q = 0; q < NLN; q++) {
+      const int ln = lane + 32 * q;
+      if (ln < L * L)
+#pragma unroll
+        for (int k = 0; k < L; k++) {
+          const int64_t l = cs * LL + k * L * L + ln;
+          C o = Lx[l];
+          o.x += acc[q][k].x;
+          o.y += acc[q][k].y;
+          Lx[l] = o;
+        }
     }
   }
 }
@@ -339,9 +412,11 @@ __global__ void __launch_bounds__(128) k_l2l(DevPlan P, int64_t s0, int64_t s1,
 // Pruned odd-size 3-D DFT (size P = 2L-1) of the zero-padded expansion
 // (circulant.hpp:96-106: M sits at the low corner of the P^3 grid):
 //   F[k0,k1,k2] = sum_{a,b,c<L} M[a,b,c] w^(k0 a + k1 b + k2 c),  w = e^{-2 pi i/P}
+// One CTA per expansion; each axis pass gives one thread one line (its L
+// inputs in registers, its P outputs computed from them).
 template <typename T, int L>
-__global__ void k_m2f(int64_t n, const typename cpx_t<T>::type* __restrict__ M,
-                      typename cpx_t<T>::type* __restrict__ F) {
+__global__ void __launch_bounds__(128) k_m2f(int64_t n, const typename cpx_t<T>::type* __restrict__ M,
+                                             typename cpx_t<T>::type* __restrict__ F) {
   typedef typename cpx_t<T>::type C;
   constexpr int P = 2 * L - 1, LL = L * L * L, PP = P * P * P;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -359,119 +434,156 @@ __global__ void k_m2f(int64_t n, const typename cpx_t<T>::type* __restrict__ M,
     __syncthreads();
     for (int i = threadIdx.x; i < LL; i += blockDim.x) Mi[i] = M[e * LL + i];
     __syncthreads();
-    for (int o = threadIdx.x; o < L * L * P; o += blockDim.x) {
-      const int ab = o / P, k2 = o % P;
-      C acc = czero<C>();
+    for (int ln = threadIdx.x; ln < L * L; ln += blockDim.x) {  // axis 2: (a,b) lines
+      C v[L];
 #pragma unroll
-      for (int c = 0; c < L; c++) cfma(acc, Mi[ab * L + c], W[(k2 * c) % P]);
-      A[o] = acc;
+      for (int c = 0; c < L; c++) v[c] = Mi[ln * L + c];
+#pragma unroll
+      for (int k2 = 0; k2 < P; k2++) {
+        C acc = v[0];
+#pragma unroll
+        for (int c = 1; c < L; c++) cfma(acc, v[c], W[(k2 * c) % P]);
+        A[ln * P + k2] = acc;
+      }
     }
     __syncthreads();
-    for (int o = threadIdx.x; o < L * P * P; o += blockDim.x) {
-      const int a = o / (P * P), k1 = (o / P) % P, k2 = o % P;
-      C acc = czero<C>();
+    for (int ln = threadIdx.x; ln < L * P; ln += blockDim.x) {  // axis 1: (a,k2) lines
+      const int a = ln / P, k2 = ln % P;
+      C v[L];
 #pragma unroll
-      for (int b = 0; b < L; b++) cfma(acc, A[(a * L + b) * P + k2], W[(k1 * b) % P]);
-      B[o] = acc;
+      for (int b = 0; b < L; b++) v[b] = A[(a * L + b) * P + k2];
+#pragma unroll
+      for (int k1 = 0; k1 < P; k1++) {
+        C acc = v[0];
+#pragma unroll
+        for (int b = 1; b < L; b++) cfma(acc, v[b], W[(k1 * b) % P]);
+        B[(a * P + k1) * P + k2] = acc;
+      }
     }
     __syncthreads();
-    for (int o = threadIdx.x; o < PP; o += blockDim.x) {
-      const int k0 = o / (P * P), k12 = o % (P * P);
-      C acc = czero<C>();
+    for (int ln = threadIdx.x; ln < P * P; ln += blockDim.x) {  // axis 0: (k1,k2) lines
+      C v[L];
 #pragma unroll
-      for (int a = 0; a < L; a++) cfma(acc, B[a * P * P + k12], W[(k0 * a) % P]);
-      F[e * PP + o] = acc;
+      for (int a = 0; a < L; a++) v[a] = B[a * P * P + ln];
+#pragma unroll
+      for (int k0 = 0; k0 < P; k0++) {
+        C acc = v[0];
+#pragma unroll
+        for (int a = 1; a < L; a++) cfma(acc, v[a], W[(k0 * a) % P]);
+        F[e * PP + k0 * P * P + ln] = acc;
+      }
     }
   }
 }
 
-// L[a,b,c] += (1/PP) sum_k J[k] conj(w)^(k0 a + k1 b + k2 c), a,b,c < L
-// (circulant.hpp:109-118: unnormalised backward DFT, gather at itilda, /PP)
-template <typename T, int L>
-__global__ void k_f2l(int64_t n, const typename cpx_t<T>::type* __restrict__ J,
-                      typename cpx_t<T>::type* __restrict__ Lx) {
+// Gather the permuted spectra used by M2L once (permutations.hpp:128-150):
+// U_k[i] = tables[key_k >> 6][perm[key_k & 63][i]].
+template <typename T>
+__global__ void k_permute_tables(int64_t n, int PP, const uint32_t* __restrict__ key, const uint16_t* __restrict__ perm,
+                                 const typename cpx_t<T>::type* __restrict__ tables,
+                                 typename cpx_t<T>::type* __restrict__ out) {
+  for (int64_t k = blockIdx.x; k < n; k += gridDim.x) {
+    const uint32_t kk = key[k];
+    const typename cpx_t<T>::type* U = tables + (int64_t)(kk >> 6) * PP;
+    const uint16_t* pm = perm + (int64_t)(kk & 63) * PP;
+    for (int i = threadIdx.x; i < PP; i += blockDim.x) out[k * PP + i] = U[pm[i]];
+  }
+}
+
+// -------------------------------------------------------------- M2L + F2L --
+// One CTA per target slot of a cone batch (M2L.hpp:115-157 target-stationary,
+// then fourier2geom circulant.hpp:109-118):
+//   J[i] = sum_{(s, k) in list(t)} U_k[i] F_s[i]          (registers)
+//   L_t[a,b,c] += (1/PP) sum_k J[k] conj(w)^(k0 a + k1 b + k2 c)   (pruned
+//   inverse DFT in shared memory, one line per thread per axis pass)
+// J never leaves the SM.
+template <typename T, int L, int NT>
+__global__ void __launch_bounds__(NT) k_m2l(DevPlan P, int64_t t0, int64_t t1, int64_t f0, int64_t f1,
+                                            const typename cpx_t<T>::type* __restrict__ F,
+                                            const typename cpx_t<T>::type* __restrict__ ptab,
+                                            typename cpx_t<T>::type* __restrict__ Lx) {
   typedef typename cpx_t<T>::type C;
-  constexpr int P = 2 * L - 1, LL = L * L * L, PP = P * P * P;
+  constexpr int PD = 2 * L - 1, LL = L * L * L, PP = PD * PD * PD, K = (PP + NT - 1) / NT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* W = reinterpret_cast<C*>(smem_raw);
-  C* Ji = W + P;
-  C* Cb = Ji + PP;
-  C* D = Cb + L * P * P;
-  for (int m = threadIdx.x; m < P; m += blockDim.x) {
+  C* Js = W + PD;
+  C* Cb = Js + PP;
+  C* D = Cb + L * PD * PD;
+  for (int m = threadIdx.x; m < PD; m += blockDim.x) {
     double s, c;
-    sincospi(2.0 * m / P, &s, &c);
+    sincospi(2.0 * m / PD, &s, &c);
     W[m].x = (T)c;
     W[m].y = (T)s;
   }
   const T inv = T(1) / T(PP);
-  for (int64_t e = blockIdx.x; e < n; e += gridDim.x) {
-    __syncthreads();
-    for (int i = threadIdx.x; i < PP; i += blockDim.x) Ji[i] = J[e * PP + i];
-    __syncthreads();
-    for (int o = threadIdx.x; o < L * P * P; o += blockDim.x) {
-      const int a = o / (P * P), k12 = o % (P * P);
-      C acc = czero<C>();
-#pragma unroll
-      for (int k0 = 0; k0 < P; k0++) cfma(acc, Ji[k0 * P * P + k12], W[(k0 * a) % P]);
-      Cb[o] = acc;
-    }
-    __syncthreads();
-    for (int o = threadIdx.x; o < L * L * P; o += blockDim.x) {
-      const int a = o / (L * P), b = (o / P) % L, k2 = o % P;
-      C acc = czero<C>();
-#pragma unroll
-      for (int k1 = 0; k1 < P; k1++) cfma(acc, Cb[(a * P + k1) * P + k2], W[(k1 * b) % P]);
-      D[o] = acc;
-    }
-    __syncthreads();
-    for (int o = threadIdx.x; o < LL; o += blockDim.x) {
-      const int ab = o / L, c = o % L;
-      C acc = czero<C>();
-#pragma unroll
-      for (int k2 = 0; k2 < P; k2++) cfma(acc, D[ab * P + k2], W[(k2 * c) % P]);
-      C v = Lx[e * LL + o];
-      v.x += acc.x * inv;
-      v.y += acc.y * inv;
-      Lx[e * LL + o] = v;
-    }
-  }
-}
-
-// -------------------------------------------------------------------- M2L --
-// One CTA per target slot of a cone batch (M2L.hpp:115-157, target-
-// stationary):  J_t[i] = sum_{(s, u, h) in list(t)} u[perm_h[i]] * F_s[i]
-template <typename T, int L, int NT>
-__global__ void __launch_bounds__(NT) k_m2l(DevPlan P, int64_t t0, int64_t t1, int64_t f0, int64_t f1,
-                                            const typename cpx_t<T>::type* __restrict__ F,
-                                            const typename cpx_t<T>::type* __restrict__ tables,
-                                            typename cpx_t<T>::type* __restrict__ J) {
-  typedef typename cpx_t<T>::type C;
-  constexpr int PD = 2 * L - 1, PP = PD * PD * PD, K = (PP + NT - 1) / NT;
   for (int64_t t = t0 + blockIdx.x; t < t1; t += gridDim.x) {
+    const int64_t eb = P.m2l_ptr[t], ee = P.m2l_ptr[t + 1];
     C acc[K];
 #pragma unroll
     for (int k = 0; k < K; k++) acc[k] = czero<C>();
-    const int64_t eb = P.m2l_ptr[t], ee = P.m2l_ptr[t + 1];
     for (int64_t e = eb; e < ee; e++) {
       const int64_t src = P.m2l_src[e];
-      const uint32_t tb = P.m2l_tab[e];
       if (src < f0 || src >= f1) {  // entry outside this cone batch: a plan bug
         if (threadIdx.x == 0) atomicExch(P.err, 1);
         continue;
       }
       const C* Fs = F + (src - f0) * PP;
-      const C* U = tables + (int64_t)(tb >> 6) * PP;
-      const uint16_t* pm = P.perm + (int64_t)(tb & 63) * PP;
+      const C* U = ptab + (int64_t)P.m2l_tab[e] * PP;
 #pragma unroll
       for (int k = 0; k < K; k++) {
         const int i = threadIdx.x + k * NT;
-        if (i < PP) cfma(acc[k], U[pm[i]], Fs[i]);
+        if (i < PP) cfma(acc[k], U[i], Fs[i]);
       }
     }
+    __syncthreads();  // the previous slot's inverse DFT is done with Js/Cb/D
 #pragma unroll
     for (int k = 0; k < K; k++) {
       const int i = threadIdx.x + k * NT;
-      if (i < PP) J[(t - t0) * PP + i] = acc[k];
+      if (i < PP) Js[i] = acc[k];
+    }
+    __syncthreads();
+    for (int ln = threadIdx.x; ln < PD * PD; ln += NT) {  // axis 0: (k1,k2) lines -> a
+      C v[PD];
+#pragma unroll
+      for (int k0 = 0; k0 < PD; k0++) v[k0] = Js[k0 * PD * PD + ln];
+#pragma unroll
+      for (int a = 0; a < L; a++) {
+        C s = v[0];
+#pragma unroll
+        for (int k0 = 1; k0 < PD; k0++) cfma(s, v[k0], W[(k0 * a) % PD]);
+        Cb[a * PD * PD + ln] = s;
+      }
+    }
+    __syncthreads();
+    for (int ln = threadIdx.x; ln < L * PD; ln += NT) {  // axis 1: (a,k2) lines -> b
+      const int a = ln / PD, k2 = ln % PD;
+      C v[PD];
+#pragma unroll
+      for (int k1 = 0; k1 < PD; k1++) v[k1] = Cb[(a * PD + k1) * PD + k2];
+#pragma unroll
+      for (int b = 0; b < L; b++) {
+        C s = v[0];
+#pragma unroll
+        for (int k1 = 1; k1 < PD; k1++) cfma(s, v[k1], W[(k1 * b) % PD]);
+        D[(a * L + b) * PD + k2] = s;
+      }
+    }
+    __syncthreads();
+    C* Lt = Lx + t * LL;
+    for (int ln = threadIdx.x; ln < L * L; ln += NT) {  // axis 2: (a,b) lines -> c
+      C v[PD];
+#pragma unroll
+      for (int k2 = 0; k2 < PD; k2++) v[k2] = D[ln * PD + k2];
+#pragma unroll
+      for (int c = 0; c < L; c++) {
+        C s = v[0];
+#pragma unroll
+        for (int k2 = 1; k2 < PD; k2++) cfma(s, v[k2], W[(k2 * c) % PD]);
+        C o = Lt[ln * L + c];
+        o.x += s.x * inv;
+        o.y += s.y * inv;
+        Lt[ln * L + c] = o;
+      }
     }
   }
 }
@@ -481,6 +593,9 @@ __global__ void __launch_bounds__(NT) k_m2l(DevPlan P, int64_t t0, int64_t t1, i
 // (dwnpass.hpp:39-47): HF (phfL2P, L2P.hpp:122-142)
 //   p_j = sum_d exp(i k d.(x_j - c)) sum_l Z(j, l) sig2_d[l] L_d[l]
 // LF (plfL2P :165-173): p_j = sum_l Z(j, l) L[l].  Writes p_far.
+// Warps take the leaf's slots in turn, lanes its particles; each lane keeps
+// its particle's 3 L basis values in registers and accumulates over the
+// warp's slots in registers; the 4 warps are summed at the end.
 template <typename T, int L>
 __global__ void __launch_bounds__(128) k_l2p(DevPlan P, const int32_t* __restrict__ leaves, int nleaves,
                                              const typename cpx_t<T>::type* __restrict__ sig2,
@@ -488,10 +603,8 @@ __global__ void __launch_bounds__(128) k_l2p(DevPlan P, const int32_t* __restric
                                              double2* __restrict__ pfar) {
   typedef typename cpx_t<T>::type C;
   constexpr int LL = L * L * L;
-  constexpr int NPB = 64;
-  __shared__ T Bs[NPB][3][L];
   __shared__ C buf[4][LL];
-  __shared__ double2 pacc[4][NPB];
+  __shared__ double2 part[4][32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int li = blockIdx.x; li < nleaves; li += gridDim.x) {
     const int c = leaves[li];
@@ -503,104 +616,225 @@ __global__ void __launch_bounds__(128) k_l2p(DevPlan P, const int32_t* __restric
     const int64_t sb = P.T_cptr[c], se = P.T_cptr[c + 1];
     const double* dirs = P.dirs + P.dir_off[h] * 3;
     const C* s2 = sig2 + P.sig_off[h];
-    for (int p0 = 0; p0 < n; p0 += NPB) {
-      const int np = min(NPB, n - p0);
-      __syncthreads();
-      for (int o = threadIdx.x; o < 3 * np; o += blockDim.x) {
-        const int p = o / 3, k = o % 3;
-        const double x = P.T_pos[3 * (int64_t)(f + p0 + p) + k] - (&ct.x)[k];
-        T b[L];
-        lagrange_all<L, T>((T)x, (T)ct.w, b);
+    for (int p0 = 0; p0 < n; p0 += 32) {
+      const int np = min(32, n - p0);
+      const int pi = f + p0 + min(lane, np - 1);
+      double xr[3];
+      T B[3][L];
 #pragma unroll
-        for (int l = 0; l < L; l++) Bs[p][k][l] = b[l];
+      for (int k = 0; k < 3; k++) {
+        xr[k] = P.T_pos[3 * (int64_t)pi + k] - (&ct.x)[k];
+        lagrange_all<L, T>((T)xr[k], (T)ct.w, B[k]);
       }
-      for (int o = threadIdx.x; o < 4 * NPB; o += blockDim.x) pacc[o / NPB][o % NPB] = make_double2(0., 0.);
-      __syncthreads();
+      double2 acc = make_double2(0., 0.);
       for (int64_t j = sb + warp; j < se; j += 4) {
         const int slot = P.T_cslot[j], d = P.T_cdir[j];
         const C* Ls = Lx + (int64_t)slot * LL;
+        __syncwarp();
         for (int l = lane; l < LL; l += 32) buf[warp][l] = hf ? cmul(s2[(int64_t)d * LL + l], Ls[l]) : Ls[l];
         __syncwarp();
-        for (int p = lane; p < np; p += 32) {
-          C acc = czero<C>();
-          for (int l = 0; l < LL; l++) {
-            const int i0 = l / (L * L), i1 = (l / L) % L, i2 = l % L;
-            rfma(acc, Bs[p][0][i0] * Bs[p][1][i1] * Bs[p][2][i2], buf[warp][l]);
+        C sum = czero<C>();
+#pragma unroll
+        for (int a = 0; a < L; a++) {
+#pragma unroll
+          for (int b = 0; b < L; b++) {
+            const T zab = B[0][a] * B[1][b];
+#pragma unroll
+            for (int cc = 0; cc < L; cc++) rfma(sum, zab * B[2][cc], buf[warp][(a * L + b) * L + cc]);
           }
-          double2 a = make_double2((double)acc.x, (double)acc.y);
-          if (hf) {
-            const double* x = P.T_pos + 3 * (int64_t)(f + p0 + p);
-            const double* dv = dirs + 3 * d;
-            double dp = 0.;
-            for (int k = 0; k < 3; k++) dp += dv[k] * (x[k] - (&ct.x)[k]);
-            a = cmul(a, expi64<double2>(P.kappa * dp));
-          }
-          pacc[warp][p].x += a.x;
-          pacc[warp][p].y += a.y;
         }
-        __syncwarp();
+        double2 v = make_double2((double)sum.x, (double)sum.y);
+        if (hf) {
+          const double* dv = dirs + 3 * d;
+          v = cmul(v, expi64<double2>(P.kappa * (dv[0] * xr[0] + dv[1] * xr[1] + dv[2] * xr[2])));
+        }
+        acc.x += v.x;
+        acc.y += v.y;
       }
       __syncthreads();
-      for (int p = threadIdx.x; p < np; p += blockDim.x) {
-        double2 s = pacc[0][p];
+      part[warp][lane] = acc;
+      __syncthreads();
+      if (threadIdx.x < np) {
+        double2 t = part[0][threadIdx.x];
         for (int w = 1; w < 4; w++) {
-          s.x += pacc[w][p].x;
-          s.y += pacc[w][p].y;
+          t.x += part[w][threadIdx.x].x;
+          t.y += part[w][threadIdx.x].y;
         }
-        pfar[f + p0 + p] = s;
+        pfar[f + p0 + threadIdx.x] = t;
       }
     }
   }
 }
 
 // -------------------------------------------------------------------- P2P --
-// Near field (P2P.hpp:43-79) on whole cells, target-stationary: one warp per
-// chunk of <= 32 target particles of one leaf.  Lanes split into groups of
-// tp >= nt lanes (one target each); groups take interleaved sources and are
-// reduced by shuffles.  Pairs with r^2 < 1e-16 contribute nothing.  Writes
-// p_near.  FP64 throughout.
-__global__ void __launch_bounds__(256) k_p2p_fp64(DevPlan P, int64_t nchunk, const int32_t* __restrict__ tfirst,
-                                                  const int32_t* __restrict__ tn, const int64_t* __restrict__ ptr,
-                                                  const int32_t* __restrict__ sfirst, const int32_t* __restrict__ sn,
-                                                  const double2* __restrict__ q, double2* __restrict__ pnear) {
-  const int lane = threadIdx.x & 31;
+// Mixed-precision near field.  The phase k r needs ~1e-7 rad absolute
+// accuracy at k r up to ~1e2, beyond FP32: the difference vector, r^2, r and
+// the reduction of k r to [-pi/4, pi/4] (quadrant n = rint(k r * 2/pi)) run
+// in FP64; sin/cos of the reduced angle are evaluated in FP32 by their Taylor
+// series to degree 9/10 (truncation < 2e-9 on [-pi/4, pi/4]), 1/(4 pi r),
+// the complex products and the per-lane accumulation (Kahan-compensated) in
+// FP32; the cross-lane reduction and the result in FP64.
+__device__ __forceinline__ void sincos_reduced(double theta, float& s, float& c) {
+  const double n = rint(theta * 0.63661977236758134308);  // 2/pi
+  const float x = (float)fma(-n, 1.5707963267948966192, theta);
+  const float x2 = x * x;
+  // sin x = x (1 - x^2/3! + x^4/5! - x^6/7! + x^8/9!)
+  float ps = fmaf(x2, 2.7557319223985893e-06f, -1.9841269841269841e-04f);
+  ps = fmaf(x2, ps, 8.3333333333333333e-03f);
+  ps = fmaf(x2, ps, -1.6666666666666667e-01f);
+  ps = fmaf(x2, ps, 1.0f);
+  const float sx = x * ps;
+  // cos x = 1 - x^2/2! + x^4/4! - x^6/6! + x^8/8! - x^10/10!
+  float pc = fmaf(x2, -2.7557319223985891e-07f, 2.4801587301587302e-05f);
+  pc = fmaf(x2, pc, -1.3888888888888889e-03f);
+  pc = fmaf(x2, pc, 4.1666666666666667e-02f);
+  pc = fmaf(x2, pc, -0.5f);
+  const float cx = fmaf(x2, pc, 1.0f);
+  const int q = ((int)n) & 3;
+  const float ss = (q & 1) ? cx : sx, cc = (q & 1) ? sx : cx;
+  s = (q & 2) ? -ss : ss;
+  c = ((q + 1) & 2) ? -cc : cc;
+}
+
+__device__ __forceinline__ void kahan_add(float& sum, float& comp, float v) {
+  const float y = v - comp;
+  const float t = sum + y;
+  comp = (t - sum) - y;
+  sum = t;
+}
+
+// Near field, tiled: one CTA (4 warps) per chunk of <= 32 target particles
+// of one leaf; CTAs take chunks from a global queue (the host orders chunks
+// by decreasing work).  The chunk's source ranges are streamed through shared
+// memory in tiles of TS particles loaded with coalesced reads; inside a warp,
+// lanes form groups of tp >= nt lanes (one target each) and the 4 warps x
+// groups take interleaved sources of the tile, two at a time.  Partial sums
+// are reduced in FP64 through shuffles and shared memory; each target is
+// written once.
+//   MIXED = false: FP64 throughout (P2P.hpp:43-79 arithmetic).
+//   MIXED = true : difference vector, r^2, r (FP32 sqrt + one FP64 Newton
+//   step) and the reduction of k r in FP64; sin/cos of the reduced angle,
+//   1/(4 pi r) and the compensated accumulation in FP32.
+template <bool MIXED, typename Q>
+__device__ __forceinline__ void p2p_pair(double x0, double x1, double x2, double sx, double sy, double sz, Q qq,
+                                         double kappa, double& pr, double& pim, float& sr, float& cr, float& si,
+                                         float& ci) {
   const double pi4m1 = 1. / (4. * 3.14159265358979323846);
-  for (int64_t ch = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); ch < nchunk;
-       ch += (int64_t)gridDim.x * (blockDim.x >> 5)) {
+  const double dx = x0 - sx, dy = x1 - sy, dz = x2 - sz;
+  const double R = fma(dx, dx, fma(dy, dy, dz * dz));
+  if (R < 1.e-16) return;  // self / duplicate pairs (P2P.hpp:66)
+  if (!MIXED) {
+    // 1/sqrt(R): FP32 estimate, two Newton steps in FP64 (quadratic: 2^-22 -> 2^-88)
+    double y = (double)rsqrtf((float)R);
+    const double hR = 0.5 * R;
+    y = y * fma(-hR * y, y, 1.5);
+    y = y * fma(-hR * y, y, 1.5);
+    const double rr = y * R * kappa;
+    const double K = y * pi4m1;
+    double sn_, cs_;
+    sincos_cw(rr, sn_, cs_);
+    cs_ *= K;
+    sn_ *= K;
+    pr = fma(cs_, (double)qq.x, fma(-sn_, (double)qq.y, pr));
+    pim = fma(cs_, (double)qq.y, fma(sn_, (double)qq.x, pim));
+  } else {
+    // r to ~1e-14 relative: FP32 reciprocal square root refined once in
+    // FP32, one Newton step for r in FP64 (rf^2 is exact in FP64)
+    const float Rf = (float)R;
+    float y = rsqrtf(Rf);
+    y = y * fmaf(-0.5f * Rf * y, y, 1.5f);
+    const float rf = Rf * y;
+    const double rr = fma(R - (double)rf * (double)rf, (double)(0.5f * y), (double)rf);
+    float s, c;
+    sincos_reduced(rr * kappa, s, c);
+    const float K = (float)pi4m1 * y;
+    c *= K;
+    s *= K;
+    kahan_add(sr, cr, fmaf(c, (float)qq.x, -s * (float)qq.y));
+    kahan_add(si, ci, fmaf(c, (float)qq.y, s * (float)qq.x));
+  }
+}
+
+template <bool MIXED>
+__global__ void __launch_bounds__(128) k_p2p_tiled(DevPlan P, int64_t nchunk, const int32_t* __restrict__ order,
+                                                   const int32_t* __restrict__ tfirst, const int32_t* __restrict__ tn,
+                                                   const int64_t* __restrict__ ptr, const int32_t* __restrict__ sfirst,
+                                                   const int32_t* __restrict__ sn, const void* __restrict__ qv,
+                                                   double2* __restrict__ pnear, unsigned long long* __restrict__ queue) {
+  constexpr int TS = 512;
+  typedef typename std::conditional<MIXED, float2, double2>::type Q;
+  const Q* q = static_cast<const Q*>(qv);
+  __shared__ double sx[TS], sy[TS], sz[TS];
+  __shared__ Q sq[TS];
+  __shared__ double2 red[4][32];
+  __shared__ int64_t cur;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) cur = (int64_t)atomicAdd(queue, 1ULL);
+    __syncthreads();
+    const int64_t k = cur;
+    if (k >= nchunk) break;
+    const int64_t ch = order[k];
     const int f = tfirst[ch], nt = tn[ch];
     int tp = 1;
     while (tp < nt) tp <<= 1;
-    const int groups = 32 / tp;
-    const int mt = lane & (tp - 1), g = lane / tp;
+    const int groups = 32 / tp, G = 4 * groups;
+    const int mt = lane & (tp - 1), gid = warp * groups + lane / tp;
     const int ti = f + min(mt, nt - 1);
     const double x0 = P.T_pos[3 * (int64_t)ti], x1 = P.T_pos[3 * (int64_t)ti + 1], x2 = P.T_pos[3 * (int64_t)ti + 2];
     double pr = 0., pim = 0.;
+    float sr = 0.f, cr = 0.f, si = 0.f, ci = 0.f;
     const int64_t rb = ptr[ch], re = ptr[ch + 1];
-    for (int64_t r = rb; r < re; r++) {
-      const int sf = sfirst[r], ns = sn[r];
-      for (int j = g; j < ns; j += groups) {
-        const int64_t sj = sf + j;
-        const double y0 = P.S_pos[3 * sj], y1 = P.S_pos[3 * sj + 1], y2 = P.S_pos[3 * sj + 2];
-        const double2 qq = q[sj];
-        const double dx = x0 - y0, dy = x1 - y1, dz = x2 - y2;
-        const double R = dx * dx + dy * dy + dz * dz;
-        double K = rsqrt(R);
-        if (R < 1.e-16) K = 0.;
-        const double rr = K * R * P.kappa;
-        K *= pi4m1;
-        double s, c;
-        sincos(rr, &s, &c);
-        c *= K;
-        s *= K;
-        pr += c * qq.x - s * qq.y;
-        pim += c * qq.y + s * qq.x;
+    int64_t r = rb;
+    int off = 0;  // position inside range r
+    while (r < re) {
+      // fill one tile from consecutive ranges (uniform control flow)
+      int fill = 0;
+      __syncthreads();
+      while (r < re && fill < TS) {
+        const int s0 = sfirst[r], ns = sn[r];
+        const int take = min(ns - off, TS - fill);
+        for (int t = threadIdx.x; t < take; t += blockDim.x) {
+          const int64_t sj = (int64_t)s0 + off + t;
+          sx[fill + t] = P.S_pos[3 * sj];
+          sy[fill + t] = P.S_pos[3 * sj + 1];
+          sz[fill + t] = P.S_pos[3 * sj + 2];
+          sq[fill + t] = q[sj];
+        }
+        fill += take;
+        off += take;
+        if (off == ns) {
+          r++;
+          off = 0;
+        }
       }
+      __syncthreads();
+      int j = gid;
+      for (; j + G < fill; j += 2 * G) {
+        p2p_pair<MIXED>(x0, x1, x2, sx[j], sy[j], sz[j], sq[j], P.kappa, pr, pim, sr, cr, si, ci);
+        p2p_pair<MIXED>(x0, x1, x2, sx[j + G], sy[j + G], sz[j + G], sq[j + G], P.kappa, pr, pim, sr, cr, si, ci);
+      }
+      if (j < fill) p2p_pair<MIXED>(x0, x1, x2, sx[j], sy[j], sz[j], sq[j], P.kappa, pr, pim, sr, cr, si, ci);
     }
-    for (int off = tp; off < 32; off <<= 1) {
-      pr += __shfl_xor_sync(0xffffffffu, pr, off);
-      pim += __shfl_xor_sync(0xffffffffu, pim, off);
+    if (MIXED) {
+      pr = (double)sr - (double)cr;
+      pim = (double)si - (double)ci;
     }
-    if (g == 0 && mt < nt) pnear[f + mt] = make_double2(pr, pim);
+    for (int o = tp; o < 32; o <<= 1) {
+      pr += __shfl_xor_sync(0xffffffffu, pr, o);
+      pim += __shfl_xor_sync(0xffffffffu, pim, o);
+    }
+    if (lane < tp) red[warp][lane] = make_double2(pr, pim);
+    __syncthreads();
+    if (threadIdx.x < nt) {
+      double2 a = red[0][threadIdx.x];
+      for (int w = 1; w < 4; w++) {
+        a.x += red[w][threadIdx.x].x;
+        a.y += red[w][threadIdx.x].y;
+      }
+      pnear[f + threadIdx.x] = a;
+    }
   }
 }
 
@@ -653,11 +887,11 @@ struct Launch {
   static constexpr int P = 2 * L - 1, LL = L * L * L, PP = P * P * P;
   static constexpr int NT = PP > 1024 ? 256 : 128;
   static size_t smem_m2f() { return sizeof(C) * (P + LL + L * L * P + L * P * P); }
-  static size_t smem_f2l() { return sizeof(C) * (P + PP + L * P * P + L * L * P); }
+  static size_t smem_m2l() { return sizeof(C) * (P + PP + L * P * P + L * L * P); }
   static cudaError_t setup() {
     cudaError_t e = cudaFuncSetAttribute(k_m2f<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_m2f());
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_f2l<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_f2l());
+    return cudaFuncSetAttribute(k_m2l<T, L, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_m2l());
   }
   static void p2m(const DevPlan& dp, const int32_t* leaves, int n, const void* q, const void* sig2, void* M,
                   cudaStream_t s) {
@@ -676,13 +910,14 @@ struct Launch {
   static void m2f(int64_t n, const void* M, void* F, cudaStream_t s) {
     if (n) k_m2f<T, L><<<grid_for(n, 1), 128, smem_m2f(), s>>>(n, (const C*)M, (C*)F);
   }
-  static void f2l(int64_t n, const void* J, void* Lx, cudaStream_t s) {
-    if (n) k_f2l<T, L><<<grid_for(n, 1), 128, smem_f2l(), s>>>(n, (const C*)J, (C*)Lx);
-  }
   static void m2l(const DevPlan& dp, int64_t t0, int64_t t1, int64_t f0, int64_t f1, const void* F,
-                  const void* tables, void* J, cudaStream_t s) {
+                  const void* ptab, void* Lx, cudaStream_t s) {
     if (t1 > t0)
-      k_m2l<T, L, NT><<<grid_for(t1 - t0, 1), NT, 0, s>>>(dp, t0, t1, f0, f1, (const C*)F, (const C*)tables, (C*)J);
+      k_m2l<T, L, NT><<<grid_for(t1 - t0, 1), NT, smem_m2l(), s>>>(dp, t0, t1, f0, f1, (const C*)F, (const C*)ptab, (C*)Lx);
+  }
+  static void permute(int64_t n, const uint32_t* key, const uint16_t* perm, const void* tables, void* out,
+                      cudaStream_t s) {
+    if (n) k_permute_tables<T><<<grid_for(n, 1), 256, 0, s>>>(n, PP, key, perm, (const C*)tables, (C*)out);
   }
   static void l2p(const DevPlan& dp, const int32_t* leaves, int n, const void* sig2, const void* Lx, double2* pfar,
                   cudaStream_t s) {
@@ -696,7 +931,7 @@ const OpTable* op_table_for(int L);
 #define DFB_OPS(T, L)                                                                                     \
   {                                                                                                       \
     Launch<T, L>::setup, Launch<T, L>::p2m, Launch<T, L>::m2m, Launch<T, L>::l2l, Launch<T, L>::m2f,       \
-        Launch<T, L>::f2l, Launch<T, L>::m2l, Launch<T, L>::l2p                                           \
+        Launch<T, L>::m2l, Launch<T, L>::l2p, Launch<T, L>::permute                                       \
   }
 
 template <>
@@ -743,9 +978,16 @@ void launch_scatter(const double2* pnear, const double2* pfar, const int32_t* pe
   k_scatter<<<(int)((n + 255) / 256), 256, 0, s>>>(pnear, pfar, perm, out, n);
 }
 
-void launch_p2p_fp64(const DevPlan& dp, int64_t nchunk, const int32_t* tfirst, const int32_t* tn, const int64_t* ptr,
-                     const int32_t* sfirst, const int32_t* sn, const double2* q, double2* pnear, cudaStream_t s) {
-  if (nchunk) k_p2p_fp64<<<grid_for(nchunk, 8, 148 * 32), 256, 0, s>>>(dp, nchunk, tfirst, tn, ptr, sfirst, sn, q, pnear);
+void launch_p2p(bool fp64, const DevPlan& dp, int64_t nchunk, const int32_t* order, const int32_t* tfirst,
+                const int32_t* tn, const int64_t* ptr, const int32_t* sfirst, const int32_t* sn, const void* q,
+                double2* pnear, unsigned long long* queue, int nsm, cudaStream_t s) {
+  if (!nchunk) return;
+  cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s);
+  const int grid = (int)std::min<int64_t>(nchunk, (int64_t)nsm * 16);
+  if (fp64)
+    k_p2p_tiled<false><<<grid, 128, 0, s>>>(dp, nchunk, order, tfirst, tn, ptr, sfirst, sn, q, pnear, queue);
+  else
+    k_p2p_tiled<true><<<grid, 128, 0, s>>>(dp, nchunk, order, tfirst, tn, ptr, sfirst, sn, q, pnear, queue);
 }
 
 void launch_direct(int64_t ns, const double* spos, const int32_t* sperm, const double2* qin, int64_t nt,

@@ -16,11 +16,14 @@ struct OpTable {
   void (*m2m)(const DevPlan&, int64_t s0, int64_t s1, const void* sig, const void* sig2, void* M, cudaStream_t);
   void (*l2l)(const DevPlan&, int64_t s0, int64_t s1, const void* sig, const void* sig2, void* Lx, cudaStream_t);
   void (*m2f)(int64_t n, const void* M, void* F, cudaStream_t);
-  void (*f2l)(int64_t n, const void* J, void* Lx, cudaStream_t);
-  void (*m2l)(const DevPlan&, int64_t t0, int64_t t1, int64_t f0, int64_t f1, const void* F, const void* tables,
-              void* J, cudaStream_t);
+  // M2L with the inverse DFT fused: adds into L of target slots [t0, t1)
+  void (*m2l)(const DevPlan&, int64_t t0, int64_t t1, int64_t f0, int64_t f1, const void* F, const void* ptab,
+              void* Lx, cudaStream_t);
   void (*l2p)(const DevPlan&, const int32_t* leaves, int n, const void* sig2, const void* Lx, double2* pfar,
               cudaStream_t);
+  // U_k = tables[key_k >> 6][perm[key_k & 63][:]] for the permuted spectra
+  void (*permute)(int64_t n, const uint32_t* key, const uint16_t* perm, const void* tables, void* out,
+                  cudaStream_t);
 };
 
 const OpTable* op_table(int L, bool fp64);
@@ -29,8 +32,11 @@ void launch_gather(bool fp64, const double2* qin, const int32_t* perm, void* q, 
                    int64_t stride_q, int nrhs, cudaStream_t s);
 void launch_scatter(const double2* pnear, const double2* pfar, const int32_t* perm, double2* out, int64_t n,
                     cudaStream_t s);
-void launch_p2p_fp64(const DevPlan& dp, int64_t nchunk, const int32_t* tfirst, const int32_t* tn, const int64_t* ptr,
-                     const int32_t* sfirst, const int32_t* sn, const double2* q, double2* pnear, cudaStream_t s);
+// Near field (k_p2p_tiled); `order` lists chunks by decreasing work, `queue`
+// is a device counter the launch resets.
+void launch_p2p(bool fp64, const DevPlan& dp, int64_t nchunk, const int32_t* order, const int32_t* tfirst,
+                const int32_t* tn, const int64_t* ptr, const int32_t* sfirst, const int32_t* sn, const void* q,
+                double2* pnear, unsigned long long* queue, int nsm, cudaStream_t s);
 void launch_direct(int64_t ns, const double* spos, const int32_t* sperm, const double2* qin, int64_t nt,
                    const double* tpos, double kappa, double2* out, cudaStream_t s);
 

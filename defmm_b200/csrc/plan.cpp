@@ -906,6 +906,20 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
     }
   }
 
+  // permuted spectra: one per (spectrum, symmetry hash) pair that occurs
+  {
+    const int64_t ntab = (int64_t)tab_nI.size();
+    std::vector<int32_t> pid(ntab * 64, -1);
+    for (uint32_t k : p.m2l_tab) pid[k] = 0;
+    p.ptab_key.clear();
+    for (int64_t k = 0; k < ntab * 64; k++)
+      if (pid[k] == 0) {
+        pid[k] = (int32_t)p.ptab_key.size();
+        p.ptab_key.push_back((uint32_t)k);
+      }
+    pfor((int64_t)p.m2l_tab.size(), 1 << 16, [&](int64_t e) { p.m2l_tab[e] = (uint32_t)pid[p.m2l_tab[e]]; });
+  }
+
   // M2M: children slots of each source slot (P2M/M2M operators, M2M.hpp:35-124)
   {
     const Slots& s = p.sS;
@@ -1008,6 +1022,19 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
         p.p2p_ptr.push_back((int64_t)p.p2p_sfirst.size());
       }
     }
+  }
+  {
+    const int64_t nch = (int64_t)p.p2p_tfirst.size();
+    std::vector<int64_t> work(nch, 0);
+    for (int64_t c = 0; c < nch; c++) {
+      int64_t ns = 0;
+      for (int64_t r = p.p2p_ptr[c]; r < p.p2p_ptr[c + 1]; r++) ns += p.p2p_sn[r];
+      work[c] = ns * 32;  // a chunk occupies its 32-lane groups whatever its size
+    }
+    p.p2p_order.resize(nch);
+    for (int64_t c = 0; c < nch; c++) p.p2p_order[c] = (int32_t)c;
+    std::stable_sort(p.p2p_order.begin(), p.p2p_order.end(),
+                     [&](int32_t a, int32_t b) { return work[a] > work[b]; });
   }
   p.t_lists = now_s() - t0;
 

@@ -85,7 +85,10 @@ struct Plan {
   // M2L, grouped by target slot (CSR over target slots)
   std::vector<int64_t> m2l_ptr;            // sT.n + 1
   std::vector<int32_t> m2l_src;            // source slot
-  std::vector<uint32_t> m2l_tab;           // (table index << 6) | hash
+  std::vector<uint32_t> m2l_tab;           // permuted spectrum id (index into ptab_key)
+  // permuted spectra actually used: (table index << 6) | hash; the device
+  // holds U_k[i] = tables[key >> 6][perm[key & 63][i]]
+  std::vector<uint32_t> ptab_key;
   // M2M children of each source slot, L2L parents of each target slot
   std::vector<int64_t> m2m_ptr;            // sS.n + 1
   std::vector<int32_t> m2m_child;          // child slot
@@ -97,6 +100,7 @@ struct Plan {
   std::vector<int32_t> p2p_tfirst, p2p_tn;   // per chunk
   std::vector<int64_t> p2p_ptr;              // chunks + 1
   std::vector<int32_t> p2p_sfirst, p2p_sn;   // source particle ranges
+  std::vector<int32_t> p2p_order;            // chunks by decreasing work (tn x sources)
   // statistics
   int64_t n_far_hf = 0, n_far_lf = 0, n_near = 0, i_near = 0;
   // Optional record of the lists for parity checks: far (t, s, lvl, cone,

@@ -40,6 +40,9 @@ typedef struct defmm_handle defmm_handle;
 #define DEFMM_PRECISION_FP64 0   /* plain FP64, the drop-in for the reference  */
 #define DEFMM_PRECISION_MIXED 1  /* FP32 bulk arithmetic, FP64 phase reduction */
 
+/* Number of visible CUDA devices (0 when there is none or no driver). */
+int defmm_device_count(void);
+
 /* IBFMM_Mat<3>::IBFMM_Mat() (interface.hpp:57). */
 defmm_handle* defmm_create(void);
 /* ~IBFMM_Mat: releases host and device memory. */
@@ -115,10 +118,15 @@ int defmm_check_full(defmm_handle* h, int64_t nsamples, uint64_t seed,
 #define DEFMM_INFO_TABLES 13
 #define DEFMM_INFO_DEVICE_BYTES 14
 #define DEFMM_INFO_LIST_RECORDS 15 /* 1 if lists were recorded (parity) */
+#define DEFMM_INFO_LAUNCHES 16     /* kernels launched by the last gemv call */
+#define DEFMM_INFO_M2L_TARGETS 17  /* target slots receiving M2L */
+#define DEFMM_INFO_LEAF_SLOTS_S 18 /* source leaf expansions (P2M outputs) */
+#define DEFMM_INFO_PERMUTED_SPECTRA 19 /* (spectrum, symmetry) pairs used by M2L */
 int defmm_info(const defmm_handle* h, int what, int64_t* value);
 
 /* Per-phase device times (ms) of the last gemv, in this order:
- * gather+P2M, M2M, M2F, M2L, F2L, L2L, L2P, P2P, scatter, total. */
+ * P2M, M2M, M2F, M2L, F2L, L2L, L2P, P2P, gather+scatter, total.
+ * F2L is fused into the M2L kernel and reads 0. */
 int defmm_phase_times(const defmm_handle* h, double ms[10]);
 
 /* Per-phase timing with CUDA events (adds synchronisation between phases;

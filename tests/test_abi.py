@@ -1,0 +1,35 @@
+"""The C-ABI library loads and exports every entry point include/defmm_b200.h
+declares (no compute call: these tests run without a GPU)."""
+import ctypes
+import os
+import re
+
+from defmm_b200 import api
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    src = open(os.path.join(ROOT, "include", "defmm_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(defmm_[a-z_0-9]+)\s*\(", src)))
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    for s in ["defmm_create", "defmm_destroy", "defmm_prcmpt", "defmm_gemv", "defmm_gemv_device",
+              "defmm_gemv_batched", "defmm_check_full", "defmm_load_inp", "defmm_add_source_particle",
+              "defmm_add_target_particle"]:
+        assert s in syms
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(api._LIB_PATH)
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_create_destroy_without_device():
+    A = api.IBFMM_Mat()
+    assert A.info("n_sources") == 0
+    del A

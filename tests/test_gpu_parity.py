@@ -1,0 +1,123 @@
+"""GPU parity: the CUDA matvec through the C ABI against the oracle (the
+C++ restatement, itself pinned to the reference by tests/test_oracle.py) and
+against the reference's golden samples.
+
+Tolerances: plain FP64 path <= 1e-12 relative L2 (the reference's own
+summation order differs, so bitwise equality is not expected); mixed
+precision <= 1e-6 relative L2 against the FP64 path.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from defmm_b200 import IBFMM_Mat, workloads as W
+from oracle import oracle as O
+from tests.golden.cases import CASES, case_inputs
+from tests.golden.gen_golden import sample_index
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+FP64_TOL = 1e-12
+MIXED_TOL = 1e-6
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def make(src, trg, L, ncrit, kappa, lvmax=-1):
+    A = IBFMM_Mat()
+    A.addSourceParticles(src)
+    A.addTargetParticles(trg)
+    A.prcmpt(L, ncrit, kappa, lvmax)
+    return A
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_fp64_matches_oracle_and_reference_samples(name, gpu):
+    src, trg, q, L, ncrit, kappa, lvmax = case_inputs(name)
+    A = make(src, trg, L, ncrit, kappa, lvmax)
+    p = A.matvec(q)
+    po = O.OracleFMM(src, trg, L, ncrit, kappa, lvmax).gemv(q)
+    assert rel(p, po) <= FP64_TOL
+    sample = np.load(os.path.join(GOLD, f"{name}_pot_sample.npy"))
+    assert rel(p[sample_index(trg.shape[0])], sample) <= FP64_TOL
+
+
+@pytest.mark.parametrize("name", ["cube20k", "cube_lf", "blobs_sphere"])
+def test_mixed_matches_fp64(name, gpu):
+    src, trg, q, L, ncrit, kappa, lvmax = case_inputs(name)
+    A = make(src, trg, L, ncrit, kappa, lvmax)
+    p64 = A.matvec(q)
+    A.set_precision("mixed")
+    p32 = A.matvec(q)
+    assert rel(p32, p64) <= MIXED_TOL
+
+
+def test_repeated_gemv_is_correct_every_time(gpu):
+    # the reference's gemv is only valid on its first call after prcmpt
+    src, trg, q, L, ncrit, kappa, lvmax = case_inputs("cube_lf")
+    A = make(src, trg, L, ncrit, kappa, lvmax)
+    p1 = A.matvec(q)
+    p2 = A.matvec(q)
+    assert np.array_equal(p1, p2)
+    p3 = A.matvec(2 * q)
+    assert rel(p3, 2 * p1) <= 1e-14
+
+
+def test_batched_rhs_equal_single(gpu):
+    src, trg, q, L, ncrit, kappa, lvmax = case_inputs("blobs_sphere")
+    A = make(src, trg, L, ncrit, kappa, lvmax)
+    Q = np.stack([q, W.charges(len(q), 9), W.charges(len(q), 10)])
+    P = A.matvec(Q)
+    for r in range(3):
+        assert np.array_equal(P[r], A.matvec(Q[r]))
+
+
+def test_device_pointer_path_matches_host_path(gpu):
+    import torch
+    src, trg, q, L, ncrit, kappa, lvmax = case_inputs("cube_lf")
+    A = make(src, trg, L, ncrit, kappa, lvmax)
+    ph = A.matvec(q)
+    dq = torch.from_numpy(q).cuda()
+    dp = torch.empty(len(trg), dtype=torch.complex128, device="cuda")
+    A.matvec_device(dq.data_ptr(), dp.data_ptr(), 1, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert np.array_equal(dp.cpu().numpy(), ph)
+
+
+def test_check_full_samples_direct_sum(gpu):
+    src, trg, q, L, ncrit, kappa, lvmax = case_inputs("cube20k")
+    A = make(src, trg, L, ncrit, kappa, lvmax)
+    p = A.matvec(q)
+    e = A.check_full(300, seed=3)
+    # order-4 interpolation: the reference's own error is ~6e-4 here
+    assert 1e-6 < e["l2"] < 3e-3
+    idx = np.sort(np.random.default_rng(0).choice(len(trg), 50, replace=False))
+    ex = O.direct(src, q, trg[idx], kappa)
+    assert rel(p[idx], ex) < 3e-3
+
+
+def test_linearity_and_accuracy_at_larger_size(gpu):
+    # size-independent properties where the oracle would take minutes
+    w = W.sphere_surface(300_000, seed=5, wavelengths=48)
+    A = make(w.points, w.points, 5, 64, w.kappa)
+    q1, q2 = W.charges(w.n, 1), W.charges(w.n, 2)
+    p1, p2 = A.matvec(q1), A.matvec(q2)
+    p12 = A.matvec(q1 + 2j * q2)
+    assert rel(p12, p1 + 2j * p2) <= 1e-13
+    e = A.check_full(200, seed=1)
+    assert e["l2"] < 1e-3
+    A.set_precision("mixed")
+    assert rel(A.matvec(q1), p1) <= MIXED_TOL
+
+
+def test_sources_and_targets_apart(gpu):
+    src = W.sphere_surface(20000, seed=3, wavelengths=8).points * 0.4
+    trg = W.cube_surface(15000, seed=6).points
+    q = W.charges(len(src), 4)
+    A = make(src, trg, 4, 48, 2 * np.pi * 8)
+    po = O.OracleFMM(src, trg, 4, 48, 2 * np.pi * 8).gemv(q)
+    assert rel(A.matvec(q), po) <= FP64_TOL
