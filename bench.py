@@ -51,6 +51,8 @@ def workload(name, rank=0):
         return W.sphere_surface(2_000_000, seed=0)
     if name == "sphere100k":
         return W.sphere_surface(100_000, seed=0, wavelengths=32)
+    if name == "sphere200k":  # config-2 points per wavelength^2, for profiling
+        return W.sphere_surface(200_000, seed=0, wavelengths=40)
     if name == "cube20k":
         return W.cube_surface(20_000, seed=0)
     raise KeyError(name)

@@ -34,7 +34,8 @@ _INFO = {
     "n_sources": 0, "n_targets": 1, "nlvl": 2, "cpt": 3, "max_stage": 4, "cells_T": 5,
     "cells_S": 6, "slots_S": 7, "slots_T": 8, "far_hf": 9, "far_lf": 10, "near": 11,
     "i_near": 12, "tables": 13, "device_bytes": 14, "list_records": 15, "launches": 16,
-    "m2l_targets": 17, "leaf_slots_S": 18, "permuted_spectra": 19,
+    "m2l_targets": 17, "leaf_slots_S": 18, "permuted_spectra": 19, "m2l_groups": 20,
+    "m2l_records": 21,
 }
 PHASES = ["p2m", "m2m", "m2f", "m2l", "f2l", "l2l", "l2p", "p2p", "scatter", "total"]
 

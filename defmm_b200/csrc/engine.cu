@@ -228,7 +228,7 @@ int upload_plan(defmm_handle* h) {
     CK(cudaMemset(e, 0, sizeof(int)));
     d.err = static_cast<int*>(e);
     void* qc = nullptr;
-    CK(cudaMalloc(&qc, sizeof(unsigned long long)));
+    CK(cudaMalloc(&qc, 2 * sizeof(unsigned long long)));  // P2P (stream 2), M2L (main stream)
     h->plan_allocs.push_back(qc);
     h->d_queue = static_cast<unsigned long long*>(qc);
     int dev = 0;
@@ -377,7 +377,7 @@ int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) 
         nl_ += 2;
         rec(h, 2 * PH_M2F + 1);
         rec(h, 2 * PH_M2L);
-        ops->m2l(d, ts0, ts1, fs0, fs1, h->F.p, h->ptab.p, h->Lx.p, s);
+        ops->m2l(d, ts0, ts1, fs0, fs1, h->F.p, h->ptab.p, h->Lx.p, h->d_queue + 1, h->nsm, s);
         rec(h, 2 * PH_M2L + 1);
         if (h->events) {
           float a;
@@ -704,6 +704,8 @@ int defmm_info(const defmm_handle* h, int what, int64_t* v) {
     case DEFMM_INFO_LIST_RECORDS: *v = p.keep_lists ? 1 : 0; break;
     case DEFMM_INFO_LAUNCHES: *v = h->launches; break;
     case DEFMM_INFO_PERMUTED_SPECTRA: *v = (int64_t)p.ptab_key.size(); break;
+    case DEFMM_INFO_M2L_GROUPS: *v = (int64_t)p.g_tslot.size(); break;
+    case DEFMM_INFO_M2L_RECORDS: *v = (int64_t)p.g_src.size(); break;
     case DEFMM_INFO_M2L_TARGETS: {
       int64_t n = 0;
       for (int64_t k = 0; k < p.sT.n; k++) n += p.m2l_ptr[k + 1] > p.m2l_ptr[k] ? 1 : 0;

@@ -498,10 +498,11 @@ __global__ void k_permute_tables(int64_t n, int PP, const uint32_t* __restrict__
 //   inverse DFT in shared memory, one line per thread per axis pass)
 // J never leaves the SM.
 template <typename T, int L, int NT>
-__global__ void __launch_bounds__(NT) k_m2l(DevPlan P, int64_t t0, int64_t t1, int64_t f0, int64_t f1,
-                                            const typename cpx_t<T>::type* __restrict__ F,
-                                            const typename cpx_t<T>::type* __restrict__ ptab,
-                                            typename cpx_t<T>::type* __restrict__ Lx) {
+__global__ void __launch_bounds__(NT, (sizeof(T) == 8 ? 512 : 1024) / NT) k_m2l(DevPlan P, int64_t t0, int64_t t1, int64_t f0, int64_t f1,
+                                                       const typename cpx_t<T>::type* __restrict__ F,
+                                                       const typename cpx_t<T>::type* __restrict__ ptab,
+                                                       typename cpx_t<T>::type* __restrict__ Lx,
+                                                       unsigned long long* __restrict__ queue) {
   typedef typename cpx_t<T>::type C;
   constexpr int PD = 2 * L - 1, LL = L * L * L, PP = PD * PD * PD, K = (PP + NT - 1) / NT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -516,11 +517,20 @@ __global__ void __launch_bounds__(NT) k_m2l(DevPlan P, int64_t t0, int64_t t1, i
     W[m].y = (T)s;
   }
   const T inv = T(1) / T(PP);
-  for (int64_t t = t0 + blockIdx.x; t < t1; t += gridDim.x) {
+  __shared__ int64_t cur;
+  // target slots are taken in order from a queue, so the slots in flight
+  // stay a contiguous window of one cone (good L2 reuse of F and U)
+  for (;;) {
+    __syncthreads();  // the previous slot's inverse DFT is done with Js/Cb/D
+    if (threadIdx.x == 0) cur = t0 + (int64_t)atomicAdd(queue, 1ULL);
+    __syncthreads();
+    const int64_t t = cur;
+    if (t >= t1) break;
     const int64_t eb = P.m2l_ptr[t], ee = P.m2l_ptr[t + 1];
     C acc[K];
 #pragma unroll
     for (int k = 0; k < K; k++) acc[k] = czero<C>();
+#pragma unroll 2
     for (int64_t e = eb; e < ee; e++) {
       const int64_t src = P.m2l_src[e];
       if (src < f0 || src >= f1) {  // entry outside this cone batch: a plan bug
@@ -532,10 +542,9 @@ __global__ void __launch_bounds__(NT) k_m2l(DevPlan P, int64_t t0, int64_t t1, i
 #pragma unroll
       for (int k = 0; k < K; k++) {
         const int i = threadIdx.x + k * NT;
-        if (i < PP) cfma(acc[k], U[i], Fs[i]);
+        if (i < PP) cfma(acc[k], __ldg(U + i), __ldg(Fs + i));
       }
     }
-    __syncthreads();  // the previous slot's inverse DFT is done with Js/Cb/D
 #pragma unroll
     for (int k = 0; k < K; k++) {
       const int i = threadIdx.x + k * NT;
@@ -633,15 +642,19 @@ __global__ void __launch_bounds__(128) k_l2p(DevPlan P, const int32_t* __restric
         __syncwarp();
         for (int l = lane; l < LL; l += 32) buf[warp][l] = hf ? cmul(s2[(int64_t)d * LL + l], Ls[l]) : Ls[l];
         __syncwarp();
+        // sum_{a,b,c} B0[a] B1[b] B2[c] X[a,b,c] = sum_a B0[a] (sum_b B1[b] (sum_c B2[c] X[a,b,c]))
         C sum = czero<C>();
 #pragma unroll
         for (int a = 0; a < L; a++) {
+          C sa = czero<C>();
 #pragma unroll
           for (int b = 0; b < L; b++) {
-            const T zab = B[0][a] * B[1][b];
+            C sb = czero<C>();
 #pragma unroll
-            for (int cc = 0; cc < L; cc++) rfma(sum, zab * B[2][cc], buf[warp][(a * L + b) * L + cc]);
+            for (int cc = 0; cc < L; cc++) rfma(sb, B[2][cc], buf[warp][(a * L + b) * L + cc]);
+            rfma(sa, B[1][b], sb);
           }
+          rfma(sum, B[0][a], sa);
         }
         double2 v = make_double2((double)sum.x, (double)sum.y);
         if (hf) {
@@ -911,9 +924,11 @@ struct Launch {
     if (n) k_m2f<T, L><<<grid_for(n, 1), 128, smem_m2f(), s>>>(n, (const C*)M, (C*)F);
   }
   static void m2l(const DevPlan& dp, int64_t t0, int64_t t1, int64_t f0, int64_t f1, const void* F,
-                  const void* ptab, void* Lx, cudaStream_t s) {
-    if (t1 > t0)
-      k_m2l<T, L, NT><<<grid_for(t1 - t0, 1), NT, smem_m2l(), s>>>(dp, t0, t1, f0, f1, (const C*)F, (const C*)ptab, (C*)Lx);
+                  const void* ptab, void* Lx, unsigned long long* queue, int nsm, cudaStream_t s) {
+    if (t1 <= t0) return;
+    cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s);
+    const int grid = (int)std::min<int64_t>(t1 - t0, (int64_t)nsm * (2048 / NT));
+    k_m2l<T, L, NT><<<grid, NT, smem_m2l(), s>>>(dp, t0, t1, f0, f1, (const C*)F, (const C*)ptab, (C*)Lx, queue);
   }
   static void permute(int64_t n, const uint32_t* key, const uint16_t* perm, const void* tables, void* out,
                       cudaStream_t s) {

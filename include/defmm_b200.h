@@ -122,6 +122,8 @@ int defmm_check_full(defmm_handle* h, int64_t nsamples, uint64_t seed,
 #define DEFMM_INFO_M2L_TARGETS 17  /* target slots receiving M2L */
 #define DEFMM_INFO_LEAF_SLOTS_S 18 /* source leaf expansions (P2M outputs) */
 #define DEFMM_INFO_PERMUTED_SPECTRA 19 /* (spectrum, symmetry) pairs used by M2L */
+#define DEFMM_INFO_M2L_GROUPS 20   /* sibling groups of target slots (blocked M2L) */
+#define DEFMM_INFO_M2L_RECORDS 21  /* distinct (group, source slot) records */
 int defmm_info(const defmm_handle* h, int what, int64_t* value);
 
 /* Per-phase device times (ms) of the last gemv, in this order:
