@@ -34,8 +34,7 @@ _INFO = {
     "n_sources": 0, "n_targets": 1, "nlvl": 2, "cpt": 3, "max_stage": 4, "cells_T": 5,
     "cells_S": 6, "slots_S": 7, "slots_T": 8, "far_hf": 9, "far_lf": 10, "near": 11,
     "i_near": 12, "tables": 13, "device_bytes": 14, "list_records": 15, "launches": 16,
-    "m2l_targets": 17, "leaf_slots_S": 18, "permuted_spectra": 19, "m2l_groups": 20,
-    "m2l_records": 21,
+    "m2l_targets": 17, "leaf_slots_S": 18, "permuted_spectra": 19,
 }
 PHASES = ["p2m", "m2m", "m2f", "m2l", "f2l", "l2l", "l2p", "p2p", "scatter", "total"]
 
@@ -74,6 +73,7 @@ def lib():
             "defmm_info": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(i64)]),
             "defmm_phase_times": (ctypes.c_int, [vp, dp]),
             "defmm_set_profiling": (ctypes.c_int, [vp, ctypes.c_int]),
+            "defmm_set_graphs": (ctypes.c_int, [vp, ctypes.c_int]),
             "defmm_keep_lists": (ctypes.c_int, [vp, ctypes.c_int]),
             "defmm_dump_tree": (ctypes.c_int, [vp, ctypes.c_int, ip, dp, ip, ctypes.POINTER(i64), ip]),
             "defmm_dump_lists": (ctypes.c_int, [vp, ip, ip, ip, ctypes.POINTER(i64)]),
@@ -153,6 +153,9 @@ class IBFMM_Mat:
 
     def set_profiling(self, on=True):
         self._check(lib().defmm_set_profiling(self._h, int(bool(on))))
+
+    def set_graphs(self, on=True):
+        self._check(lib().defmm_set_graphs(self._h, int(bool(on))))
 
     def keep_lists(self, on=True):
         self._check(lib().defmm_keep_lists(self._h, int(bool(on))))

@@ -60,6 +60,15 @@ struct defmm_handle {
   bool events = false;
   bool has_out = false;
   int64_t launches = 0;  // kernels launched by the last gemv call
+  // CUDA graph of one matvec, replayed while (precision, input, output,
+  // stream) stay the same
+  bool use_graphs = true;
+  cudaGraphExec_t gexec = nullptr;
+  const void* g_in = nullptr;
+  void* g_out = nullptr;
+  cudaStream_t g_stream = nullptr;
+  int g_prec = -1;
+  int64_t g_launches = 0;
 
   int fail(int code, const std::string& m) {
     err = m;
@@ -121,7 +130,14 @@ std::vector<int32_t> to_i32(const std::vector<V>& v) {
   return std::vector<int32_t>(v.begin(), v.end());
 }
 
+void drop_graph(defmm_handle* h) {
+  if (h->gexec) cudaGraphExecDestroy(h->gexec);
+  h->gexec = nullptr;
+  h->g_prec = -1;
+}
+
 void free_plan_device(defmm_handle* h) {
+  drop_graph(h);
   for (void* p : h->plan_allocs) cudaFree(p);
   h->plan_allocs.clear();
   free_buf(h->M);
@@ -245,6 +261,7 @@ int upload_plan(defmm_handle* h) {
 // Allocate / convert the arrays whose element type follows the precision.
 int prepare_precision(defmm_handle* h) {
   if (h->ops_prec == h->precision) return 0;
+  drop_graph(h);
   Plan& p = h->plan;
   const bool fp64 = h->precision == DEFMM_PRECISION_FP64;
   const size_t cs = fp64 ? 16 : 8;
@@ -437,6 +454,46 @@ int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) 
   return 0;
 }
 
+// One matvec on stream s, replaying a captured graph when possible.
+int matvec(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) {
+  if (!h->use_graphs || h->events) return run_gemv(h, qin, out, s);
+  if (h->gexec && h->g_in == qin && h->g_out == out && h->g_stream == s && h->g_prec == h->precision) {
+    CK(cudaGraphLaunch(h->gexec, s));
+    h->launches += h->g_launches;
+    return 0;
+  }
+  drop_graph(h);
+  CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  const int64_t before = h->launches;
+  int st = run_gemv(h, qin, out, s);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(s, &g);
+  if (st) {
+    if (g) cudaGraphDestroy(g);
+    return st;
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    h->use_graphs = false;  // capture not possible here: run directly from now on
+    return run_gemv(h, qin, out, s);
+  }
+  e = cudaGraphInstantiate(&h->gexec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    h->gexec = nullptr;
+    h->use_graphs = false;
+    return run_gemv(h, qin, out, s);
+  }
+  h->g_in = qin;
+  h->g_out = out;
+  h->g_stream = s;
+  h->g_prec = h->precision;
+  h->g_launches = h->launches - before;
+  CK(cudaGraphLaunch(h->gexec, s));
+  return 0;
+}
+
 int ensure_device(defmm_handle* h) {
   if (h->device >= 0) return 0;
   int n = 0;
@@ -531,6 +588,13 @@ int defmm_load_inp(defmm_handle* h, const char* path, int64_t nparts, int which)
   return 0;
 }
 
+int defmm_set_graphs(defmm_handle* h, int on) {
+  if (!h) return DEFMM_ERR_ARG;
+  h->use_graphs = on != 0;
+  if (!h->use_graphs && h->device >= 0) drop_graph(h);
+  return 0;
+}
+
 int defmm_set_profiling(defmm_handle* h, int on) {
   if (!h) return DEFMM_ERR_ARG;
   h->events = on != 0;
@@ -594,7 +658,7 @@ int defmm_gemv_device(defmm_handle* h, const void* d_in, void* d_out, int64_t nr
   h->launches = 0;
   const int64_t nS = (int64_t)h->plan.S.perm.size(), nT = (int64_t)h->plan.T.perm.size();
   for (int64_t r = 0; r < nrhs; r++) {
-    st = run_gemv(h, (const double2*)d_in + r * nS, (double2*)d_out + r * nT, s);
+    st = matvec(h, (const double2*)d_in + r * nS, (double2*)d_out + r * nT, s);
     if (st) return st;
   }
   return 0;
@@ -611,7 +675,7 @@ int defmm_gemv_batched(defmm_handle* h, int64_t nrhs, const double* in, double* 
   h->launches = 0;
   for (int64_t r = 0; r < nrhs; r++) {
     CK(cudaMemcpyAsync(h->qin.p, in + 2 * r * nS, 16 * nS, cudaMemcpyHostToDevice, h->st));
-    st = run_gemv(h, (const double2*)h->qin.p, (double2*)h->out.p, h->st);
+    st = matvec(h, (const double2*)h->qin.p, (double2*)h->out.p, h->st);
     if (st) return st;
     CK(cudaMemcpyAsync(out + 2 * r * nT, h->out.p, 16 * nT, cudaMemcpyDeviceToHost, h->st));
   }
@@ -704,8 +768,6 @@ int defmm_info(const defmm_handle* h, int what, int64_t* v) {
     case DEFMM_INFO_LIST_RECORDS: *v = p.keep_lists ? 1 : 0; break;
     case DEFMM_INFO_LAUNCHES: *v = h->launches; break;
     case DEFMM_INFO_PERMUTED_SPECTRA: *v = (int64_t)p.ptab_key.size(); break;
-    case DEFMM_INFO_M2L_GROUPS: *v = (int64_t)p.g_tslot.size(); break;
-    case DEFMM_INFO_M2L_RECORDS: *v = (int64_t)p.g_src.size(); break;
     case DEFMM_INFO_M2L_TARGETS: {
       int64_t n = 0;
       for (int64_t k = 0; k < p.sT.n; k++) n += p.m2l_ptr[k + 1] > p.m2l_ptr[k] ? 1 : 0;

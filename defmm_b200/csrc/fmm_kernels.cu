@@ -287,14 +287,42 @@ __global__ void __launch_bounds__(128) k_m2m(DevPlan P, int64_t s0, int64_t s1,
     for (int q = 0; q < NLN; q++)
 #pragma unroll
       for (int k = 0; k < L; k++) acc[q][k] = czero<C>();
-    for (int64_t e = eb; e < ee; e++) {
-      const int cs = P.m2m_child[e];
-      const int cc = P.sS_cell[cs];
-      const double4 cct = P.S_ctr[cc];
-      const double v[3] = {cct.x - pct.x, cct.y - pct.y, cct.z - pct.z};
-      const C* Mc = M + (int64_t)cs * LL;
+    // children metadata fetched by lane (<= 8 children), broadcast below
+    const int nch = (int)(ee - eb);
+    int my_cs = 0;
+    double4 my_ct = make_double4(0., 0., 0., 0.);
+    if (lane < nch) {
+      my_cs = P.m2m_child[eb + lane];
+      my_ct = P.S_ctr[P.sS_cell[my_cs]];
+    }
+    constexpr int NV = (LL + 31) / 32;
+    C nxt[NV];  // next child's expansion, prefetched
+    {
+      const int cs0 = __shfl_sync(0xffffffffu, my_cs, 0);
+#pragma unroll
+      for (int m = 0; m < NV; m++) {
+        const int l = lane + 32 * m;
+        nxt[m] = l < LL ? M[(int64_t)cs0 * LL + l] : czero<C>();
+      }
+    }
+    for (int e = 0; e < nch; e++) {
+      const double cx = __shfl_sync(0xffffffffu, my_ct.x, e), cy = __shfl_sync(0xffffffffu, my_ct.y, e),
+                   cz = __shfl_sync(0xffffffffu, my_ct.z, e);
+      const double v[3] = {cx - pct.x, cy - pct.y, cz - pct.z};
       __syncwarp();
-      for (int l = lane; l < LL; l += 32) sbuf[warp][0][l] = hf ? cmul(sg[l], Mc[l]) : Mc[l];
+#pragma unroll
+      for (int m = 0; m < NV; m++) {
+        const int l = lane + 32 * m;
+        if (l < LL) sbuf[warp][0][l] = hf ? cmul(sg[l], nxt[m]) : nxt[m];
+      }
+      if (e + 1 < nch) {
+        const int csn = __shfl_sync(0xffffffffu, my_cs, e + 1);
+#pragma unroll
+        for (int m = 0; m < NV; m++) {
+          const int l = lane + 32 * m;
+          if (l < LL) nxt[m] = M[(int64_t)csn * LL + l];
+        }
+      }
       __syncwarp();
       C res[NLN][L];
       Sep<T, L>::run(mats, v[0] < 0. ? 0 : 1, v[1] < 0. ? 0 : 1, v[2] < 0. ? 0 : 1, sbuf[warp][0],
@@ -361,14 +389,41 @@ __global__ void __launch_bounds__(128) k_l2l(DevPlan P, int64_t s0, int64_t s1,
     for (int q = 0; q < NLN; q++)
 #pragma unroll
       for (int k = 0; k < L; k++) acc[q][k] = czero<C>();
-    for (int64_t e = eb; e < ee; e++) {
-      const int ps = P.l2l_parent[e];
-      const int d = P.sT_dir[ps];
-      const C* Lp = Lx + (int64_t)ps * LL;
+    // parents' slots and directions fetched by lane (<= 6 per child slot)
+    const int npa = (int)(ee - eb);
+    int my_ps = 0, my_d = 0;
+    if (lane < npa) {
+      my_ps = P.l2l_parent[eb + lane];
+      my_d = P.sT_dir[my_ps];
+    }
+    constexpr int NV = (LL + 31) / 32;
+    C nxt[NV];
+    {
+      const int ps0 = __shfl_sync(0xffffffffu, my_ps, 0);
+#pragma unroll
+      for (int m = 0; m < NV; m++) {
+        const int l = lane + 32 * m;
+        nxt[m] = l < LL ? Lx[(int64_t)ps0 * LL + l] : czero<C>();
+      }
+    }
+    for (int e = 0; e < npa; e++) {
+      const int d = __shfl_sync(0xffffffffu, my_d, e);
       const C* sg = sig + P.sig_off[h] + (int64_t)(hf ? d : 0) * LL;
       const C* sgq = sig2 + P.sig_off[h] + (int64_t)(hf ? d : 0) * LL;
       __syncwarp();
-      for (int l = lane; l < LL; l += 32) sbuf[warp][0][l] = hf ? cmul(sgq[l], Lp[l]) : Lp[l];
+#pragma unroll
+      for (int m = 0; m < NV; m++) {
+        const int l = lane + 32 * m;
+        if (l < LL) sbuf[warp][0][l] = hf ? cmul(sgq[l], nxt[m]) : nxt[m];
+      }
+      if (e + 1 < npa) {
+        const int psn = __shfl_sync(0xffffffffu, my_ps, e + 1);
+#pragma unroll
+        for (int m = 0; m < NV; m++) {
+          const int l = lane + 32 * m;
+          if (l < LL) nxt[m] = Lx[(int64_t)psn * LL + l];
+        }
+      }
       __syncwarp();
       C res[NLN][L];
       Sep<T, L>::run(mats, sg0, sg1, sg2i, sbuf[warp][0], sbuf[warp][1], res, lane);
@@ -412,29 +467,41 @@ __global__ void __launch_bounds__(128) k_l2l(DevPlan P, int64_t s0, int64_t s1,
 // Pruned odd-size 3-D DFT (size P = 2L-1) of the zero-padded expansion
 // (circulant.hpp:96-106: M sits at the low corner of the P^3 grid):
 //   F[k0,k1,k2] = sum_{a,b,c<L} M[a,b,c] w^(k0 a + k1 b + k2 c),  w = e^{-2 pi i/P}
-// One CTA per expansion; each axis pass gives one thread one line (its L
-// inputs in registers, its P outputs computed from them).
+// One warp per expansion (several per CTA); each axis pass gives one lane one
+// line (its L inputs in registers, its P outputs computed from them).
 template <typename T, int L>
-__global__ void __launch_bounds__(128) k_m2f(int64_t n, const typename cpx_t<T>::type* __restrict__ M,
+struct M2FCfg {
+  typedef typename cpx_t<T>::type C;
+  static constexpr int P = 2 * L - 1, LL = L * L * L;
+  static constexpr int PER_WARP = P + LL + L * L * P + L * P * P;  // complex elements
+  // warps per CTA so that a CTA's shared memory stays within ~48 KB
+  static constexpr int NW0 = (int)(49152 / (PER_WARP * sizeof(C)));
+  static constexpr int NW = NW0 < 1 ? 1 : (NW0 > 8 ? 8 : NW0);
+};
+
+template <typename T, int L>
+__global__ void __launch_bounds__(256) k_m2f(int64_t n, const typename cpx_t<T>::type* __restrict__ M,
                                              typename cpx_t<T>::type* __restrict__ F) {
   typedef typename cpx_t<T>::type C;
   constexpr int P = 2 * L - 1, LL = L * L * L, PP = P * P * P;
+  constexpr int NW = M2FCfg<T, L>::NW, PER = M2FCfg<T, L>::PER_WARP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* W = reinterpret_cast<C*>(smem_raw);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  C* W = reinterpret_cast<C*>(smem_raw) + warp * PER;
   C* Mi = W + P;
   C* A = Mi + LL;
   C* B = A + L * L * P;
-  for (int m = threadIdx.x; m < P; m += blockDim.x) {
+  for (int m = lane; m < P; m += 32) {
     double s, c;
     sincospi(-2.0 * m / P, &s, &c);
     W[m].x = (T)c;
     W[m].y = (T)s;
   }
-  for (int64_t e = blockIdx.x; e < n; e += gridDim.x) {
-    __syncthreads();
-    for (int i = threadIdx.x; i < LL; i += blockDim.x) Mi[i] = M[e * LL + i];
-    __syncthreads();
-    for (int ln = threadIdx.x; ln < L * L; ln += blockDim.x) {  // axis 2: (a,b) lines
+  for (int64_t e = (int64_t)blockIdx.x * NW + warp; e < n; e += (int64_t)gridDim.x * NW) {
+    __syncwarp();
+    for (int i = lane; i < LL; i += 32) Mi[i] = M[e * LL + i];
+    __syncwarp();
+    for (int ln = lane; ln < L * L; ln += 32) {  // axis 2: (a,b) lines
       C v[L];
 #pragma unroll
       for (int c = 0; c < L; c++) v[c] = Mi[ln * L + c];
@@ -446,8 +513,8 @@ __global__ void __launch_bounds__(128) k_m2f(int64_t n, const typename cpx_t<T>:
         A[ln * P + k2] = acc;
       }
     }
-    __syncthreads();
-    for (int ln = threadIdx.x; ln < L * P; ln += blockDim.x) {  // axis 1: (a,k2) lines
+    __syncwarp();
+    for (int ln = lane; ln < L * P; ln += 32) {  // axis 1: (a,k2) lines
       const int a = ln / P, k2 = ln % P;
       C v[L];
 #pragma unroll
@@ -460,8 +527,8 @@ __global__ void __launch_bounds__(128) k_m2f(int64_t n, const typename cpx_t<T>:
         B[(a * P + k1) * P + k2] = acc;
       }
     }
-    __syncthreads();
-    for (int ln = threadIdx.x; ln < P * P; ln += blockDim.x) {  // axis 0: (k1,k2) lines
+    __syncwarp();
+    for (int ln = lane; ln < P * P; ln += 32) {  // axis 0: (k1,k2) lines
       C v[L];
 #pragma unroll
       for (int a = 0; a < L; a++) v[a] = B[a * P * P + ln];
@@ -682,39 +749,35 @@ __global__ void __launch_bounds__(128) k_l2p(DevPlan P, const int32_t* __restric
 // -------------------------------------------------------------------- P2P --
 // Mixed-precision near field.  The phase k r needs ~1e-7 rad absolute
 // accuracy at k r up to ~1e2, beyond FP32: the difference vector, r^2, r and
-// the reduction of k r to [-pi/4, pi/4] (quadrant n = rint(k r * 2/pi)) run
-// in FP64; sin/cos of the reduced angle are evaluated in FP32 by their Taylor
-// series to degree 9/10 (truncation < 2e-9 on [-pi/4, pi/4]), 1/(4 pi r),
-// the complex products and the per-lane accumulation (Kahan-compensated) in
-// FP32; the cross-lane reduction and the result in FP64.
+// the reduction of k r to [-pi/2, pi/2] (n = rint(k r / pi)) run in FP64;
+// sin/cos of the reduced angle are evaluated in FP32 by their Taylor series
+// to degree 13/12, 1/(4 pi r) and the complex products in FP32; every
+// product is accumulated in FP64.
 __device__ __forceinline__ void sincos_reduced(double theta, float& s, float& c) {
-  const double n = rint(theta * 0.63661977236758134308);  // 2/pi
-  const float x = (float)fma(-n, 1.5707963267948966192, theta);
+  // theta = n pi + x, |x| <= pi/2 (FP64 reduction; n pi exact inside the FMA)
+  const double n = rint(theta * 0.31830988618379067154);  // 1/pi
+  const float x = (float)fma(-n, 3.14159265358979323846, theta);
   const float x2 = x * x;
-  // sin x = x (1 - x^2/3! + x^4/5! - x^6/7! + x^8/9!)
-  float ps = fmaf(x2, 2.7557319223985893e-06f, -1.9841269841269841e-04f);
+  // sin x = x (1 - x^2/3! + ... + x^12/13!), cos x = 1 - x^2/2! + ... + x^12/12!
+  // (Taylor; truncation < 7e-10 on [-pi/2, pi/2])
+  float ps = fmaf(x2, 1.6059043836821613e-10f, -2.5052108385441720e-08f);
+  ps = fmaf(x2, ps, 2.7557319223985893e-06f);
+  ps = fmaf(x2, ps, -1.9841269841269841e-04f);
   ps = fmaf(x2, ps, 8.3333333333333333e-03f);
   ps = fmaf(x2, ps, -1.6666666666666667e-01f);
   ps = fmaf(x2, ps, 1.0f);
-  const float sx = x * ps;
-  // cos x = 1 - x^2/2! + x^4/4! - x^6/6! + x^8/8! - x^10/10!
-  float pc = fmaf(x2, -2.7557319223985891e-07f, 2.4801587301587302e-05f);
+  float pc = fmaf(x2, 2.0876756987868099e-09f, -2.7557319223985891e-07f);
+  pc = fmaf(x2, pc, 2.4801587301587302e-05f);
   pc = fmaf(x2, pc, -1.3888888888888889e-03f);
   pc = fmaf(x2, pc, 4.1666666666666667e-02f);
   pc = fmaf(x2, pc, -0.5f);
-  const float cx = fmaf(x2, pc, 1.0f);
-  const int q = ((int)n) & 3;
-  const float ss = (q & 1) ? cx : sx, cc = (q & 1) ? sx : cx;
-  s = (q & 2) ? -ss : ss;
-  c = ((q + 1) & 2) ? -cc : cc;
+  pc = fmaf(x2, pc, 1.0f);
+  // (-1)^n on both
+  const float sg = (__double2int_rn(n) & 1) ? -1.0f : 1.0f;
+  s = sg * x * ps;
+  c = sg * pc;
 }
 
-__device__ __forceinline__ void kahan_add(float& sum, float& comp, float v) {
-  const float y = v - comp;
-  const float t = sum + y;
-  comp = (t - sum) - y;
-  sum = t;
-}
 
 // Near field, tiled: one CTA (4 warps) per chunk of <= 32 target particles
 // of one leaf; CTAs take chunks from a global queue (the host orders chunks
@@ -727,13 +790,15 @@ __device__ __forceinline__ void kahan_add(float& sum, float& comp, float v) {
 //   MIXED = false: FP64 throughout (P2P.hpp:43-79 arithmetic).
 //   MIXED = true : difference vector, r^2, r (FP32 sqrt + one FP64 Newton
 //   step) and the reduction of k r in FP64; sin/cos of the reduced angle,
-//   1/(4 pi r) and the compensated accumulation in FP32.
-template <bool MIXED, typename Q>
-__device__ __forceinline__ void p2p_pair(double x0, double x1, double x2, double sx, double sy, double sz, Q qq,
-                                         double kappa, double& pr, double& pim, float& sr, float& cr, float& si,
-                                         float& ci) {
+//   1/(4 pi r) and the complex products in FP32, accumulated in FP64.
+// One source/target interaction.  Source record in shared memory: a = (x, y),
+// b = (z, charge) with the FP32 charge bits in b.y (mixed) or the FP64
+// charge in c (FP64 path).
+template <bool MIXED>
+__device__ __forceinline__ void p2p_pair(double x0, double x1, double x2, double2 a, double2 b, double2 qd,
+                                         double kappa, double& pr, double& pim) {
   const double pi4m1 = 1. / (4. * 3.14159265358979323846);
-  const double dx = x0 - sx, dy = x1 - sy, dz = x2 - sz;
+  const double dx = x0 - a.x, dy = x1 - a.y, dz = x2 - b.x;
   const double R = fma(dx, dx, fma(dy, dy, dz * dz));
   if (R < 1.e-16) return;  // self / duplicate pairs (P2P.hpp:66)
   if (!MIXED) {
@@ -748,8 +813,8 @@ __device__ __forceinline__ void p2p_pair(double x0, double x1, double x2, double
     sincos_cw(rr, sn_, cs_);
     cs_ *= K;
     sn_ *= K;
-    pr = fma(cs_, (double)qq.x, fma(-sn_, (double)qq.y, pr));
-    pim = fma(cs_, (double)qq.y, fma(sn_, (double)qq.x, pim));
+    pr = fma(cs_, qd.x, fma(-sn_, qd.y, pr));
+    pim = fma(cs_, qd.y, fma(sn_, qd.x, pim));
   } else {
     // r to ~1e-14 relative: FP32 reciprocal square root refined once in
     // FP32, one Newton step for r in FP64 (rf^2 is exact in FP64)
@@ -763,8 +828,9 @@ __device__ __forceinline__ void p2p_pair(double x0, double x1, double x2, double
     const float K = (float)pi4m1 * y;
     c *= K;
     s *= K;
-    kahan_add(sr, cr, fmaf(c, (float)qq.x, -s * (float)qq.y));
-    kahan_add(si, ci, fmaf(c, (float)qq.y, s * (float)qq.x));
+    const float2 q = *reinterpret_cast<const float2*>(&b.y);
+    pr += (double)fmaf(c, q.x, -s * q.y);
+    pim += (double)fmaf(c, q.y, s * q.x);
   }
 }
 
@@ -777,8 +843,8 @@ __global__ void __launch_bounds__(128) k_p2p_tiled(DevPlan P, int64_t nchunk, co
   constexpr int TS = 512;
   typedef typename std::conditional<MIXED, float2, double2>::type Q;
   const Q* q = static_cast<const Q*>(qv);
-  __shared__ double sx[TS], sy[TS], sz[TS];
-  __shared__ Q sq[TS];
+  __shared__ double2 sa[TS], sb[TS];
+  __shared__ double2 sc[MIXED ? 1 : TS];
   __shared__ double2 red[4][32];
   __shared__ int64_t cur;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -797,7 +863,6 @@ __global__ void __launch_bounds__(128) k_p2p_tiled(DevPlan P, int64_t nchunk, co
     const int ti = f + min(mt, nt - 1);
     const double x0 = P.T_pos[3 * (int64_t)ti], x1 = P.T_pos[3 * (int64_t)ti + 1], x2 = P.T_pos[3 * (int64_t)ti + 2];
     double pr = 0., pim = 0.;
-    float sr = 0.f, cr = 0.f, si = 0.f, ci = 0.f;
     const int64_t rb = ptr[ch], re = ptr[ch + 1];
     int64_t r = rb;
     int off = 0;  // position inside range r
@@ -810,10 +875,17 @@ __global__ void __launch_bounds__(128) k_p2p_tiled(DevPlan P, int64_t nchunk, co
         const int take = min(ns - off, TS - fill);
         for (int t = threadIdx.x; t < take; t += blockDim.x) {
           const int64_t sj = (int64_t)s0 + off + t;
-          sx[fill + t] = P.S_pos[3 * sj];
-          sy[fill + t] = P.S_pos[3 * sj + 1];
-          sz[fill + t] = P.S_pos[3 * sj + 2];
-          sq[fill + t] = q[sj];
+          const double* y = P.S_pos + 3 * sj;
+          sa[fill + t] = make_double2(y[0], y[1]);
+          if (MIXED) {
+            const float2 qq = *reinterpret_cast<const float2*>(&q[sj]);
+            double qbits;
+            *reinterpret_cast<float2*>(&qbits) = qq;
+            sb[fill + t] = make_double2(y[2], qbits);
+          } else {
+            sb[fill + t] = make_double2(y[2], 0.);
+            sc[fill + t] = *reinterpret_cast<const double2*>(&q[sj]);
+          }
         }
         fill += take;
         off += take;
@@ -825,14 +897,10 @@ __global__ void __launch_bounds__(128) k_p2p_tiled(DevPlan P, int64_t nchunk, co
       __syncthreads();
       int j = gid;
       for (; j + G < fill; j += 2 * G) {
-        p2p_pair<MIXED>(x0, x1, x2, sx[j], sy[j], sz[j], sq[j], P.kappa, pr, pim, sr, cr, si, ci);
-        p2p_pair<MIXED>(x0, x1, x2, sx[j + G], sy[j + G], sz[j + G], sq[j + G], P.kappa, pr, pim, sr, cr, si, ci);
+        p2p_pair<MIXED>(x0, x1, x2, sa[j], sb[j], MIXED ? sb[j] : sc[j], P.kappa, pr, pim);
+        p2p_pair<MIXED>(x0, x1, x2, sa[j + G], sb[j + G], MIXED ? sb[j + G] : sc[j + G], P.kappa, pr, pim);
       }
-      if (j < fill) p2p_pair<MIXED>(x0, x1, x2, sx[j], sy[j], sz[j], sq[j], P.kappa, pr, pim, sr, cr, si, ci);
-    }
-    if (MIXED) {
-      pr = (double)sr - (double)cr;
-      pim = (double)si - (double)ci;
+      if (j < fill) p2p_pair<MIXED>(x0, x1, x2, sa[j], sb[j], MIXED ? sb[j] : sc[j], P.kappa, pr, pim);
     }
     for (int o = tp; o < 32; o <<= 1) {
       pr += __shfl_xor_sync(0xffffffffu, pr, o);
@@ -899,7 +967,7 @@ struct Launch {
   typedef typename cpx_t<T>::type C;
   static constexpr int P = 2 * L - 1, LL = L * L * L, PP = P * P * P;
   static constexpr int NT = PP > 1024 ? 256 : 128;
-  static size_t smem_m2f() { return sizeof(C) * (P + LL + L * L * P + L * P * P); }
+  static size_t smem_m2f() { return sizeof(C) * M2FCfg<T, L>::PER_WARP * M2FCfg<T, L>::NW; }
   static size_t smem_m2l() { return sizeof(C) * (P + PP + L * P * P + L * L * P); }
   static cudaError_t setup() {
     cudaError_t e = cudaFuncSetAttribute(k_m2f<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_m2f());
@@ -921,7 +989,8 @@ struct Launch {
     if (s1 > s0) k_l2l<T, L><<<grid_for(s1 - s0, NW), 32 * NW, 0, s>>>(dp, s0, s1, (const C*)sig, (const C*)sig2, (C*)Lx);
   }
   static void m2f(int64_t n, const void* M, void* F, cudaStream_t s) {
-    if (n) k_m2f<T, L><<<grid_for(n, 1), 128, smem_m2f(), s>>>(n, (const C*)M, (C*)F);
+    constexpr int NW = M2FCfg<T, L>::NW;
+    if (n) k_m2f<T, L><<<grid_for(n, NW), 32 * NW, smem_m2f(), s>>>(n, (const C*)M, (C*)F);
   }
   static void m2l(const DevPlan& dp, int64_t t0, int64_t t1, int64_t f0, int64_t f1, const void* F,
                   const void* ptab, void* Lx, unsigned long long* queue, int nsm, cudaStream_t s) {

@@ -921,74 +921,6 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
     pfor((int64_t)p.m2l_tab.size(), 1 << 16, [&](int64_t e) { p.m2l_tab[e] = (uint32_t)pid[p.m2l_tab[e]]; });
   }
 
-  // sibling groups for the blocked M2L kernel
-  {
-    const Slots& sT = p.sT;
-    std::vector<int64_t> gstart;  // group starts over target slots with M2L work
-    for (int l = 0; l < nlvl; l++) {
-      const auto& cb = sT.cone_begin[l];
-      for (size_t c = 0; c + 1 < cb.size(); c++) {
-        int64_t k = cb[c];
-        while (k < cb[c + 1]) {
-          const int32_t par = p.T.parent[sT.cell[k]];
-          int64_t e = k + 1;
-          while (e < cb[c + 1] && e - k < 8 && p.T.parent[sT.cell[e]] == par) e++;
-          gstart.push_back(k);
-          k = e;
-        }
-      }
-    }
-    const int64_t ng = (int64_t)gstart.size();
-    p.g_tslot.resize(ng);
-    p.g_n.resize(ng);
-    std::vector<int64_t> nrec(ng + 1, 0), npair(ng + 1, 0);
-    std::vector<std::vector<int32_t>> rs(ng);
-    std::vector<std::vector<uint8_t>> rm(ng);
-    std::vector<std::vector<uint32_t>> rp(ng);
-    pfor(ng, 256, [&](int64_t g) {
-      const int64_t t0 = gstart[g];
-      const int64_t t1 = g + 1 < ng ? std::min(gstart[g + 1], t0 + 8) : std::min(sT.n, t0 + 8);
-      // members are the consecutive slots [t0, t0 + n) with the group's parent
-      int n = 0;
-      while (t0 + n < t1 && (n == 0 || p.T.parent[sT.cell[t0 + n]] == p.T.parent[sT.cell[t0]])) n++;
-      p.g_tslot[g] = t0;
-      p.g_n[g] = (int8_t)n;
-      std::vector<std::tuple<int32_t, int, uint32_t>> ent;
-      for (int m = 0; m < n; m++)
-        for (int64_t e = p.m2l_ptr[t0 + m]; e < p.m2l_ptr[t0 + m + 1]; e++)
-          ent.emplace_back(p.m2l_src[e], m, p.m2l_tab[e]);
-      std::sort(ent.begin(), ent.end());
-      for (size_t i = 0; i < ent.size();) {
-        size_t j = i;
-        uint8_t mask = 0;
-        while (j < ent.size() && std::get<0>(ent[j]) == std::get<0>(ent[i])) {
-          mask |= (uint8_t)(1u << std::get<1>(ent[j]));
-          rp[g].push_back(std::get<2>(ent[j]));
-          j++;
-        }
-        rs[g].push_back(std::get<0>(ent[i]));
-        rm[g].push_back(mask);
-        i = j;
-      }
-      nrec[g + 1] = (int64_t)rs[g].size();
-      npair[g + 1] = (int64_t)rp[g].size();
-    });
-    for (int64_t g = 0; g < ng; g++) {
-      nrec[g + 1] += nrec[g];
-      npair[g + 1] += npair[g];
-    }
-    p.g_rptr = nrec;
-    p.g_pptr = npair;
-    p.g_src.resize(nrec[ng]);
-    p.g_mask.resize(nrec[ng]);
-    p.g_ptab.resize(npair[ng]);
-    pfor(ng, 256, [&](int64_t g) {
-      std::copy(rs[g].begin(), rs[g].end(), p.g_src.begin() + nrec[g]);
-      std::copy(rm[g].begin(), rm[g].end(), p.g_mask.begin() + nrec[g]);
-      std::copy(rp[g].begin(), rp[g].end(), p.g_ptab.begin() + npair[g]);
-    });
-  }
-
   // M2M: children slots of each source slot (P2M/M2M operators, M2M.hpp:35-124)
   {
     const Slots& s = p.sS;

@@ -89,17 +89,6 @@ struct Plan {
   // permuted spectra actually used: (table index << 6) | hash; the device
   // holds U_k[i] = tables[key >> 6][perm[key & 63][i]]
   std::vector<uint32_t> ptab_key;
-  // M2L by sibling groups: consecutive target slots of one level and cone
-  // whose cells share a parent (<= 8).  Per group, the union of the
-  // members' sources as records (source slot, member mask); the permuted
-  // spectrum of every (record, member) pair follows in mask-bit order.
-  std::vector<int64_t> g_tslot;            // first target slot of the group
-  std::vector<int8_t> g_n;                 // members
-  std::vector<int64_t> g_rptr;             // groups + 1 -> records
-  std::vector<int64_t> g_pptr;             // groups + 1 -> pair spectra
-  std::vector<int32_t> g_src;              // per record: source slot
-  std::vector<uint8_t> g_mask;             // per record: members using it
-  std::vector<uint32_t> g_ptab;            // per pair: permuted spectrum id
   // M2M children of each source slot, L2L parents of each target slot
   std::vector<int64_t> m2m_ptr;            // sS.n + 1
   std::vector<int32_t> m2m_child;          // child slot

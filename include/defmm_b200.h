@@ -122,14 +122,17 @@ int defmm_check_full(defmm_handle* h, int64_t nsamples, uint64_t seed,
 #define DEFMM_INFO_M2L_TARGETS 17  /* target slots receiving M2L */
 #define DEFMM_INFO_LEAF_SLOTS_S 18 /* source leaf expansions (P2M outputs) */
 #define DEFMM_INFO_PERMUTED_SPECTRA 19 /* (spectrum, symmetry) pairs used by M2L */
-#define DEFMM_INFO_M2L_GROUPS 20   /* sibling groups of target slots (blocked M2L) */
-#define DEFMM_INFO_M2L_RECORDS 21  /* distinct (group, source slot) records */
 int defmm_info(const defmm_handle* h, int what, int64_t* value);
 
 /* Per-phase device times (ms) of the last gemv, in this order:
  * P2M, M2M, M2F, M2L, F2L, L2L, L2P, P2P, gather+scatter, total.
  * F2L is fused into the M2L kernel and reads 0. */
 int defmm_phase_times(const defmm_handle* h, double ms[10]);
+
+/* Replay repeated matvecs from a captured CUDA graph (default on): the
+ * first gemv with a given precision, input, output and stream captures the
+ * launch sequence, later ones replay it.  on = 0 / 1. */
+int defmm_set_graphs(defmm_handle* h, int on);
 
 /* Per-phase timing with CUDA events (adds synchronisation between phases;
  * off by default).  on = 0 / 1. */

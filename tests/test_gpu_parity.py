@@ -121,3 +121,19 @@ def test_sources_and_targets_apart(gpu):
     A = make(src, trg, 4, 48, 2 * np.pi * 8)
     po = O.OracleFMM(src, trg, 4, 48, 2 * np.pi * 8).gemv(q)
     assert rel(A.matvec(q), po) <= FP64_TOL
+
+
+def test_graph_replay_equals_direct_launches(gpu):
+    # repeated matvecs replay a captured CUDA graph; results must not change
+    src, trg, q, L, ncrit, kappa, lvmax = case_inputs("cube_lf")
+    A = make(src, trg, L, ncrit, kappa, lvmax)
+    A.set_graphs(False)
+    p_direct = A.matvec(q)
+    A.set_graphs(True)
+    p1 = A.matvec(q)  # captures
+    p2 = A.matvec(q)  # replays
+    q2 = W.charges(len(q), 77)
+    p3 = A.matvec(q2)  # replays with new input data in the same buffers
+    assert np.array_equal(p1, p_direct) and np.array_equal(p2, p_direct)
+    A.set_graphs(False)
+    assert np.array_equal(p3, A.matvec(q2))
