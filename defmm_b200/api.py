@@ -70,6 +70,7 @@ def lib():
             "defmm_gemv_device": (ctypes.c_int, [vp, vp, vp, i64, vp]),
             "defmm_gemv_batched": (ctypes.c_int, [vp, i64, dp, dp]),
             "defmm_check_full": (ctypes.c_int, [vp, i64, ctypes.c_uint64, dp]),
+            "defmm_direct_noalloc": (ctypes.c_int, [vp, vp, i64, vp, vp]),
             "defmm_info": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(i64)]),
             "defmm_phase_times": (ctypes.c_int, [vp, dp]),
             "defmm_set_profiling": (ctypes.c_int, [vp, ctypes.c_int]),
@@ -178,6 +179,14 @@ class IBFMM_Mat:
         err = np.zeros(3)
         self._check(lib().defmm_check_full(self._h, int(nsamples), int(seed), _dp(err)))
         return {"linf": err[0], "l1": err[1], "l2": err[2]}
+
+    def direct_noalloc(self, d_targets, nt, d_out, stream=0):
+        """FP64 direct sums at `nt` device target points (nt x 3 float64)
+        into `d_out` (nt complex128), charges of the last host matvec; no
+        device allocation, nt <= 262144, calls on one device must not
+        overlap.  Enqueued on `stream` without synchronising."""
+        self._check(lib().defmm_direct_noalloc(self._h, ctypes.c_void_p(d_targets), int(nt),
+                                               ctypes.c_void_p(d_out), ctypes.c_void_p(stream) if stream else None))
 
     # -- introspection
     def info(self, what=None):

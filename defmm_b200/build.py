@@ -16,9 +16,9 @@ LIB = os.path.join(HERE, "libdefmm_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU = ["fmm_kernels.cu", "engine.cu"]
+CU = ["fmm_kernels.cu", "engine.cu", "noalloc.cu"]
 CPP = ["plan.cpp"]
-HEADERS = ["plan.hpp", "kernels.cuh", "fmm_kernels.h"]
+HEADERS = ["plan.hpp", "kernels.cuh", "fmm_kernels.h", "engine_internal.h"]
 
 
 def _newer(target, deps):

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "../../include/defmm_b200.h"
+#include "engine_internal.h"
 #include "fmm_kernels.h"
 #include "plan.hpp"
 
@@ -839,3 +840,18 @@ int defmm_dump_lists(const defmm_handle* h, int32_t* far_hf, int32_t* far_lf, in
 }
 
 }  // extern "C"
+
+int dfb::handle_view(defmm_handle* h, dfb::HandleView* v) {
+  if (!h || !v) return DEFMM_ERR_ARG;
+  if (!h->built || !h->has_out || !h->qin.p) return h->fail(DEFMM_ERR_ARG, "direct sums need a host gemv first");
+  v->device = h->device;
+  v->stream = h->st;
+  v->nS = (int64_t)h->plan.S.perm.size();
+  v->S_pos = h->dp.S_pos;
+  v->S_perm = h->dp.S_perm;
+  v->qin = (const double2*)h->qin.p;
+  v->kappa = h->plan.kappa;
+  return 0;
+}
+
+int dfb::handle_fail(defmm_handle* h, int code, const char* msg) { return h->fail(code, msg); }
