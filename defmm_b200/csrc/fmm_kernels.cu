@@ -834,6 +834,56 @@ __device__ __forceinline__ void p2p_pair(double x0, double x1, double x2, double
   }
 }
 
+// Compensated (Kahan) FP32 summation: s - c carries the sum.
+__device__ __forceinline__ void kahan_add(float& s, float& c, float x) {
+  const float y = x - c;
+  const float t = s + y;
+  c = (t - s) - y;
+  s = t;
+}
+
+// Mixed-precision interaction with FP32 compensated accumulators (the FP64
+// path keeps p2p_pair<false>).  r = sqrt(R): FP32 reciprocal square root
+// refined once in FP32 (used for 1/(4 pi r)), widened and refined once in
+// FP64 (relative error ~1e-14) for k r.  k r = n pi + x with n read from the
+// low mantissa bits of k r / pi + 1.5 * 2^52 (exact for k r / pi < 2^51) and
+// x = k r - n pi in FP64; sin/cos of x by the FP32 Taylor polynomials of
+// sincos_reduced, (-1)^n applied to both.
+__device__ __forceinline__ void p2p_pair_mixed(double x0, double x1, double x2, double2 a, double2 b, double kappa,
+                                               float& sr, float& cr, float& si, float& ci) {
+  const double dx = x0 - a.x, dy = x1 - a.y, dz = x2 - b.x;
+  const double R = fma(dx, dx, fma(dy, dy, dz * dz));
+  if (R < 1.e-16) return;  // self / duplicate pairs (P2P.hpp:66)
+  const float Rf = (float)R;
+  float y = rsqrtf(Rf);
+  y = y * fmaf(-0.5f * Rf * y, y, 1.5f);
+  double yd = (double)y;
+  yd = yd * fma(-0.5 * R * yd, yd, 1.5);
+  const double theta = R * yd * kappa;
+  const double t = fma(theta, 0.31830988618379067154, 6755399441055744.0);  // + 1.5 * 2^52
+  const double n = t - 6755399441055744.0;
+  const int odd = __double2loint(t) & 1;
+  const float x = (float)fma(-n, 3.14159265358979323846, theta);
+  const float xx = x * x;
+  float ps = fmaf(xx, 1.6059043836821613e-10f, -2.5052108385441720e-08f);
+  ps = fmaf(xx, ps, 2.7557319223985893e-06f);
+  ps = fmaf(xx, ps, -1.9841269841269841e-04f);
+  ps = fmaf(xx, ps, 8.3333333333333333e-03f);
+  ps = fmaf(xx, ps, -1.6666666666666667e-01f);
+  ps = fmaf(xx, ps, 1.0f);
+  float pc = fmaf(xx, 2.0876756987868099e-09f, -2.7557319223985891e-07f);
+  pc = fmaf(xx, pc, 2.4801587301587302e-05f);
+  pc = fmaf(xx, pc, -1.3888888888888889e-03f);
+  pc = fmaf(xx, pc, 4.1666666666666667e-02f);
+  pc = fmaf(xx, pc, -0.5f);
+  pc = fmaf(xx, pc, 1.0f);
+  const float K = odd ? -0.0795774715459476679f * y : 0.0795774715459476679f * y;  // (-1)^n / (4 pi r)
+  const float c = pc * K, s = x * ps * K;
+  const float2 q = *reinterpret_cast<const float2*>(&b.y);
+  kahan_add(sr, cr, fmaf(c, q.x, -s * q.y));
+  kahan_add(si, ci, fmaf(c, q.y, s * q.x));
+}
+
 template <bool MIXED>
 __global__ void __launch_bounds__(128) k_p2p_tiled(DevPlan P, int64_t nchunk, const int32_t* __restrict__ order,
                                                    const int32_t* __restrict__ tfirst, const int32_t* __restrict__ tn,
@@ -863,6 +913,7 @@ __global__ void __launch_bounds__(128) k_p2p_tiled(DevPlan P, int64_t nchunk, co
     const int ti = f + min(mt, nt - 1);
     const double x0 = P.T_pos[3 * (int64_t)ti], x1 = P.T_pos[3 * (int64_t)ti + 1], x2 = P.T_pos[3 * (int64_t)ti + 2];
     double pr = 0., pim = 0.;
+    float sr = 0.f, cr = 0.f, si = 0.f, ci = 0.f;  // mixed: compensated FP32 sums
     const int64_t rb = ptr[ch], re = ptr[ch + 1];
     int64_t r = rb;
     int off = 0;  // position inside range r
@@ -896,11 +947,23 @@ __global__ void __launch_bounds__(128) k_p2p_tiled(DevPlan P, int64_t nchunk, co
       }
       __syncthreads();
       int j = gid;
-      for (; j + G < fill; j += 2 * G) {
-        p2p_pair<MIXED>(x0, x1, x2, sa[j], sb[j], MIXED ? sb[j] : sc[j], P.kappa, pr, pim);
-        p2p_pair<MIXED>(x0, x1, x2, sa[j + G], sb[j + G], MIXED ? sb[j + G] : sc[j + G], P.kappa, pr, pim);
+      if constexpr (MIXED) {
+        for (; j + G < fill; j += 2 * G) {
+          p2p_pair_mixed(x0, x1, x2, sa[j], sb[j], P.kappa, sr, cr, si, ci);
+          p2p_pair_mixed(x0, x1, x2, sa[j + G], sb[j + G], P.kappa, sr, cr, si, ci);
+        }
+        if (j < fill) p2p_pair_mixed(x0, x1, x2, sa[j], sb[j], P.kappa, sr, cr, si, ci);
+      } else {
+        for (; j + G < fill; j += 2 * G) {
+          p2p_pair<false>(x0, x1, x2, sa[j], sb[j], sc[j], P.kappa, pr, pim);
+          p2p_pair<false>(x0, x1, x2, sa[j + G], sb[j + G], sc[j + G], P.kappa, pr, pim);
+        }
+        if (j < fill) p2p_pair<false>(x0, x1, x2, sa[j], sb[j], sc[j], P.kappa, pr, pim);
       }
-      if (j < fill) p2p_pair<MIXED>(x0, x1, x2, sa[j], sb[j], MIXED ? sb[j] : sc[j], P.kappa, pr, pim);
+    }
+    if constexpr (MIXED) {
+      pr = (double)sr - (double)cr;
+      pim = (double)si - (double)ci;
     }
     for (int o = tp; o < 32; o <<= 1) {
       pr += __shfl_xor_sync(0xffffffffu, pr, o);
