@@ -52,6 +52,13 @@ struct defmm_handle {
   const int64_t* d_p2p_ptr = nullptr;
   const int32_t* d_p2p_order = nullptr;
   unsigned long long* d_queue = nullptr;
+  // symmetric near field (Plan::self_*, sym_*, red_*)
+  const int64_t *d_self_ptr = nullptr, *d_sym_ptr = nullptr, *d_sym_soff = nullptr, *d_red_base = nullptr;
+  const int32_t *d_self_sfirst = nullptr, *d_self_sn = nullptr, *d_self_order = nullptr;
+  const int32_t *d_sym_sfirst = nullptr, *d_sym_sn = nullptr, *d_sym_order = nullptr;
+  const int32_t *d_red_first = nullptr, *d_red_n = nullptr, *d_red_nin = nullptr;
+  DevBuf pscr;           // source-side partial sums (one complex per slot)
+  bool use_sym = false;  // this precision runs the symmetric near field
   int nsm = 148;
   int64_t nchunk = 0;
   size_t dev_bytes = 0;
@@ -153,6 +160,8 @@ void free_plan_device(defmm_handle* h) {
   free_buf(h->qin);
   free_buf(h->out);
   free_buf(h->chk);
+  free_buf(h->pscr);
+  h->use_sym = false;
   h->ops_prec = -1;
   h->dev_bytes = 0;
   h->has_out = false;
@@ -236,6 +245,21 @@ int upload_plan(defmm_handle* h) {
   UP(p.p2p_sfirst, h->d_sfirst);
   UP(p.p2p_sn, h->d_sn);
   UP(p.p2p_order, h->d_p2p_order);
+  if (p.p2p_sym) {
+    UP(p.self_ptr, h->d_self_ptr);
+    UP(p.self_sfirst, h->d_self_sfirst);
+    UP(p.self_sn, h->d_self_sn);
+    UP(p.self_order, h->d_self_order);
+    UP(p.sym_ptr, h->d_sym_ptr);
+    UP(p.sym_sfirst, h->d_sym_sfirst);
+    UP(p.sym_sn, h->d_sym_sn);
+    UP(p.sym_soff, h->d_sym_soff);
+    UP(p.sym_order, h->d_sym_order);
+    UP(p.red_first, h->d_red_first);
+    UP(p.red_n, h->d_red_n);
+    UP(p.red_nin, h->d_red_nin);
+    UP(p.red_base, h->d_red_base);
+  }
   h->nchunk = (int64_t)p.p2p_tfirst.size();
 #undef UP
   {
@@ -316,6 +340,19 @@ int prepare_precision(defmm_handle* h) {
   if ((st = ensure(h, h->M, std::max<int64_t>(1, p.sS.n) * p.LL * cs)) ||
       (st = ensure(h, h->Lx, std::max<int64_t>(1, p.sT.n) * p.LL * cs)) || (st = ensure(h, h->q, nS * cs)))
     return st;
+  // symmetric near field when its scratch takes at most 40% of the free
+  // memory (otherwise every interaction is evaluated from both sides)
+  free_buf(h->pscr);
+  h->use_sym = false;
+  if (p.p2p_sym && p.sym_scratch > 0) {
+    size_t fr0 = 0, tot0 = 0;
+    CK(cudaMemGetInfo(&fr0, &tot0));
+    const size_t b = (size_t)p.sym_scratch * cs;
+    if (b <= (size_t)(0.4 * (double)fr0)) {
+      if ((st = ensure(h, h->pscr, b))) return st;
+      h->use_sym = true;
+    }
+  }
   // F batch buffer: at least the largest cone of any level, at most about
   // half of the free memory
   int64_t need = 1, want = 0;
@@ -364,8 +401,20 @@ int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) 
   CK(cudaEventRecord(ready, s));
   CK(cudaStreamWaitEvent(sn, ready, 0));
   if (h->events) cudaEventRecord(h->ev[2 * PH_P2P], sn);
-  dfb::launch_p2p(fp64, d, h->nchunk, h->d_p2p_order, h->d_tfirst, h->d_tn, h->d_p2p_ptr, h->d_sfirst, h->d_sn,
-                  h->q.p, (double2*)h->pnear.p, h->d_queue, h->nsm, sn);
+  if (h->use_sym) {  // own leaves, then symmetric blocks, then the mirrored partial sums
+    dfb::launch_p2p(fp64, d, (int64_t)p.self_order.size(), h->d_self_order, h->d_tfirst, h->d_tn, h->d_self_ptr,
+                    h->d_self_sfirst, h->d_self_sn, h->q.p, (double2*)h->pnear.p, h->d_queue, h->nsm, sn);
+    dfb::launch_p2p_sym(fp64, d, (int64_t)p.sym_order.size(), h->d_sym_order, h->d_tfirst, h->d_tn, h->d_sym_ptr,
+                        h->d_sym_sfirst, h->d_sym_sn, h->d_sym_soff, h->q.p, (double2*)h->pnear.p, h->pscr.p,
+                        h->d_queue, h->nsm, sn);
+    dfb::launch_p2p_reduce(fp64, (int64_t)p.red_first.size(), h->d_red_first, h->d_red_n, h->d_red_nin,
+                           h->d_red_base, h->pscr.p, (double2*)h->pnear.p, h->nsm, sn);
+    nl_ += (p.self_order.empty() ? 0 : 1) + (p.sym_order.empty() ? 0 : 1) + (p.red_first.empty() ? 0 : 1) -
+           (h->nchunk ? 1 : 0);
+  } else {
+    dfb::launch_p2p(fp64, d, h->nchunk, h->d_p2p_order, h->d_tfirst, h->d_tn, h->d_p2p_ptr, h->d_sfirst, h->d_sn,
+                    h->q.p, (double2*)h->pnear.p, h->d_queue, h->nsm, sn);
+  }
   if (h->events) cudaEventRecord(h->ev[2 * PH_P2P + 1], sn);
   // upward pass
   rec(h, 2 * PH_P2M);

@@ -982,6 +982,228 @@ __global__ void __launch_bounds__(128) k_p2p_tiled(DevPlan P, int64_t nchunk, co
   }
 }
 
+// ----------------------------------------------------- symmetric near field --
+// G(x, y) = exp(i k r) / (4 pi r) of one pair (0 for R < 1e-16, P2P.hpp:66),
+// with the arithmetic of p2p_pair<false> (FP64) or p2p_pair_mixed (FP32
+// after the FP64 r and k r reduction).
+__device__ __forceinline__ double2 green64(double dx, double dy, double dz, double kappa) {
+  const double R = fma(dx, dx, fma(dy, dy, dz * dz));
+  if (R < 1.e-16) return make_double2(0., 0.);
+  const double pi4m1 = 1. / (4. * 3.14159265358979323846);
+  double y = (double)rsqrtf((float)R);
+  const double hR = 0.5 * R;
+  y = y * fma(-hR * y, y, 1.5);
+  y = y * fma(-hR * y, y, 1.5);
+  const double K = y * pi4m1;
+  double sn_, cs_;
+  sincos_cw(y * R * kappa, sn_, cs_);
+  return make_double2(cs_ * K, sn_ * K);
+}
+__device__ __forceinline__ float2 green32(double dx, double dy, double dz, double kappa) {
+  const double R = fma(dx, dx, fma(dy, dy, dz * dz));
+  if (R < 1.e-16) return make_float2(0.f, 0.f);
+  const float Rf = (float)R;
+  float y = rsqrtf(Rf);
+  y = y * fmaf(-0.5f * Rf * y, y, 1.5f);
+  double yd = (double)y;
+  yd = yd * fma(-0.5 * R * yd, yd, 1.5);
+  const double theta = R * yd * kappa;
+  const double t = fma(theta, 0.31830988618379067154, 6755399441055744.0);  // + 1.5 * 2^52
+  const double n = t - 6755399441055744.0;
+  const int odd = __double2loint(t) & 1;
+  const float x = (float)fma(-n, 3.14159265358979323846, theta);
+  const float xx = x * x;
+  float ps = fmaf(xx, 1.6059043836821613e-10f, -2.5052108385441720e-08f);
+  ps = fmaf(xx, ps, 2.7557319223985893e-06f);
+  ps = fmaf(xx, ps, -1.9841269841269841e-04f);
+  ps = fmaf(xx, ps, 8.3333333333333333e-03f);
+  ps = fmaf(xx, ps, -1.6666666666666667e-01f);
+  ps = fmaf(xx, ps, 1.0f);
+  float pc = fmaf(xx, 2.0876756987868099e-09f, -2.7557319223985891e-07f);
+  pc = fmaf(xx, pc, 2.4801587301587302e-05f);
+  pc = fmaf(xx, pc, -1.3888888888888889e-03f);
+  pc = fmaf(xx, pc, 4.1666666666666667e-02f);
+  pc = fmaf(xx, pc, -0.5f);
+  pc = fmaf(xx, pc, 1.0f);
+  const float K = odd ? -0.0795774715459476679f * y : 0.0795774715459476679f * y;
+  return make_float2(pc * K, x * ps * K);
+}
+
+// Symmetric blocks of the near field (Plan::sym_*): one CTA (4 warps) per
+// chunk of <= 32 targets, taken from a queue.  A warp splits into segments
+// of tp = nextpow2(nt) lanes; lane l of a segment owns source l of the
+// segment's tp-source sub-tile and, over tp steps, meets every target
+// i = (l + step) mod tp.  One evaluation of G feeds both
+//   the target's partial  (an accumulator that moves one lane down per step
+//                          and ends in lane i), and
+//   the source's partial  (lane-local),
+// so each mirrored pair of interactions costs one kernel evaluation.  Target
+// partials are added to pnear (after the self blocks); source partials go to
+// scratch and are added per source leaf by k_p2p_reduce.
+template <bool MIXED>
+__global__ void __launch_bounds__(128) k_p2p_sym(DevPlan P, int64_t nwork, const int32_t* __restrict__ order,
+                                                 const int32_t* __restrict__ tfirst, const int32_t* __restrict__ tn,
+                                                 const int64_t* __restrict__ ptr, const int32_t* __restrict__ sfirst,
+                                                 const int32_t* __restrict__ sn, const int64_t* __restrict__ soff,
+                                                 const void* __restrict__ qv, double2* __restrict__ pnear,
+                                                 void* __restrict__ scratch, unsigned long long* __restrict__ queue) {
+  typedef typename std::conditional<MIXED, float2, double2>::type Q;
+  constexpr int RMAX = 64;
+  const Q* q = static_cast<const Q*>(qv);
+  Q* scr = static_cast<Q*>(scratch);
+  __shared__ double tx[32], ty[32], tz[32];
+  __shared__ Q tq[32];
+  __shared__ int32_t rpre[RMAX + 1], rfst[RMAX];
+  __shared__ int64_t roff[RMAX];
+  __shared__ double2 red[4][32];
+  __shared__ int64_t cur;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) cur = (int64_t)atomicAdd(queue, 1ULL);
+    __syncthreads();
+    const int64_t k = cur;
+    if (k >= nwork) break;
+    const int64_t ch = order[k];
+    const int f = tfirst[ch], nt = tn[ch];
+    int tp = 4;
+    while (tp < nt) tp <<= 1;
+    const int ls = lane & (tp - 1);
+    if (threadIdx.x < 32) {
+      const int t = threadIdx.x;
+      if (t < nt) {
+        const double* x = P.T_pos + 3 * (int64_t)(f + t);
+        tx[t] = x[0];
+        ty[t] = x[1];
+        tz[t] = x[2];
+        tq[t] = q[f + t];
+      } else {
+        tx[t] = ty[t] = tz[t] = 0.;
+        tq[t] = Q{0, 0};
+      }
+    }
+    float sr = 0.f, cr = 0.f, si = 0.f, ci = 0.f;  // mixed: compensated target sums
+    double pr = 0., pim = 0.;                      // FP64 target sums
+    const int64_t rb = ptr[ch], re = ptr[ch + 1];
+    for (int64_t r0 = rb; r0 < re; r0 += RMAX) {
+      const int nr = (int)min((int64_t)RMAX, re - r0);
+      __syncthreads();  // previous batch of ranges (and the target arrays) settled
+      if (threadIdx.x == 0) {
+        int a = 0;
+        for (int m = 0; m < nr; m++) {
+          rpre[m] = a;
+          rfst[m] = sfirst[r0 + m];
+          roff[m] = soff[r0 + m];
+          a += sn[r0 + m];
+        }
+        rpre[nr] = a;
+      }
+      __syncthreads();
+      const int ntot = rpre[nr];
+      for (int base = warp * 32; base < ntot; base += 4 * 32) {
+        const int jj = base + lane;
+        const bool vj = jj < ntot;
+        double yx = 0., yy = 0., yz = 0.;
+        Q qj = Q{0, 0};
+        int64_t sidx = 0;
+        if (vj) {
+          int lo = 0, hi = nr - 1;  // last range with rpre <= jj
+          while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (rpre[mid] <= jj) lo = mid; else hi = mid - 1;
+          }
+          const int o = jj - rpre[lo];
+          const int64_t sj = (int64_t)rfst[lo] + o;
+          sidx = roff[lo] + o;
+          const double* y = P.S_pos + 3 * sj;
+          yx = y[0];
+          yy = y[1];
+          yz = y[2];
+          qj = q[sj];
+        }
+        Q accD = Q{0, 0}, accT = Q{0, 0};
+        for (int st = 0; st < tp; st++) {
+          const int i = (ls + st) & (tp - 1);
+          if (vj && i < nt) {
+            if constexpr (MIXED) {
+              const float2 g = green32(tx[i] - yx, ty[i] - yy, tz[i] - yz, P.kappa);
+              const float2 qi = tq[i];
+              accD.x = fmaf(g.x, qj.x, fmaf(-g.y, qj.y, accD.x));
+              accD.y = fmaf(g.x, qj.y, fmaf(g.y, qj.x, accD.y));
+              accT.x = fmaf(g.x, qi.x, fmaf(-g.y, qi.y, accT.x));
+              accT.y = fmaf(g.x, qi.y, fmaf(g.y, qi.x, accT.y));
+            } else {
+              const double2 g = green64(tx[i] - yx, ty[i] - yy, tz[i] - yz, P.kappa);
+              const double2 qi = tq[i];
+              accD.x = fma(g.x, qj.x, fma(-g.y, qj.y, accD.x));
+              accD.y = fma(g.x, qj.y, fma(g.y, qj.x, accD.y));
+              accT.x = fma(g.x, qi.x, fma(-g.y, qi.y, accT.x));
+              accT.y = fma(g.x, qi.y, fma(g.y, qi.x, accT.y));
+            }
+          }
+          accD.x = __shfl_sync(0xffffffffu, accD.x, ls + 1, tp);
+          accD.y = __shfl_sync(0xffffffffu, accD.y, ls + 1, tp);
+        }
+        if constexpr (MIXED) {
+          kahan_add(sr, cr, accD.x);
+          kahan_add(si, ci, accD.y);
+        } else {
+          pr += accD.x;
+          pim += accD.y;
+        }
+        if (vj) scr[sidx] = accT;
+      }
+    }
+    if constexpr (MIXED) {
+      pr = (double)sr - (double)cr;
+      pim = (double)si - (double)ci;
+    }
+    for (int o = tp; o < 32; o <<= 1) {  // segments of the warp hold the same targets
+      pr += __shfl_xor_sync(0xffffffffu, pr, o);
+      pim += __shfl_xor_sync(0xffffffffu, pim, o);
+    }
+    if (lane < tp) red[warp][lane] = make_double2(pr, pim);
+    __syncthreads();
+    if (threadIdx.x < nt) {
+      double2 a = red[0][threadIdx.x];
+      for (int w = 1; w < 4; w++) {
+        a.x += red[w][threadIdx.x].x;
+        a.y += red[w][threadIdx.x].y;
+      }
+      double2 o = pnear[f + threadIdx.x];
+      o.x += a.x;
+      o.y += a.y;
+      pnear[f + threadIdx.x] = o;
+    }
+  }
+}
+
+// Source-side partial sums of the symmetric blocks, per source leaf in a
+// fixed order (Plan::red_*): p_j += sum_k scratch[base + k n + (j - first)].
+template <bool MIXED>
+__global__ void k_p2p_reduce(int64_t nleaf, const int32_t* __restrict__ first, const int32_t* __restrict__ n,
+                             const int32_t* __restrict__ nin, const int64_t* __restrict__ base,
+                             const void* __restrict__ scratch, double2* __restrict__ pnear) {
+  typedef typename std::conditional<MIXED, float2, double2>::type Q;
+  const Q* scr = static_cast<const Q*>(scratch);
+  for (int64_t l = blockIdx.x; l < nleaf; l += gridDim.x) {
+    const int nl = n[l], ni = nin[l];
+    const int64_t b = base[l];
+    for (int j = threadIdx.x; j < nl; j += blockDim.x) {
+      double ar = 0., ai = 0.;
+      for (int k = 0; k < ni; k++) {
+        const Q v = scr[b + (int64_t)k * nl + j];
+        ar += (double)v.x;
+        ai += (double)v.y;
+      }
+      double2 o = pnear[first[l] + j];
+      o.x += ar;
+      o.y += ai;
+      pnear[first[l] + j] = o;
+    }
+  }
+}
+
 // ------------------------------------------------------------ direct sum --
 // FP64 direct sum at sampled targets (CheckFULL arithmetic,
 // interface.hpp:178-221): one warp per target, lanes over sources.
@@ -1135,6 +1357,31 @@ void launch_p2p(bool fp64, const DevPlan& dp, int64_t nchunk, const int32_t* ord
     k_p2p_tiled<false><<<grid, 128, 0, s>>>(dp, nchunk, order, tfirst, tn, ptr, sfirst, sn, q, pnear, queue);
   else
     k_p2p_tiled<true><<<grid, 128, 0, s>>>(dp, nchunk, order, tfirst, tn, ptr, sfirst, sn, q, pnear, queue);
+}
+
+void launch_p2p_sym(bool fp64, const DevPlan& dp, int64_t nwork, const int32_t* order, const int32_t* tfirst,
+                    const int32_t* tn, const int64_t* ptr, const int32_t* sfirst, const int32_t* sn,
+                    const int64_t* soff, const void* q, double2* pnear, void* scratch, unsigned long long* queue,
+                    int nsm, cudaStream_t s) {
+  if (nwork <= 0) return;
+  cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s);
+  const int grid = (int)std::min<int64_t>(nwork, (int64_t)nsm * 16);
+  if (fp64)
+    k_p2p_sym<false><<<grid, 128, 0, s>>>(dp, nwork, order, tfirst, tn, ptr, sfirst, sn, soff, q, pnear, scratch,
+                                          queue);
+  else
+    k_p2p_sym<true><<<grid, 128, 0, s>>>(dp, nwork, order, tfirst, tn, ptr, sfirst, sn, soff, q, pnear, scratch,
+                                         queue);
+}
+
+void launch_p2p_reduce(bool fp64, int64_t nleaf, const int32_t* first, const int32_t* n, const int32_t* nin,
+                       const int64_t* base, const void* scratch, double2* pnear, int nsm, cudaStream_t s) {
+  if (nleaf <= 0) return;
+  const int grid = (int)std::min<int64_t>(nleaf, (int64_t)nsm * 16);
+  if (fp64)
+    k_p2p_reduce<false><<<grid, 64, 0, s>>>(nleaf, first, n, nin, base, scratch, pnear);
+  else
+    k_p2p_reduce<true><<<grid, 64, 0, s>>>(nleaf, first, n, nin, base, scratch, pnear);
 }
 
 void launch_direct(int64_t ns, const double* spos, const int32_t* sperm, const double2* qin, int64_t nt,

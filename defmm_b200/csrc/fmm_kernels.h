@@ -37,6 +37,16 @@ void launch_scatter(const double2* pnear, const double2* pfar, const int32_t* pe
 void launch_p2p(bool fp64, const DevPlan& dp, int64_t nchunk, const int32_t* order, const int32_t* tfirst,
                 const int32_t* tn, const int64_t* ptr, const int32_t* sfirst, const int32_t* sn, const void* q,
                 double2* pnear, unsigned long long* queue, int nsm, cudaStream_t s);
+// Symmetric near field: symmetric blocks (k_p2p_sym, adds the target side to
+// pnear and writes the source side to scratch) and the per-leaf reduction of
+// the scratch into pnear (k_p2p_reduce).  Scratch holds double2 (fp64) or
+// float2 (mixed) partial sums.
+void launch_p2p_sym(bool fp64, const DevPlan& dp, int64_t nwork, const int32_t* order, const int32_t* tfirst,
+                    const int32_t* tn, const int64_t* ptr, const int32_t* sfirst, const int32_t* sn,
+                    const int64_t* soff, const void* q, double2* pnear, void* scratch, unsigned long long* queue,
+                    int nsm, cudaStream_t s);
+void launch_p2p_reduce(bool fp64, int64_t nleaf, const int32_t* first, const int32_t* n, const int32_t* nin,
+                       const int64_t* base, const void* scratch, double2* pnear, int nsm, cudaStream_t s);
 void launch_direct(int64_t ns, const double* spos, const int32_t* sperm, const double2* qin, int64_t nt,
                    const double* tpos, double kappa, double2* out, cudaStream_t s);
 

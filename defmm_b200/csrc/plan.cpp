@@ -575,6 +575,87 @@ void level_slots(const Plan& p, int l, const LevelFlags& F, Slots& s,
   s.n += tot;
 }
 
+// Symmetric decomposition of the near field (Plan::self_*, sym_*, red_*),
+// for one tree holding both sources and targets.  Source ranges are unions
+// of whole leaves, and a leaf's own range is always present (its self pair).
+void build_symmetric_near(Plan& p) {
+  const Tree& T = p.T;
+  const int64_t nch = (int64_t)p.p2p_tfirst.size();
+  std::vector<int32_t> leaf_at(T.pos.size() / 3, -1);  // particle -> leaf
+  for (int64_t c = 0; c < T.ncell; c++)
+    if (T.leaf(c))
+      for (int32_t k = 0; k < T.nprt[c]; k++) leaf_at[T.first[c] + k] = (int32_t)c;
+  p.self_ptr.assign(1, 0);
+  p.self_sfirst.clear();
+  p.self_sn.clear();
+  p.sym_ptr.assign(1, 0);
+  p.sym_sfirst.clear();
+  p.sym_sn.clear();
+  std::vector<int32_t> sym_leaf;
+  for (int64_t ch = 0; ch < nch; ch++) {
+    const int32_t lf = leaf_at[p.p2p_tfirst[ch]];
+    const int32_t a0 = T.first[lf], a1 = a0 + T.nprt[lf];
+    for (int64_t r = p.p2p_ptr[ch]; r < p.p2p_ptr[ch + 1]; r++) {
+      const int32_t s0 = p.p2p_sfirst[r], s1 = s0 + p.p2p_sn[r];
+      if (s0 < a1 && s1 > a0) {  // the own leaf
+        p.self_sfirst.push_back(a0);
+        p.self_sn.push_back(a1 - a0);
+      }
+      for (int32_t j = std::max(s0, a1); j < s1;) {  // source leaves after the own leaf
+        const int32_t sl = leaf_at[j];
+        p.sym_sfirst.push_back(j);
+        p.sym_sn.push_back(T.nprt[sl]);
+        sym_leaf.push_back(sl);
+        j += T.nprt[sl];
+      }
+    }
+    p.self_ptr.push_back((int64_t)p.self_sfirst.size());
+    p.sym_ptr.push_back((int64_t)p.sym_sfirst.size());
+  }
+  // scratch: per source leaf, one row of its particles per incoming block,
+  // rows in chunk order
+  std::vector<int32_t> nin(T.ncell, 0);
+  for (int32_t sl : sym_leaf) nin[sl]++;
+  std::vector<int64_t> base(T.ncell, 0);
+  int64_t tot = 0;
+  p.red_first.clear();
+  p.red_n.clear();
+  p.red_nin.clear();
+  p.red_base.clear();
+  for (int64_t c = 0; c < T.ncell; c++)
+    if (nin[c]) {
+      base[c] = tot;
+      p.red_first.push_back(T.first[c]);
+      p.red_n.push_back(T.nprt[c]);
+      p.red_nin.push_back(nin[c]);
+      p.red_base.push_back(tot);
+      tot += (int64_t)nin[c] * T.nprt[c];
+    }
+  p.sym_scratch = tot;
+  std::fill(nin.begin(), nin.end(), 0);
+  p.sym_soff.resize(sym_leaf.size());
+  for (size_t r = 0; r < sym_leaf.size(); r++) {
+    const int32_t sl = sym_leaf[r];
+    p.sym_soff[r] = base[sl] + (int64_t)(nin[sl]++) * T.nprt[sl];
+  }
+  // work orders: a chunk occupies tp = nextpow2(tn) lanes per source
+  std::vector<int64_t> ws(nch, 0), wy(nch, 0);
+  for (int64_t ch = 0; ch < nch; ch++) {
+    int tp = 4;
+    while (tp < p.p2p_tn[ch]) tp <<= 1;
+    for (int64_t r = p.self_ptr[ch]; r < p.self_ptr[ch + 1]; r++) ws[ch] += (int64_t)p.self_sn[r] * 32;
+    for (int64_t r = p.sym_ptr[ch]; r < p.sym_ptr[ch + 1]; r++) wy[ch] += (int64_t)p.sym_sn[r] * tp;
+  }
+  auto order = [&](const std::vector<int64_t>& w, std::vector<int32_t>& o) {
+    o.clear();
+    for (int64_t ch = 0; ch < nch; ch++)
+      if (w[ch]) o.push_back((int32_t)ch);
+    std::stable_sort(o.begin(), o.end(), [&](int32_t a, int32_t b) { return w[a] > w[b]; });
+  };
+  order(ws, p.self_order);
+  order(wy, p.sym_order);
+}
+
 }  // namespace
 
 int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
@@ -603,6 +684,7 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
   p.ncrit = ncrit;
   p.lvmax = lvmax;
   p.kappa = kappa;
+  p.p2p_sym = ns == nt && (src == trg || std::memcmp(src, trg, sizeof(double) * 3 * (size_t)ns) == 0);
   double t0 = now_s();
   // particles.hpp:79-100 (getBounds): one cube around targets and sources
   {
@@ -1037,6 +1119,7 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
     std::stable_sort(p.p2p_order.begin(), p.p2p_order.end(),
                      [&](int32_t a, int32_t b) { return work[a] > work[b]; });
   }
+  if (p.p2p_sym) build_symmetric_near(p);
   p.t_lists = now_s() - t0;
 
   // transfer spectra, FP64 (circulant.hpp:133-144)

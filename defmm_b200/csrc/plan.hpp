@@ -101,6 +101,23 @@ struct Plan {
   std::vector<int64_t> p2p_ptr;              // chunks + 1
   std::vector<int32_t> p2p_sfirst, p2p_sn;   // source particle ranges
   std::vector<int32_t> p2p_order;            // chunks by decreasing work (tn x sources)
+  // Symmetric near field (sources and targets are the same points, so the
+  // particle interactions come in mirrored pairs): each chunk keeps its own
+  // leaf as a plain block (self_*) and the source leaves after its leaf in
+  // tree order as symmetric blocks (sym_*); one evaluation of G(x_i, y_j)
+  // then serves p_i and p_j.  The mirrored part (sources before the leaf)
+  // is dropped: it arrives from the other leaf's chunks, as partial sums
+  // written to scratch at sym_soff and reduced per source leaf (red_*) in a
+  // fixed order.
+  bool p2p_sym = false;
+  std::vector<int64_t> self_ptr;             // chunks + 1
+  std::vector<int32_t> self_sfirst, self_sn, self_order;
+  std::vector<int64_t> sym_ptr;              // chunks + 1 into sym ranges (one source leaf each)
+  std::vector<int32_t> sym_sfirst, sym_sn, sym_order;
+  std::vector<int64_t> sym_soff;             // scratch slot of the range's first source
+  std::vector<int32_t> red_first, red_n, red_nin;  // per source leaf with partial sums
+  std::vector<int64_t> red_base;
+  int64_t sym_scratch = 0;                   // scratch slots (one complex each)
   // statistics
   int64_t n_far_hf = 0, n_far_lf = 0, n_near = 0, i_near = 0;
   // Optional record of the lists for parity checks: far (t, s, lvl, cone,
