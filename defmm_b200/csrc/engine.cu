@@ -36,7 +36,8 @@ struct defmm_handle {
   std::string err;
   // device state
   int device = -1;
-  cudaStream_t st = nullptr, st2 = nullptr;
+  cudaStream_t st = nullptr, st2 = nullptr;  // own stream; near field
+  cudaStream_t cur = nullptr;                // stream of the gemv in progress (phase events)
   std::vector<void*> plan_allocs;  // freed when the plan is rebuilt
   DevPlan dp;
   const dfb::OpTable* ops = nullptr;
@@ -51,12 +52,16 @@ struct defmm_handle {
   const int32_t *d_tfirst = nullptr, *d_tn = nullptr, *d_sfirst = nullptr, *d_sn = nullptr;
   const int64_t* d_p2p_ptr = nullptr;
   const int32_t* d_p2p_order = nullptr;
+  const int32_t *d_p2p_item_chunk = nullptr, *d_sym_item_chunk = nullptr;
+  const int64_t *d_p2p_chunk_items = nullptr, *d_sym_chunk_items = nullptr;
+  double2* d_tpart = nullptr;  // near-field item partial sums (32 per item)
   unsigned long long* d_queue = nullptr;
   // symmetric near field (Plan::self_*, sym_*, red_*)
-  const int64_t *d_self_ptr = nullptr, *d_sym_ptr = nullptr, *d_sym_soff = nullptr, *d_red_base = nullptr;
+  const int64_t *d_self_ptr = nullptr, *d_sym_ptr = nullptr, *d_sym_soff = nullptr, *d_red_ptr = nullptr,
+                *d_red_off = nullptr;
   const int32_t *d_self_sfirst = nullptr, *d_self_sn = nullptr, *d_self_order = nullptr;
   const int32_t *d_sym_sfirst = nullptr, *d_sym_sn = nullptr, *d_sym_order = nullptr;
-  const int32_t *d_red_first = nullptr, *d_red_n = nullptr, *d_red_nin = nullptr;
+  const int32_t *d_red_first = nullptr, *d_red_n = nullptr;
   DevBuf pscr;           // source-side partial sums (one complex per slot)
   bool use_sym = false;  // this precision runs the symmetric near field
   int nsm = 148;
@@ -245,7 +250,11 @@ int upload_plan(defmm_handle* h) {
   UP(p.p2p_sfirst, h->d_sfirst);
   UP(p.p2p_sn, h->d_sn);
   UP(p.p2p_order, h->d_p2p_order);
+  UP(p.p2p_item_chunk, h->d_p2p_item_chunk);
+  UP(p.p2p_chunk_items, h->d_p2p_chunk_items);
   if (p.p2p_sym) {
+    UP(p.sym_item_chunk, h->d_sym_item_chunk);
+    UP(p.sym_chunk_items, h->d_sym_chunk_items);
     UP(p.self_ptr, h->d_self_ptr);
     UP(p.self_sfirst, h->d_self_sfirst);
     UP(p.self_sn, h->d_self_sn);
@@ -257,8 +266,8 @@ int upload_plan(defmm_handle* h) {
     UP(p.sym_order, h->d_sym_order);
     UP(p.red_first, h->d_red_first);
     UP(p.red_n, h->d_red_n);
-    UP(p.red_nin, h->d_red_nin);
-    UP(p.red_base, h->d_red_base);
+    UP(p.red_ptr, h->d_red_ptr);
+    UP(p.red_off, h->d_red_off);
   }
   h->nchunk = (int64_t)p.p2p_tfirst.size();
 #undef UP
@@ -268,6 +277,12 @@ int upload_plan(defmm_handle* h) {
     h->plan_allocs.push_back(e);
     CK(cudaMemset(e, 0, sizeof(int)));
     d.err = static_cast<int*>(e);
+    const size_t nitem = std::max<size_t>(1, std::max(p.p2p_item_chunk.size(), p.sym_item_chunk.size()));
+    void* tp = nullptr;
+    CK(cudaMalloc(&tp, nitem * 32 * sizeof(double2)));
+    h->plan_allocs.push_back(tp);
+    h->dev_bytes += nitem * 32 * sizeof(double2);
+    h->d_tpart = static_cast<double2*>(tp);
     void* qc = nullptr;
     CK(cudaMalloc(&qc, 2 * sizeof(unsigned long long)));  // P2P (stream 2), M2L (main stream)
     h->plan_allocs.push_back(qc);
@@ -340,17 +355,24 @@ int prepare_precision(defmm_handle* h) {
   if ((st = ensure(h, h->M, std::max<int64_t>(1, p.sS.n) * p.LL * cs)) ||
       (st = ensure(h, h->Lx, std::max<int64_t>(1, p.sT.n) * p.LL * cs)) || (st = ensure(h, h->q, nS * cs)))
     return st;
-  // symmetric near field when its scratch takes at most 40% of the free
-  // memory (otherwise every interaction is evaluated from both sides)
+  // symmetric near field when its scratch takes at most 70% of the free
+  // memory and can be allocated (otherwise every interaction is evaluated
+  // from both sides)
   free_buf(h->pscr);
   h->use_sym = false;
   if (p.p2p_sym && p.sym_scratch > 0) {
     size_t fr0 = 0, tot0 = 0;
     CK(cudaMemGetInfo(&fr0, &tot0));
     const size_t b = (size_t)p.sym_scratch * cs;
-    if (b <= (size_t)(0.4 * (double)fr0)) {
-      if ((st = ensure(h, h->pscr, b))) return st;
-      h->use_sym = true;
+    if (b <= (size_t)(0.7 * (double)fr0)) {
+      void* ptr = nullptr;
+      if (cudaMalloc(&ptr, b) == cudaSuccess) {
+        h->pscr.p = ptr;
+        h->pscr.bytes = b;
+        h->use_sym = true;
+      } else {
+        cudaGetLastError();
+      }
     }
   }
   // F batch buffer: at least the largest cone of any level, at most about
@@ -375,7 +397,7 @@ int prepare_precision(defmm_handle* h) {
 }
 
 void rec(defmm_handle* h, int i) {
-  if (h->events) cudaEventRecord(h->ev[i], h->st);
+  if (h->events) cudaEventRecord(h->ev[i], h->cur);
 }
 
 // One matvec, everything on the device: qin (user order) -> out (user order).
@@ -386,43 +408,50 @@ int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) 
   const dfb::OpTable* ops = h->ops;
   const int64_t nS = (int64_t)p.S.perm.size(), nT = (int64_t)p.T.perm.size();
   const int nl = p.lv.nlvl;
-  h->st = s;
+  h->cur = s;
   int64_t nl_ = 0;
   rec(h, 2 * PH_TOTAL);
   dfb::launch_gather(fp64, qin, d.S_perm, h->q.p, nS, 0, 0, 1, s);
-  nl_ += 1 + (h->nchunk ? 1 : 0) + (p.p2m_leaf.empty() ? 0 : 1) + (p.l2p_leaf.empty() ? 0 : 1) + 1;
+  nl_ += 1 + (p.p2m_leaf.empty() ? 0 : 1) + (p.l2p_leaf.empty() ? 0 : 1) + 1;
   CK(cudaMemsetAsync(h->pfar.p, 0, 16 * nT, s));
   CK(cudaMemsetAsync(h->pnear.p, 0, 16 * nT, s));
   CK(cudaMemsetAsync(h->Lx.p, 0, h->Lx.bytes, s));
   // near field on the second stream, overlapping the far field
   // (profiling runs it on the main stream so that phase times do not overlap)
   cudaStream_t sn = h->events ? s : h->st2;
+  const cudaStream_t sf = s;
   cudaEvent_t ready = h->ev_ready;
   CK(cudaEventRecord(ready, s));
   CK(cudaStreamWaitEvent(sn, ready, 0));
   if (h->events) cudaEventRecord(h->ev[2 * PH_P2P], sn);
   if (h->use_sym) {  // own leaves, then symmetric blocks, then the mirrored partial sums
-    dfb::launch_p2p(fp64, d, (int64_t)p.self_order.size(), h->d_self_order, h->d_tfirst, h->d_tn, h->d_self_ptr,
-                    h->d_self_sfirst, h->d_self_sn, h->q.p, (double2*)h->pnear.p, h->d_queue, h->nsm, sn);
-    dfb::launch_p2p_sym(fp64, d, (int64_t)p.sym_order.size(), h->d_sym_order, h->d_tfirst, h->d_tn, h->d_sym_ptr,
-                        h->d_sym_sfirst, h->d_sym_sn, h->d_sym_soff, h->q.p, (double2*)h->pnear.p, h->pscr.p,
-                        h->d_queue, h->nsm, sn);
-    dfb::launch_p2p_reduce(fp64, (int64_t)p.red_first.size(), h->d_red_first, h->d_red_n, h->d_red_nin,
-                           h->d_red_base, h->pscr.p, (double2*)h->pnear.p, h->nsm, sn);
-    nl_ += (p.self_order.empty() ? 0 : 1) + (p.sym_order.empty() ? 0 : 1) + (p.red_first.empty() ? 0 : 1) -
-           (h->nchunk ? 1 : 0);
-  } else {
-    dfb::launch_p2p(fp64, d, h->nchunk, h->d_p2p_order, h->d_tfirst, h->d_tn, h->d_p2p_ptr, h->d_sfirst, h->d_sn,
-                    h->q.p, (double2*)h->pnear.p, h->d_queue, h->nsm, sn);
+    dfb::launch_p2p(fp64, d, (int64_t)p.self_order.size(), h->d_self_order, nullptr, h->d_tfirst, h->d_tn,
+                    h->d_self_ptr, h->d_self_sfirst, h->d_self_sn, h->q.p, (double2*)h->pnear.p, nullptr,
+                    h->d_queue, h->nsm, sn);
+    dfb::launch_p2p_sym(fp64, d, (int64_t)p.sym_order.size(), h->d_sym_order, h->d_sym_item_chunk, h->d_tfirst,
+                        h->d_tn, h->d_sym_ptr, h->d_sym_sfirst, h->d_sym_sn, h->d_sym_soff, h->q.p, h->d_tpart,
+                        h->pscr.p, h->d_queue, h->nsm, sn);
+    dfb::launch_p2p_items(h->nchunk, h->d_tfirst, h->d_tn, h->d_sym_chunk_items, h->d_tpart, (double2*)h->pnear.p,
+                          h->nsm, sn);
+    dfb::launch_p2p_reduce(fp64, (int64_t)p.red_first.size(), h->d_red_first, h->d_red_n, h->d_red_ptr,
+                           h->d_red_off, h->pscr.p, (double2*)h->pnear.p, h->nsm, sn);
+    nl_ += (p.self_order.empty() ? 0 : 1) + (p.sym_order.empty() ? 0 : 2) + (p.red_first.empty() ? 0 : 1);
+  } else {  // every interaction from the target side, in items
+    dfb::launch_p2p(fp64, d, (int64_t)p.p2p_order.size(), h->d_p2p_order, h->d_p2p_item_chunk, h->d_tfirst, h->d_tn,
+                    h->d_p2p_ptr, h->d_sfirst, h->d_sn, h->q.p, (double2*)h->pnear.p, h->d_tpart, h->d_queue,
+                    h->nsm, sn);
+    dfb::launch_p2p_items(h->nchunk, h->d_tfirst, h->d_tn, h->d_p2p_chunk_items, h->d_tpart, (double2*)h->pnear.p,
+                          h->nsm, sn);
+    nl_ += p.p2p_order.empty() ? 0 : 2;
   }
   if (h->events) cudaEventRecord(h->ev[2 * PH_P2P + 1], sn);
   // upward pass
   rec(h, 2 * PH_P2M);
-  ops->p2m(d, h->d_p2m_leaf, (int)p.p2m_leaf.size(), h->q.p, h->sig2.p, h->M.p, s);
+  ops->p2m(d, h->d_p2m_leaf, (int)p.p2m_leaf.size(), h->q.p, h->sig2.p, h->M.p, sf);
   rec(h, 2 * PH_P2M + 1);
   rec(h, 2 * PH_M2M);
   for (int l = nl - 2; l >= p.lv.max_stage; l--) {
-    ops->m2m(d, p.sS.lvl_begin[l], p.sS.lvl_begin[l + 1], h->sig.p, h->sig2.p, h->M.p, s);
+    ops->m2m(d, p.sS.lvl_begin[l], p.sS.lvl_begin[l + 1], h->sig.p, h->sig2.p, h->M.p, sf);
     nl_ += p.sS.lvl_begin[l + 1] > p.sS.lvl_begin[l] ? 1 : 0;
   }
   rec(h, 2 * PH_M2M + 1);
@@ -440,11 +469,11 @@ int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) 
       const int64_t fs0 = cS[c0], fs1 = cS[c1], ts0 = cT[c0], ts1 = cT[c1];
       if (ts1 > ts0 && fs1 > fs0) {
         rec(h, 2 * PH_M2F);
-        ops->m2f(fs1 - fs0, (const char*)h->M.p + fs0 * p.LL * cs, h->F.p, s);
+        ops->m2f(fs1 - fs0, (const char*)h->M.p + fs0 * p.LL * cs, h->F.p, sf);
         nl_ += 2;
         rec(h, 2 * PH_M2F + 1);
         rec(h, 2 * PH_M2L);
-        ops->m2l(d, ts0, ts1, fs0, fs1, h->F.p, h->ptab.p, h->Lx.p, h->d_queue + 1, h->nsm, s);
+        ops->m2l(d, ts0, ts1, fs0, fs1, h->F.p, h->ptab.p, h->Lx.p, h->d_queue + 1, h->nsm, sf);
         rec(h, 2 * PH_M2L + 1);
         if (h->events) {
           float a;
@@ -459,7 +488,7 @@ int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) 
     }
     if (l + 1 < nl) {
       rec(h, 2 * PH_L2L);
-      ops->l2l(d, p.sT.lvl_begin[l + 1], p.sT.lvl_begin[l + 2], h->sig.p, h->sig2.p, h->Lx.p, s);
+      ops->l2l(d, p.sT.lvl_begin[l + 1], p.sT.lvl_begin[l + 2], h->sig.p, h->sig2.p, h->Lx.p, sf);
       nl_ += p.sT.lvl_begin[l + 2] > p.sT.lvl_begin[l + 1] ? 1 : 0;
       rec(h, 2 * PH_L2L + 1);
       if (h->events) {
@@ -471,11 +500,10 @@ int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) 
     }
   }
   rec(h, 2 * PH_L2P);
-  ops->l2p(d, h->d_l2p_leaf, (int)p.l2p_leaf.size(), h->sig2.p, h->Lx.p, (double2*)h->pfar.p, s);
+  ops->l2p(d, h->d_l2p_leaf, (int)p.l2p_leaf.size(), h->sig2.p, h->Lx.p, (double2*)h->pfar.p, sf);
   rec(h, 2 * PH_L2P + 1);
-  cudaEvent_t done = h->ev_done;
-  CK(cudaEventRecord(done, sn));
-  CK(cudaStreamWaitEvent(s, done, 0));
+  CK(cudaEventRecord(h->ev_done, sn));
+  CK(cudaStreamWaitEvent(s, h->ev_done, 0));
   rec(h, 2 * PH_SCATTER);
   dfb::launch_scatter((const double2*)h->pnear.p, (const double2*)h->pfar.p, d.T_perm, out, nT, s);
   rec(h, 2 * PH_SCATTER + 1);

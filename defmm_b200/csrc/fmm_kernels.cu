@@ -779,9 +779,9 @@ __device__ __forceinline__ void sincos_reduced(double theta, float& s, float& c)
 }
 
 
-// Near field, tiled: one CTA (4 warps) per chunk of <= 32 target particles
-// of one leaf; CTAs take chunks from a global queue (the host orders chunks
-// by decreasing work).  The chunk's source ranges are streamed through shared
+// Near field, tiled: one CTA (4 warps) per work item (part of the sources of
+// one chunk of <= 32 target particles of one leaf); CTAs take items from a
+// global queue in the host's order of decreasing work.  The chunk's source ranges are streamed through shared
 // memory in tiles of TS particles loaded with coalesced reads; inside a warp,
 // lanes form groups of tp >= nt lanes (one target each) and the 4 warps x
 // groups take interleaved sources of the tile, two at a time.  Partial sums
@@ -885,11 +885,13 @@ __device__ __forceinline__ void p2p_pair_mixed(double x0, double x1, double x2, 
 }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(128) k_p2p_tiled(DevPlan P, int64_t nchunk, const int32_t* __restrict__ order,
+__global__ void __launch_bounds__(128) k_p2p_tiled(DevPlan P, int64_t nitem, const int32_t* __restrict__ order,
+                                                   const int32_t* __restrict__ item_chunk,
                                                    const int32_t* __restrict__ tfirst, const int32_t* __restrict__ tn,
                                                    const int64_t* __restrict__ ptr, const int32_t* __restrict__ sfirst,
                                                    const int32_t* __restrict__ sn, const void* __restrict__ qv,
-                                                   double2* __restrict__ pnear, unsigned long long* __restrict__ queue) {
+                                                   double2* __restrict__ pnear, double2* __restrict__ tpart,
+                                                   unsigned long long* __restrict__ queue) {
   constexpr int TS = 512;
   typedef typename std::conditional<MIXED, float2, double2>::type Q;
   const Q* q = static_cast<const Q*>(qv);
@@ -903,8 +905,9 @@ __global__ void __launch_bounds__(128) k_p2p_tiled(DevPlan P, int64_t nchunk, co
     if (threadIdx.x == 0) cur = (int64_t)atomicAdd(queue, 1ULL);
     __syncthreads();
     const int64_t k = cur;
-    if (k >= nchunk) break;
-    const int64_t ch = order[k];
+    if (k >= nitem) break;
+    const int64_t it = order[k];
+    const int64_t ch = item_chunk ? item_chunk[it] : it;
     const int f = tfirst[ch], nt = tn[ch];
     int tp = 1;
     while (tp < nt) tp <<= 1;
@@ -914,7 +917,7 @@ __global__ void __launch_bounds__(128) k_p2p_tiled(DevPlan P, int64_t nchunk, co
     const double x0 = P.T_pos[3 * (int64_t)ti], x1 = P.T_pos[3 * (int64_t)ti + 1], x2 = P.T_pos[3 * (int64_t)ti + 2];
     double pr = 0., pim = 0.;
     float sr = 0.f, cr = 0.f, si = 0.f, ci = 0.f;  // mixed: compensated FP32 sums
-    const int64_t rb = ptr[ch], re = ptr[ch + 1];
+    const int64_t rb = ptr[it], re = ptr[it + 1];
     int64_t r = rb;
     int off = 0;  // position inside range r
     while (r < re) {
@@ -977,8 +980,32 @@ __global__ void __launch_bounds__(128) k_p2p_tiled(DevPlan P, int64_t nchunk, co
         a.x += red[w][threadIdx.x].x;
         a.y += red[w][threadIdx.x].y;
       }
-      pnear[f + threadIdx.x] = a;
+      if (tpart)
+        tpart[it * 32 + threadIdx.x] = a;  // item partial, added per chunk by k_p2p_items
+      else
+        pnear[f + threadIdx.x] = a;
     }
+  }
+}
+
+// Item partial sums of the near field into p, per chunk in item order.
+__global__ void k_p2p_items(int64_t nchunk, const int32_t* __restrict__ tfirst, const int32_t* __restrict__ tn,
+                            const int64_t* __restrict__ chunk_items, const double2* __restrict__ tpart,
+                            double2* __restrict__ pnear) {
+  const int t = threadIdx.x & 31;
+  for (int64_t ch = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); ch < nchunk;
+       ch += (int64_t)gridDim.x * (blockDim.x >> 5)) {
+    if (t >= tn[ch]) continue;
+    double ar = 0., ai = 0.;
+    for (int64_t it = chunk_items[ch]; it < chunk_items[ch + 1]; it++) {
+      const double2 v = tpart[it * 32 + t];
+      ar += v.x;
+      ai += v.y;
+    }
+    double2 o = pnear[tfirst[ch] + t];
+    o.x += ar;
+    o.y += ai;
+    pnear[tfirst[ch] + t] = o;
   }
 }
 
@@ -1030,7 +1057,8 @@ __device__ __forceinline__ float2 green32(double dx, double dy, double dz, doubl
 }
 
 // Symmetric blocks of the near field (Plan::sym_*): one CTA (4 warps) per
-// chunk of <= 32 targets, taken from a queue.  A warp splits into segments
+// work item (part of the sources of one chunk of <= 32 targets), items taken
+// from a queue in the host's order of decreasing work.  A warp splits into segments
 // of tp = nextpow2(nt) lanes; lane l of a segment owns source l of the
 // segment's tp-source sub-tile and, over tp steps, meets every target
 // i = (l + step) mod tp.  One evaluation of G feeds both
@@ -1038,17 +1066,18 @@ __device__ __forceinline__ float2 green32(double dx, double dy, double dz, doubl
 //                          and ends in lane i), and
 //   the source's partial  (lane-local),
 // so each mirrored pair of interactions costs one kernel evaluation.  Target
-// partials are added to pnear (after the self blocks); source partials go to
-// scratch and are added per source leaf by k_p2p_reduce.
+// partials of the item go to tpart (added per chunk by k_p2p_items); source
+// partials go to scratch and are added per source leaf by k_p2p_reduce.
 template <bool MIXED>
 __global__ void __launch_bounds__(128) k_p2p_sym(DevPlan P, int64_t nwork, const int32_t* __restrict__ order,
+                                                 const int32_t* __restrict__ item_chunk,
                                                  const int32_t* __restrict__ tfirst, const int32_t* __restrict__ tn,
                                                  const int64_t* __restrict__ ptr, const int32_t* __restrict__ sfirst,
                                                  const int32_t* __restrict__ sn, const int64_t* __restrict__ soff,
-                                                 const void* __restrict__ qv, double2* __restrict__ pnear,
+                                                 const void* __restrict__ qv, double2* __restrict__ tpart,
                                                  void* __restrict__ scratch, unsigned long long* __restrict__ queue) {
   typedef typename std::conditional<MIXED, float2, double2>::type Q;
-  constexpr int RMAX = 64;
+  constexpr int RMAX = 128;
   const Q* q = static_cast<const Q*>(qv);
   Q* scr = static_cast<Q*>(scratch);
   __shared__ double tx[32], ty[32], tz[32];
@@ -1064,7 +1093,8 @@ __global__ void __launch_bounds__(128) k_p2p_sym(DevPlan P, int64_t nwork, const
     __syncthreads();
     const int64_t k = cur;
     if (k >= nwork) break;
-    const int64_t ch = order[k];
+    const int64_t it = order[k];
+    const int64_t ch = item_chunk[it];
     const int f = tfirst[ch], nt = tn[ch];
     int tp = 4;
     while (tp < nt) tp <<= 1;
@@ -1084,19 +1114,28 @@ __global__ void __launch_bounds__(128) k_p2p_sym(DevPlan P, int64_t nwork, const
     }
     float sr = 0.f, cr = 0.f, si = 0.f, ci = 0.f;  // mixed: compensated target sums
     double pr = 0., pim = 0.;                      // FP64 target sums
-    const int64_t rb = ptr[ch], re = ptr[ch + 1];
+    const int64_t rb = ptr[it], re = ptr[it + 1];
     for (int64_t r0 = rb; r0 < re; r0 += RMAX) {
       const int nr = (int)min((int64_t)RMAX, re - r0);
       __syncthreads();  // previous batch of ranges (and the target arrays) settled
-      if (threadIdx.x == 0) {
-        int a = 0;
-        for (int m = 0; m < nr; m++) {
-          rpre[m] = a;
-          rfst[m] = sfirst[r0 + m];
-          roff[m] = soff[r0 + m];
-          a += sn[r0 + m];
+      for (int m = threadIdx.x; m < nr; m += blockDim.x) {
+        rfst[m] = sfirst[r0 + m];
+        roff[m] = soff[r0 + m];
+        rpre[m + 1] = sn[r0 + m];
+      }
+      __syncthreads();
+      if (warp == 0) {  // inclusive scan of the range lengths
+        int carry = 0;
+        for (int b0 = 0; b0 < nr; b0 += 32) {
+          int v = b0 + lane < nr ? rpre[b0 + lane + 1] : 0;
+          for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += u;
+          }
+          if (b0 + lane < nr) rpre[b0 + lane + 1] = carry + v;
+          carry += __shfl_sync(0xffffffffu, v, 31);
         }
-        rpre[nr] = a;
+        if (lane == 0) rpre[0] = 0;
       }
       __syncthreads();
       const int ntot = rpre[nr];
@@ -1170,29 +1209,26 @@ __global__ void __launch_bounds__(128) k_p2p_sym(DevPlan P, int64_t nwork, const
         a.x += red[w][threadIdx.x].x;
         a.y += red[w][threadIdx.x].y;
       }
-      double2 o = pnear[f + threadIdx.x];
-      o.x += a.x;
-      o.y += a.y;
-      pnear[f + threadIdx.x] = o;
+      tpart[it * 32 + threadIdx.x] = a;
     }
   }
 }
 
 // Source-side partial sums of the symmetric blocks, per source leaf in a
-// fixed order (Plan::red_*): p_j += sum_k scratch[base + k n + (j - first)].
+// fixed order (Plan::red_*): p_j += sum_k scratch[off_k + (j - first)].
 template <bool MIXED>
 __global__ void k_p2p_reduce(int64_t nleaf, const int32_t* __restrict__ first, const int32_t* __restrict__ n,
-                             const int32_t* __restrict__ nin, const int64_t* __restrict__ base,
+                             const int64_t* __restrict__ rptr, const int64_t* __restrict__ roff,
                              const void* __restrict__ scratch, double2* __restrict__ pnear) {
   typedef typename std::conditional<MIXED, float2, double2>::type Q;
   const Q* scr = static_cast<const Q*>(scratch);
   for (int64_t l = blockIdx.x; l < nleaf; l += gridDim.x) {
-    const int nl = n[l], ni = nin[l];
-    const int64_t b = base[l];
+    const int nl = n[l];
+    const int64_t kb = rptr[l], ke = rptr[l + 1];
     for (int j = threadIdx.x; j < nl; j += blockDim.x) {
       double ar = 0., ai = 0.;
-      for (int k = 0; k < ni; k++) {
-        const Q v = scr[b + (int64_t)k * nl + j];
+      for (int64_t k = kb; k < ke; k++) {
+        const Q v = scr[roff[k] + j];
         ar += (double)v.x;
         ai += (double)v.y;
       }
@@ -1347,41 +1383,50 @@ void launch_scatter(const double2* pnear, const double2* pfar, const int32_t* pe
   k_scatter<<<(int)((n + 255) / 256), 256, 0, s>>>(pnear, pfar, perm, out, n);
 }
 
-void launch_p2p(bool fp64, const DevPlan& dp, int64_t nchunk, const int32_t* order, const int32_t* tfirst,
-                const int32_t* tn, const int64_t* ptr, const int32_t* sfirst, const int32_t* sn, const void* q,
-                double2* pnear, unsigned long long* queue, int nsm, cudaStream_t s) {
-  if (!nchunk) return;
+void launch_p2p(bool fp64, const DevPlan& dp, int64_t nitem, const int32_t* order, const int32_t* item_chunk,
+                const int32_t* tfirst, const int32_t* tn, const int64_t* ptr, const int32_t* sfirst, const int32_t* sn,
+                const void* q, double2* pnear, double2* tpart, unsigned long long* queue, int nsm, cudaStream_t s) {
+  if (!nitem) return;
   cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s);
-  const int grid = (int)std::min<int64_t>(nchunk, (int64_t)nsm * 16);
+  const int grid = (int)std::min<int64_t>(nitem, (int64_t)nsm * 16);
   if (fp64)
-    k_p2p_tiled<false><<<grid, 128, 0, s>>>(dp, nchunk, order, tfirst, tn, ptr, sfirst, sn, q, pnear, queue);
+    k_p2p_tiled<false><<<grid, 128, 0, s>>>(dp, nitem, order, item_chunk, tfirst, tn, ptr, sfirst, sn, q, pnear,
+                                            tpart, queue);
   else
-    k_p2p_tiled<true><<<grid, 128, 0, s>>>(dp, nchunk, order, tfirst, tn, ptr, sfirst, sn, q, pnear, queue);
+    k_p2p_tiled<true><<<grid, 128, 0, s>>>(dp, nitem, order, item_chunk, tfirst, tn, ptr, sfirst, sn, q, pnear,
+                                           tpart, queue);
 }
 
-void launch_p2p_sym(bool fp64, const DevPlan& dp, int64_t nwork, const int32_t* order, const int32_t* tfirst,
-                    const int32_t* tn, const int64_t* ptr, const int32_t* sfirst, const int32_t* sn,
-                    const int64_t* soff, const void* q, double2* pnear, void* scratch, unsigned long long* queue,
-                    int nsm, cudaStream_t s) {
+void launch_p2p_items(int64_t nchunk, const int32_t* tfirst, const int32_t* tn, const int64_t* chunk_items,
+                      const double2* tpart, double2* pnear, int nsm, cudaStream_t s) {
+  if (nchunk <= 0) return;
+  const int grid = (int)std::min<int64_t>((nchunk + 3) / 4, (int64_t)nsm * 16);
+  k_p2p_items<<<grid, 128, 0, s>>>(nchunk, tfirst, tn, chunk_items, tpart, pnear);
+}
+
+void launch_p2p_sym(bool fp64, const DevPlan& dp, int64_t nwork, const int32_t* order, const int32_t* item_chunk,
+                    const int32_t* tfirst, const int32_t* tn, const int64_t* ptr, const int32_t* sfirst,
+                    const int32_t* sn, const int64_t* soff, const void* q, double2* tpart, void* scratch,
+                    unsigned long long* queue, int nsm, cudaStream_t s) {
   if (nwork <= 0) return;
   cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s);
   const int grid = (int)std::min<int64_t>(nwork, (int64_t)nsm * 16);
   if (fp64)
-    k_p2p_sym<false><<<grid, 128, 0, s>>>(dp, nwork, order, tfirst, tn, ptr, sfirst, sn, soff, q, pnear, scratch,
-                                          queue);
+    k_p2p_sym<false><<<grid, 128, 0, s>>>(dp, nwork, order, item_chunk, tfirst, tn, ptr, sfirst, sn, soff, q, tpart,
+                                          scratch, queue);
   else
-    k_p2p_sym<true><<<grid, 128, 0, s>>>(dp, nwork, order, tfirst, tn, ptr, sfirst, sn, soff, q, pnear, scratch,
-                                         queue);
+    k_p2p_sym<true><<<grid, 128, 0, s>>>(dp, nwork, order, item_chunk, tfirst, tn, ptr, sfirst, sn, soff, q, tpart,
+                                         scratch, queue);
 }
 
-void launch_p2p_reduce(bool fp64, int64_t nleaf, const int32_t* first, const int32_t* n, const int32_t* nin,
-                       const int64_t* base, const void* scratch, double2* pnear, int nsm, cudaStream_t s) {
+void launch_p2p_reduce(bool fp64, int64_t nleaf, const int32_t* first, const int32_t* n, const int64_t* rptr,
+                       const int64_t* roff, const void* scratch, double2* pnear, int nsm, cudaStream_t s) {
   if (nleaf <= 0) return;
   const int grid = (int)std::min<int64_t>(nleaf, (int64_t)nsm * 16);
   if (fp64)
-    k_p2p_reduce<false><<<grid, 64, 0, s>>>(nleaf, first, n, nin, base, scratch, pnear);
+    k_p2p_reduce<false><<<grid, 64, 0, s>>>(nleaf, first, n, rptr, roff, scratch, pnear);
   else
-    k_p2p_reduce<true><<<grid, 64, 0, s>>>(nleaf, first, n, nin, base, scratch, pnear);
+    k_p2p_reduce<true><<<grid, 64, 0, s>>>(nleaf, first, n, rptr, roff, scratch, pnear);
 }
 
 void launch_direct(int64_t ns, const double* spos, const int32_t* sperm, const double2* qin, int64_t nt,

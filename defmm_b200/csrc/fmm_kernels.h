@@ -32,21 +32,26 @@ void launch_gather(bool fp64, const double2* qin, const int32_t* perm, void* q, 
                    int64_t stride_q, int nrhs, cudaStream_t s);
 void launch_scatter(const double2* pnear, const double2* pfar, const int32_t* perm, double2* out, int64_t n,
                     cudaStream_t s);
-// Near field (k_p2p_tiled); `order` lists chunks by decreasing work, `queue`
-// is a device counter the launch resets.
-void launch_p2p(bool fp64, const DevPlan& dp, int64_t nchunk, const int32_t* order, const int32_t* tfirst,
-                const int32_t* tn, const int64_t* ptr, const int32_t* sfirst, const int32_t* sn, const void* q,
-                double2* pnear, unsigned long long* queue, int nsm, cudaStream_t s);
-// Symmetric near field: symmetric blocks (k_p2p_sym, adds the target side to
-// pnear and writes the source side to scratch) and the per-leaf reduction of
+// Near field (k_p2p_tiled) over work items; `order` lists items by
+// decreasing work, `queue` is a device counter the launch resets.  With
+// item_chunk == nullptr items are chunks and sums are stored into pnear;
+// otherwise item partial sums go to tpart (32 per item) and
+// launch_p2p_items adds them per chunk, in item order.
+void launch_p2p(bool fp64, const DevPlan& dp, int64_t nitem, const int32_t* order, const int32_t* item_chunk,
+                const int32_t* tfirst, const int32_t* tn, const int64_t* ptr, const int32_t* sfirst, const int32_t* sn,
+                const void* q, double2* pnear, double2* tpart, unsigned long long* queue, int nsm, cudaStream_t s);
+void launch_p2p_items(int64_t nchunk, const int32_t* tfirst, const int32_t* tn, const int64_t* chunk_items,
+                      const double2* tpart, double2* pnear, int nsm, cudaStream_t s);
+// Symmetric near field: symmetric blocks over items (k_p2p_sym: the target
+// side to tpart, the source side to scratch) and the per-leaf reduction of
 // the scratch into pnear (k_p2p_reduce).  Scratch holds double2 (fp64) or
 // float2 (mixed) partial sums.
-void launch_p2p_sym(bool fp64, const DevPlan& dp, int64_t nwork, const int32_t* order, const int32_t* tfirst,
-                    const int32_t* tn, const int64_t* ptr, const int32_t* sfirst, const int32_t* sn,
-                    const int64_t* soff, const void* q, double2* pnear, void* scratch, unsigned long long* queue,
-                    int nsm, cudaStream_t s);
-void launch_p2p_reduce(bool fp64, int64_t nleaf, const int32_t* first, const int32_t* n, const int32_t* nin,
-                       const int64_t* base, const void* scratch, double2* pnear, int nsm, cudaStream_t s);
+void launch_p2p_sym(bool fp64, const DevPlan& dp, int64_t nwork, const int32_t* order, const int32_t* item_chunk,
+                    const int32_t* tfirst, const int32_t* tn, const int64_t* ptr, const int32_t* sfirst,
+                    const int32_t* sn, const int64_t* soff, const void* q, double2* tpart, void* scratch,
+                    unsigned long long* queue, int nsm, cudaStream_t s);
+void launch_p2p_reduce(bool fp64, int64_t nleaf, const int32_t* first, const int32_t* n, const int64_t* rptr,
+                       const int64_t* roff, const void* scratch, double2* pnear, int nsm, cudaStream_t s);
 void launch_direct(int64_t ns, const double* spos, const int32_t* sperm, const double2* qin, int64_t nt,
                    const double* tpos, double kappa, double2* out, cudaStream_t s);
 

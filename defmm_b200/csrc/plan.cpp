@@ -578,6 +578,7 @@ void level_slots(const Plan& p, int l, const LevelFlags& F, Slots& s,
 // Symmetric decomposition of the near field (Plan::self_*, sym_*, red_*),
 // for one tree holding both sources and targets.  Source ranges are unions
 // of whole leaves, and a leaf's own range is always present (its self pair).
+// Scratch is chunk-major: a chunk's symmetric ranges take consecutive slots.
 void build_symmetric_near(Plan& p) {
   const Tree& T = p.T;
   const int64_t nch = (int64_t)p.p2p_tfirst.size();
@@ -591,7 +592,8 @@ void build_symmetric_near(Plan& p) {
   p.sym_ptr.assign(1, 0);
   p.sym_sfirst.clear();
   p.sym_sn.clear();
-  std::vector<int32_t> sym_leaf;
+  p.sym_soff.clear();
+  int64_t tot = 0;
   for (int64_t ch = 0; ch < nch; ch++) {
     const int32_t lf = leaf_at[p.p2p_tfirst[ch]];
     const int32_t a0 = T.first[lf], a1 = a0 + T.nprt[lf];
@@ -601,59 +603,99 @@ void build_symmetric_near(Plan& p) {
         p.self_sfirst.push_back(a0);
         p.self_sn.push_back(a1 - a0);
       }
-      for (int32_t j = std::max(s0, a1); j < s1;) {  // source leaves after the own leaf
-        const int32_t sl = leaf_at[j];
-        p.sym_sfirst.push_back(j);
-        p.sym_sn.push_back(T.nprt[sl]);
-        sym_leaf.push_back(sl);
-        j += T.nprt[sl];
+      const int32_t b0 = std::max(s0, a1);
+      if (b0 < s1) {  // source leaves after the own leaf
+        p.sym_sfirst.push_back(b0);
+        p.sym_sn.push_back(s1 - b0);
+        p.sym_soff.push_back(tot);
+        tot += s1 - b0;
       }
     }
     p.self_ptr.push_back((int64_t)p.self_sfirst.size());
     p.sym_ptr.push_back((int64_t)p.sym_sfirst.size());
   }
-  // scratch: per source leaf, one row of its particles per incoming block,
-  // rows in chunk order
-  std::vector<int32_t> nin(T.ncell, 0);
-  for (int32_t sl : sym_leaf) nin[sl]++;
-  std::vector<int64_t> base(T.ncell, 0);
-  int64_t tot = 0;
+  p.sym_scratch = tot;
+  // rows per source leaf, in chunk order
+  std::vector<int64_t> cnt(T.ncell + 1, 0);
+  for (size_t r = 0; r < p.sym_sfirst.size(); r++)
+    for (int32_t j = p.sym_sfirst[r]; j < p.sym_sfirst[r] + p.sym_sn[r]; j += T.nprt[leaf_at[j]]) cnt[leaf_at[j]]++;
+  std::vector<int64_t> lpos(T.ncell, -1);
   p.red_first.clear();
   p.red_n.clear();
-  p.red_nin.clear();
-  p.red_base.clear();
+  p.red_ptr.assign(1, 0);
   for (int64_t c = 0; c < T.ncell; c++)
-    if (nin[c]) {
-      base[c] = tot;
+    if (cnt[c]) {
+      lpos[c] = p.red_ptr.back();
       p.red_first.push_back(T.first[c]);
       p.red_n.push_back(T.nprt[c]);
-      p.red_nin.push_back(nin[c]);
-      p.red_base.push_back(tot);
-      tot += (int64_t)nin[c] * T.nprt[c];
+      p.red_ptr.push_back(p.red_ptr.back() + cnt[c]);
     }
-  p.sym_scratch = tot;
-  std::fill(nin.begin(), nin.end(), 0);
-  p.sym_soff.resize(sym_leaf.size());
-  for (size_t r = 0; r < sym_leaf.size(); r++) {
-    const int32_t sl = sym_leaf[r];
-    p.sym_soff[r] = base[sl] + (int64_t)(nin[sl]++) * T.nprt[sl];
-  }
-  // work orders: a chunk occupies tp = nextpow2(tn) lanes per source
-  std::vector<int64_t> ws(nch, 0), wy(nch, 0);
+  p.red_off.assign(p.red_ptr.back(), 0);
+  for (size_t r = 0; r < p.sym_sfirst.size(); r++)
+    for (int32_t j = p.sym_sfirst[r]; j < p.sym_sfirst[r] + p.sym_sn[r]; j += T.nprt[leaf_at[j]])
+      p.red_off[lpos[leaf_at[j]]++] = p.sym_soff[r] + (j - p.sym_sfirst[r]);
+  // self blocks by decreasing work
+  std::vector<int64_t> ws(nch, 0);
+  for (int64_t ch = 0; ch < nch; ch++)
+    for (int64_t r = p.self_ptr[ch]; r < p.self_ptr[ch + 1]; r++) ws[ch] += p.self_sn[r];
+  p.self_order.clear();
+  for (int64_t ch = 0; ch < nch; ch++)
+    if (ws[ch]) p.self_order.push_back((int32_t)ch);
+  std::stable_sort(p.self_order.begin(), p.self_order.end(), [&](int32_t a, int32_t b) { return ws[a] > ws[b]; });
+}
+
+// Cut every chunk's source ranges (CSR `ptr` over chunks) into items of at
+// most kItemSources sources, in place: ptr becomes a CSR over items, ranges
+// are split at item boundaries (with their scratch slots, if any); `chunk`
+// maps items to chunks, `items` chunks to their consecutive items, and
+// `order` lists items by decreasing work (sources x lanes per source).
+void split_items(const Plan& p, std::vector<int64_t>& ptr, std::vector<int32_t>& sf, std::vector<int32_t>& sn,
+                 std::vector<int64_t>* soff, std::vector<int32_t>& chunk, std::vector<int64_t>& items,
+                 std::vector<int32_t>& order, bool lanes_by_chunk) {
+  constexpr int64_t SP = Plan::kItemSources;
+  const int64_t nch = (int64_t)ptr.size() - 1;
+  std::vector<int64_t> nptr{0};
+  std::vector<int32_t> nsf, nsn;
+  std::vector<int64_t> nso;
+  std::vector<int64_t> work;
+  chunk.clear();
+  items.assign(1, 0);
   for (int64_t ch = 0; ch < nch; ch++) {
-    int tp = 4;
-    while (tp < p.p2p_tn[ch]) tp <<= 1;
-    for (int64_t r = p.self_ptr[ch]; r < p.self_ptr[ch + 1]; r++) ws[ch] += (int64_t)p.self_sn[r] * 32;
-    for (int64_t r = p.sym_ptr[ch]; r < p.sym_ptr[ch + 1]; r++) wy[ch] += (int64_t)p.sym_sn[r] * tp;
+    int tp = 32;
+    if (lanes_by_chunk) {
+      tp = 4;
+      while (tp < p.p2p_tn[ch]) tp <<= 1;
+    }
+    int64_t fill = 0;
+    for (int64_t r = ptr[ch]; r < ptr[ch + 1]; r++)
+      for (int32_t o = 0; o < sn[r];) {
+        const int32_t take = (int32_t)std::min<int64_t>(sn[r] - o, SP - fill);
+        nsf.push_back(sf[r] + o);
+        nsn.push_back(take);
+        if (soff) nso.push_back((*soff)[r] + o);
+        fill += take;
+        o += take;
+        if (fill == SP) {
+          nptr.push_back((int64_t)nsf.size());
+          chunk.push_back((int32_t)ch);
+          work.push_back(fill * tp);
+          fill = 0;
+        }
+      }
+    if (fill) {
+      nptr.push_back((int64_t)nsf.size());
+      chunk.push_back((int32_t)ch);
+      work.push_back(fill * tp);
+    }
+    items.push_back((int64_t)chunk.size());
   }
-  auto order = [&](const std::vector<int64_t>& w, std::vector<int32_t>& o) {
-    o.clear();
-    for (int64_t ch = 0; ch < nch; ch++)
-      if (w[ch]) o.push_back((int32_t)ch);
-    std::stable_sort(o.begin(), o.end(), [&](int32_t a, int32_t b) { return w[a] > w[b]; });
-  };
-  order(ws, p.self_order);
-  order(wy, p.sym_order);
+  ptr.swap(nptr);
+  sf.swap(nsf);
+  sn.swap(nsn);
+  if (soff) soff->swap(nso);
+  order.resize(chunk.size());
+  for (size_t k = 0; k < order.size(); k++) order[k] = (int32_t)k;
+  std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return work[a] > work[b]; });
 }
 
 }  // namespace
@@ -1106,20 +1148,13 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
       }
     }
   }
-  {
-    const int64_t nch = (int64_t)p.p2p_tfirst.size();
-    std::vector<int64_t> work(nch, 0);
-    for (int64_t c = 0; c < nch; c++) {
-      int64_t ns = 0;
-      for (int64_t r = p.p2p_ptr[c]; r < p.p2p_ptr[c + 1]; r++) ns += p.p2p_sn[r];
-      work[c] = ns * 32;  // a chunk occupies its 32-lane groups whatever its size
-    }
-    p.p2p_order.resize(nch);
-    for (int64_t c = 0; c < nch; c++) p.p2p_order[c] = (int32_t)c;
-    std::stable_sort(p.p2p_order.begin(), p.p2p_order.end(),
-                     [&](int32_t a, int32_t b) { return work[a] > work[b]; });
+  if (p.p2p_sym) {
+    build_symmetric_near(p);
+    split_items(p, p.sym_ptr, p.sym_sfirst, p.sym_sn, &p.sym_soff, p.sym_item_chunk, p.sym_chunk_items,
+                p.sym_order, true);
   }
-  if (p.p2p_sym) build_symmetric_near(p);
+  split_items(p, p.p2p_ptr, p.p2p_sfirst, p.p2p_sn, nullptr, p.p2p_item_chunk, p.p2p_chunk_items, p.p2p_order,
+              false);
   p.t_lists = now_s() - t0;
 
   // transfer spectra, FP64 (circulant.hpp:133-144)

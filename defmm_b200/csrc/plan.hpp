@@ -96,11 +96,18 @@ struct Plan {
   std::vector<int32_t> l2l_parent;         // parent slot
   // leaves at precomputed levels (P2M sources / L2P targets)
   std::vector<int32_t> p2m_leaf, l2p_leaf;
-  // near field, grouped by target leaf chunk (<= 32 targets per chunk)
+  // near field, grouped by target leaf chunk (<= 32 targets per chunk); a
+  // chunk's source ranges are cut into work items of at most kItemSources
+  // sources (a coarse leaf next to a large subtree can meet most of the
+  // points), each item yields partial sums for its chunk's targets, added per
+  // chunk in item order
+  static constexpr int kItemSources = 8192;
   std::vector<int32_t> p2p_tfirst, p2p_tn;   // per chunk
-  std::vector<int64_t> p2p_ptr;              // chunks + 1
+  std::vector<int64_t> p2p_ptr;              // items + 1
   std::vector<int32_t> p2p_sfirst, p2p_sn;   // source particle ranges
-  std::vector<int32_t> p2p_order;            // chunks by decreasing work (tn x sources)
+  std::vector<int32_t> p2p_item_chunk;       // per item
+  std::vector<int64_t> p2p_chunk_items;      // chunks + 1 (a chunk's items are consecutive)
+  std::vector<int32_t> p2p_order;            // items by decreasing work
   // Symmetric near field (sources and targets are the same points, so the
   // particle interactions come in mirrored pairs): each chunk keeps its own
   // leaf as a plain block (self_*) and the source leaves after its leaf in
@@ -112,11 +119,15 @@ struct Plan {
   bool p2p_sym = false;
   std::vector<int64_t> self_ptr;             // chunks + 1
   std::vector<int32_t> self_sfirst, self_sn, self_order;
-  std::vector<int64_t> sym_ptr;              // chunks + 1 into sym ranges (one source leaf each)
+  std::vector<int64_t> sym_ptr;              // items + 1 into sym ranges
   std::vector<int32_t> sym_sfirst, sym_sn, sym_order;
   std::vector<int64_t> sym_soff;             // scratch slot of the range's first source
-  std::vector<int32_t> red_first, red_n, red_nin;  // per source leaf with partial sums
-  std::vector<int64_t> red_base;
+  std::vector<int32_t> sym_item_chunk;       // per item
+  std::vector<int64_t> sym_chunk_items;      // chunks + 1
+  // per source leaf receiving partial sums: its particles and the scratch
+  // rows to add (row k covers the leaf's particles at red_off[k] + j)
+  std::vector<int32_t> red_first, red_n;
+  std::vector<int64_t> red_ptr, red_off;     // leaves + 1 into red_off (chunk order)
   int64_t sym_scratch = 0;                   // scratch slots (one complex each)
   // statistics
   int64_t n_far_hf = 0, n_far_lf = 0, n_near = 0, i_near = 0;
