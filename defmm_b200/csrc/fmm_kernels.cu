@@ -1216,25 +1216,63 @@ __global__ void __launch_bounds__(128) k_p2p_sym(DevPlan P, int64_t nwork, const
 
 // Source-side partial sums of the symmetric blocks, per source leaf in a
 // fixed order (Plan::red_*): p_j += sum_k scratch[off_k + (j - first)].
+// One CTA per leaf: 4 groups of 64 threads (one particle each) sum
+// contiguous quarters of the leaf's rows, row offsets staged in shared
+// memory and four rows in flight per thread; the quarters are added in order.
 template <bool MIXED>
-__global__ void k_p2p_reduce(int64_t nleaf, const int32_t* __restrict__ first, const int32_t* __restrict__ n,
-                             const int64_t* __restrict__ rptr, const int64_t* __restrict__ roff,
-                             const void* __restrict__ scratch, double2* __restrict__ pnear) {
+__global__ void __launch_bounds__(256) k_p2p_reduce(int64_t nleaf, const int32_t* __restrict__ first,
+                                                    const int32_t* __restrict__ n, const int64_t* __restrict__ rptr,
+                                                    const int64_t* __restrict__ roff, const void* __restrict__ scratch,
+                                                    double2* __restrict__ pnear) {
   typedef typename std::conditional<MIXED, float2, double2>::type Q;
+  constexpr int RB = 256;  // row offsets staged per round
   const Q* scr = static_cast<const Q*>(scratch);
-  for (int64_t l = blockIdx.x; l < nleaf; l += gridDim.x) {
-    const int nl = n[l];
+  __shared__ int64_t so[RB];
+  __shared__ double2 part[4][64];
+  const int g = threadIdx.x >> 6, jl = threadIdx.x & 63;
+  // (leaf, block of 64 particles): leaves of more than 64 particles take
+  // several passes
+  for (int64_t l = blockIdx.x; l < nleaf; l += gridDim.x)
+  for (int j0 = 0; j0 < n[l]; j0 += 64) {
+    const int nl = n[l], j = j0 + jl;
     const int64_t kb = rptr[l], ke = rptr[l + 1];
-    for (int j = threadIdx.x; j < nl; j += blockDim.x) {
-      double ar = 0., ai = 0.;
-      for (int64_t k = kb; k < ke; k++) {
-        const Q v = scr[roff[k] + j];
-        ar += (double)v.x;
-        ai += (double)v.y;
+    double ar = 0., ai = 0.;
+    __syncthreads();  // the previous pass is done with part[][]
+    for (int64_t k0 = kb; k0 < ke; k0 += RB) {
+      const int nr = (int)min((int64_t)RB, ke - k0);
+      __syncthreads();
+      for (int t = threadIdx.x; t < nr; t += blockDim.x) so[t] = roff[k0 + t];
+      __syncthreads();
+      // group g takes rows [g*nr/4, (g+1)*nr/4) of this round
+      const int r0 = g * nr / 4, r1 = (g + 1) * nr / 4;
+      if (j < nl) {
+        int r = r0;
+        for (; r + 4 <= r1; r += 4) {
+          const Q v0 = scr[so[r] + j], v1 = scr[so[r + 1] + j], v2 = scr[so[r + 2] + j], v3 = scr[so[r + 3] + j];
+          ar += (double)v0.x;
+          ai += (double)v0.y;
+          ar += (double)v1.x;
+          ai += (double)v1.y;
+          ar += (double)v2.x;
+          ai += (double)v2.y;
+          ar += (double)v3.x;
+          ai += (double)v3.y;
+        }
+        for (; r < r1; r++) {
+          const Q v = scr[so[r] + j];
+          ar += (double)v.x;
+          ai += (double)v.y;
+        }
       }
+    }
+    part[g][jl] = make_double2(ar, ai);
+    __syncthreads();
+    if (g == 0 && j < nl) {
       double2 o = pnear[first[l] + j];
-      o.x += ar;
-      o.y += ai;
+      for (int q = 0; q < 4; q++) {
+        o.x += part[q][jl].x;
+        o.y += part[q][jl].y;
+      }
       pnear[first[l] + j] = o;
     }
   }
@@ -1424,9 +1462,9 @@ void launch_p2p_reduce(bool fp64, int64_t nleaf, const int32_t* first, const int
   if (nleaf <= 0) return;
   const int grid = (int)std::min<int64_t>(nleaf, (int64_t)nsm * 16);
   if (fp64)
-    k_p2p_reduce<false><<<grid, 64, 0, s>>>(nleaf, first, n, rptr, roff, scratch, pnear);
+    k_p2p_reduce<false><<<grid, 256, 0, s>>>(nleaf, first, n, rptr, roff, scratch, pnear);
   else
-    k_p2p_reduce<true><<<grid, 64, 0, s>>>(nleaf, first, n, rptr, roff, scratch, pnear);
+    k_p2p_reduce<true><<<grid, 256, 0, s>>>(nleaf, first, n, rptr, roff, scratch, pnear);
 }
 
 void launch_direct(int64_t ns, const double* spos, const int32_t* sperm, const double2* qin, int64_t nt,
