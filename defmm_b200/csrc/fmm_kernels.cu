@@ -70,6 +70,44 @@ __device__ __forceinline__ C expi64(double a) {
   return r;
 }
 
+// exp(i a) for the FP32 path: a = n pi + x reduced in FP64 (n from the low
+// mantissa bits of a / pi + 1.5 * 2^52, exact for |a / pi| < 2^51, any sign),
+// sin/cos of x in FP32 by Taylor polynomials of degree 13/12 on
+// [-pi/2, pi/2] (truncation < 7e-10), (-1)^n applied to both.
+__device__ __forceinline__ float2 expi_reduced(double a) {
+  const double t = fma(a, 0.31830988618379067154, 6755399441055744.0);
+  const double n = t - 6755399441055744.0;
+  const int odd = __double2loint(t) & 1;
+  const float x = (float)fma(-n, 3.14159265358979323846, a);
+  const float xx = x * x;
+  float ps = fmaf(xx, 1.6059043836821613e-10f, -2.5052108385441720e-08f);
+  ps = fmaf(xx, ps, 2.7557319223985893e-06f);
+  ps = fmaf(xx, ps, -1.9841269841269841e-04f);
+  ps = fmaf(xx, ps, 8.3333333333333333e-03f);
+  ps = fmaf(xx, ps, -1.6666666666666667e-01f);
+  ps = fmaf(xx, ps, 1.0f);
+  float pc = fmaf(xx, 2.0876756987868099e-09f, -2.7557319223985891e-07f);
+  pc = fmaf(xx, pc, 2.4801587301587302e-05f);
+  pc = fmaf(xx, pc, -1.3888888888888889e-03f);
+  pc = fmaf(xx, pc, 4.1666666666666667e-02f);
+  pc = fmaf(xx, pc, -0.5f);
+  pc = fmaf(xx, pc, 1.0f);
+  const float sg = odd ? -1.0f : 1.0f;
+  return make_float2(sg * pc, sg * x * ps);
+}
+
+// Plane-wave phase exp(i a) at the precision of the complex type.
+template <typename C>
+__device__ __forceinline__ C expi(double a);
+template <>
+__device__ __forceinline__ double2 expi<double2>(double a) {
+  return expi64<double2>(a);
+}
+template <>
+__device__ __forceinline__ float2 expi<float2>(double a) {
+  return expi_reduced(a);
+}
+
 // ------------------------------------------------------------- gather/scatter
 template <typename T>
 __global__ void k_gather(const double2* __restrict__ qin, const int32_t* __restrict__ perm,
@@ -146,7 +184,7 @@ __global__ void __launch_bounds__(128) k_p2m(DevPlan P, const int32_t* __restric
             const double* dv = dirs + 3 * d;
             double dp = 0.;
             for (int k = 0; k < 3; k++) dp += dv[k] * (y[k] - (&ct.x)[k]);
-            C e = expi64<C>(-P.kappa * dp);
+            C e = expi<C>(-P.kappa * dp);
             w = cmul(w, e);
           }
           wq[warp][p] = w;
@@ -328,7 +366,7 @@ __global__ void __launch_bounds__(128) k_m2m(DevPlan P, int64_t s0, int64_t s1,
       Sep<T, L>::run(mats, v[0] < 0. ? 0 : 1, v[1] < 0. ? 0 : 1, v[2] < 0. ? 0 : 1, sbuf[warp][0],
                      sbuf[warp][1], res, lane);
       if (hf) {
-        const C ph = expi64<C>(-P.kappa * (dv[0] * v[0] + dv[1] * v[1] + dv[2] * v[2]));
+        const C ph = expi<C>(-P.kappa * (dv[0] * v[0] + dv[1] * v[1] + dv[2] * v[2]));
 #pragma unroll
         for (int q = 0; q < NLN; q++)
 #pragma unroll
@@ -429,7 +467,7 @@ __global__ void __launch_bounds__(128) k_l2l(DevPlan P, int64_t s0, int64_t s1,
       Sep<T, L>::run(mats, sg0, sg1, sg2i, sbuf[warp][0], sbuf[warp][1], res, lane);
       if (hf) {
         const double* dv = P.dirs + 3 * (P.dir_off[h] + d);
-        const C ph = expi64<C>(P.kappa * (v[0] * dv[0] + v[1] * dv[1] + v[2] * dv[2]));
+        const C ph = expi<C>(P.kappa * (v[0] * dv[0] + v[1] * dv[1] + v[2] * dv[2]));
 #pragma unroll
         for (int q = 0; q < NLN; q++) {
           const int ln = lane + 32 * q;
@@ -723,11 +761,11 @@ __global__ void __launch_bounds__(128) k_l2p(DevPlan P, const int32_t* __restric
           }
           rfma(sum, B[0][a], sa);
         }
-        double2 v = make_double2((double)sum.x, (double)sum.y);
         if (hf) {
           const double* dv = dirs + 3 * d;
-          v = cmul(v, expi64<double2>(P.kappa * (dv[0] * xr[0] + dv[1] * xr[1] + dv[2] * xr[2])));
+          sum = cmul(sum, expi<C>(P.kappa * (dv[0] * xr[0] + dv[1] * xr[1] + dv[2] * xr[2])));
         }
+        const double2 v = make_double2((double)sum.x, (double)sum.y);
         acc.x += v.x;
         acc.y += v.y;
       }
