@@ -1051,10 +1051,12 @@ __global__ void k_p2p_items(int64_t nchunk, const int32_t* __restrict__ tfirst, 
 // G(x, y) = exp(i k r) / (4 pi r) of one pair (0 for R < 1e-16, P2P.hpp:66),
 // with the arithmetic of p2p_pair<false> (FP64) or p2p_pair_mixed (FP32
 // after the FP64 r and k r reduction).
+// Branch-free: a pair with R < 1e-16 is evaluated at R = 1 and scaled by 0.
 __device__ __forceinline__ double2 green64(double dx, double dy, double dz, double kappa) {
-  const double R = fma(dx, dx, fma(dy, dy, dz * dz));
-  if (R < 1.e-16) return make_double2(0., 0.);
-  const double pi4m1 = 1. / (4. * 3.14159265358979323846);
+  const double R0 = fma(dx, dx, fma(dy, dy, dz * dz));
+  const bool skip = R0 < 1.e-16;
+  const double R = skip ? 1. : R0;
+  const double pi4m1 = skip ? 0. : 1. / (4. * 3.14159265358979323846);
   double y = (double)rsqrtf((float)R);
   const double hR = 0.5 * R;
   y = y * fma(-hR * y, y, 1.5);
@@ -1065,8 +1067,9 @@ __device__ __forceinline__ double2 green64(double dx, double dy, double dz, doub
   return make_double2(cs_ * K, sn_ * K);
 }
 __device__ __forceinline__ float2 green32(double dx, double dy, double dz, double kappa) {
-  const double R = fma(dx, dx, fma(dy, dy, dz * dz));
-  if (R < 1.e-16) return make_float2(0.f, 0.f);
+  const double R0 = fma(dx, dx, fma(dy, dy, dz * dz));
+  const bool skip = R0 < 1.e-16;
+  const double R = skip ? 1. : R0;
   const float Rf = (float)R;
   float y = rsqrtf(Rf);
   y = y * fmaf(-0.5f * Rf * y, y, 1.5f);
@@ -1090,8 +1093,44 @@ __device__ __forceinline__ float2 green32(double dx, double dy, double dz, doubl
   pc = fmaf(xx, pc, 4.1666666666666667e-02f);
   pc = fmaf(xx, pc, -0.5f);
   pc = fmaf(xx, pc, 1.0f);
-  const float K = odd ? -0.0795774715459476679f * y : 0.0795774715459476679f * y;
+  const float K0 = odd ? -0.0795774715459476679f * y : 0.0795774715459476679f * y;
+  const float K = skip ? 0.f : K0;
   return make_float2(pc * K, x * ps * K);
+}
+
+// tp steps of a symmetric block: lane ls owns one source (y, qj) and meets
+// target (ls + step) mod tp; the target's running sum moves one lane down per
+// step.  TP = 32 fixes the segment width at compile time.
+template <bool MIXED, int TP>
+__device__ __forceinline__ void sym_steps(int ls, int tp_rt, double yx, double yy, double yz,
+                                          typename std::conditional<MIXED, float2, double2>::type qj,
+                                          const double* tx, const double* ty, const double* tz,
+                                          const typename std::conditional<MIXED, float2, double2>::type* tq,
+                                          double kappa, typename std::conditional<MIXED, float2, double2>::type& accD,
+                                          typename std::conditional<MIXED, float2, double2>::type& accT) {
+  const int tp = TP ? TP : tp_rt;
+  constexpr int UNR = MIXED ? 4 : 1;
+#pragma unroll UNR
+  for (int st = 0; st < tp; st++) {
+    const int i = (ls + st) & (tp - 1);
+    if constexpr (MIXED) {
+      const float2 g = green32(tx[i] - yx, ty[i] - yy, tz[i] - yz, kappa);
+      const float2 qi = tq[i];
+      accD.x = fmaf(g.x, qj.x, fmaf(-g.y, qj.y, accD.x));
+      accD.y = fmaf(g.x, qj.y, fmaf(g.y, qj.x, accD.y));
+      accT.x = fmaf(g.x, qi.x, fmaf(-g.y, qi.y, accT.x));
+      accT.y = fmaf(g.x, qi.y, fmaf(g.y, qi.x, accT.y));
+    } else {
+      const double2 g = green64(tx[i] - yx, ty[i] - yy, tz[i] - yz, kappa);
+      const double2 qi = tq[i];
+      accD.x = fma(g.x, qj.x, fma(-g.y, qj.y, accD.x));
+      accD.y = fma(g.x, qj.y, fma(g.y, qj.x, accD.y));
+      accT.x = fma(g.x, qi.x, fma(-g.y, qi.y, accT.x));
+      accT.y = fma(g.x, qi.y, fma(g.y, qi.x, accT.y));
+    }
+    accD.x = __shfl_sync(0xffffffffu, accD.x, ls + 1, tp);
+    accD.y = __shfl_sync(0xffffffffu, accD.y, ls + 1, tp);
+  }
 }
 
 // Symmetric blocks of the near field (Plan::sym_*): one CTA (4 warps) per
@@ -1199,28 +1238,12 @@ __global__ void __launch_bounds__(128) k_p2p_sym(DevPlan P, int64_t nwork, const
           qj = q[sj];
         }
         Q accD = Q{0, 0}, accT = Q{0, 0};
-        for (int st = 0; st < tp; st++) {
-          const int i = (ls + st) & (tp - 1);
-          if (vj && i < nt) {
-            if constexpr (MIXED) {
-              const float2 g = green32(tx[i] - yx, ty[i] - yy, tz[i] - yz, P.kappa);
-              const float2 qi = tq[i];
-              accD.x = fmaf(g.x, qj.x, fmaf(-g.y, qj.y, accD.x));
-              accD.y = fmaf(g.x, qj.y, fmaf(g.y, qj.x, accD.y));
-              accT.x = fmaf(g.x, qi.x, fmaf(-g.y, qi.y, accT.x));
-              accT.y = fmaf(g.x, qi.y, fmaf(g.y, qi.x, accT.y));
-            } else {
-              const double2 g = green64(tx[i] - yx, ty[i] - yy, tz[i] - yz, P.kappa);
-              const double2 qi = tq[i];
-              accD.x = fma(g.x, qj.x, fma(-g.y, qj.y, accD.x));
-              accD.y = fma(g.x, qj.y, fma(g.y, qj.x, accD.y));
-              accT.x = fma(g.x, qi.x, fma(-g.y, qi.y, accT.x));
-              accT.y = fma(g.x, qi.y, fma(g.y, qi.x, accT.y));
-            }
-          }
-          accD.x = __shfl_sync(0xffffffffu, accD.x, ls + 1, tp);
-          accD.y = __shfl_sync(0xffffffffu, accD.y, ls + 1, tp);
-        }
+        // no validity tests: padded targets and missing sources carry zero
+        // charges, and their target sums are never stored
+        if (tp == 32)
+          sym_steps<MIXED, 32>(ls, 32, yx, yy, yz, qj, tx, ty, tz, tq, P.kappa, accD, accT);
+        else
+          sym_steps<MIXED, 0>(ls, tp, yx, yy, yz, qj, tx, ty, tz, tq, P.kappa, accD, accT);
         if constexpr (MIXED) {
           kahan_add(sr, cr, accD.x);
           kahan_add(si, ci, accD.y);
