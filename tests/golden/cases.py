@@ -11,6 +11,9 @@ Each case exercises a different part of the reference's method:
 * ``blobs_sphere`` -- distinct sources (Gaussian blobs) and targets (a
   sphere), order 4, leaf size 40.
 * ``sphere_l6`` -- sphere surface, 30,000 points, 16 wavelengths, order 6.
+* ``cube_laplace`` -- cube surface at k = 0: the reference's Laplace kernel
+  1/(4 pi r) (thetis_kernels.hpp:35) through the same method, every level
+  low-frequency.
 """
 from __future__ import annotations
 
@@ -24,7 +27,7 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspa
 
 from defmm_b200 import workloads as W  # noqa: E402
 
-CASES = ["cube20k", "cube_lf", "fixed_depth", "blobs_sphere", "sphere_l6"]
+CASES = ["cube20k", "cube_lf", "fixed_depth", "blobs_sphere", "sphere_l6", "cube_laplace"]
 
 
 def case_inputs(name):
@@ -45,4 +48,7 @@ def case_inputs(name):
     if name == "sphere_l6":
         p = W.sphere_surface(30000, seed=9).points
         return p, p, W.charges(len(p), 5), 6, 64, 2 * math.pi * 8, -1
+    if name == "cube_laplace":
+        p = W.cube_surface(20000, seed=2).points
+        return p, p, W.charges(len(p), 5), 4, 64, 0.0, -1
     raise KeyError(name)

@@ -11,7 +11,7 @@ synthetic cases and stores, per case, compact pins of what it produced:
   checksums (sum, sum of squared moduli, a seeded random projection).
 
 Usage (in the container that has the reference checkout):
-    python tests/golden/gen_golden.py
+    python tests/golden/gen_golden.py [case ...]   # default: every case
 """
 from __future__ import annotations
 
@@ -55,9 +55,9 @@ def sample_index(n, m=500):
     return np.sort(np.random.default_rng(777).choice(n, size=min(m, n), replace=False))
 
 
-def main():
+def main(names):
     from oracle import refrun
-    for name in CASES:
+    for name in names:
         src, trg, q, L, ncrit, kappa, lvmax = case_inputs(name)
         r = refrun.run(src, trg, q, L, ncrit, kappa, lvmax)
         idx = sample_index(trg.shape[0])
@@ -81,4 +81,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:] or CASES)

@@ -46,7 +46,7 @@ def test_fp64_matches_oracle_and_reference_samples(name, gpu):
     assert rel(p[sample_index(trg.shape[0])], sample) <= FP64_TOL
 
 
-@pytest.mark.parametrize("name", ["cube20k", "cube_lf", "blobs_sphere"])
+@pytest.mark.parametrize("name", ["cube20k", "cube_lf", "blobs_sphere", "cube_laplace"])
 def test_mixed_matches_fp64(name, gpu):
     src, trg, q, L, ncrit, kappa, lvmax = case_inputs(name)
     A = make(src, trg, L, ncrit, kappa, lvmax)
@@ -137,3 +137,19 @@ def test_graph_replay_equals_direct_launches(gpu):
     assert np.array_equal(p1, p_direct) and np.array_equal(p2, p_direct)
     A.set_graphs(False)
     assert np.array_equal(p3, A.matvec(q2))
+
+
+def test_laplace_kernel_is_the_zero_wavenumber_operator(gpu):
+    # thetis_kernels.hpp:35: Laplace(R) = 1 / (4 pi R), the Helmholtz kernel
+    # at k = 0; every level is low-frequency.  Against explicit 1/(4 pi r) sums.
+    src, trg, q, L, ncrit, kappa, lvmax = case_inputs("cube_laplace")
+    A = make(src, trg, L, ncrit, kappa, lvmax)
+    assert A.info("cpt") == 0 and A.info("far_hf") == 0
+    p = A.matvec(q)
+    idx = np.sort(np.random.default_rng(1).choice(len(trg), 200, replace=False))
+    d = trg[idx][:, None, :] - src[None, :, :]
+    r2 = (d * d).sum(-1)
+    G = np.where(r2 < 1e-16, 0.0, 1.0 / (4 * np.pi * np.sqrt(np.where(r2 < 1e-16, 1.0, r2))))
+    ex = G @ q
+    assert rel(p[idx], ex) < 2e-3  # order-4 interpolation error
+
