@@ -700,70 +700,12 @@ void split_items(const Plan& p, std::vector<int64_t>& ptr, std::vector<int32_t>&
 
 }  // namespace
 
-int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
-               int64_t nt, int L, int ncrit, double kappa, int lvmax,
-               std::string& err) {
-  if (ns <= 0 || nt <= 0) {
-    err = "empty source or target set";
-    return -1;
-  }
-  if (L < 2 || L > 8) {
-    err = "interpolation order must be in [2, 8]";
-    return -1;
-  }
-  if (lvmax < 0 && ncrit < 1) {
-    err = "leaf size must be positive";
-    return -1;
-  }
-  if (ns >= (int64_t(1) << 31) || nt >= (int64_t(1) << 31)) {
-    err = "too many particles";
-    return -1;
-  }
-  p.L = L;
-  p.P = 2 * L - 1;
-  p.LL = L * L * L;
-  p.PP = p.P * p.P * p.P;
-  p.ncrit = ncrit;
-  p.lvmax = lvmax;
-  p.kappa = kappa;
-  p.p2p_sym = ns == nt && (src == trg || std::memcmp(src, trg, sizeof(double) * 3 * (size_t)ns) == 0);
-  double t0 = now_s();
-  // particles.hpp:79-100 (getBounds): one cube around targets and sources
-  {
-    double mn[3], mx[3];
-    for (int k = 0; k < 3; k++) mn[k] = mx[k] = trg[k];
-    auto upd = [&](const double* x, int64_t n) {
-      for (int64_t i = 0; i < n; i++)
-        for (int k = 0; k < 3; k++) {
-          const double a = x[3 * i + k];
-          mn[k] = mn[k] < a ? mn[k] : a;
-          mx[k] = mx[k] > a ? mx[k] : a;
-        }
-    };
-    upd(trg, nt);
-    upd(src, ns);
-    for (int k = 0; k < 3; k++) p.box_ctr[k] = (mn[k] + mx[k]) / 2.;
-    double a = p.box_ctr[0] - mn[0], b = mx[0] - p.box_ctr[0];
-    for (int k = 1; k < 3; k++) {
-      a = a > p.box_ctr[k] - mn[k] ? a : p.box_ctr[k] - mn[k];
-      b = b > mx[k] - p.box_ctr[k] ? b : mx[k] - p.box_ctr[k];
-    }
-    p.box_rad = std::max(a, b);
-  }
-  int st = build_tree(p.T, trg, nt, p.box_ctr, p.box_rad, ncrit, lvmax, err);
-  if (st) return st;
-  st = build_tree(p.S, src, ns, p.box_ctr, p.box_rad, ncrit, lvmax, err);
-  if (st) return st;
-  p.t_tree = now_s() - t0;
-  t0 = now_s();
-  st = init_levels(p, err);
-  if (st) return st;
-  init_directions(p);
-  init_small_tables(p);
-  init_signatures(p);
+// The level walk on the host (see LevelWalk): frontier pairs level by level
+// in depth-first order, multi-threaded per level.
+int walk_levels_host(Plan& p, LevelWalk& walk) {
   const Levels& v = p.lv;
   const int nlvl = v.nlvl;
-
+  const double kappa = p.kappa;
   // per-level cell lists (DFS order) and level-local indices
   auto level_lists = [&](const Tree& tr, std::vector<std::vector<int64_t>>& lists,
                          std::vector<int32_t>& loc) {
@@ -787,16 +729,16 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
   p.sS.cone_begin.assign(nlvl, {});
 
   // M2L entries per level before grouping by target slot
-  struct FarLevel {
-    std::vector<int32_t> ts, ss;
-    std::vector<uint32_t> tab;
-  };
-  std::vector<FarLevel> far(nlvl);
-  std::vector<std::pair<int32_t, int32_t>> near_pairs;
+  walk.far_ts.assign(nlvl, {});
+  walk.far_ss.assign(nlvl, {});
+  walk.far_tab.assign(nlvl, {});
+  auto& near_pairs = walk.near_pairs;
+  auto& tab_nI = walk.tab_nI;
+  near_pairs.clear();
+  tab_nI.clear();
   std::vector<int32_t> denseT, denseS, denseT_prev, denseS_prev;
   LevelFlags fT_prev, fS_prev;
   int64_t table_count = 0;
-  std::vector<std::array<int32_t, 3>> tab_nI;
 
   // frontier of the dual traversal (hrzpass.hpp:62-91), kept in the
   // reference's depth-first order
@@ -947,17 +889,19 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
           const int M = v.nCellMax[l];
           p.tab_iz.push_back(((int64_t)a * M + b) * M + c);
         }
-      FarLevel& fl = far[l];
-      fl.ts.resize(nf);
-      fl.ss.resize(nf);
-      fl.tab.resize(nf);
+      auto& fts = walk.far_ts[l];
+      auto& fss = walk.far_ss[l];
+      auto& ftab = walk.far_tab[l];
+      fts.resize(nf);
+      fss.resize(nf);
+      ftab.resize(nf);
       pfor(nf, 4096, [&](int64_t i) {
         const int64_t lt = locT[fpairs[i].first], ls = locS[fpairs[i].second];
         const int32_t ts = hf ? denseT[lt * nd + cone[i]] : denseT[lt];
         const int32_t ss = hf ? denseS[ls * nd + cone[i]] : denseS[ls];
-        fl.ts[i] = ts;
-        fl.ss[i] = ss;
-        fl.tab[i] = ((uint32_t)tid[fi[i]] << 6) | hs[i];
+        fts[i] = ts;
+        fss[i] = ss;
+        ftab[i] = ((uint32_t)tid[fi[i]] << 6) | hs[i];
       });
       if (p.keep_lists) {
         for (int64_t i = 0; i < nf; i++) {
@@ -988,6 +932,78 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
   }
   p.sT.lvl_begin[nlvl] = p.sT.n;
   p.sS.lvl_begin[nlvl] = p.sS.n;
+  return 0;
+}
+
+int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
+               int64_t nt, int L, int ncrit, double kappa, int lvmax,
+               std::string& err, LevelWalker* walker) {
+  if (ns <= 0 || nt <= 0) {
+    err = "empty source or target set";
+    return -1;
+  }
+  if (L < 2 || L > 8) {
+    err = "interpolation order must be in [2, 8]";
+    return -1;
+  }
+  if (lvmax < 0 && ncrit < 1) {
+    err = "leaf size must be positive";
+    return -1;
+  }
+  if (ns >= (int64_t(1) << 31) || nt >= (int64_t(1) << 31)) {
+    err = "too many particles";
+    return -1;
+  }
+  p.L = L;
+  p.P = 2 * L - 1;
+  p.LL = L * L * L;
+  p.PP = p.P * p.P * p.P;
+  p.ncrit = ncrit;
+  p.lvmax = lvmax;
+  p.kappa = kappa;
+  p.p2p_sym = ns == nt && (src == trg || std::memcmp(src, trg, sizeof(double) * 3 * (size_t)ns) == 0);
+  double t0 = now_s();
+  // particles.hpp:79-100 (getBounds): one cube around targets and sources
+  {
+    double mn[3], mx[3];
+    for (int k = 0; k < 3; k++) mn[k] = mx[k] = trg[k];
+    auto upd = [&](const double* x, int64_t n) {
+      for (int64_t i = 0; i < n; i++)
+        for (int k = 0; k < 3; k++) {
+          const double a = x[3 * i + k];
+          mn[k] = mn[k] < a ? mn[k] : a;
+          mx[k] = mx[k] > a ? mx[k] : a;
+        }
+    };
+    upd(trg, nt);
+    upd(src, ns);
+    for (int k = 0; k < 3; k++) p.box_ctr[k] = (mn[k] + mx[k]) / 2.;
+    double a = p.box_ctr[0] - mn[0], b = mx[0] - p.box_ctr[0];
+    for (int k = 1; k < 3; k++) {
+      a = a > p.box_ctr[k] - mn[k] ? a : p.box_ctr[k] - mn[k];
+      b = b > mx[k] - p.box_ctr[k] ? b : mx[k] - p.box_ctr[k];
+    }
+    p.box_rad = std::max(a, b);
+  }
+  int st = build_tree(p.T, trg, nt, p.box_ctr, p.box_rad, ncrit, lvmax, err);
+  if (st) return st;
+  st = build_tree(p.S, src, ns, p.box_ctr, p.box_rad, ncrit, lvmax, err);
+  if (st) return st;
+  p.t_tree = now_s() - t0;
+  t0 = now_s();
+  st = init_levels(p, err);
+  if (st) return st;
+  init_directions(p);
+  init_small_tables(p);
+  init_signatures(p);
+  const Levels& v = p.lv;
+  const int nlvl = v.nlvl;
+
+  LevelWalk w;
+  st = (walker && !p.keep_lists) ? walker->walk(p, w, err) : walk_levels_host(p, w);
+  if (st) return st;
+  auto& near_pairs = w.near_pairs;
+  auto& tab_nI = w.tab_nI;
 
   // per-cell direction/slot CSR for both trees
   auto cell_csr = [&](const Tree& tr, Slots& s) {
@@ -1012,22 +1028,21 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
   {
     p.m2l_ptr.assign(p.sT.n + 1, 0);
     for (int l = 0; l < nlvl; l++)
-      for (int32_t ts : far[l].ts) p.m2l_ptr[ts + 1]++;
+      for (int32_t ts : w.far_ts[l]) p.m2l_ptr[ts + 1]++;
     for (int64_t k = 0; k < p.sT.n; k++) p.m2l_ptr[k + 1] += p.m2l_ptr[k];
     const int64_t tot = p.m2l_ptr[p.sT.n];
     p.m2l_src.resize(tot);
     p.m2l_tab.resize(tot);
     std::vector<int64_t> pos(p.m2l_ptr.begin(), p.m2l_ptr.end() - 1);
     for (int l = 0; l < nlvl; l++) {
-      FarLevel& fl = far[l];
-      for (size_t i = 0; i < fl.ts.size(); i++) {
-        const int64_t q = pos[fl.ts[i]]++;
-        p.m2l_src[q] = fl.ss[i];
-        p.m2l_tab[q] = fl.tab[i];
+      for (size_t i = 0; i < w.far_ts[l].size(); i++) {
+        const int64_t q = pos[w.far_ts[l][i]]++;
+        p.m2l_src[q] = w.far_ss[l][i];
+        p.m2l_tab[q] = w.far_tab[l][i];
       }
-      FarLevel().ts.swap(fl.ts);
-      std::vector<int32_t>().swap(fl.ss);
-      std::vector<uint32_t>().swap(fl.tab);
+      std::vector<int32_t>().swap(w.far_ts[l]);
+      std::vector<int32_t>().swap(w.far_ss[l]);
+      std::vector<uint32_t>().swap(w.far_tab[l]);
     }
   }
 

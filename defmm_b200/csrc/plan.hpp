@@ -8,9 +8,11 @@
 // is level-wise and multi-threaded instead of the reference's recursions.
 #pragma once
 
+#include <array>
 #include <complex>
 #include <cstdint>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace dfb {
@@ -138,13 +140,33 @@ struct Plan {
   double t_tree = 0, t_lists = 0, t_tables = 0;
 };
 
-// Build the plan; returns 0 or a negative status with `err` set.
+// Result of the level-by-level dual traversal (hrzpass.hpp:62-143 with the
+// blank passes, dwnpass.hpp:81-109): besides what it fills in the plan (slots
+// sS/sT without their per-cell CSR, tab_lvl/tab_iz, far counts, list
+// records), the far entries of every level and the near pairs, both in the
+// reference's depth-first order.
+struct LevelWalk {
+  std::vector<std::pair<int32_t, int32_t>> near_pairs;
+  std::vector<std::array<int32_t, 3>> tab_nI;  // fundamental index per table
+  std::vector<std::vector<int32_t>> far_ts, far_ss;  // per level: slots
+  std::vector<std::vector<uint32_t>> far_tab;        // per level: (table << 6) | hash
+};
+
+// Another implementation of the level walk (the device one); it must produce
+// exactly the host walk's results.  Returns 0 or a negative status.
+struct LevelWalker {
+  virtual ~LevelWalker() = default;
+  virtual int walk(Plan& p, LevelWalk& w, std::string& err) = 0;
+};
+
+// Build the plan; returns 0 or a negative status with `err` set.  With a
+// walker (and no list records requested) the level walk runs there.
 //   -2: coincident points keep a cell above ncrit (the reference recurses
 //       without end, sort.hpp:98-162)
 //   -3: the tree is too shallow for any M2L level (frequency.hpp:114-120)
 //   -1: invalid arguments
 int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
                int64_t nt, int L, int ncrit, double kappa, int lvmax,
-               std::string& err);
+               std::string& err, LevelWalker* walker = nullptr);
 
 }  // namespace dfb
