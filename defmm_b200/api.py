@@ -34,7 +34,7 @@ _INFO = {
     "n_sources": 0, "n_targets": 1, "nlvl": 2, "cpt": 3, "max_stage": 4, "cells_T": 5,
     "cells_S": 6, "slots_S": 7, "slots_T": 8, "far_hf": 9, "far_lf": 10, "near": 11,
     "i_near": 12, "tables": 13, "device_bytes": 14, "list_records": 15, "launches": 16,
-    "m2l_targets": 17, "leaf_slots_S": 18, "permuted_spectra": 19,
+    "m2l_targets": 17, "leaf_slots_S": 18, "permuted_spectra": 19, "plan_walk_device": 20, "plan_ms": 21,
 }
 PHASES = ["p2m", "m2m", "m2f", "m2l", "f2l", "l2l", "l2p", "p2p", "scatter", "total"]
 
@@ -76,6 +76,7 @@ def lib():
             "defmm_set_profiling": (ctypes.c_int, [vp, ctypes.c_int]),
             "defmm_set_graphs": (ctypes.c_int, [vp, ctypes.c_int]),
             "defmm_keep_lists": (ctypes.c_int, [vp, ctypes.c_int]),
+            "defmm_set_plan_device": (ctypes.c_int, [vp, ctypes.c_int]),
             "defmm_dump_tree": (ctypes.c_int, [vp, ctypes.c_int, ip, dp, ip, ctypes.POINTER(i64), ip]),
             "defmm_dump_lists": (ctypes.c_int, [vp, ip, ip, ip, ctypes.POINTER(i64)]),
         }
@@ -151,6 +152,10 @@ class IBFMM_Mat:
         if isinstance(mode, str):
             mode = {"fp64": PRECISION_FP64, "mixed": PRECISION_MIXED}[mode]
         self._check(lib().defmm_set_precision(self._h, int(mode)))
+
+    def set_plan_device(self, on=True):
+        """Run prcmpt's level walk on the GPU (default) or on the host."""
+        self._check(lib().defmm_set_plan_device(self._h, int(bool(on))))
 
     def set_profiling(self, on=True):
         self._check(lib().defmm_set_profiling(self._h, int(bool(on))))

@@ -16,9 +16,12 @@ LIB = os.path.join(HERE, "libdefmm_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU = ["fmm_kernels.cu", "engine.cu", "noalloc.cu"]
+CU = ["fmm_kernels.cu", "engine.cu", "noalloc.cu", "plan_device.cu"]
+# the device level walk reproduces the host plan's floating-point decisions:
+# no FMA contraction there
+CU_FLAGS = {"plan_device.cu": ["--fmad=false"]}
 CPP = ["plan.cpp"]
-HEADERS = ["plan.hpp", "kernels.cuh", "fmm_kernels.h", "engine_internal.h"]
+HEADERS = ["plan.hpp", "kernels.cuh", "fmm_kernels.h", "engine_internal.h", "plan_device.hpp"]
 
 
 def _newer(target, deps):
@@ -40,7 +43,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
         objs.append(obj)
         if force or _newer(obj, [src] + hdrs):
             jobs.append([NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
-                         "-Xptxas", "-v" if verbose else "-O3", "-c", src, "-o", obj])
+                         *CU_FLAGS.get(f, []), "-Xptxas", "-v" if verbose else "-O3", "-c", src, "-o", obj])
     for f in CPP:
         src = os.path.join(CSRC, f)
         obj = os.path.join(BUILD, f + ".o")

@@ -11,6 +11,7 @@
 #include "engine_internal.h"
 #include "fmm_kernels.h"
 #include "plan.hpp"
+#include "plan_device.hpp"
 
 using dfb::DevPlan;
 using dfb::Plan;
@@ -32,6 +33,8 @@ struct defmm_handle {
   bool built = false;
   bool uploaded = false;
   bool keep_lists = false;
+  bool plan_device = true;   // run the plan's level walk on the GPU when one is present
+  bool walked_on_device = false;
   int precision = DEFMM_PRECISION_FP64;
   std::string err;
   // device state
@@ -679,6 +682,12 @@ int defmm_set_profiling(defmm_handle* h, int on) {
   return 0;
 }
 
+int defmm_set_plan_device(defmm_handle* h, int on) {
+  if (!h) return DEFMM_ERR_ARG;
+  h->plan_device = on != 0;
+  return 0;
+}
+
 int defmm_keep_lists(defmm_handle* h, int on) {
   if (!h) return DEFMM_ERR_ARG;
   h->keep_lists = on != 0;
@@ -698,9 +707,22 @@ int defmm_prcmpt(defmm_handle* h, int L, int Ncrit, double kappa, int lvMAX) {
   h->plan = Plan();
   h->plan.keep_lists = h->keep_lists;
   std::string e;
+  // the level walk on the GPU when there is one (list records for parity
+  // checks come from the host walk)
+  dfb::LevelWalker* walker = nullptr;
+  h->walked_on_device = false;
+  if (h->plan_device && !h->keep_lists) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) == cudaSuccess && n > 0 && ensure_device(h) == 0 &&
+        cudaSetDevice(h->device) == cudaSuccess)
+      walker = dfb::device_level_walker();
+    cudaGetLastError();
+    h->err.clear();
+  }
   int st = dfb::build_plan(h->plan, h->src.data(), (int64_t)h->src.size() / 3, h->trg.data(),
-                           (int64_t)h->trg.size() / 3, L, Ncrit, kappa, lvMAX, e);
-  if (st) return h->fail(st, e);
+                           (int64_t)h->trg.size() / 3, L, Ncrit, kappa, lvMAX, e, walker);
+  if (st) return h->fail(st == -4 ? DEFMM_ERR_CUDA : st == -5 ? DEFMM_ERR_MEMORY : st, e);
+  h->walked_on_device = walker != nullptr;
   if (h->plan.lv.nlvl > 32) return h->fail(DEFMM_ERR_DEPTH, "more than 32 tree levels");
   h->built = true;
   return 0;
@@ -846,6 +868,8 @@ int defmm_info(const defmm_handle* h, int what, int64_t* v) {
     case DEFMM_INFO_LIST_RECORDS: *v = p.keep_lists ? 1 : 0; break;
     case DEFMM_INFO_LAUNCHES: *v = h->launches; break;
     case DEFMM_INFO_PERMUTED_SPECTRA: *v = (int64_t)p.ptab_key.size(); break;
+    case DEFMM_INFO_PLAN_WALK_DEVICE: *v = h->walked_on_device ? 1 : 0; break;
+    case DEFMM_INFO_PLAN_MS: *v = (int64_t)(1e3 * (p.t_tree + p.t_lists + p.t_tables)); break;
     case DEFMM_INFO_M2L_TARGETS: {
       int64_t n = 0;
       for (int64_t k = 0; k < p.sT.n; k++) n += p.m2l_ptr[k + 1] > p.m2l_ptr[k] ? 1 : 0;

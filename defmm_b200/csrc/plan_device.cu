@@ -1,0 +1,600 @@
+// The level walk of the plan (LevelWalk: dual traversal, cones, effective
+// directions, slots, far entries) on the GPU, level by level.  Same results
+// as the host walk in plan.cpp, bit for bit: every floating-point decision
+// (admissibility hrzpass.hpp:52-56, the cone of a translation
+// newdirections.hpp:175-185) uses the host's IEEE operations in the host's
+// order with explicit round-to-nearest intrinsics (no contraction), every
+// list keeps the reference's depth-first order (stable compaction by prefix
+// sums), and the cone of a translation comes from its first pair in that
+// order (M2L.hpp:189-197).
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cstring>
+
+#include "plan.hpp"
+#include "plan_device.hpp"
+
+namespace dfb {
+namespace {
+
+__constant__ int8_t c_axis_order[8][3] = {{0, 1, 2}, {1, 0, 2}, {0, 1, 2}, {1, 2, 0},
+                                          {0, 2, 1}, {0, 1, 2}, {2, 0, 1}, {2, 1, 0}};
+
+struct DTree {
+  const int32_t* idx;  // 3 per cell
+  const double* ctr;   // 3 per cell
+  const double* rad;
+  const int64_t* son_ptr;
+  const int32_t* sons;
+  const int32_t* parent;
+  const int32_t* loc;  // level-local index
+};
+
+// sqrt((0 + x x) + y y) + z z), as the host's norm3 without contraction
+__device__ __forceinline__ double dnorm3(double x, double y, double z) {
+  double t = __dadd_rn(0.0, __dmul_rn(x, x));
+  t = __dadd_rn(t, __dmul_rn(y, y));
+  t = __dadd_rn(t, __dmul_rn(z, z));
+  return __dsqrt_rn(t);
+}
+
+// 0 far, 1 near, 2 split (with the children count)
+__global__ void k_classify(int64_t nf, const int2* __restrict__ F, DTree T, DTree S, int prec, int hf, double kappa,
+                           int32_t* __restrict__ isfar, int32_t* __restrict__ isnear, int64_t* __restrict__ nch) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= nf) return;
+  const int t = F[i].x, s = F[i].y;
+  bool far = false;
+  if (prec) {
+    if (hf) {  // MACgeomhf
+      const double dx = __dsub_rn(T.ctr[3 * t], S.ctr[3 * s]), dy = __dsub_rn(T.ctr[3 * t + 1], S.ctr[3 * s + 1]),
+                   dz = __dsub_rn(T.ctr[3 * t + 2], S.ctr[3 * s + 2]);
+      const double tt = __dmul_rn(2., S.rad[s]);
+      const double tmp = __dmul_rn(1. - 1.e-8, __dsub_rn(dnorm3(dx, dy, dz), tt));
+      const double a = __dmul_rn(__dmul_rn(tt, tt), kappa);
+      const double mx = (a < tt) ? tt : a;
+      far = tmp >= mx;
+    } else {  // MAClist
+      int test = 0, ncmp = 3;
+      for (int k = 0; k < 3; k++) {
+        const int d = T.idx[3 * t + k] - S.idx[3 * s + k];
+        ncmp -= d ? 0 : 1;
+        test += d < 0 ? -d : d;
+      }
+      far = test > ncmp;
+    }
+  }
+  const int64_t nt = T.son_ptr[t + 1] - T.son_ptr[t], ns = S.son_ptr[s + 1] - S.son_ptr[s];
+  const bool near = !far && (nt == 0 || ns == 0);
+  isfar[i] = far ? 1 : 0;
+  isnear[i] = near ? 1 : 0;
+  nch[i] = (!far && !near) ? nt * ns : 0;
+}
+
+__global__ void k_scatter(int64_t nf, const int2* __restrict__ F, DTree T, DTree S, const int32_t* __restrict__ isfar,
+                          const int32_t* __restrict__ pfar, const int32_t* __restrict__ isnear,
+                          const int32_t* __restrict__ pnear, const int64_t* __restrict__ nch,
+                          const int64_t* __restrict__ pch, int2* __restrict__ far_out, int2* __restrict__ near_out,
+                          int2* __restrict__ next) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= nf) return;
+  const int2 pr = F[i];
+  if (isfar[i]) {
+    far_out[pfar[i]] = pr;
+  } else if (isnear[i]) {
+    near_out[pnear[i]] = pr;
+  } else if (nch[i]) {
+    const int64_t ta = T.son_ptr[pr.x], tb = T.son_ptr[pr.x + 1], sa = S.son_ptr[pr.y], sb = S.son_ptr[pr.y + 1];
+    int64_t o = pch[i];
+    for (int64_t a = ta; a < tb; a++)
+      for (int64_t b = sa; b < sb; b++) next[o++] = make_int2(T.sons[a], S.sons[b]);
+  }
+}
+
+__device__ __forceinline__ void diz(const DTree& T, const DTree& S, int2 pr, int* iZ) {
+  for (int k = 0; k < 3; k++) iZ[k] = T.idx[3 * pr.x + k] - S.idx[3 * pr.y + k];
+}
+
+__global__ void k_maxdiff(int64_t nf, const int2* __restrict__ P, DTree T, DTree S, int* __restrict__ m) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int v = 0;
+  if (i < nf) {
+    int iZ[3];
+    diz(T, S, P[i], iZ);
+    for (int k = 0; k < 3; k++) v = max(v, iZ[k] < 0 ? -iZ[k] : iZ[k]);
+  }
+  for (int o = 16; o; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0 && v) atomicMax(m, v);
+}
+
+__device__ __forceinline__ int64_t zkey(const DTree& T, const DTree& S, int2 pr, int m) {
+  int iZ[3];
+  diz(T, S, pr, iZ);
+  const int64_t w = 2 * m + 1;
+  return ((int64_t)(iZ[0] + m) * w + (iZ[1] + m)) * w + (iZ[2] + m);
+}
+
+__global__ void k_firstpos(int64_t nf, const int2* __restrict__ P, DTree T, DTree S, int m,
+                           unsigned long long* __restrict__ first) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= nf) return;
+  atomicMin(first + zkey(T, S, P[i], m), (unsigned long long)i);
+}
+
+// the cone of each translation: direction nearest to the normalised centre
+// difference of its first pair, lowest index on ties (one block per key)
+__global__ void k_cones(int64_t nkeys, const unsigned long long* __restrict__ first, const int2* __restrict__ P,
+                        DTree T, DTree S, const double* __restrict__ dirs, int nd, int16_t* __restrict__ key_cone) {
+  __shared__ double bd[256];
+  __shared__ int bi[256];
+  for (int64_t k = blockIdx.x; k < nkeys; k += gridDim.x) {
+    const unsigned long long f = first[k];
+    if (f == ~0ULL) continue;  // uniform over the block
+    const int2 pr = P[f];
+    double u[3];
+    for (int q = 0; q < 3; q++) u[q] = __dsub_rn(T.ctr[3 * pr.x + q], S.ctr[3 * pr.y + q]);
+    const double n = dnorm3(u[0], u[1], u[2]);
+    for (int q = 0; q < 3; q++) u[q] = __ddiv_rn(u[q], n);
+    double best = 1.e30;
+    int ind = -1;
+    for (int i = threadIdx.x; i < nd; i += blockDim.x) {  // increasing i: strict < keeps the lowest
+      const double d = dnorm3(__dsub_rn(dirs[3 * i], u[0]), __dsub_rn(dirs[3 * i + 1], u[1]),
+                              __dsub_rn(dirs[3 * i + 2], u[2]));
+      if (d < best) {
+        best = d;
+        ind = i;
+      }
+    }
+    bd[threadIdx.x] = best;
+    bi[threadIdx.x] = ind;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o; o >>= 1) {
+      if ((int)threadIdx.x < o) {
+        const double d2 = bd[threadIdx.x + o];
+        const int i2 = bi[threadIdx.x + o];
+        if (i2 >= 0 && (d2 < bd[threadIdx.x] || (d2 == bd[threadIdx.x] && (bi[threadIdx.x] < 0 || i2 < bi[threadIdx.x])))) {
+          bd[threadIdx.x] = d2;
+          bi[threadIdx.x] = i2;
+        }
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) key_cone[k] = (int16_t)bi[0];
+    __syncthreads();
+  }
+}
+
+__global__ void k_cone_of(int64_t nf, const int2* __restrict__ P, DTree T, DTree S, int m,
+                          const int16_t* __restrict__ key_cone, int16_t* __restrict__ cone) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= nf) return;
+  cone[i] = key_cone[zkey(T, S, P[i], m)];
+}
+
+__global__ void k_flags(int64_t nf, const int2* __restrict__ P, DTree T, DTree S, const int16_t* __restrict__ cone,
+                        int nd, uint8_t* __restrict__ effT, uint8_t* __restrict__ effS) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= nf) return;
+  const int c = cone[i];
+  effT[(int64_t)T.loc[P[i].x] * nd + c] = 1;
+  effS[(int64_t)S.loc[P[i].y] * nd + c] = 1;
+}
+
+// child flag dt set when any of the parent's 4 dt..4 dt + 3 is (dwnpass.hpp:81-109)
+__global__ void k_propagate(int64_t nc, const int32_t* __restrict__ cells, DTree Tr, int nd, int pnd,
+                            const uint8_t* __restrict__ prev, uint8_t* __restrict__ eff) {
+  const int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (w >= nc * nd) return;
+  const int64_t i = w / nd;
+  const int dt = (int)(w % nd);
+  const int par = Tr.parent[cells[i]];
+  const uint8_t* pe = prev + (int64_t)Tr.loc[par] * pnd + 4 * dt;
+  if (pe[0] | pe[1] | pe[2] | pe[3]) eff[w] = 1;
+}
+
+// d-major copy of the flags for the cone-major slot numbering
+__global__ void k_transpose(int64_t nc, int nd, const uint8_t* __restrict__ eff, int32_t* __restrict__ fl) {
+  const int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (w >= nc * nd) return;
+  const int64_t d = w / nc, c = w % nc;
+  fl[w] = eff[c * nd + d];
+}
+
+__global__ void k_slots_hf(int64_t nc, int nd, const uint8_t* __restrict__ eff, const int32_t* __restrict__ pos,
+                           const int32_t* __restrict__ cells, int64_t base, int32_t* __restrict__ dense,
+                           int32_t* __restrict__ scell, int32_t* __restrict__ sdir) {
+  const int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (w >= nc * nd) return;
+  const int64_t c = w / nd;
+  const int d = (int)(w % nd);
+  if (!eff[w]) {
+    dense[w] = -1;
+    return;
+  }
+  const int64_t r = pos[(int64_t)d * nc + c];
+  dense[w] = (int32_t)(base + r);
+  scell[r] = cells[c];
+  sdir[r] = d;
+}
+
+__global__ void k_tabflags(int64_t nf, const int2* __restrict__ P, DTree T, DTree S, int m, int32_t* __restrict__ used) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= nf) return;
+  int iZ[3];
+  diz(T, S, P[i], iZ);
+  const int a0 = abs(iZ[0]), a1 = abs(iZ[1]), a2 = abs(iZ[2]);
+  const int h1 = (a0 < a1 ? 1 : 0) | (a0 < a2 ? 2 : 0) | (a1 < a2 ? 4 : 0);
+  int nI[3];
+  for (int k = 0; k < 3; k++) nI[k] = abs(iZ[c_axis_order[h1][k]]);
+  used[((int64_t)nI[0] * (m + 1) + nI[1]) * (m + 1) + nI[2]] = 1;
+}
+
+__global__ void k_entries(int64_t nf, const int2* __restrict__ P, DTree T, DTree S, int m, int hf, int nd,
+                          const int16_t* __restrict__ cone, const int32_t* __restrict__ denseT,
+                          const int32_t* __restrict__ denseS, const int32_t* __restrict__ tidpos, int64_t tbase,
+                          int32_t* __restrict__ ts, int32_t* __restrict__ ss, uint32_t* __restrict__ tab) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= nf) return;
+  const int2 pr = P[i];
+  int iZ[3];
+  diz(T, S, pr, iZ);
+  const int a0 = abs(iZ[0]), a1 = abs(iZ[1]), a2 = abs(iZ[2]);
+  const int h1 = (a0 < a1 ? 1 : 0) | (a0 < a2 ? 2 : 0) | (a1 < a2 ? 4 : 0);
+  const int h0 = (iZ[0] < 0 ? 1 : 0) | (iZ[1] < 0 ? 2 : 0) | (iZ[2] < 0 ? 4 : 0);
+  int nI[3];
+  for (int k = 0; k < 3; k++) nI[k] = abs(iZ[c_axis_order[h1][k]]);
+  const int64_t fi = ((int64_t)nI[0] * (m + 1) + nI[1]) * (m + 1) + nI[2];
+  const int64_t lt = T.loc[pr.x], ls = S.loc[pr.y];
+  ts[i] = hf ? denseT[lt * nd + cone[i]] : denseT[lt];
+  ss[i] = hf ? denseS[ls * nd + cone[i]] : denseS[ls];
+  tab[i] = ((uint32_t)(tbase + tidpos[fi]) << 6) | (uint32_t)(h0 + (h1 << 3));
+}
+
+inline unsigned nblk(int64_t n, int b = 256) { return (unsigned)std::max<int64_t>(1, (n + b - 1) / b); }
+
+// Device buffers of one walk; everything is freed at the end.
+struct Arena {
+  std::vector<void*> all;
+  ~Arena() {
+    for (void* p : all) cudaFree(p);
+  }
+  template <typename T>
+  T* get(size_t n) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, std::max<size_t>(1, n) * sizeof(T)) != cudaSuccess) return nullptr;
+    all.push_back(p);
+    return static_cast<T*>(p);
+  }
+  void drop(void* p) {
+    auto it = std::find(all.begin(), all.end(), p);
+    if (it != all.end()) {
+      cudaFree(p);
+      all.erase(it);
+    }
+  }
+};
+
+struct DeviceWalker final : LevelWalker {
+  int walk(Plan& p, LevelWalk& w, std::string& err) override;
+};
+
+#define DW_CK(call)                                                          \
+  do {                                                                       \
+    cudaError_t e_ = (call);                                                 \
+    if (e_ != cudaSuccess) {                                                 \
+      err = std::string("device plan: ") + #call + ": " + cudaGetErrorString(e_); \
+      return -4;                                                             \
+    }                                                                        \
+  } while (0)
+#define DW_ALLOC(ptr, T, n)                                      \
+  do {                                                           \
+    ptr = A.get<T>(n);                                           \
+    if (!ptr) {                                                  \
+      cudaGetLastError();                                        \
+      err = "device plan: out of device memory";                 \
+      return -5;                                                 \
+    }                                                            \
+  } while (0)
+
+template <typename T>
+int upload_vec(Arena& A, const std::vector<T>& v, const T** out, std::string& err) {
+  T* p = nullptr;
+  DW_ALLOC(p, T, v.size());
+  if (!v.empty()) DW_CK(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  *out = p;
+  return 0;
+}
+
+int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
+  const Levels& v = p.lv;
+  const int nlvl = v.nlvl;
+  Arena A;
+  // cells per level (DFS order) and level-local indices, as the host walk
+  std::vector<std::vector<int32_t>> lcT(nlvl), lcS(nlvl);
+  std::vector<int32_t> locT(p.T.ncell), locS(p.S.ncell);
+  for (int64_t c = 0; c < p.T.ncell; c++) {
+    locT[c] = (int32_t)lcT[p.T.lvl[c]].size();
+    lcT[p.T.lvl[c]].push_back((int32_t)c);
+  }
+  for (int64_t c = 0; c < p.S.ncell; c++) {
+    locS[c] = (int32_t)lcS[p.S.lvl[c]].size();
+    lcS[p.S.lvl[c]].push_back((int32_t)c);
+  }
+  auto dtree = [&](const Tree& tr, const std::vector<int32_t>& loc, DTree& d) -> int {
+    int st;
+    if ((st = upload_vec(A, tr.idx, &d.idx, err)) || (st = upload_vec(A, tr.ctr, &d.ctr, err)) ||
+        (st = upload_vec(A, tr.rad, &d.rad, err)) || (st = upload_vec(A, tr.son_ptr, &d.son_ptr, err)) ||
+        (st = upload_vec(A, tr.sons, &d.sons, err)) || (st = upload_vec(A, tr.parent, &d.parent, err)) ||
+        (st = upload_vec(A, loc, &d.loc, err)))
+      return st;
+    return 0;
+  };
+  DTree T{}, S{};
+  int st;
+  if ((st = dtree(p.T, locT, T)) || (st = dtree(p.S, locS, S))) return st;
+
+  p.sT = Slots();
+  p.sS = Slots();
+  p.sT.lvl_begin.assign(nlvl + 1, 0);
+  p.sS.lvl_begin.assign(nlvl + 1, 0);
+  p.sT.cone_begin.assign(nlvl, {});
+  p.sS.cone_begin.assign(nlvl, {});
+  walk.far_ts.assign(nlvl, {});
+  walk.far_ss.assign(nlvl, {});
+  walk.far_tab.assign(nlvl, {});
+  walk.near_pairs.clear();
+  walk.tab_nI.clear();
+
+  void* tmp = nullptr;
+  size_t tmp_bytes = 0;
+  auto scan = [&](auto* in, auto* out, int64_t n) -> int {
+    size_t need = 0;
+    DW_CK(cub::DeviceScan::ExclusiveSum(nullptr, need, in, out, n));
+    if (need > tmp_bytes) {
+      if (tmp) A.drop(tmp);
+      tmp = A.get<char>(need);
+      if (!tmp) {
+        err = "device plan: out of device memory";
+        return -5;
+      }
+      tmp_bytes = need;
+    }
+    DW_CK(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, in, out, n));
+    return 0;
+  };
+  auto last = [&](const auto* arr, int64_t i, auto& out) -> int {
+    DW_CK(cudaMemcpy(&out, arr + i, sizeof(out), cudaMemcpyDeviceToHost));
+    return 0;
+  };
+
+  // directions of all stages, one device table
+  std::vector<int64_t> dir_off(p.dirs.size() + 1, 0);
+  std::vector<double> alld;
+  for (size_t e = 0; e < p.dirs.size(); e++) {
+    dir_off[e] = (int64_t)(alld.size() / 3);
+    alld.insert(alld.end(), p.dirs[e].begin(), p.dirs[e].end());
+  }
+  const double* d_dirs = nullptr;
+  if ((st = upload_vec(A, alld, &d_dirs, err))) return st;
+
+  std::vector<int2> near_h;
+  int64_t table_count = 0;
+  int2* F = nullptr;
+  DW_ALLOC(F, int2, 1);
+  const int2 root = make_int2(0, 0);
+  DW_CK(cudaMemcpy(F, &root, sizeof(int2), cudaMemcpyHostToDevice));
+  int64_t nfr = 1;
+  uint8_t *prevT = nullptr, *prevS = nullptr;  // flags of the previous level
+  for (int l = 0; l < nlvl; l++) {
+    const bool prec = v.prec[l], hf = l > 0 && v.isHF[l];
+    // 1. classify and compact: far pairs, near pairs, next frontier
+    int32_t *isfar, *isnear, *pfar, *pnear;
+    int64_t *nch, *pch;
+    DW_ALLOC(isfar, int32_t, nfr + 1);
+    DW_ALLOC(isnear, int32_t, nfr + 1);
+    DW_ALLOC(pfar, int32_t, nfr + 1);
+    DW_ALLOC(pnear, int32_t, nfr + 1);
+    DW_ALLOC(nch, int64_t, nfr + 1);
+    DW_ALLOC(pch, int64_t, nfr + 1);
+    if (nfr) k_classify<<<nblk(nfr), 256>>>(nfr, F, T, S, prec ? 1 : 0, hf ? 1 : 0, p.kappa, isfar, isnear, nch);
+    DW_CK(cudaGetLastError());
+    DW_CK(cudaMemset(isfar + nfr, 0, sizeof(int32_t)));
+    DW_CK(cudaMemset(isnear + nfr, 0, sizeof(int32_t)));
+    DW_CK(cudaMemset(nch + nfr, 0, sizeof(int64_t)));
+    if ((st = scan(isfar, pfar, nfr + 1)) || (st = scan(isnear, pnear, nfr + 1)) || (st = scan(nch, pch, nfr + 1)))
+      return st;
+    int32_t nf = 0, nn = 0;
+    int64_t nx = 0;
+    if ((st = last(pfar, nfr, nf)) || (st = last(pnear, nfr, nn)) || (st = last(pch, nfr, nx))) return st;
+    int2 *fp, *np_, *next;
+    DW_ALLOC(fp, int2, nf);
+    DW_ALLOC(np_, int2, nn);
+    DW_ALLOC(next, int2, nx);
+    if (nfr)
+      k_scatter<<<nblk(nfr), 256>>>(nfr, F, T, S, isfar, pfar, isnear, pnear, nch, pch, fp, np_, next);
+    DW_CK(cudaGetLastError());
+    if (nn) {
+      const size_t o = near_h.size();
+      near_h.resize(o + nn);
+      DW_CK(cudaMemcpy(near_h.data() + o, np_, (size_t)nn * sizeof(int2), cudaMemcpyDeviceToHost));
+    }
+    for (void* q : {(void*)isfar, (void*)isnear, (void*)pfar, (void*)pnear, (void*)nch, (void*)pch, (void*)np_, (void*)F})
+      A.drop(q);
+    F = next;
+    nfr = nx;
+    if (hf) p.n_far_hf += nf; else p.n_far_lf += nf;
+
+    // 2. fundamental index bound and (HF) the cone of each far pair
+    int m = 0;
+    int16_t* cone = nullptr;
+    const int nd = v.nDir[l];
+    if (nf) {
+      int* dm;
+      DW_ALLOC(dm, int, 1);
+      DW_CK(cudaMemset(dm, 0, sizeof(int)));
+      k_maxdiff<<<nblk(nf), 256>>>(nf, fp, T, S, dm);
+      DW_CK(cudaGetLastError());
+      DW_CK(cudaMemcpy(&m, dm, sizeof(int), cudaMemcpyDeviceToHost));
+      A.drop(dm);
+    }
+    if (hf && nf) {
+      const int64_t wk = 2 * (int64_t)m + 1, nk = wk * wk * wk;
+      unsigned long long* first;
+      int16_t* kc;
+      DW_ALLOC(first, unsigned long long, nk);
+      DW_ALLOC(kc, int16_t, nk);
+      DW_ALLOC(cone, int16_t, nf);
+      DW_CK(cudaMemset(first, 0xff, nk * sizeof(unsigned long long)));
+      k_firstpos<<<nblk(nf), 256>>>(nf, fp, T, S, m, first);
+      const int h = v.HFStage[l];
+      k_cones<<<(unsigned)std::min<int64_t>(nk, 65535), 256>>>(nk, first, fp, T, S, d_dirs + 3 * dir_off[h],
+                                                              (int)(p.dirs[h].size() / 3), kc);
+      k_cone_of<<<nblk(nf), 256>>>(nf, fp, T, S, m, kc, cone);
+      DW_CK(cudaGetLastError());
+      A.drop(first);
+      A.drop(kc);
+    }
+
+    // 3. effective directions of this level (+ propagation from the parent level)
+    const bool hfprec = v.prec[l] && v.isHF[l];
+    const int64_t ncT = (int64_t)lcT[l].size(), ncS = (int64_t)lcS[l].size();
+    uint8_t *effT = nullptr, *effS = nullptr;
+    const int32_t *cellsT = nullptr, *cellsS = nullptr;
+    if ((st = upload_vec(A, lcT[l], &cellsT, err)) || (st = upload_vec(A, lcS[l], &cellsS, err))) return st;
+    if (hfprec) {
+      DW_ALLOC(effT, uint8_t, ncT * nd);
+      DW_ALLOC(effS, uint8_t, ncS * nd);
+      DW_CK(cudaMemset(effT, 0, std::max<int64_t>(1, ncT * nd)));
+      DW_CK(cudaMemset(effS, 0, std::max<int64_t>(1, ncS * nd)));
+      if (hf && nf) k_flags<<<nblk(nf), 256>>>(nf, fp, T, S, cone, nd, effT, effS);
+      if (!v.noHF && l > 0 && v.isHF[l - 1] && v.prec[l - 1] && prevT && prevS) {
+        const int pnd = v.nDir[l - 1];
+        if (ncT) k_propagate<<<nblk(ncT * nd), 256>>>(ncT, cellsT, T, nd, pnd, prevT, effT);
+        if (ncS) k_propagate<<<nblk(ncS * nd), 256>>>(ncS, cellsS, S, nd, pnd, prevS, effS);
+      }
+      DW_CK(cudaGetLastError());
+    }
+
+    // 4. slots of this level (cone-major, cells in DFS order)
+    int32_t *denseT = nullptr, *denseS = nullptr;
+    auto slots = [&](Slots& sl, const std::vector<int32_t>& cells, const int32_t* dcells, int64_t nc,
+                     const uint8_t* eff, int32_t*& dense) -> int {
+      sl.lvl_begin[l] = sl.n;
+      if (!v.prec[l]) {
+        sl.cone_begin[l].assign(2, sl.n);
+        return 0;
+      }
+      if (!v.isHF[l]) {  // one LF expansion per cell
+        sl.cone_begin[l] = {sl.n, sl.n + nc};
+        std::vector<int32_t> dh(nc);
+        for (int64_t i = 0; i < nc; i++) {
+          sl.cell.push_back(cells[i]);
+          sl.dir.push_back(-1);
+          dh[i] = (int32_t)(sl.n + i);
+        }
+        const int32_t* dd = nullptr;
+        int s2 = upload_vec(A, dh, &dd, err);
+        if (s2) return s2;
+        dense = const_cast<int32_t*>(dd);
+        sl.n += nc;
+        return 0;
+      }
+      int32_t *fl, *pos, *scell, *sdir;
+      const int64_t tot = nc * nd;
+      DW_ALLOC(fl, int32_t, tot + 1);
+      DW_ALLOC(pos, int32_t, tot + 1);
+      DW_ALLOC(dense, int32_t, tot);
+      if (tot) k_transpose<<<nblk(tot), 256>>>(nc, nd, eff, fl);
+      DW_CK(cudaMemset(fl + tot, 0, sizeof(int32_t)));
+      int s2 = scan(fl, pos, tot + 1);
+      if (s2) return s2;
+      int32_t cnt = 0;
+      if ((s2 = last(pos, tot, cnt))) return s2;
+      DW_ALLOC(scell, int32_t, cnt);
+      DW_ALLOC(sdir, int32_t, cnt);
+      if (tot) k_slots_hf<<<nblk(tot), 256>>>(nc, nd, eff, pos, dcells, sl.n, dense, scell, sdir);
+      DW_CK(cudaGetLastError());
+      // cone starts: pos at (d, 0)
+      std::vector<int32_t> ph(tot + 1);
+      DW_CK(cudaMemcpy(ph.data(), pos, (tot + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost));
+      sl.cone_begin[l].assign(nd + 1, 0);
+      for (int d = 0; d < nd; d++) sl.cone_begin[l][d] = sl.n + ph[(int64_t)d * nc];
+      sl.cone_begin[l][nd] = sl.n + cnt;
+      const size_t o = sl.cell.size();
+      sl.cell.resize(o + cnt);
+      sl.dir.resize(o + cnt);
+      DW_CK(cudaMemcpy(sl.cell.data() + o, scell, (size_t)cnt * sizeof(int32_t), cudaMemcpyDeviceToHost));
+      DW_CK(cudaMemcpy(sl.dir.data() + o, sdir, (size_t)cnt * sizeof(int32_t), cudaMemcpyDeviceToHost));
+      A.drop(fl);
+      A.drop(pos);
+      A.drop(scell);
+      A.drop(sdir);
+      sl.n += cnt;
+      return 0;
+    };
+    if ((st = slots(p.sT, lcT[l], cellsT, ncT, effT, denseT)) || (st = slots(p.sS, lcS[l], cellsS, ncS, effS, denseS)))
+      return st;
+
+    // 5. transfer-spectrum ids per fundamental index and the far entries
+    if (nf) {
+      const int64_t nkey = (int64_t)(m + 1) * (m + 1) * (m + 1);
+      int32_t *used, *tpos, *ts, *ss;
+      uint32_t* tab;
+      DW_ALLOC(used, int32_t, nkey + 1);
+      DW_ALLOC(tpos, int32_t, nkey + 1);
+      DW_CK(cudaMemset(used, 0, (nkey + 1) * sizeof(int32_t)));
+      k_tabflags<<<nblk(nf), 256>>>(nf, fp, T, S, m, used);
+      DW_CK(cudaGetLastError());
+      if ((st = scan(used, tpos, nkey + 1))) return st;
+      std::vector<int32_t> uh(nkey);
+      DW_CK(cudaMemcpy(uh.data(), used, nkey * sizeof(int32_t), cudaMemcpyDeviceToHost));
+      const int64_t tbase = table_count;
+      for (int64_t k = 0; k < nkey; k++)
+        if (uh[k]) {
+          table_count++;
+          const int a = (int)(k / ((m + 1) * (m + 1))), b = (int)((k / (m + 1)) % (m + 1)), c = (int)(k % (m + 1));
+          walk.tab_nI.push_back({a, b, c});
+          p.tab_lvl.push_back(l);
+          const int M = v.nCellMax[l];
+          p.tab_iz.push_back(((int64_t)a * M + b) * M + c);
+        }
+      DW_ALLOC(ts, int32_t, nf);
+      DW_ALLOC(ss, int32_t, nf);
+      DW_ALLOC(tab, uint32_t, nf);
+      k_entries<<<nblk(nf), 256>>>(nf, fp, T, S, m, hf ? 1 : 0, nd, cone, denseT, denseS, tpos, tbase, ts, ss, tab);
+      DW_CK(cudaGetLastError());
+      walk.far_ts[l].resize(nf);
+      walk.far_ss[l].resize(nf);
+      walk.far_tab[l].resize(nf);
+      DW_CK(cudaMemcpy(walk.far_ts[l].data(), ts, (size_t)nf * 4, cudaMemcpyDeviceToHost));
+      DW_CK(cudaMemcpy(walk.far_ss[l].data(), ss, (size_t)nf * 4, cudaMemcpyDeviceToHost));
+      DW_CK(cudaMemcpy(walk.far_tab[l].data(), tab, (size_t)nf * 4, cudaMemcpyDeviceToHost));
+      for (void* q : {(void*)used, (void*)tpos, (void*)ts, (void*)ss, (void*)tab}) A.drop(q);
+    }
+    if (cone) A.drop(cone);
+    A.drop(fp);
+    if (denseT) A.drop(denseT);
+    if (denseS) A.drop(denseS);
+    A.drop(const_cast<int32_t*>(cellsT));
+    A.drop(const_cast<int32_t*>(cellsS));
+    if (prevT) A.drop(prevT);
+    if (prevS) A.drop(prevS);
+    prevT = effT;
+    prevS = effS;
+  }
+  p.sT.lvl_begin[nlvl] = p.sT.n;
+  p.sS.lvl_begin[nlvl] = p.sS.n;
+  walk.near_pairs.resize(near_h.size());
+  for (size_t i = 0; i < near_h.size(); i++) walk.near_pairs[i] = {near_h[i].x, near_h[i].y};
+  return 0;
+}
+
+}  // namespace
+
+LevelWalker* device_level_walker() {
+  static DeviceWalker w;
+  return &w;
+}
+
+}  // namespace dfb

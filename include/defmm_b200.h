@@ -66,13 +66,15 @@ int defmm_load_inp(defmm_handle* h, const char* path, int64_t nparts, int which)
 /* IBFMM_Mat<3>::prcmpt(int L, int Ncrit, flt kappa, int lvMAX = -1)
  * (interface.hpp:100-151): build both octrees (leaf = fewer than Ncrit
  * particles, or fixed depth lvMAX when lvMAX >= 0), the frequency regime,
- * cones, interaction lists, expansion slots and transfer spectra on the host
- * (multi-threaded).  2 <= L <= 8. */
+ * cones, interaction lists, expansion slots and transfer spectra; the level
+ * walk (dual traversal, cones, effective directions, slots, far entries) runs
+ * on the GPU when one is present (defmm_set_plan_device), the rest on the
+ * host (multi-threaded).  2 <= L <= 8. */
 int defmm_prcmpt(defmm_handle* h, int L, int Ncrit, double kappa, int lvMAX);
 
 /* Copy the plan to the current CUDA device (done by the first gemv when not
- * called explicitly; prcmpt itself runs on the host only, so the plan can be
- * inspected without a GPU). */
+ * called explicitly; without a GPU prcmpt runs entirely on the host, so the
+ * plan can be inspected without one). */
 int defmm_upload(defmm_handle* h);
 
 /* Select the matvec arithmetic (DEFMM_PRECISION_*); default FP64.
@@ -140,6 +142,8 @@ int defmm_direct_noalloc(defmm_handle* h, const double* d_targets, int64_t nt,
 #define DEFMM_INFO_M2L_TARGETS 17  /* target slots receiving M2L */
 #define DEFMM_INFO_LEAF_SLOTS_S 18 /* source leaf expansions (P2M outputs) */
 #define DEFMM_INFO_PERMUTED_SPECTRA 19 /* (spectrum, symmetry) pairs used by M2L */
+#define DEFMM_INFO_PLAN_WALK_DEVICE 20 /* 1 if prcmpt's level walk ran on the GPU */
+#define DEFMM_INFO_PLAN_MS 21          /* prcmpt time (tree, lists, spectra), ms */
 int defmm_info(const defmm_handle* h, int what, int64_t* value);
 
 /* Per-phase device times (ms) of the last gemv, in this order:
@@ -159,6 +163,13 @@ int defmm_set_profiling(defmm_handle* h, int on);
 /* Record the interaction lists at the next prcmpt (costs host memory; for
  * parity checks against the reference). */
 int defmm_keep_lists(defmm_handle* h, int on);
+
+/* No counterpart in the reference (its precomputation is host-only).  on != 0
+ * (the default): prcmpt runs the level walk of the plan — dual traversal,
+ * cones, effective directions, slots, far-field entries — on the GPU when one
+ * is present, with results identical to the host walk; on == 0: always on
+ * the host.  List records (defmm_keep_lists) always come from the host walk. */
+int defmm_set_plan_device(defmm_handle* h, int on);
 
 /* Tree dump in the layout of the reference's cell array (SourceRoot /
  * TargetRoot, interface.hpp:174-175; cells in depth-first pre-order):
