@@ -196,7 +196,9 @@ def main():
     t0 = time.perf_counter()
     A.prcmpt(w.order, w.ncrit, w.kappa)
     setup_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
     A.upload()
+    upload_s = time.perf_counter() - t0
     info = A.info()
     # a dedicated stream: torch's default stream is the legacy NULL stream,
     # which the library's non-blocking streams would not order against
@@ -317,6 +319,8 @@ def main():
             "gpu_launches": res[head]["launches"],
             "phases_ms": phases,
             "setup_s": setup_s,
+            "setup": {"prcmpt_s": setup_s, "level_walk_s": info["plan_walk_ms"] / 1e3,
+                      "level_walk_on_gpu": bool(info["plan_walk_device"]), "upload_s": upload_s},
             "plan": {k: info[k] for k in ["nlvl", "cpt", "slots_S", "slots_T", "far_hf", "far_lf", "near",
                                           "i_near", "tables", "permuted_spectra", "device_bytes"]},
         }

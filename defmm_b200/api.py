@@ -35,6 +35,7 @@ _INFO = {
     "cells_S": 6, "slots_S": 7, "slots_T": 8, "far_hf": 9, "far_lf": 10, "near": 11,
     "i_near": 12, "tables": 13, "device_bytes": 14, "list_records": 15, "launches": 16,
     "m2l_targets": 17, "leaf_slots_S": 18, "permuted_spectra": 19, "plan_walk_device": 20, "plan_ms": 21,
+    "plan_walk_ms": 22,
 }
 PHASES = ["p2m", "m2m", "m2f", "m2l", "f2l", "l2l", "l2p", "p2p", "scatter", "total"]
 

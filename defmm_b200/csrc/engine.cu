@@ -219,8 +219,14 @@ int upload_plan(defmm_handle* h) {
   UP(p.l2l_ptr, d.l2l_ptr);
   UP(p.l2l_parent, d.l2l_parent);
   UP(p.m2l_ptr, d.m2l_ptr);
-  UP(p.m2l_src, d.m2l_src);
-  UP(p.m2l_tab, d.m2l_tab);
+  if (p.dev_m2l_src) {  // built on the device by prcmpt
+    d.m2l_src = static_cast<const int32_t*>(p.dev_m2l_src);
+    d.m2l_tab = static_cast<const uint32_t*>(p.dev_m2l_tab);
+    h->dev_bytes += (size_t)p.n_m2l * 8;
+  } else {
+    UP(p.m2l_src, d.m2l_src);
+    UP(p.m2l_tab, d.m2l_tab);
+  }
   UP(p.perm, d.perm);
   UP(p.ptab_key, h->d_ptab_key);
   std::vector<double> mats;
@@ -723,6 +729,9 @@ int defmm_prcmpt(defmm_handle* h, int L, int Ncrit, double kappa, int lvMAX) {
                            (int64_t)h->trg.size() / 3, L, Ncrit, kappa, lvMAX, e, walker);
   if (st) return h->fail(st == -4 ? DEFMM_ERR_CUDA : st == -5 ? DEFMM_ERR_MEMORY : st, e);
   h->walked_on_device = walker != nullptr;
+  // M2L entries the walk left on the device belong to this handle's plan
+  if (h->plan.dev_m2l_src) h->plan_allocs.push_back(h->plan.dev_m2l_src);
+  if (h->plan.dev_m2l_tab) h->plan_allocs.push_back(h->plan.dev_m2l_tab);
   if (h->plan.lv.nlvl > 32) return h->fail(DEFMM_ERR_DEPTH, "more than 32 tree levels");
   h->built = true;
   return 0;
@@ -870,6 +879,7 @@ int defmm_info(const defmm_handle* h, int what, int64_t* v) {
     case DEFMM_INFO_PERMUTED_SPECTRA: *v = (int64_t)p.ptab_key.size(); break;
     case DEFMM_INFO_PLAN_WALK_DEVICE: *v = h->walked_on_device ? 1 : 0; break;
     case DEFMM_INFO_PLAN_MS: *v = (int64_t)(1e3 * (p.t_tree + p.t_lists + p.t_tables)); break;
+    case DEFMM_INFO_PLAN_WALK_MS: *v = (int64_t)(1e3 * p.t_walk); break;
     case DEFMM_INFO_M2L_TARGETS: {
       int64_t n = 0;
       for (int64_t k = 0; k < p.sT.n; k++) n += p.m2l_ptr[k + 1] > p.m2l_ptr[k] ? 1 : 0;

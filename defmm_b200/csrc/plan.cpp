@@ -1000,8 +1000,10 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
   const int nlvl = v.nlvl;
 
   LevelWalk w;
+  const double tw = now_s();
   st = (walker && !p.keep_lists) ? walker->walk(p, w, err) : walk_levels_host(p, w);
   if (st) return st;
+  p.t_walk = now_s() - tw;
   auto& near_pairs = w.near_pairs;
   auto& tab_nI = w.tab_nI;
 
@@ -1025,7 +1027,7 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
   cell_csr(p.S, p.sS);
 
   // M2L grouped by target slot (stable: depth-first order within a slot)
-  {
+  if (!w.m2l_done) {
     p.m2l_ptr.assign(p.sT.n + 1, 0);
     for (int l = 0; l < nlvl; l++)
       for (int32_t ts : w.far_ts[l]) p.m2l_ptr[ts + 1]++;
@@ -1047,7 +1049,7 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
   }
 
   // permuted spectra: one per (spectrum, symmetry hash) pair that occurs
-  {
+  if (!w.m2l_done) {
     const int64_t ntab = (int64_t)tab_nI.size();
     std::vector<int32_t> pid(ntab * 64, -1);
     for (uint32_t k : p.m2l_tab) pid[k] = 0;

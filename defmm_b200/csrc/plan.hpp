@@ -91,6 +91,13 @@ struct Plan {
   // permuted spectra actually used: (table index << 6) | hash; the device
   // holds U_k[i] = tables[key >> 6][perm[key & 63][i]]
   std::vector<uint32_t> ptab_key;
+  // M2L entries already on the device (built there by the level walk):
+  // int32 source slots and uint32 permuted-spectrum ids, n_m2l each, in
+  // m2l_ptr order; the host copies m2l_src / m2l_tab stay empty.  The
+  // operator that owns the plan releases them.
+  void* dev_m2l_src = nullptr;
+  void* dev_m2l_tab = nullptr;
+  int64_t n_m2l = 0;
   // M2M children of each source slot, L2L parents of each target slot
   std::vector<int64_t> m2m_ptr;            // sS.n + 1
   std::vector<int32_t> m2m_child;          // child slot
@@ -137,7 +144,7 @@ struct Plan {
   // iz, hash) and near (t, s) in the reference's HorizontalPass order.
   bool keep_lists = false;
   std::vector<int32_t> rec_far_hf, rec_far_lf, rec_near;
-  double t_tree = 0, t_lists = 0, t_tables = 0;
+  double t_tree = 0, t_lists = 0, t_tables = 0, t_walk = 0;  // t_walk: part of t_lists
 };
 
 // Result of the level-by-level dual traversal (hrzpass.hpp:62-143 with the
@@ -150,6 +157,10 @@ struct LevelWalk {
   std::vector<std::array<int32_t, 3>> tab_nI;  // fundamental index per table
   std::vector<std::vector<int32_t>> far_ts, far_ss;  // per level: slots
   std::vector<std::vector<uint32_t>> far_tab;        // per level: (table << 6) | hash
+  // Set by a walker that also grouped the far entries by target slot itself
+  // (the M2L CSR with permuted-spectrum ids): it fills Plan::m2l_ptr and
+  // ptab_key and leaves the entries in Plan::dev_m2l_src / dev_m2l_tab.
+  bool m2l_done = false;
 };
 
 // Another implementation of the level walk (the device one); it must produce

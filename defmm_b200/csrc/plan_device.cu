@@ -251,6 +251,33 @@ __global__ void k_entries(int64_t nf, const int2* __restrict__ P, DTree T, DTree
   tab[i] = ((uint32_t)(tbase + tidpos[fi]) << 6) | (uint32_t)(h0 + (h1 << 3));
 }
 
+__global__ void k_iota(int64_t n, int32_t* __restrict__ v) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) v[i] = (int32_t)i;
+}
+
+__global__ void k_count(int64_t n, const int32_t* __restrict__ key, int32_t* __restrict__ cnt) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) atomicAdd(cnt + key[i], 1);
+}
+
+// entries in sorted order; marks the (table, hash) keys that occur
+__global__ void k_gather_entries(int64_t n, const int32_t* __restrict__ order, const int32_t* __restrict__ ss,
+                                 const uint32_t* __restrict__ tab, int32_t* __restrict__ src,
+                                 uint32_t* __restrict__ key, int32_t* __restrict__ used) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int32_t o = order[i];
+  src[i] = ss[o];
+  key[i] = tab[o];
+  used[tab[o]] = 1;
+}
+
+__global__ void k_renumber(int64_t n, const int32_t* __restrict__ pid, uint32_t* __restrict__ key) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) key[i] = (uint32_t)pid[key[i]];
+}
+
 inline unsigned nblk(int64_t n, int b = 256) { return (unsigned)std::max<int64_t>(1, (n + b - 1) / b); }
 
 // Device buffers of one walk; everything is freed at the end.
@@ -380,6 +407,10 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
 
   std::vector<int2> near_h;
   int64_t table_count = 0;
+  std::vector<int32_t*> lv_ts, lv_ss;  // far entries per level, on the device
+  std::vector<uint32_t*> lv_tab;
+  std::vector<int64_t> lv_n;
+  std::vector<int> lv_level;
   int2* F = nullptr;
   DW_ALLOC(F, int2, 1);
   const int2 root = make_int2(0, 0);
@@ -564,13 +595,12 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
       DW_ALLOC(tab, uint32_t, nf);
       k_entries<<<nblk(nf), 256>>>(nf, fp, T, S, m, hf ? 1 : 0, nd, cone, denseT, denseS, tpos, tbase, ts, ss, tab);
       DW_CK(cudaGetLastError());
-      walk.far_ts[l].resize(nf);
-      walk.far_ss[l].resize(nf);
-      walk.far_tab[l].resize(nf);
-      DW_CK(cudaMemcpy(walk.far_ts[l].data(), ts, (size_t)nf * 4, cudaMemcpyDeviceToHost));
-      DW_CK(cudaMemcpy(walk.far_ss[l].data(), ss, (size_t)nf * 4, cudaMemcpyDeviceToHost));
-      DW_CK(cudaMemcpy(walk.far_tab[l].data(), tab, (size_t)nf * 4, cudaMemcpyDeviceToHost));
-      for (void* q : {(void*)used, (void*)tpos, (void*)ts, (void*)ss, (void*)tab}) A.drop(q);
+      lv_ts.push_back(ts);  // kept on the device for the M2L grouping below
+      lv_ss.push_back(ss);
+      lv_tab.push_back(tab);
+      lv_n.push_back(nf);
+      lv_level.push_back(l);
+      for (void* q : {(void*)used, (void*)tpos}) A.drop(q);
     }
     if (cone) A.drop(cone);
     A.drop(fp);
@@ -587,6 +617,108 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
   p.sS.lvl_begin[nlvl] = p.sS.n;
   walk.near_pairs.resize(near_h.size());
   for (size_t i = 0; i < near_h.size(); i++) walk.near_pairs[i] = {near_h[i].x, near_h[i].y};
+
+  // M2L entries grouped by target slot: a stable radix sort of all levels'
+  // entries (level order, then walk order) by target slot, as the host's
+  // counting placement; then the permuted-spectrum ids (one per
+  // (table, hash) key that occurs, in increasing key order)
+  int64_t n = 0;
+  for (int64_t c : lv_n) n += c;
+  if (n >= ((int64_t)1 << 31) - 1) {  // beyond 32-bit sort indices: the host groups the entries
+    for (size_t q = 0; q < lv_n.size(); q++) {
+      const int l = lv_level[q];
+      walk.far_ts[l].resize(lv_n[q]);
+      walk.far_ss[l].resize(lv_n[q]);
+      walk.far_tab[l].resize(lv_n[q]);
+      DW_CK(cudaMemcpy(walk.far_ts[l].data(), lv_ts[q], lv_n[q] * 4, cudaMemcpyDeviceToHost));
+      DW_CK(cudaMemcpy(walk.far_ss[l].data(), lv_ss[q], lv_n[q] * 4, cudaMemcpyDeviceToHost));
+      DW_CK(cudaMemcpy(walk.far_tab[l].data(), lv_tab[q], lv_n[q] * 4, cudaMemcpyDeviceToHost));
+    }
+    return 0;
+  }
+  int32_t *all_ts, *all_ss, *idx, *keys_out, *idx_out, *cnt, *used, *pid;
+  uint32_t* all_tab;
+  DW_ALLOC(all_ts, int32_t, n);
+  DW_ALLOC(all_ss, int32_t, n);
+  DW_ALLOC(all_tab, uint32_t, n);
+  {
+    int64_t o = 0;
+    for (size_t k = 0; k < lv_n.size(); k++) {
+      DW_CK(cudaMemcpy(all_ts + o, lv_ts[k], lv_n[k] * 4, cudaMemcpyDeviceToDevice));
+      DW_CK(cudaMemcpy(all_ss + o, lv_ss[k], lv_n[k] * 4, cudaMemcpyDeviceToDevice));
+      DW_CK(cudaMemcpy(all_tab + o, lv_tab[k], lv_n[k] * 4, cudaMemcpyDeviceToDevice));
+      A.drop(lv_ts[k]);
+      A.drop(lv_ss[k]);
+      A.drop(lv_tab[k]);
+      o += lv_n[k];
+    }
+  }
+  DW_ALLOC(idx, int32_t, n);
+  DW_ALLOC(keys_out, int32_t, n);
+  DW_ALLOC(idx_out, int32_t, n);
+  if (n) k_iota<<<nblk(n), 256>>>(n, idx);
+  int bits = 1;
+  while (bits < 31 && ((int64_t)1 << bits) <= p.sT.n) bits++;
+  {
+    size_t need = 0;
+    DW_CK(cub::DeviceRadixSort::SortPairs(nullptr, need, all_ts, keys_out, idx, idx_out, n, 0, bits));
+    char* t2 = A.get<char>(need);
+    if (!t2) {
+      err = "device plan: out of device memory";
+      return -5;
+    }
+    DW_CK(cub::DeviceRadixSort::SortPairs(t2, need, all_ts, keys_out, idx, idx_out, n, 0, bits));
+    A.drop(t2);
+  }
+  const int64_t nslot = p.sT.n, ntab = (int64_t)walk.tab_nI.size() * 64;
+  DW_ALLOC(cnt, int32_t, nslot + 1);
+  DW_ALLOC(used, int32_t, ntab + 1);
+  DW_ALLOC(pid, int32_t, ntab + 1);
+  DW_CK(cudaMemset(cnt, 0, (nslot + 1) * sizeof(int32_t)));
+  DW_CK(cudaMemset(used, 0, (ntab + 1) * sizeof(int32_t)));
+  void *src_out = nullptr, *key_out = nullptr;  // handed to the plan's owner
+  DW_CK(cudaMalloc(&src_out, std::max<int64_t>(1, n) * sizeof(int32_t)));
+  if (cudaMalloc(&key_out, std::max<int64_t>(1, n) * sizeof(uint32_t)) != cudaSuccess) {
+    cudaFree(src_out);
+    cudaGetLastError();
+    err = "device plan: out of device memory";
+    return -5;
+  }
+  auto fail_out = [&](int code) {
+    cudaFree(src_out);
+    cudaFree(key_out);
+    return code;
+  };
+  if (n) {
+    k_count<<<nblk(n), 256>>>(n, all_ts, cnt);
+    k_gather_entries<<<nblk(n), 256>>>(n, idx_out, all_ss, all_tab, (int32_t*)src_out, (uint32_t*)key_out, used);
+  }
+  if (cudaGetLastError() != cudaSuccess) return fail_out(-4);
+  int32_t* pos = nullptr;
+  pos = A.get<int32_t>(nslot + 1);
+  if (!pos) return fail_out(-5);
+  if ((st = scan(cnt, pos, nslot + 1)) || (st = scan(used, pid, ntab + 1))) return fail_out(st);
+  if (n) k_renumber<<<nblk(n), 256>>>(n, pid, (uint32_t*)key_out);
+  if (cudaDeviceSynchronize() != cudaSuccess) {
+    cudaGetLastError();
+    err = "device plan: M2L grouping failed";
+    return fail_out(-4);
+  }
+  std::vector<int32_t> ph(nslot + 1), uh(ntab);
+  if (cudaMemcpy(ph.data(), pos, (nslot + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      (ntab && cudaMemcpy(uh.data(), used, ntab * sizeof(int32_t), cudaMemcpyDeviceToHost) != cudaSuccess)) {
+    cudaGetLastError();
+    err = "device plan: copy of the M2L grouping failed";
+    return fail_out(-4);
+  }
+  p.m2l_ptr.assign(ph.begin(), ph.end());
+  p.ptab_key.clear();
+  for (int64_t k = 0; k < ntab; k++)
+    if (uh[k]) p.ptab_key.push_back((uint32_t)k);
+  p.dev_m2l_src = src_out;
+  p.dev_m2l_tab = key_out;
+  p.n_m2l = n;
+  walk.m2l_done = true;
   return 0;
 }
 

@@ -144,6 +144,7 @@ int defmm_direct_noalloc(defmm_handle* h, const double* d_targets, int64_t nt,
 #define DEFMM_INFO_PERMUTED_SPECTRA 19 /* (spectrum, symmetry) pairs used by M2L */
 #define DEFMM_INFO_PLAN_WALK_DEVICE 20 /* 1 if prcmpt's level walk ran on the GPU */
 #define DEFMM_INFO_PLAN_MS 21          /* prcmpt time (tree, lists, spectra), ms */
+#define DEFMM_INFO_PLAN_WALK_MS 22     /* of which the level walk, ms */
 int defmm_info(const defmm_handle* h, int what, int64_t* value);
 
 /* Per-phase device times (ms) of the last gemv, in this order:
