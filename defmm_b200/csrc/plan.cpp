@@ -1062,51 +1062,64 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
     pfor((int64_t)p.m2l_tab.size(), 1 << 16, [&](int64_t e) { p.m2l_tab[e] = (uint32_t)pid[p.m2l_tab[e]]; });
   }
 
+  // CSR over slots from a per-slot visitor visit(k, emit): counted, then
+  // filled, both passes in parallel over slots
+  auto slot_csr = [&](int64_t n, auto visit, std::vector<int64_t>& ptr, std::vector<int32_t>& out) {
+    std::vector<int32_t> cnt(n, 0);
+    pfor(n, 4096, [&](int64_t k) {
+      int32_t c = 0;
+      visit(k, [&](int64_t) { c++; });
+      cnt[k] = c;
+    });
+    ptr.assign(n + 1, 0);
+    for (int64_t k = 0; k < n; k++) ptr[k + 1] = ptr[k] + cnt[k];
+    out.resize(ptr[n]);
+    pfor(n, 4096, [&](int64_t k) {
+      int64_t o = ptr[k];
+      visit(k, [&](int64_t x) { out[o++] = (int32_t)x; });
+    });
+  };
   // M2M: children slots of each source slot (P2M/M2M operators, M2M.hpp:35-124)
   {
     const Slots& s = p.sS;
-    std::vector<std::vector<int32_t>> ch(s.n);
-    pfor(s.n, 1024, [&](int64_t k) {
-      const int64_t c = s.cell[k];
-      const int l = p.S.lvl[c];
-      if (!v.prec[l] || p.S.leaf(c)) return;
-      const int d = s.dir[k];
-      const bool hfd = v.isHF[l] && v.HFStage[l] > 0;
-      for (int64_t a = p.S.son_ptr[c]; a < p.S.son_ptr[c + 1]; a++) {
-        const int64_t cs = s.slot_of(p.S.sons[a], hfd ? d / 4 : -1);
-        if (cs >= 0) ch[k].push_back((int32_t)cs);
-      }
-    });
-    p.m2m_ptr.assign(s.n + 1, 0);
-    for (int64_t k = 0; k < s.n; k++) p.m2m_ptr[k + 1] = p.m2m_ptr[k] + (int64_t)ch[k].size();
-    p.m2m_child.resize(p.m2m_ptr[s.n]);
-    for (int64_t k = 0; k < s.n; k++)
-      std::copy(ch[k].begin(), ch[k].end(), p.m2m_child.begin() + p.m2m_ptr[k]);
+    slot_csr(
+        s.n,
+        [&](int64_t k, auto emit) {
+          const int64_t c = s.cell[k];
+          const int l = p.S.lvl[c];
+          if (!v.prec[l] || p.S.leaf(c)) return;
+          const int d = s.dir[k];
+          const bool hfd = v.isHF[l] && v.HFStage[l] > 0;
+          for (int64_t a = p.S.son_ptr[c]; a < p.S.son_ptr[c + 1]; a++) {
+            const int64_t cs = s.slot_of(p.S.sons[a], hfd ? d / 4 : -1);
+            if (cs >= 0) emit(cs);
+          }
+        },
+        p.m2m_ptr, p.m2m_child);
   }
   // L2L: parent slots feeding each target slot (L2L.hpp:35-127)
   {
     const Slots& s = p.sT;
-    std::vector<std::vector<int32_t>> par(s.n);
-    pfor(s.n, 1024, [&](int64_t k) {
-      const int64_t c = s.cell[k];
-      const int64_t pc = p.T.parent[c];
-      if (pc < 0) return;
-      const int l = p.T.lvl[pc];
-      if (!v.prec[l]) return;
-      const int dt = s.dir[k];
-      const int64_t b = s.cell_ptr[pc], e = s.cell_ptr[pc + 1];
-      if (v.isHF[l] && v.HFStage[l] > 0) {  // parent directions 4dt..4dt+3
-        for (int64_t j = b; j < e; j++)
-          if (s.cell_dirs[j] / 4 == dt) par[k].push_back((int32_t)s.cell_slots[j]);
-      } else {  // HFStage-0 parent: all its directions; LF parent: its expansion
-        for (int64_t j = b; j < e; j++) par[k].push_back((int32_t)s.cell_slots[j]);
-      }
-    });
-    p.l2l_ptr.assign(s.n + 1, 0);
-    for (int64_t k = 0; k < s.n; k++) p.l2l_ptr[k + 1] = p.l2l_ptr[k] + (int64_t)par[k].size();
-    p.l2l_parent.resize(p.l2l_ptr[s.n]);
-    for (int64_t k = 0; k < s.n; k++)
-      std::copy(par[k].begin(), par[k].end(), p.l2l_parent.begin() + p.l2l_ptr[k]);
+    slot_csr(
+        s.n,
+        [&](int64_t k, auto emit) {
+          const int64_t c = s.cell[k];
+          const int64_t pc = p.T.parent[c];
+          if (pc < 0) return;
+          const int l = p.T.lvl[pc];
+          if (!v.prec[l]) return;
+          const int dt = s.dir[k];
+          const int64_t b = s.cell_ptr[pc], e = s.cell_ptr[pc + 1];
+          if (v.isHF[l] && v.HFStage[l] > 0) {  // parent directions 4dt..4dt+3
+            // cell_dirs of the parent are increasing: binary search the run
+            const int32_t* cd = s.cell_dirs.data();
+            int64_t j = std::lower_bound(cd + b, cd + e, 4 * dt) - cd;
+            for (; j < e && cd[j] / 4 == dt; j++) emit(s.cell_slots[j]);
+          } else {  // HFStage-0 parent: all its directions; LF parent: its expansion
+            for (int64_t j = b; j < e; j++) emit(s.cell_slots[j]);
+          }
+        },
+        p.l2l_ptr, p.l2l_parent);
   }
   // leaves holding expansions (upwpass.hpp:39-47, dwnpass.hpp:39-47)
   for (int64_t c = 0; c < p.S.ncell; c++)
