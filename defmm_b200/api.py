@@ -78,6 +78,9 @@ def lib():
             "defmm_set_graphs": (ctypes.c_int, [vp, ctypes.c_int]),
             "defmm_keep_lists": (ctypes.c_int, [vp, ctypes.c_int]),
             "defmm_set_plan_device": (ctypes.c_int, [vp, ctypes.c_int]),
+            "defmm_batch_create": (vp, [i64, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.c_int]),
+            "defmm_batch_launch": (ctypes.c_int, [vp, vp]),
+            "defmm_batch_destroy": (None, [vp]),
             "defmm_dump_tree": (ctypes.c_int, [vp, ctypes.c_int, ip, dp, ip, ctypes.POINTER(i64), ip]),
             "defmm_dump_lists": (ctypes.c_int, [vp, ip, ip, ip, ctypes.POINTER(i64)]),
         }
@@ -230,6 +233,38 @@ class IBFMM_Mat:
         nr = np.zeros((n[2], 2), np.int32)
         self._check(lib().defmm_dump_lists(self._h, _ip(fh), _ip(fl), _ip(nr), n))
         return nr, fh, fl
+
+
+class Batch:
+    """Several operators applied by one graph launch (defmm_batch_*): ops[i]
+    maps the device vector at d_in[i] to d_out[i] (pointers as ints, e.g.
+    torch.Tensor.data_ptr()).  Creating the batch runs every member once.
+    `lanes` chains run concurrently; the matvecs of one chain run in turn."""
+
+    def __init__(self, ops, d_in, d_out, lanes=1):
+        n = len(ops)
+        if not (n == len(d_in) == len(d_out)) or n == 0:
+            raise ValueError("one input and one output per operator")
+        hs = (ctypes.c_void_p * n)(*[op._h for op in ops])
+        ins = (ctypes.c_void_p * n)(*d_in)
+        outs = (ctypes.c_void_p * n)(*d_out)
+        self._ops = list(ops)  # members must outlive the batch
+        if lanes < 1:
+            raise ValueError("lanes must be >= 1")
+        self._b = lib().defmm_batch_create(n, hs, ins, outs, int(lanes))
+        if not self._b:
+            msgs = "; ".join(lib().defmm_last_error(op._h).decode() for op in ops if lib().defmm_last_error(op._h))
+            raise DefmmError(-4, "batch creation failed" + (": " + msgs if msgs else ""))
+
+    def launch(self, stream=0):
+        st = lib().defmm_batch_launch(self._b, ctypes.c_void_p(stream) if stream else None)
+        if st != 0:
+            raise DefmmError(st, "batch launch failed")
+
+    def __del__(self):
+        if getattr(self, "_b", None):
+            lib().defmm_batch_destroy(self._b)
+            self._b = None
 
 
 def SourceRoot(A):

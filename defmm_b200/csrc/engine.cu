@@ -79,6 +79,7 @@ struct defmm_handle {
   // CUDA graph of one matvec, replayed while (precision, input, output,
   // stream) stay the same
   bool use_graphs = true;
+  cudaGraph_t graph = nullptr;  // the captured matvec behind gexec (child node of batches)
   cudaGraphExec_t gexec = nullptr;
   const void* g_in = nullptr;
   void* g_out = nullptr;
@@ -148,7 +149,9 @@ std::vector<int32_t> to_i32(const std::vector<V>& v) {
 
 void drop_graph(defmm_handle* h) {
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
+  if (h->graph) cudaGraphDestroy(h->graph);
   h->gexec = nullptr;
+  h->graph = nullptr;
   h->g_prec = -1;
 }
 
@@ -565,7 +568,7 @@ int matvec(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) {
     return run_gemv(h, qin, out, s);
   }
   e = cudaGraphInstantiate(&h->gexec, g, 0);
-  cudaGraphDestroy(g);
+  h->graph = g;  // kept: batches embed it as a child graph
   if (e != cudaSuccess) {
     cudaGetLastError();
     h->gexec = nullptr;
@@ -771,6 +774,86 @@ int defmm_gemv_device(defmm_handle* h, const void* d_in, void* d_out, int64_t nr
     if (st) return st;
   }
   return 0;
+}
+
+}  // extern "C"
+
+// Several operators' matvecs as one graph: each handle's captured matvec is
+// an independent child node, so independent problems share the GPU.
+struct defmm_batch {
+  cudaGraphExec_t exec = nullptr;
+  int device = -1;
+};
+
+extern "C" {
+
+defmm_batch* defmm_batch_create(int64_t n, defmm_handle* const* hs, const void* const* d_in, void* const* d_out,
+                                int lanes) {
+  if (n < 1 || !hs || !d_in || !d_out || lanes < 1) return nullptr;
+  for (int64_t i = 0; i < n; i++)
+    if (!hs[i]) return nullptr;
+  cudaGraph_t parent = nullptr;
+  if (cudaGraphCreate(&parent, 0) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  // longest-first onto the lane with the fewest points so far; within a
+  // lane each matvec waits for the previous one
+  const int nl = (int)std::min<int64_t>(lanes, n);
+  std::vector<int64_t> order(n);
+  for (int64_t i = 0; i < n; i++) order[i] = i;
+  auto pts = [&](int64_t i) { return (int64_t)(hs[i]->plan.S.perm.size() + hs[i]->plan.T.perm.size()); };
+  std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return pts(a) > pts(b); });
+  std::vector<int64_t> load(nl, 0);
+  std::vector<cudaGraphNode_t> tail(nl, nullptr);
+  int device = -1;
+  for (int64_t i : order) {
+    defmm_handle* h = hs[i];
+    const int lane = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    load[lane] += pts(i);
+    bool ok = h && d_in[i] && d_out[i] && h->built && h->use_graphs;
+    // one run on the handle's own stream captures (and runs) its matvec
+    if (ok)
+      ok = defmm_gemv_device(h, d_in[i], d_out[i], 1, nullptr) == 0 && cudaStreamSynchronize(h->st) == cudaSuccess &&
+           h->graph && h->g_in == d_in[i] && h->g_out == d_out[i] && (device < 0 || h->device == device);
+    cudaGraphNode_t node;
+    if (ok)
+      ok = cudaGraphAddChildGraphNode(&node, parent, tail[lane] ? &tail[lane] : nullptr, tail[lane] ? 1 : 0,
+                                      h->graph) == cudaSuccess;
+    if (ok) tail[lane] = node;
+    if (!ok) {
+      if (h && h->err.empty()) h->err = "batch: this operator's matvec could not be captured as a graph";
+      cudaGetLastError();
+      cudaGraphDestroy(parent);
+      return nullptr;
+    }
+    device = h->device;
+  }
+  defmm_batch* b = new defmm_batch;
+  b->device = device;
+  cudaError_t e = cudaGraphInstantiate(&b->exec, parent, 0);
+  cudaGraphDestroy(parent);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    delete b;
+    return nullptr;
+  }
+  return b;
+}
+
+int defmm_batch_launch(defmm_batch* b, void* stream) {
+  if (!b || !b->exec) return DEFMM_ERR_ARG;
+  if (cudaSetDevice(b->device) != cudaSuccess || cudaGraphLaunch(b->exec, (cudaStream_t)stream) != cudaSuccess) {
+    cudaGetLastError();
+    return DEFMM_ERR_CUDA;
+  }
+  return 0;
+}
+
+void defmm_batch_destroy(defmm_batch* b) {
+  if (!b) return;
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  delete b;
 }
 
 int defmm_gemv_batched(defmm_handle* h, int64_t nrhs, const double* in, double* out) {

@@ -126,6 +126,32 @@ def gaussian_blobs(n: int, seed: int = 0, nblobs: int = 8, sigma: float = 0.05,
                     2.0 * math.pi * wavelengths / math.sqrt(3.0), order, ncrit)
 
 
+def ragged_problems(count: int = 48, seed: int = 0) -> list:
+    """Independent problems of uneven size for one batched launch: N
+    log-uniform in [5,000, 250,000]; geometry cycling cube surface / sphere
+    surface / 8 Gaussian blobs (sigma 0.05) in the unit cube; 8-128
+    wavelengths across the diameter (log-uniform, capped so that the surface
+    keeps >= 25 points per square wavelength and the tree reaches a level
+    with far-field work); order 4-6; leaf size 64."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(round(math.exp(rng.uniform(math.log(5e3), math.log(2.5e5)))))
+        wl = math.exp(rng.uniform(math.log(8.0), math.log(128.0)))
+        wl = max(2.0, min(wl, math.sqrt(n / (25.0 * math.pi))))
+        order = 4 + i % 3
+        g = i % 3
+        if g == 0:
+            c = cube_surface(n, seed=seed * 1000 + i)
+            w = Workload("cube_surface", c.points, 2.0 * math.pi * wl / math.sqrt(3.0), order, 64)
+        elif g == 1:
+            w = sphere_surface(n, seed=seed * 1000 + i, wavelengths=wl, order=order)
+        else:
+            w = gaussian_blobs(n, seed=seed * 1000 + i, wavelengths=wl, order=order)
+        out.append(w)
+    return out
+
+
 def charges(n: int, seed: int = 1, nrhs: int | None = None) -> np.ndarray:
     """Complex charges, real and imaginary parts uniform in [-1, 1]."""
     rng = np.random.default_rng(seed)

@@ -92,6 +92,25 @@ int defmm_gemv(defmm_handle* h, const double* in, double* out);
 int defmm_gemv_device(defmm_handle* h, const void* d_in, void* d_out,
                       int64_t nrhs, void* stream);
 
+/* No counterpart in the reference.  Independent operators (handles of
+ * problems of any sizes, orders and wavenumbers) applied together: each
+ * handle's matvec is captured as a CUDA graph (one run on its own stream, on
+ * d_in[i] -> d_out[i], device pointers as in defmm_gemv_device) and becomes a
+ * node of one graph, so one launch runs all of them.  The members are spread
+ * over `lanes` >= 1 chains (largest first, onto the chain with the fewest
+ * points so far): matvecs of one chain run in turn, chains run concurrently.
+ * The handles and buffers must outlive the batch; after prcmpt or
+ * defmm_set_precision on a member, create the batch again.  Returns NULL on
+ * failure (see the members' defmm_last_error). */
+typedef struct defmm_batch defmm_batch;
+defmm_batch* defmm_batch_create(int64_t n, defmm_handle* const* hs,
+                                const void* const* d_in, void* const* d_out,
+                                int lanes);
+/* One launch of every member's matvec on `stream` (a cudaStream_t; NULL is
+ * the legacy default stream), without synchronising. */
+int defmm_batch_launch(defmm_batch* b, void* stream);
+void defmm_batch_destroy(defmm_batch* b);
+
 /* Many right-hand sides at once (host vectors, rhs-major). */
 int defmm_gemv_batched(defmm_handle* h, int64_t nrhs, const double* in,
                        double* out);
