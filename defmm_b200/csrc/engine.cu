@@ -232,10 +232,6 @@ int upload_plan(defmm_handle* h) {
   }
   UP(p.perm, d.perm);
   UP(p.ptab_key, h->d_ptab_key);
-  std::vector<double> mats;
-  for (int k = 0; k < 2; k++) mats.insert(mats.end(), p.m2m[k].begin(), p.m2m[k].end());
-  for (int k = 0; k < 2; k++) mats.insert(mats.end(), p.l2l[k].begin(), p.l2l[k].end());
-  UP(mats, d.mats);
   std::vector<double> dirs;
   for (size_t e = 0; e < p.dirs.size() && e < 32; e++) {
     d.dir_off[e] = (int64_t)(dirs.size() / 3);
@@ -326,7 +322,10 @@ int prepare_precision(defmm_handle* h) {
   free_buf(h->ptab);
   h->ops = dfb::op_table(p.L, fp64);
   if (!h->ops) return h->fail(DEFMM_ERR_ARG, "unsupported order");
-  CK(h->ops->setup());
+  std::vector<double> mats;
+  for (int k = 0; k < 2; k++) mats.insert(mats.end(), p.m2m[k].begin(), p.m2m[k].end());
+  for (int k = 0; k < 2; k++) mats.insert(mats.end(), p.l2l[k].begin(), p.l2l[k].end());
+  CK(h->ops->setup(mats.data()));
   auto put = [&](DevBuf& b, const dfb::cplx* src, size_t n) -> int {
     int st = ensure(h, b, std::max<size_t>(1, n) * cs);
     if (st) return st;

@@ -4,7 +4,11 @@
 #include "fmm_kernels.h"
 
 #include <algorithm>
+#include <mutex>
+#include <set>
 #include <type_traits>
+#include <utility>
+#include <vector>
 
 namespace dfb {
 
@@ -108,6 +112,59 @@ __device__ __forceinline__ float2 expi<float2>(double a) {
   return expi_reduced(a);
 }
 
+// --------------------------------------------------------- constant tables --
+// Per order L = 2..8: the four L x L interpolation matrices (m2m[0], m2m[1],
+// l2l[0], l2l[1]; A(k, p) at k + p L) and the twiddles exp(-2 pi i m / P),
+// P = 2L - 1.  Every use sits in a fully unrolled loop, so the operands are
+// immediate constant-bank addresses rather than shared-memory loads.
+constexpr int kMinOrder = 2, kMaxOrder = 8;
+__host__ __device__ constexpr int mat_off(int L) {
+  int s = 0;
+  for (int l = kMinOrder; l < L; l++) s += 4 * l * l;
+  return s;
+}
+__host__ __device__ constexpr int tw_off(int L) {
+  int s = 0;
+  for (int l = kMinOrder; l < L; l++) s += 2 * l - 1;
+  return s;
+}
+__constant__ double c_mat64[mat_off(kMaxOrder + 1)];
+__constant__ float c_mat32[mat_off(kMaxOrder + 1)];
+__constant__ double c_tw64[2 * tw_off(kMaxOrder + 1)];
+__constant__ float c_tw32[2 * tw_off(kMaxOrder + 1)];
+
+template <typename T>
+__device__ __forceinline__ T cmat(int i);
+template <>
+__device__ __forceinline__ double cmat<double>(int i) {
+  return c_mat64[i];
+}
+template <>
+__device__ __forceinline__ float cmat<float>(int i) {
+  return c_mat32[i];
+}
+// twiddle exp(-2 pi i m / P) of order L, m in [0, P)
+template <typename T, int L>
+__device__ __forceinline__ typename cpx_t<T>::type ctw(int m) {
+  typename cpx_t<T>::type r;
+  if constexpr (sizeof(T) == 8) {
+    r.x = c_tw64[2 * (tw_off(L) + m)];
+    r.y = c_tw64[2 * (tw_off(L) + m) + 1];
+  } else {
+    r.x = c_tw32[2 * (tw_off(L) + m)];
+    r.y = c_tw32[2 * (tw_off(L) + m) + 1];
+  }
+  return r;
+}
+// acc += v * conj(w)
+template <typename C>
+__device__ __forceinline__ void cfmac(C& acc, C v, C w) {
+  acc.x = fma(v.x, w.x, acc.x);
+  acc.x = fma(v.y, w.y, acc.x);
+  acc.y = fma(v.y, w.x, acc.y);
+  acc.y = fma(-v.x, w.y, acc.y);
+}
+
 // ------------------------------------------------------------- gather/scatter
 template <typename T>
 __global__ void k_gather(const double2* __restrict__ qin, const int32_t* __restrict__ perm,
@@ -136,23 +193,120 @@ __global__ void k_scatter(const double2* __restrict__ pnear, const double2* __re
 }
 
 // -------------------------------------------------------------------- P2M --
-// One CTA (4 warps) per source leaf at a precomputed level (upwpass.hpp:39-47).
 // HF leaf (phfP2M, P2M.hpp:114-131), per effective direction d:
 //   M_d[l] = conj(sig2_d[l]) * sum_j Z(l, j) exp(-i k d.(y_j - c)) q_j
 // LF leaf (plfP2M, P2M.hpp:134-136): M[l] = sum_j Z(l, j) q_j,
 // with Z(l, j) = prod_k S_{I_k(l)}(y_jk - c_k) the leaf's interpolation matrix
 // (mapOnTrees.hpp:37-83).
+//
+// Per leaf this is the small GEMM  M[l][s] = sum_j Z[j][l] W[j][s],
+// W[j][s] = q_j exp(-i k d_s.(y_j - c)).  One CTA per leaf, in chunks of NPB
+// points: Z[j][l] is built once per chunk in shared memory (point-major, l
+// padded to LLP = 32 R); each warp takes S of the leaf's slots at a time,
+// writes their W column block, and every lane accumulates an R x S register
+// tile (expansion entries R lane .. R lane + R - 1, all S slots) over the
+// chunk's points: per point one R-wide load of Z and S broadcast loads of W
+// feed 2 R S FMAs.
+template <typename T, int L>
+struct P2MCfg {
+  static constexpr int LL = L * L * L;
+  static constexpr int R = L >= 5 ? 4 * ((LL + 127) / 128) : (LL + 31) / 32;  // entries per lane
+  static constexpr int LLP = 32 * R;
+  static constexpr int S0 = (sizeof(T) == 4 ? 32 : 16) / R;
+  static constexpr int S = S0 < 1 ? 1 : (S0 > (sizeof(T) == 4 ? 8 : 4) ? (sizeof(T) == 4 ? 8 : 4) : S0);
+  static constexpr int NPB0 = 65536 / (LLP * (int)sizeof(T));
+  static constexpr int NPB = NPB0 > 64 ? 64 : NPB0;  // points per chunk
+  typedef typename cpx_t<T>::type C;
+  // shared memory: Z, basis values, point offsets, charges, W blocks of 4 warps
+  static constexpr size_t smem() {
+    return sizeof(T) * (size_t)NPB * LLP + sizeof(double) * NPB * 3 + sizeof(T) * NPB * 3 * L + sizeof(C) * NPB +
+           sizeof(C) * 4 * NPB * S;
+  }
+};
+
+template <typename T, int L, int SS>
+__device__ __forceinline__ void p2m_group(const DevPlan& P, int64_t j0, int ns, bool hf, bool first, int np,
+                                          const T* __restrict__ Zs, const double* __restrict__ yc,
+                                          const typename cpx_t<T>::type* __restrict__ qs,
+                                          typename cpx_t<T>::type* __restrict__ Ws, const double* dirs,
+                                          const typename cpx_t<T>::type* __restrict__ s2,
+                                          typename cpx_t<T>::type* __restrict__ M, int lane) {
+  typedef typename cpx_t<T>::type C;
+  typedef P2MCfg<T, L> G;
+  constexpr int R = G::R, LLP = G::LLP, LL = G::LL;
+  __syncwarp();
+  for (int idx = lane; idx < np * SS; idx += 32) {
+    const int j = idx / SS, s = idx % SS;
+    C w = qs[j];
+    if (s >= ns) {
+      w = czero<C>();
+    } else if (hf) {
+      const double* dv = dirs + 3 * P.S_cdir[j0 + s];
+      double dp = 0.;
+      for (int k = 0; k < 3; k++) dp += dv[k] * yc[3 * j + k];
+      w = cmul(w, expi<C>(-P.kappa * dp));
+    }
+    Ws[j * SS + s] = w;
+  }
+  __syncwarp();
+  C acc[R][SS];
+#pragma unroll
+  for (int r = 0; r < R; r++)
+#pragma unroll
+    for (int s = 0; s < SS; s++) acc[r][s] = czero<C>();
+  const T* zl = Zs + lane * R;
+  for (int j = 0; j < np; j++) {
+    T z[R];
+    C w[SS];
+#pragma unroll
+    for (int r = 0; r < R; r++) z[r] = zl[j * LLP + r];
+#pragma unroll
+    for (int s = 0; s < SS; s++) w[s] = Ws[j * SS + s];
+#pragma unroll
+    for (int r = 0; r < R; r++)
+#pragma unroll
+      for (int s = 0; s < SS; s++) rfma(acc[r][s], z[r], w[s]);
+  }
+#pragma unroll
+  for (int s = 0; s < SS; s++) {
+    if (s < ns) {
+      const int slot = P.S_cslot[j0 + s], d = P.S_cdir[j0 + s];
+#pragma unroll
+      for (int r = 0; r < R; r++) {
+        const int l = lane * R + r;
+        if (l < LL) {
+          const C a = hf ? cmulc(s2[(int64_t)d * LL + l], acc[r][s]) : acc[r][s];
+          C* out = M + (int64_t)slot * LL + l;
+          if (first) {
+            *out = a;
+          } else {
+            C o = *out;
+            o.x += a.x;
+            o.y += a.y;
+            *out = o;
+          }
+        }
+      }
+    }
+  }
+}
+
 template <typename T, int L>
 __global__ void __launch_bounds__(128) k_p2m(DevPlan P, const int32_t* __restrict__ leaves, int nleaves,
                                              const typename cpx_t<T>::type* __restrict__ q,
                                              const typename cpx_t<T>::type* __restrict__ sig2,
                                              typename cpx_t<T>::type* __restrict__ M) {
   typedef typename cpx_t<T>::type C;
-  constexpr int LL = L * L * L;
-  constexpr int NPB = 64;
-  __shared__ T Bs[NPB][3][L];
-  __shared__ C wq[4][NPB];
+  typedef P2MCfg<T, L> G;
+  constexpr int LL = G::LL, LLP = G::LLP, NPB = G::NPB, S = G::S;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* Zs = reinterpret_cast<T*>(smem_raw);
+  double* yc = reinterpret_cast<double*>(Zs + (size_t)NPB * LLP);
+  T* Bs = reinterpret_cast<T*>(yc + NPB * 3);
+  C* qs = reinterpret_cast<C*>(Bs + NPB * 3 * L);
+  C* Wall = qs + NPB;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  C* Ws = Wall + warp * NPB * S;
   for (int li = blockIdx.x; li < nleaves; li += gridDim.x) {
     const int c = leaves[li];
     const int n = P.S_nprt[c], f = P.S_first[c];
@@ -161,54 +315,39 @@ __global__ void __launch_bounds__(128) k_p2m(DevPlan P, const int32_t* __restric
     const bool hf = P.ishf[lv] != 0;
     const int h = P.hfstage[lv];
     const int64_t sb = P.S_cptr[c], se = P.S_cptr[c + 1];
+    const int nslots = (int)(se - sb);
     const double* dirs = P.dirs + P.dir_off[h] * 3;
     const C* s2 = sig2 + P.sig_off[h];
     for (int p0 = 0; p0 < n; p0 += NPB) {
       const int np = min(NPB, n - p0);
-      __syncthreads();
+      __syncthreads();  // the previous chunk's Z, W are no longer read
       for (int o = threadIdx.x; o < 3 * np; o += blockDim.x) {
         const int p = o / 3, k = o % 3;
         const double x = P.S_pos[3 * (int64_t)(f + p0 + p) + k] - (&ct.x)[k];
+        yc[o] = x;
         T b[L];
         lagrange_all<L, T>((T)x, (T)ct.w, b);
 #pragma unroll
-        for (int l = 0; l < L; l++) Bs[p][k][l] = b[l];
+        for (int l = 0; l < L; l++) Bs[(p * 3 + k) * L + l] = b[l];
+      }
+      for (int p = threadIdx.x; p < np; p += blockDim.x) qs[p] = q[f + p0 + p];
+      __syncthreads();
+      for (int o = threadIdx.x; o < np * LLP; o += blockDim.x) {
+        const int p = o / LLP, l = o % LLP;
+        T z = 0;
+        if (l < LL) {
+          const int i0 = l / (L * L), i1 = (l / L) % L, i2 = l % L;
+          z = Bs[(p * 3 + 0) * L + i0] * Bs[(p * 3 + 1) * L + i1] * Bs[(p * 3 + 2) * L + i2];
+        }
+        Zs[o] = z;
       }
       __syncthreads();
-      for (int64_t j = sb + warp; j < se; j += 4) {
-        const int slot = P.S_cslot[j], d = P.S_cdir[j];
-        for (int p = lane; p < np; p += 32) {
-          C w = q[f + p0 + p];
-          if (hf) {
-            const double* y = P.S_pos + 3 * (int64_t)(f + p0 + p);
-            const double* dv = dirs + 3 * d;
-            double dp = 0.;
-            for (int k = 0; k < 3; k++) dp += dv[k] * (y[k] - (&ct.x)[k]);
-            C e = expi<C>(-P.kappa * dp);
-            w = cmul(w, e);
-          }
-          wq[warp][p] = w;
-        }
-        __syncwarp();
-        for (int l = lane; l < LL; l += 32) {
-          const int i0 = l / (L * L), i1 = (l / L) % L, i2 = l % L;
-          C acc = czero<C>();
-          for (int p = 0; p < np; p++) {
-            const T z = Bs[p][0][i0] * Bs[p][1][i1] * Bs[p][2][i2];
-            rfma(acc, z, wq[warp][p]);
-          }
-          if (hf) acc = cmulc(s2[(int64_t)d * LL + l], acc);
-          C* out = M + (int64_t)slot * LL + l;
-          if (p0 == 0) {
-            *out = acc;
-          } else {
-            C o = *out;
-            o.x += acc.x;
-            o.y += acc.y;
-            *out = o;
-          }
-        }
-        __syncwarp();
+      for (int g0 = warp * S; g0 < nslots; g0 += 4 * S) {
+        const int ns = min(S, nslots - g0);
+        if (ns == 1)
+          p2m_group<T, L, 1>(P, sb + g0, 1, hf, p0 == 0, np, Zs, yc, qs, Ws, dirs, s2, M, lane);
+        else
+          p2m_group<T, L, S>(P, sb + g0, ns, hf, p0 == 0, np, Zs, yc, qs, Ws, dirs, s2, M, lane);
       }
     }
   }
@@ -217,56 +356,58 @@ __global__ void __launch_bounds__(128) k_p2m(DevPlan P, const int32_t* __restric
 // ------------------------------------------------ separable 3-D transfer --
 // out[a,b,c] = sum A_s0(a,a') A_s1(b,b') A_s2(c,c') in[a',b',c'] computed in
 // three axis passes (axis 2, 1, 0 as interpolation.hpp:311-361); A(k, p) is
-// stored column-major mat[k + p*L].  One warp; in every pass a lane owns
-// whole lines (L inputs in registers -> L outputs).  After the last pass lane
-// ln holds the outputs (a, b, c) for a = 0..L-1 of its line(s) (b, c) = ln.
-template <typename T, int L>
-struct XferCfg {
-  // warps per CTA so that 2 LL-vectors per warp fit in 40 KB of shared memory
-  static constexpr int NW = (2 * L * L * L * (int)sizeof(typename cpx_t<T>::type) * 4 <= 40960) ? 4 : 2;
-};
-
-template <typename T, int L>
+// matrix 2*ROLE + s of the order's constant table (ROLE 0: M2M, 1: L2L).
+// One warp per transfer; lane ln owns line(s) ln, ln + 32 of each pass:
+//   axis 2 on (a, b) lines: input in registers (v), output to buf
+//   axis 1 on (a, c) lines: in place in buf (a lane's line is its own)
+//   axis 0 on (b, c) lines: from buf to registers (res)
+// The branch on each s is warp-uniform and keeps the matrix indices
+// compile-time constants.
+template <typename T, int L, int ROLE>
 struct Sep {
   typedef typename cpx_t<T>::type C;
   static constexpr int NLN = (L * L + 31) / 32;  // lines per lane
-  __device__ static __forceinline__ void run(const T* mats, int sg0, int sg1, int sg2, C* buf, C* buf2,
+  template <int MI>
+  __device__ static __forceinline__ void line(const C (&v)[L], C (&o)[L]) {
+    constexpr int B = mat_off(L) + MI * L * L;
+#pragma unroll
+    for (int k = 0; k < L; k++) {
+      C acc = czero<C>();
+#pragma unroll
+      for (int p = 0; p < L; p++) rfma(acc, cmat<T>(B + k + p * L), v[p]);
+      o[k] = acc;
+    }
+  }
+  __device__ static __forceinline__ void apply(int s, const C (&v)[L], C (&o)[L]) {
+    if (s)
+      line<2 * ROLE + 1>(v, o);
+    else
+      line<2 * ROLE>(v, o);
+  }
+  __device__ static __forceinline__ void run(int sg0, int sg1, int sg2, const C (&v)[NLN][L], C* buf,
                                              C (&res)[NLN][L], int lane) {
-    const T* m2 = mats + sg2 * L * L;
-    const T* m1 = mats + sg1 * L * L;
-    const T* m0 = mats + sg0 * L * L;
 #pragma unroll
     for (int q = 0; q < NLN; q++) {  // axis 2: lines (a, b)
       const int ln = lane + 32 * q;
       if (ln < L * L) {
-        C v[L];
+        C o[L];
+        apply(sg2, v[q], o);
 #pragma unroll
-        for (int p = 0; p < L; p++) v[p] = buf[ln * L + p];
-#pragma unroll
-        for (int k = 0; k < L; k++) {
-          C acc = czero<C>();
-#pragma unroll
-          for (int p = 0; p < L; p++) rfma(acc, m2[k + p * L], v[p]);
-          buf2[ln * L + k] = acc;
-        }
+        for (int k = 0; k < L; k++) buf[ln * L + k] = o[k];
       }
     }
     __syncwarp();
 #pragma unroll
-    for (int q = 0; q < NLN; q++) {  // axis 1: lines (a, c)
+    for (int q = 0; q < NLN; q++) {  // axis 1: lines (a, c), in place
       const int ln = lane + 32 * q;
       if (ln < L * L) {
         const int a = ln / L, c = ln % L;
-        C v[L];
+        C w[L], o[L];
 #pragma unroll
-        for (int p = 0; p < L; p++) v[p] = buf2[(a * L + p) * L + c];
+        for (int p = 0; p < L; p++) w[p] = buf[(a * L + p) * L + c];
+        apply(sg1, w, o);
 #pragma unroll
-        for (int k = 0; k < L; k++) {
-          C acc = czero<C>();
-#pragma unroll
-          for (int p = 0; p < L; p++) rfma(acc, m1[k + p * L], v[p]);
-          buf[(a * L + k) * L + c] = acc;
-        }
+        for (int k = 0; k < L; k++) buf[(a * L + k) * L + c] = o[k];
       }
     }
     __syncwarp();
@@ -274,16 +415,10 @@ struct Sep {
     for (int q = 0; q < NLN; q++) {  // axis 0: lines (b, c)
       const int ln = lane + 32 * q;
       if (ln < L * L) {
-        C v[L];
+        C w[L];
 #pragma unroll
-        for (int p = 0; p < L; p++) v[p] = buf[p * L * L + ln];
-#pragma unroll
-        for (int k = 0; k < L; k++) {
-          C acc = czero<C>();
-#pragma unroll
-          for (int p = 0; p < L; p++) rfma(acc, m0[k + p * L], v[p]);
-          res[q][k] = acc;
-        }
+        for (int p = 0; p < L; p++) w[p] = buf[p * L * L + ln];
+        apply(sg0, w, res[q]);
       }
     }
     __syncwarp();
@@ -295,17 +430,19 @@ struct Sep {
 //   HF parent, direction d (hfM2Mblock M2M.hpp:76-105 / lf2hfM2M :108-124):
 //     M_d = conj(sig2_d) o sum_c exp(-i k d.v_c) A_{v_c}(sig_d o M_c)
 //   LF parent (lfM2M :35-41): M = sum_c A_{v_c}(M_c);   v_c = ctr_c - ctr_parent
+// A lane reads its (a, b) lines of each child's expansion straight into
+// registers (the next child's are prefetched during the current transfer).
+constexpr int kXferWarps = 4;  // warps (transfers in flight) per CTA
+
 template <typename T, int L>
-__global__ void __launch_bounds__(128) k_m2m(DevPlan P, int64_t s0, int64_t s1,
-                                             const typename cpx_t<T>::type* __restrict__ sig,
-                                             const typename cpx_t<T>::type* __restrict__ sig2,
-                                             typename cpx_t<T>::type* __restrict__ M) {
+__global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 4 ? 6 : (L == 5 ? 5 : 3)) : (L <= 5 ? 3 : 1)) k_m2m(DevPlan P, int64_t s0, int64_t s1,
+                                                         const typename cpx_t<T>::type* __restrict__ sig,
+                                                         const typename cpx_t<T>::type* __restrict__ sig2,
+                                                         typename cpx_t<T>::type* __restrict__ M) {
   typedef typename cpx_t<T>::type C;
-  constexpr int LL = L * L * L, NW = XferCfg<T, L>::NW, NLN = Sep<T, L>::NLN;
-  __shared__ T mats[2 * L * L];
-  __shared__ C sbuf[NW][2][LL];
-  for (int i = threadIdx.x; i < 2 * L * L; i += blockDim.x) mats[i] = (T)P.mats[i];
-  __syncthreads();
+  typedef Sep<T, L, 0> S;
+  constexpr int LL = L * L * L, NW = kXferWarps, NLN = S::NLN;
+  __shared__ C sbuf[NW][LL];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int64_t ps = s0 + blockIdx.x * NW + warp; ps < s1; ps += (int64_t)gridDim.x * NW) {
     const int64_t eb = P.m2m_ptr[ps], ee = P.m2m_ptr[ps + 1];
@@ -320,11 +457,19 @@ __global__ void __launch_bounds__(128) k_m2m(DevPlan P, int64_t s0, int64_t s1,
     double dv[3] = {0., 0., 0.};
     if (hf)
       for (int k = 0; k < 3; k++) dv[k] = P.dirs[3 * (P.dir_off[h] + d) + k];
-    C acc[NLN][L];
+    // with one line per lane (L <= 5) the parent's signature line and the
+    // next child's lines stay in registers; larger orders reload them
+    constexpr bool REG = NLN == 1;
+    C acc[NLN][L], sgr[REG ? NLN : 1][L];
 #pragma unroll
-    for (int q = 0; q < NLN; q++)
+    for (int q = 0; q < NLN; q++) {
+      const int ln = lane + 32 * q;
 #pragma unroll
-      for (int k = 0; k < L; k++) acc[q][k] = czero<C>();
+      for (int k = 0; k < L; k++) {
+        acc[q][k] = czero<C>();
+        if (REG) sgr[0][k] = (hf && ln < L * L) ? sg[ln * L + k] : czero<C>();
+      }
+    }
     // children metadata fetched by lane (<= 8 children), broadcast below
     const int nch = (int)(ee - eb);
     int my_cs = 0;
@@ -333,38 +478,40 @@ __global__ void __launch_bounds__(128) k_m2m(DevPlan P, int64_t s0, int64_t s1,
       my_cs = P.m2m_child[eb + lane];
       my_ct = P.S_ctr[P.sS_cell[my_cs]];
     }
-    constexpr int NV = (LL + 31) / 32;
-    C nxt[NV];  // next child's expansion, prefetched
-    {
-      const int cs0 = __shfl_sync(0xffffffffu, my_cs, 0);
+    C nxt[REG ? NLN : 1][L];  // next child's (a, b) lines, prefetched
+    if (REG) {
+      const C* Mc = M + (int64_t)__shfl_sync(0xffffffffu, my_cs, 0) * LL;
 #pragma unroll
-      for (int m = 0; m < NV; m++) {
-        const int l = lane + 32 * m;
-        nxt[m] = l < LL ? M[(int64_t)cs0 * LL + l] : czero<C>();
-      }
+      for (int k = 0; k < L; k++) nxt[0][k] = lane < L * L ? Mc[lane * L + k] : czero<C>();
     }
     for (int e = 0; e < nch; e++) {
       const double cx = __shfl_sync(0xffffffffu, my_ct.x, e), cy = __shfl_sync(0xffffffffu, my_ct.y, e),
                    cz = __shfl_sync(0xffffffffu, my_ct.z, e);
       const double v[3] = {cx - pct.x, cy - pct.y, cz - pct.z};
-      __syncwarp();
+      C in[NLN][L];
+      if (REG) {
 #pragma unroll
-      for (int m = 0; m < NV; m++) {
-        const int l = lane + 32 * m;
-        if (l < LL) sbuf[warp][0][l] = hf ? cmul(sg[l], nxt[m]) : nxt[m];
-      }
-      if (e + 1 < nch) {
-        const int csn = __shfl_sync(0xffffffffu, my_cs, e + 1);
+        for (int k = 0; k < L; k++) in[0][k] = hf ? cmul(sgr[0][k], nxt[0][k]) : nxt[0][k];
+        if (e + 1 < nch) {
+          const C* Mc = M + (int64_t)__shfl_sync(0xffffffffu, my_cs, e + 1) * LL;
 #pragma unroll
-        for (int m = 0; m < NV; m++) {
-          const int l = lane + 32 * m;
-          if (l < LL) nxt[m] = M[(int64_t)csn * LL + l];
+          for (int k = 0; k < L; k++)
+            if (lane < L * L) nxt[0][k] = Mc[lane * L + k];
+        }
+      } else {
+        const C* Mc = M + (int64_t)__shfl_sync(0xffffffffu, my_cs, e) * LL;
+#pragma unroll
+        for (int q = 0; q < NLN; q++) {
+          const int ln = lane + 32 * q;
+#pragma unroll
+          for (int k = 0; k < L; k++) {
+            const C m = ln < L * L ? Mc[ln * L + k] : czero<C>();
+            in[q][k] = (hf && ln < L * L) ? cmul(sg[ln * L + k], m) : m;
+          }
         }
       }
-      __syncwarp();
       C res[NLN][L];
-      Sep<T, L>::run(mats, v[0] < 0. ? 0 : 1, v[1] < 0. ? 0 : 1, v[2] < 0. ? 0 : 1, sbuf[warp][0],
-                     sbuf[warp][1], res, lane);
+      S::run(v[0] < 0. ? 0 : 1, v[1] < 0. ? 0 : 1, v[2] < 0. ? 0 : 1, in, sbuf[warp], res, lane);
       if (hf) {
         const C ph = expi<C>(-P.kappa * (dv[0] * v[0] + dv[1] * v[1] + dv[2] * v[2]));
 #pragma unroll
@@ -400,16 +547,14 @@ __global__ void __launch_bounds__(128) k_m2m(DevPlan P, int64_t s0, int64_t s1,
 //     L_c += sum_d exp(i k v.d) conj(sig_d) o B_v(sig2_d o L_d)
 //   LF parent (lfL2L :35-41): L_c += B_v(L_p);   v = ctr_child - ctr_parent
 template <typename T, int L>
-__global__ void __launch_bounds__(128) k_l2l(DevPlan P, int64_t s0, int64_t s1,
-                                             const typename cpx_t<T>::type* __restrict__ sig,
-                                             const typename cpx_t<T>::type* __restrict__ sig2,
-                                             typename cpx_t<T>::type* __restrict__ Lx) {
+__global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 5 ? 6 : 3) : (L <= 5 ? 3 : 1)) k_l2l(DevPlan P, int64_t s0, int64_t s1,
+                                                         const typename cpx_t<T>::type* __restrict__ sig,
+                                                         const typename cpx_t<T>::type* __restrict__ sig2,
+                                                         typename cpx_t<T>::type* __restrict__ Lx) {
   typedef typename cpx_t<T>::type C;
-  constexpr int LL = L * L * L, NW = XferCfg<T, L>::NW, NLN = Sep<T, L>::NLN;
-  __shared__ T mats[2 * L * L];
-  __shared__ C sbuf[NW][2][LL];
-  for (int i = threadIdx.x; i < 2 * L * L; i += blockDim.x) mats[i] = (T)P.mats[2 * L * L + i];
-  __syncthreads();
+  typedef Sep<T, L, 1> S;
+  constexpr int LL = L * L * L, NW = kXferWarps, NLN = S::NLN;
+  __shared__ C sbuf[NW][LL];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int64_t cs = s0 + blockIdx.x * NW + warp; cs < s1; cs += (int64_t)gridDim.x * NW) {
     const int64_t eb = P.l2l_ptr[cs], ee = P.l2l_ptr[cs + 1];
@@ -434,37 +579,43 @@ __global__ void __launch_bounds__(128) k_l2l(DevPlan P, int64_t s0, int64_t s1,
       my_ps = P.l2l_parent[eb + lane];
       my_d = P.sT_dir[my_ps];
     }
-    constexpr int NV = (LL + 31) / 32;
-    C nxt[NV];
-    {
-      const int ps0 = __shfl_sync(0xffffffffu, my_ps, 0);
+    // with one line per lane (L <= 5) the next parent's lines are
+    // prefetched into registers; larger orders load them when used
+    constexpr bool REG = NLN == 1;
+    C nxt[REG ? NLN : 1][L];
+    if (REG) {
+      const C* Lp = Lx + (int64_t)__shfl_sync(0xffffffffu, my_ps, 0) * LL;
 #pragma unroll
-      for (int m = 0; m < NV; m++) {
-        const int l = lane + 32 * m;
-        nxt[m] = l < LL ? Lx[(int64_t)ps0 * LL + l] : czero<C>();
-      }
+      for (int k = 0; k < L; k++) nxt[0][k] = lane < L * L ? Lp[lane * L + k] : czero<C>();
     }
     for (int e = 0; e < npa; e++) {
       const int d = __shfl_sync(0xffffffffu, my_d, e);
       const C* sg = sig + P.sig_off[h] + (int64_t)(hf ? d : 0) * LL;
       const C* sgq = sig2 + P.sig_off[h] + (int64_t)(hf ? d : 0) * LL;
-      __syncwarp();
+      C in[NLN][L];
+      if (REG) {
 #pragma unroll
-      for (int m = 0; m < NV; m++) {
-        const int l = lane + 32 * m;
-        if (l < LL) sbuf[warp][0][l] = hf ? cmul(sgq[l], nxt[m]) : nxt[m];
-      }
-      if (e + 1 < npa) {
-        const int psn = __shfl_sync(0xffffffffu, my_ps, e + 1);
+        for (int k = 0; k < L; k++) in[0][k] = (hf && lane < L * L) ? cmul(sgq[lane * L + k], nxt[0][k]) : nxt[0][k];
+        if (e + 1 < npa) {
+          const C* Lp = Lx + (int64_t)__shfl_sync(0xffffffffu, my_ps, e + 1) * LL;
 #pragma unroll
-        for (int m = 0; m < NV; m++) {
-          const int l = lane + 32 * m;
-          if (l < LL) nxt[m] = Lx[(int64_t)psn * LL + l];
+          for (int k = 0; k < L; k++)
+            if (lane < L * L) nxt[0][k] = Lp[lane * L + k];
+        }
+      } else {
+        const C* Lp = Lx + (int64_t)__shfl_sync(0xffffffffu, my_ps, e) * LL;
+#pragma unroll
+        for (int q = 0; q < NLN; q++) {
+          const int ln = lane + 32 * q;
+#pragma unroll
+          for (int k = 0; k < L; k++) {
+            const C m = ln < L * L ? Lp[ln * L + k] : czero<C>();
+            in[q][k] = (hf && ln < L * L) ? cmul(sgq[ln * L + k], m) : m;
+          }
         }
       }
-      __syncwarp();
       C res[NLN][L];
-      Sep<T, L>::run(mats, sg0, sg1, sg2i, sbuf[warp][0], sbuf[warp][1], res, lane);
+      S::run(sg0, sg1, sg2i, in, sbuf[warp], res, lane);
       if (hf) {
         const double* dv = P.dirs + 3 * (P.dir_off[h] + d);
         const C ph = expi<C>(P.kappa * (v[0] * dv[0] + v[1] * dv[1] + v[2] * dv[2]));
@@ -511,7 +662,7 @@ template <typename T, int L>
 struct M2FCfg {
   typedef typename cpx_t<T>::type C;
   static constexpr int P = 2 * L - 1, LL = L * L * L;
-  static constexpr int PER_WARP = P + LL + L * L * P + L * P * P;  // complex elements
+  static constexpr int PER_WARP = LL + L * L * P + L * P * P;  // complex elements
   // warps per CTA so that a CTA's shared memory stays within ~48 KB
   static constexpr int NW0 = (int)(49152 / (PER_WARP * sizeof(C)));
   static constexpr int NW = NW0 < 1 ? 1 : (NW0 > 8 ? 8 : NW0);
@@ -525,16 +676,9 @@ __global__ void __launch_bounds__(256) k_m2f(int64_t n, const typename cpx_t<T>:
   constexpr int NW = M2FCfg<T, L>::NW, PER = M2FCfg<T, L>::PER_WARP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  C* W = reinterpret_cast<C*>(smem_raw) + warp * PER;
-  C* Mi = W + P;
+  C* Mi = reinterpret_cast<C*>(smem_raw) + warp * PER;
   C* A = Mi + LL;
   C* B = A + L * L * P;
-  for (int m = lane; m < P; m += 32) {
-    double s, c;
-    sincospi(-2.0 * m / P, &s, &c);
-    W[m].x = (T)c;
-    W[m].y = (T)s;
-  }
   for (int64_t e = (int64_t)blockIdx.x * NW + warp; e < n; e += (int64_t)gridDim.x * NW) {
     __syncwarp();
     for (int i = lane; i < LL; i += 32) Mi[i] = M[e * LL + i];
@@ -547,7 +691,7 @@ __global__ void __launch_bounds__(256) k_m2f(int64_t n, const typename cpx_t<T>:
       for (int k2 = 0; k2 < P; k2++) {
         C acc = v[0];
 #pragma unroll
-        for (int c = 1; c < L; c++) cfma(acc, v[c], W[(k2 * c) % P]);
+        for (int c = 1; c < L; c++) cfma(acc, v[c], ctw<T, L>((k2 * c) % P));
         A[ln * P + k2] = acc;
       }
     }
@@ -561,7 +705,7 @@ __global__ void __launch_bounds__(256) k_m2f(int64_t n, const typename cpx_t<T>:
       for (int k1 = 0; k1 < P; k1++) {
         C acc = v[0];
 #pragma unroll
-        for (int b = 1; b < L; b++) cfma(acc, v[b], W[(k1 * b) % P]);
+        for (int b = 1; b < L; b++) cfma(acc, v[b], ctw<T, L>((k1 * b) % P));
         B[(a * P + k1) * P + k2] = acc;
       }
     }
@@ -574,7 +718,7 @@ __global__ void __launch_bounds__(256) k_m2f(int64_t n, const typename cpx_t<T>:
       for (int k0 = 0; k0 < P; k0++) {
         C acc = v[0];
 #pragma unroll
-        for (int a = 1; a < L; a++) cfma(acc, v[a], W[(k0 * a) % P]);
+        for (int a = 1; a < L; a++) cfma(acc, v[a], ctw<T, L>((k0 * a) % P));
         F[e * PP + k0 * P * P + ln] = acc;
       }
     }
@@ -611,16 +755,9 @@ __global__ void __launch_bounds__(NT, (sizeof(T) == 8 ? 512 : 1024) / NT) k_m2l(
   typedef typename cpx_t<T>::type C;
   constexpr int PD = 2 * L - 1, LL = L * L * L, PP = PD * PD * PD, K = (PP + NT - 1) / NT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* W = reinterpret_cast<C*>(smem_raw);
-  C* Js = W + PD;
+  C* Js = reinterpret_cast<C*>(smem_raw);
   C* Cb = Js + PP;
   C* D = Cb + L * PD * PD;
-  for (int m = threadIdx.x; m < PD; m += blockDim.x) {
-    double s, c;
-    sincospi(2.0 * m / PD, &s, &c);
-    W[m].x = (T)c;
-    W[m].y = (T)s;
-  }
   const T inv = T(1) / T(PP);
   __shared__ int64_t cur;
   // target slots are taken in order from a queue, so the slots in flight
@@ -664,7 +801,7 @@ __global__ void __launch_bounds__(NT, (sizeof(T) == 8 ? 512 : 1024) / NT) k_m2l(
       for (int a = 0; a < L; a++) {
         C s = v[0];
 #pragma unroll
-        for (int k0 = 1; k0 < PD; k0++) cfma(s, v[k0], W[(k0 * a) % PD]);
+        for (int k0 = 1; k0 < PD; k0++) cfmac(s, v[k0], ctw<T, L>((k0 * a) % PD));
         Cb[a * PD * PD + ln] = s;
       }
     }
@@ -678,7 +815,7 @@ __global__ void __launch_bounds__(NT, (sizeof(T) == 8 ? 512 : 1024) / NT) k_m2l(
       for (int b = 0; b < L; b++) {
         C s = v[0];
 #pragma unroll
-        for (int k1 = 1; k1 < PD; k1++) cfma(s, v[k1], W[(k1 * b) % PD]);
+        for (int k1 = 1; k1 < PD; k1++) cfmac(s, v[k1], ctw<T, L>((k1 * b) % PD));
         D[(a * L + b) * PD + k2] = s;
       }
     }
@@ -692,7 +829,7 @@ __global__ void __launch_bounds__(NT, (sizeof(T) == 8 ? 512 : 1024) / NT) k_m2l(
       for (int c = 0; c < L; c++) {
         C s = v[0];
 #pragma unroll
-        for (int k2 = 1; k2 < PD; k2++) cfma(s, v[k2], W[(k2 * c) % PD]);
+        for (int k2 = 1; k2 < PD; k2++) cfmac(s, v[k2], ctw<T, L>((k2 * c) % PD));
         C o = Lt[ln * L + c];
         o.x += s.x * inv;
         o.y += s.y * inv;
@@ -1374,6 +1511,56 @@ __global__ void k_direct(int64_t ns, const double* __restrict__ spos, const int3
 
 // ---------------------------------------------------------------- launch --
 namespace {
+// twiddles exp(-2 pi i m / P) of every order, computed on the device
+__global__ void k_twiddles(double* tw) {
+  for (int L = kMinOrder; L <= kMaxOrder; L++) {
+    const int P = 2 * L - 1;
+    for (int m = threadIdx.x; m < P; m += blockDim.x) {
+      double s, c;
+      sincospi(-2.0 * m / P, &s, &c);
+      tw[2 * (tw_off(L) + m)] = c;
+      tw[2 * (tw_off(L) + m) + 1] = s;
+    }
+  }
+}
+
+// Constant tables of the current device: twiddles of every order on first
+// use, the interpolation matrices of order L (m2m[0], m2m[1], l2l[0], l2l[1];
+// they depend on L only) on first use of L.  Later calls write nothing, so
+// kernels of other operators in flight never see a table change.
+cudaError_t upload_tables(int L, const double* mats) {
+  static std::mutex mu;
+  static std::set<std::pair<int, int>> done;  // (device, L); L = 0: twiddles
+  std::lock_guard<std::mutex> lock(mu);
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (!done.count({dev, 0})) {
+    constexpr int n = 2 * tw_off(kMaxOrder + 1);
+    double* d = nullptr;
+    if ((e = cudaMalloc(&d, n * sizeof(double))) != cudaSuccess) return e;
+    k_twiddles<<<1, 32>>>(d);
+    std::vector<double> h64(n);
+    e = cudaMemcpy(h64.data(), d, n * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return e;
+    std::vector<float> h32(h64.begin(), h64.end());
+    if ((e = cudaMemcpyToSymbol(c_tw64, h64.data(), n * sizeof(double))) != cudaSuccess ||
+        (e = cudaMemcpyToSymbol(c_tw32, h32.data(), n * sizeof(float))) != cudaSuccess)
+      return e;
+    done.insert({dev, 0});
+  }
+  if (!done.count({dev, L})) {
+    const int n = 4 * L * L;
+    std::vector<float> m32(mats, mats + n);
+    if ((e = cudaMemcpyToSymbol(c_mat64, mats, n * sizeof(double), mat_off(L) * sizeof(double))) != cudaSuccess ||
+        (e = cudaMemcpyToSymbol(c_mat32, m32.data(), n * sizeof(float), mat_off(L) * sizeof(float))) != cudaSuccess)
+      return e;
+    done.insert({dev, L});
+  }
+  return cudaSuccess;
+}
+
 int grid_for(int64_t n, int per_block, int cap = 148 * 64) {
   int64_t g = (n + per_block - 1) / per_block;
   if (g < 1) g = 1;
@@ -1388,24 +1575,30 @@ struct Launch {
   static constexpr int P = 2 * L - 1, LL = L * L * L, PP = P * P * P;
   static constexpr int NT = PP > 1024 ? 256 : 128;
   static size_t smem_m2f() { return sizeof(C) * M2FCfg<T, L>::PER_WARP * M2FCfg<T, L>::NW; }
-  static size_t smem_m2l() { return sizeof(C) * (P + PP + L * P * P + L * L * P); }
-  static cudaError_t setup() {
+  static size_t smem_m2l() { return sizeof(C) * (PP + L * P * P + L * L * P); }
+  static cudaError_t setup(const double* mats) {
+    cudaError_t e0 = upload_tables(L, mats);
+    if (e0 != cudaSuccess) return e0;
     cudaError_t e = cudaFuncSetAttribute(k_m2f<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_m2f());
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_p2m<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P2MCfg<T, L>::smem());
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_m2l<T, L, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_m2l());
   }
   static void p2m(const DevPlan& dp, const int32_t* leaves, int n, const void* q, const void* sig2, void* M,
                   cudaStream_t s) {
-    if (n) k_p2m<T, L><<<grid_for(n, 1), 128, 0, s>>>(dp, leaves, n, (const C*)q, (const C*)sig2, (C*)M);
+    if (n)
+      k_p2m<T, L><<<grid_for(n, 1), 128, P2MCfg<T, L>::smem(), s>>>(dp, leaves, n, (const C*)q, (const C*)sig2,
+                                                                    (C*)M);
   }
   static void m2m(const DevPlan& dp, int64_t s0, int64_t s1, const void* sig, const void* sig2, void* M,
                   cudaStream_t s) {
-    constexpr int NW = XferCfg<T, L>::NW;
+    constexpr int NW = kXferWarps;
     if (s1 > s0) k_m2m<T, L><<<grid_for(s1 - s0, NW), 32 * NW, 0, s>>>(dp, s0, s1, (const C*)sig, (const C*)sig2, (C*)M);
   }
   static void l2l(const DevPlan& dp, int64_t s0, int64_t s1, const void* sig, const void* sig2, void* Lx,
                   cudaStream_t s) {
-    constexpr int NW = XferCfg<T, L>::NW;
+    constexpr int NW = kXferWarps;
     if (s1 > s0) k_l2l<T, L><<<grid_for(s1 - s0, NW), 32 * NW, 0, s>>>(dp, s0, s1, (const C*)sig, (const C*)sig2, (C*)Lx);
   }
   static void m2f(int64_t n, const void* M, void* F, cudaStream_t s) {

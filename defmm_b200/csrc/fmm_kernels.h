@@ -11,7 +11,9 @@ namespace dfb {
 // Per-(precision, order) launchers of the expansion phases.  Complex arrays
 // are passed untyped; their element type is double2 (FP64) or float2.
 struct OpTable {
-  cudaError_t (*setup)();
+  // per-order kernel attributes and constant tables; mats = m2m[0], m2m[1],
+  // l2l[0], l2l[1] (L*L each, A(k, p) at k + p*L)
+  cudaError_t (*setup)(const double* mats);
   void (*p2m)(const DevPlan&, const int32_t* leaves, int n, const void* q, const void* sig2, void* M, cudaStream_t);
   void (*m2m)(const DevPlan&, int64_t s0, int64_t s1, const void* sig, const void* sig2, void* M, cudaStream_t);
   void (*l2l)(const DevPlan&, int64_t s0, int64_t s1, const void* sig, const void* sig2, void* Lx, cudaStream_t);

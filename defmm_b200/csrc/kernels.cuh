@@ -67,7 +67,6 @@ struct DevPlan {
   const int32_t *m2m_child, *l2l_parent, *m2l_src;
   const uint32_t* m2l_tab;
   const uint16_t* perm;
-  const double* mats;                          // m2m[0], m2m[1], l2l[0], l2l[1] (L*L each)
   const double* dirs;                          // all stages, 3 per direction
   int64_t dir_off[32];                         // per stage
   int64_t sig_off[32];                         // per stage, in complex elements
