@@ -962,51 +962,42 @@ __device__ __forceinline__ void sincos_reduced(double theta, float& s, float& c)
 // groups take interleaved sources of the tile, two at a time.  Partial sums
 // are reduced in FP64 through shuffles and shared memory; each target is
 // written once.
-//   MIXED = false: FP64 throughout (P2P.hpp:43-79 arithmetic).
-//   MIXED = true : difference vector, r^2, r (FP32 sqrt + one FP64 Newton
-//   step) and the reduction of k r in FP64; sin/cos of the reduced angle,
-//   1/(4 pi r) and the complex products in FP32, accumulated in FP64.
-// One source/target interaction.  Source record in shared memory: a = (x, y),
-// b = (z, charge) with the FP32 charge bits in b.y (mixed) or the FP64
-// charge in c (FP64 path).
-template <bool MIXED>
-__device__ __forceinline__ void p2p_pair(double x0, double x1, double x2, double2 a, double2 b, double2 qd,
-                                         double kappa, double& pr, double& pim) {
+//   MIXED = false: FP64 throughout (P2P.hpp:43-79 arithmetic, p2p_pair64).
+//   MIXED = true : difference vector, r^2, 1/r and the reduction of k r in
+//   FP64; sin/cos of the reduced angle, 1/(4 pi r) and the complex products
+//   in FP32 with compensated sums (p2p_pair_mixed).
+// Source record in shared memory: a = (x, y), b = (z, charge) with the FP32
+// charge bits in b.y (mixed) or the FP64 charge in c (FP64 path).
+
+// Approximate FP64 reciprocal square root (the PTX instruction
+// rsqrt.approx.ftz.f64, about FP32 accuracy); callers refine it by Newton
+// steps y <- y (3/2 - R y^2 / 2), each of which doubles the correct bits.
+__device__ __forceinline__ double rsqrt_approx64(double x) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  return y;
+}
+
+// One FP64 source/target interaction.
+__device__ __forceinline__ void p2p_pair64(double x0, double x1, double x2, double2 a, double2 b, double2 qd,
+                                           double kappa, double& pr, double& pim) {
   const double pi4m1 = 1. / (4. * 3.14159265358979323846);
   const double dx = x0 - a.x, dy = x1 - a.y, dz = x2 - b.x;
   const double R = fma(dx, dx, fma(dy, dy, dz * dz));
   if (R < 1.e-16) return;  // self / duplicate pairs (P2P.hpp:66)
-  if (!MIXED) {
-    // 1/sqrt(R): FP32 estimate, two Newton steps in FP64 (quadratic: 2^-22 -> 2^-88)
-    double y = (double)rsqrtf((float)R);
-    const double hR = 0.5 * R;
-    y = y * fma(-hR * y, y, 1.5);
-    y = y * fma(-hR * y, y, 1.5);
-    const double rr = y * R * kappa;
-    const double K = y * pi4m1;
-    double sn_, cs_;
-    sincos_cw(rr, sn_, cs_);
-    cs_ *= K;
-    sn_ *= K;
-    pr = fma(cs_, qd.x, fma(-sn_, qd.y, pr));
-    pim = fma(cs_, qd.y, fma(sn_, qd.x, pim));
-  } else {
-    // r to ~1e-14 relative: FP32 reciprocal square root refined once in
-    // FP32, one Newton step for r in FP64 (rf^2 is exact in FP64)
-    const float Rf = (float)R;
-    float y = rsqrtf(Rf);
-    y = y * fmaf(-0.5f * Rf * y, y, 1.5f);
-    const float rf = Rf * y;
-    const double rr = fma(R - (double)rf * (double)rf, (double)(0.5f * y), (double)rf);
-    float s, c;
-    sincos_reduced(rr * kappa, s, c);
-    const float K = (float)pi4m1 * y;
-    c *= K;
-    s *= K;
-    const float2 q = *reinterpret_cast<const float2*>(&b.y);
-    pr += (double)fmaf(c, q.x, -s * q.y);
-    pim += (double)fmaf(c, q.y, s * q.x);
-  }
+  // 1/sqrt(R): approximate FP64 estimate, two Newton steps (quadratic)
+  double y = rsqrt_approx64(R);
+  const double hR = 0.5 * R;
+  y = y * fma(-hR * y, y, 1.5);
+  y = y * fma(-hR * y, y, 1.5);
+  const double rr = y * R * kappa;
+  const double K = y * pi4m1;
+  double sn_, cs_;
+  sincos_cw(rr, sn_, cs_);
+  cs_ *= K;
+  sn_ *= K;
+  pr = fma(cs_, qd.x, fma(-sn_, qd.y, pr));
+  pim = fma(cs_, qd.y, fma(sn_, qd.x, pim));
 }
 
 // Compensated (Kahan) FP32 summation: s - c carries the sum.
@@ -1018,9 +1009,9 @@ __device__ __forceinline__ void kahan_add(float& s, float& c, float x) {
 }
 
 // Mixed-precision interaction with FP32 compensated accumulators (the FP64
-// path keeps p2p_pair<false>).  r = sqrt(R): FP32 reciprocal square root
-// refined once in FP32 (used for 1/(4 pi r)), widened and refined once in
-// FP64 (relative error ~1e-14) for k r.  k r = n pi + x with n read from the
+// path keeps p2p_pair<false>).  1/r: approximate FP64 reciprocal square root
+// refined once in FP64 (relative error ~1e-14), used for k r, and rounded to
+// FP32 for 1/(4 pi r).  k r = n pi + x with n read from the
 // low mantissa bits of k r / pi + 1.5 * 2^52 (exact for k r / pi < 2^51) and
 // x = k r - n pi in FP64; sin/cos of x by the FP32 Taylor polynomials of
 // sincos_reduced, (-1)^n applied to both.
@@ -1029,11 +1020,9 @@ __device__ __forceinline__ void p2p_pair_mixed(double x0, double x1, double x2, 
   const double dx = x0 - a.x, dy = x1 - a.y, dz = x2 - b.x;
   const double R = fma(dx, dx, fma(dy, dy, dz * dz));
   if (R < 1.e-16) return;  // self / duplicate pairs (P2P.hpp:66)
-  const float Rf = (float)R;
-  float y = rsqrtf(Rf);
-  y = y * fmaf(-0.5f * Rf * y, y, 1.5f);
-  double yd = (double)y;
+  double yd = rsqrt_approx64(R);
   yd = yd * fma(-0.5 * R * yd, yd, 1.5);
+  const float y = (float)yd;
   const double theta = R * yd * kappa;
   const double t = fma(theta, 0.31830988618379067154, 6755399441055744.0);  // + 1.5 * 2^52
   const double n = t - 6755399441055744.0;
@@ -1133,10 +1122,10 @@ __global__ void __launch_bounds__(128) k_p2p_tiled(DevPlan P, int64_t nitem, con
         if (j < fill) p2p_pair_mixed(x0, x1, x2, sa[j], sb[j], P.kappa, sr, cr, si, ci);
       } else {
         for (; j + G < fill; j += 2 * G) {
-          p2p_pair<false>(x0, x1, x2, sa[j], sb[j], sc[j], P.kappa, pr, pim);
-          p2p_pair<false>(x0, x1, x2, sa[j + G], sb[j + G], sc[j + G], P.kappa, pr, pim);
+          p2p_pair64(x0, x1, x2, sa[j], sb[j], sc[j], P.kappa, pr, pim);
+          p2p_pair64(x0, x1, x2, sa[j + G], sb[j + G], sc[j + G], P.kappa, pr, pim);
         }
-        if (j < fill) p2p_pair<false>(x0, x1, x2, sa[j], sb[j], sc[j], P.kappa, pr, pim);
+        if (j < fill) p2p_pair64(x0, x1, x2, sa[j], sb[j], sc[j], P.kappa, pr, pim);
       }
     }
     if constexpr (MIXED) {
@@ -1194,7 +1183,7 @@ __device__ __forceinline__ double2 green64(double dx, double dy, double dz, doub
   const bool skip = R0 < 1.e-16;
   const double R = skip ? 1. : R0;
   const double pi4m1 = skip ? 0. : 1. / (4. * 3.14159265358979323846);
-  double y = (double)rsqrtf((float)R);
+  double y = rsqrt_approx64(R);
   const double hR = 0.5 * R;
   y = y * fma(-hR * y, y, 1.5);
   y = y * fma(-hR * y, y, 1.5);
@@ -1207,11 +1196,9 @@ __device__ __forceinline__ float2 green32(double dx, double dy, double dz, doubl
   const double R0 = fma(dx, dx, fma(dy, dy, dz * dz));
   const bool skip = R0 < 1.e-16;
   const double R = skip ? 1. : R0;
-  const float Rf = (float)R;
-  float y = rsqrtf(Rf);
-  y = y * fmaf(-0.5f * Rf * y, y, 1.5f);
-  double yd = (double)y;
+  double yd = rsqrt_approx64(R);
   yd = yd * fma(-0.5 * R * yd, yd, 1.5);
+  const float y = (float)yd;
   const double theta = R * yd * kappa;
   const double t = fma(theta, 0.31830988618379067154, 6755399441055744.0);  // + 1.5 * 2^52
   const double n = t - 6755399441055744.0;
