@@ -213,6 +213,104 @@ def run_ragged(args, torch):
     batches.clear()
 
 
+def run_spheroid(args, torch):
+    """Spheroid with semi-axes (1, 0.5, 0.25), N = 4,000,000, density
+    1 + 4|z|, 256 wavelengths along the long axis, order 6, leaf 96, mixed
+    precision only: the FP64 path would hold M and L for 2 x 33.3M
+    expansion slots of 216 entries (230 GB), beyond the 180 GB of one B200.
+    Accuracy: FP64 direct sums at 2,000 seeded targets."""
+    from defmm_b200 import IBFMM_Mat, workloads as W
+    w = W.spheroid(4_000_000, seed=0)
+    q = W.charges(w.n, 1)
+    A = IBFMM_Mat()
+    A.set_precision("mixed")
+    A.addSourceParticles(w.points)
+    A.addTargetParticles(w.points)
+    t0 = time.perf_counter()
+    A.prcmpt(w.order, w.ncrit, w.kappa)
+    setup_s = time.perf_counter() - t0
+    A.upload()
+    info = A.info()
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    dq = torch.from_numpy(q).to("cuda")
+    dp = torch.empty(w.n, dtype=torch.complex128, device="cuda")
+    for _ in range(args.warmup):
+        A.matvec_device(dq.data_ptr(), dp.data_ptr(), 1, stream.cuda_stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(0) as ck:
+        e0.record(stream)
+        for _ in range(args.steps):
+            A.matvec_device(dq.data_ptr(), dp.data_ptr(), 1, stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    A.matvec(q)
+    chk = A.check_full(2000, seed=7)
+    A.set_profiling(True)
+    A.matvec_device(dq.data_ptr(), dp.data_ptr(), 1, stream.cuda_stream)
+    torch.cuda.synchronize()
+    phases = A.phase_times()
+    A.set_profiling(False)
+    line = {"metric": "FMM matvec points/s, mixed precision, spheroid", "impl": "ours",
+            "value": w.n / (ms * 1e-3), "unit": "points/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "dtype": "f32+f64",
+            "data": "synthetic",
+            "config": {"workload": "spheroid4m", "n_points": w.n, "kappa": w.kappa, "order": w.order,
+                       "leaf_size": w.ncrit, "precision": "mixed",
+                       "fp64": "not run: M and L would need 230 GB"},
+            "accuracy": {"direct_sum_2000_targets": chk}, "clocks": ck.summary(), "phases_ms": phases,
+            "setup_s": setup_s, "device_bytes": A.info("device_bytes"),
+            "plan": {k: info[k] for k in ["nlvl", "cpt", "slots_S", "slots_T", "far_hf", "near", "i_near",
+                                          "tables", "permuted_spectra"]}}
+    print(json.dumps(line), flush=True)
+
+
+def run_orders(args, torch):
+    """Error against FP64 direct sums (2,000 seeded targets) and time per
+    matvec for orders 4-7, FP64 and mixed, on the spheroid at the 4M
+    workload's points per square wavelength: N = 500,000, 90.5 wavelengths
+    along the long axis, leaf 96."""
+    from defmm_b200 import IBFMM_Mat, workloads as W
+    n = 500_000
+    rows = []
+    for L in (4, 5, 6, 7):
+        w = W.spheroid(n, seed=0, order=L, wavelengths=256.0 * math.sqrt(n / 4_000_000))
+        q = W.charges(w.n, 1)
+        A = IBFMM_Mat()
+        A.addSourceParticles(w.points)
+        A.addTargetParticles(w.points)
+        A.prcmpt(w.order, w.ncrit, w.kappa)
+        stream = torch.cuda.Stream()
+        dq = torch.from_numpy(q).to("cuda")
+        dp = torch.empty(w.n, dtype=torch.complex128, device="cuda")
+        row = {"order": L}
+        out = {}
+        for prec in ("fp64", "mixed"):
+            A.set_precision(prec)
+            for _ in range(args.warmup):
+                A.matvec_device(dq.data_ptr(), dp.data_ptr(), 1, stream.cuda_stream)
+            stream.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                A.matvec_device(dq.data_ptr(), dp.data_ptr(), 1, stream.cuda_stream)
+            e1.record(stream)
+            stream.synchronize()
+            out[prec] = A.matvec(q)
+            row[prec] = {"ms": e0.elapsed_time(e1) / args.steps, "vs_direct": A.check_full(2000, seed=7)}
+        row["mixed_vs_fp64_rel_l2"] = float(np.linalg.norm(out["mixed"] - out["fp64"]) / np.linalg.norm(out["fp64"]))
+        rows.append(row)
+        del A
+    line = {"metric": "FMM error vs FP64 direct sums and ms per matvec by order, spheroid", "impl": "ours",
+            "unit": "relative error", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "data": "synthetic",
+            "config": {"workload": "spheroid_orders", "n_points": n, "leaf_size": 96,
+                       "wavelengths_long_axis": 256.0 * math.sqrt(n / 4_000_000)},
+            "orders": rows}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -244,9 +342,10 @@ def main():
         if dist:
             dist.barrier()
 
-    if args.workload == "ragged48":
+    if args.workload in ("ragged48", "spheroid4m", "spheroid_orders"):
         if rank == 0:
-            run_ragged(args, torch)
+            {"ragged48": run_ragged, "spheroid4m": run_spheroid, "spheroid_orders": run_orders}[args.workload](
+                args, torch)
         return
 
     from defmm_b200 import IBFMM_Mat, replicas, workloads as W

@@ -1225,10 +1225,11 @@ __device__ __forceinline__ float2 green32(double dx, double dy, double dz, doubl
 // tp steps of a symmetric block: lane ls owns one source (y, qj) and meets
 // target (ls + step) mod tp; the target's running sum moves one lane down per
 // step.  TP = 32 fixes the segment width at compile time.
-// Target records in shared memory: (x, y, z, w) with w the FP32 charge's
-// bits (mixed path; two 16-byte loads per step) or unused (FP64 path, the
-// charge in tq).  Entry j holds target j mod tp (j < 64), so step st of lane
-// ls reads entry ls + st without wrapping arithmetic.
+// Target records in shared memory as two 16-byte arrays, (x, y) and (z, w)
+// with w the FP32 charge's bits (mixed path) or unused (FP64 path, the charge
+// in tq): one conflict-free 16-byte load from each per step.  Entry j holds
+// target j mod tp (j < 64), so step st of lane ls reads entry ls + st without
+// wrapping arithmetic.
 __device__ __forceinline__ float2 charge_bits(double w) {
   const long long b = __double_as_longlong(w);
   return make_float2(__int_as_float((int)(b & 0xffffffffLL)), __int_as_float((int)(b >> 32)));
@@ -1240,25 +1241,27 @@ __device__ __forceinline__ double charge_word(float2 q) {
 template <bool MIXED, int TP>
 __device__ __forceinline__ void sym_steps(int ls, int tp_rt, double yx, double yy, double yz,
                                           typename std::conditional<MIXED, float2, double2>::type qj,
-                                          const double4* tr, const double2* tq, double kappa,
+                                          const double2* trxy, const double2* trzw, const double2* tq,
+                                          double kappa,
                                           typename std::conditional<MIXED, float2, double2>::type& accD,
                                           typename std::conditional<MIXED, float2, double2>::type& accT) {
   const int tp = TP ? TP : tp_rt;
   constexpr int UNR = MIXED ? 4 : 1;
 #pragma unroll UNR
-  const double4* trl = tr + ls;
+  const double2* txy = trxy + ls;
+  const double2* tzw = trzw + ls;
   const double2* tql = tq + ls;
   for (int st = 0; st < tp; st++) {
-    const double4 t = trl[st];
+    const double2 a = txy[st], b = tzw[st];
     if constexpr (MIXED) {
-      const float2 g = green32(t.x - yx, t.y - yy, t.z - yz, kappa);
-      const float2 qi = charge_bits(t.w);
+      const float2 g = green32(a.x - yx, a.y - yy, b.x - yz, kappa);
+      const float2 qi = charge_bits(b.y);
       accD.x = fmaf(g.x, qj.x, fmaf(-g.y, qj.y, accD.x));
       accD.y = fmaf(g.x, qj.y, fmaf(g.y, qj.x, accD.y));
       accT.x = fmaf(g.x, qi.x, fmaf(-g.y, qi.y, accT.x));
       accT.y = fmaf(g.x, qi.y, fmaf(g.y, qi.x, accT.y));
     } else {
-      const double2 g = green64(t.x - yx, t.y - yy, t.z - yz, kappa);
+      const double2 g = green64(a.x - yx, a.y - yy, b.x - yz, kappa);
       const double2 qi = tql[st];
       accD.x = fma(g.x, qj.x, fma(-g.y, qj.y, accD.x));
       accD.y = fma(g.x, qj.y, fma(g.y, qj.x, accD.y));
@@ -1294,7 +1297,7 @@ __global__ void __launch_bounds__(128) k_p2p_sym(DevPlan P, int64_t nwork, const
   constexpr int RMAX = 128;
   const Q* q = static_cast<const Q*>(qv);
   Q* scr = static_cast<Q*>(scratch);
-  __shared__ double4 tr[64];
+  __shared__ double2 trxy[64], trzw[64];
   __shared__ double2 tq[64];  // FP64 path: target charges
   __shared__ int32_t rpre[RMAX + 1], rfst[RMAX];
   __shared__ int64_t roff[RMAX];
@@ -1324,9 +1327,11 @@ __global__ void __launch_bounds__(128) k_p2p_sym(DevPlan P, int64_t nwork, const
         } else {
           tq[j] = qt;
         }
-        tr[j] = make_double4(x[0], x[1], x[2], w);
+        trxy[j] = make_double2(x[0], x[1]);
+        trzw[j] = make_double2(x[2], w);
       } else {
-        tr[j] = make_double4(0., 0., 0., 0.);
+        trxy[j] = make_double2(0., 0.);
+        trzw[j] = make_double2(0., 0.);
         tq[j] = make_double2(0., 0.);
       }
     }
@@ -1382,9 +1387,9 @@ __global__ void __launch_bounds__(128) k_p2p_sym(DevPlan P, int64_t nwork, const
         // no validity tests: padded targets and missing sources carry zero
         // charges, and their target sums are never stored
         if (tp == 32)
-          sym_steps<MIXED, 32>(ls, 32, yx, yy, yz, qj, tr, tq, P.kappa, accD, accT);
+          sym_steps<MIXED, 32>(ls, 32, yx, yy, yz, qj, trxy, trzw, tq, P.kappa, accD, accT);
         else
-          sym_steps<MIXED, 0>(ls, tp, yx, yy, yz, qj, tr, tq, P.kappa, accD, accT);
+          sym_steps<MIXED, 0>(ls, tp, yx, yy, yz, qj, trxy, trzw, tq, P.kappa, accD, accT);
         if constexpr (MIXED) {
           kahan_add(sr, cr, accD.x);
           kahan_add(si, ci, accD.y);

@@ -97,7 +97,8 @@ def sphere_surface(n: int = 2_000_000, seed: int = 0, wavelengths: float = 128.0
                     2.0 * math.pi * wavelengths / 2.0, order, ncrit)
 
 
-def spheroid(n: int = 4_000_000, seed: int = 0, order: int = 6, ncrit: int = 96) -> Workload:
+def spheroid(n: int = 4_000_000, seed: int = 0, order: int = 6, ncrit: int = 96,
+             wavelengths: float = 256.0) -> Workload:
     rng = np.random.default_rng(seed)
     a = np.array([1.0, 0.5, 0.25])
     out = []
@@ -112,7 +113,7 @@ def spheroid(n: int = 4_000_000, seed: int = 0, order: int = 6, ncrit: int = 96)
         need -= out[-1].shape[0]
     pts = np.concatenate(out)[:n]
     return Workload("spheroid", np.ascontiguousarray(pts),
-                    2.0 * math.pi * 256.0 / 2.0, order, ncrit)
+                    2.0 * math.pi * wavelengths / 2.0, order, ncrit)
 
 
 def gaussian_blobs(n: int, seed: int = 0, nblobs: int = 8, sigma: float = 0.05,
