@@ -267,6 +267,46 @@ def run_spheroid(args, torch):
     print(json.dumps(line), flush=True)
 
 
+def run_rhs64(args, torch):
+    """64 right-hand sides (complex charges with FP32-representable parts
+    uniform in [-1, 1]) on the 2M-point sphere (k = 2 pi 64, order 5, leaf
+    64), mixed precision: one defmm_gemv_device call with nrhs = 64 per step
+    (each right-hand side replays the operator's captured graph)."""
+    from defmm_b200 import IBFMM_Mat, workloads as W
+    w = W.sphere_surface(2_000_000, seed=0)
+    nrhs = 64
+    Q = W.charges(w.n, 5, nrhs=nrhs).astype(np.complex64).astype(np.complex128)
+    A = IBFMM_Mat()
+    A.set_precision("mixed")
+    A.addSourceParticles(w.points)
+    A.addTargetParticles(w.points)
+    A.prcmpt(w.order, w.ncrit, w.kappa)
+    stream = torch.cuda.Stream()
+    dq = torch.from_numpy(Q).to("cuda")
+    dp = torch.empty((nrhs, w.n), dtype=torch.complex128, device="cuda")
+    for _ in range(max(1, args.warmup - 2)):
+        A.matvec_device(dq.data_ptr(), dp.data_ptr(), nrhs, stream.cuda_stream)
+    stream.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(0) as ck:
+        e0.record(stream)
+        for _ in range(args.steps):
+            A.matvec_device(dq.data_ptr(), dp.data_ptr(), nrhs, stream.cuda_stream)
+        e1.record(stream)
+        stream.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    one = A.matvec(Q[nrhs - 1])
+    same = bool(np.array_equal(dp[nrhs - 1].cpu().numpy(), one))
+    line = {"metric": "FMM matvec points/s over 64 right-hand sides, mixed precision", "impl": "ours",
+            "value": nrhs * w.n / (ms * 1e-3), "unit": "points/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "ms_per_rhs": ms / nrhs, "higher_is_better": True,
+            "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": "rhs64", "n_points": w.n, "nrhs": nrhs, "kappa": w.kappa, "order": w.order,
+                       "leaf_size": w.ncrit, "precision": "mixed"},
+            "last_rhs_equals_single_call": same, "clocks": ck.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def run_orders(args, torch):
     """Error against FP64 direct sums (2,000 seeded targets) and time per
     matvec for orders 4-7, FP64 and mixed, on the spheroid at the 4M
@@ -342,10 +382,11 @@ def main():
         if dist:
             dist.barrier()
 
-    if args.workload in ("ragged48", "spheroid4m", "spheroid_orders"):
+    extra = {"ragged48": run_ragged, "spheroid4m": run_spheroid, "spheroid_orders": run_orders,
+             "rhs64": run_rhs64}
+    if args.workload in extra:
         if rank == 0:
-            {"ragged48": run_ragged, "spheroid4m": run_spheroid, "spheroid_orders": run_orders}[args.workload](
-                args, torch)
+            extra[args.workload](args, torch)
         return
 
     from defmm_b200 import IBFMM_Mat, replicas, workloads as W

@@ -83,6 +83,12 @@ def lib():
             "defmm_batch_destroy": (None, [vp]),
             "defmm_dump_tree": (ctypes.c_int, [vp, ctypes.c_int, ip, dp, ip, ctypes.POINTER(i64), ip]),
             "defmm_dump_lists": (ctypes.c_int, [vp, ip, ip, ip, ctypes.POINTER(i64)]),
+            "defmm_mlp_forward": (ctypes.c_int, [vp, vp, i64, vp, vp, vp, vp]),
+            "defmm_mlp_backward": (ctypes.c_int, [vp, vp, vp, vp, vp, vp, vp, ctypes.c_float, i64, vp, vp, vp,
+                                                  vp]),
+            "defmm_mlp_adam": (ctypes.c_int, [vp, vp, vp, vp, i64, ctypes.c_float, ctypes.c_float, vp]),
+            "defmm_mlp_to_bf16": (ctypes.c_int, [vp, vp, vp]),
+            "defmm_mlp_infer_bf16": (ctypes.c_int, [vp, vp, i64, vp, vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)

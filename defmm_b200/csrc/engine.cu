@@ -51,6 +51,7 @@ struct defmm_handle {
   int64_t f_cap = 0;  // source slots per F batch buffer
   // FP64 vectors
   DevBuf pnear, pfar, qin, out, chk;
+  DevBuf rin, rout;  // staging of device multi-RHS calls (defmm_gemv_device, nrhs > 1)
   const int32_t *d_p2m_leaf = nullptr, *d_l2p_leaf = nullptr;
   const int32_t *d_tfirst = nullptr, *d_tn = nullptr, *d_sfirst = nullptr, *d_sn = nullptr;
   const int64_t* d_p2p_ptr = nullptr;
@@ -170,6 +171,8 @@ void free_plan_device(defmm_handle* h) {
   free_buf(h->pfar);
   free_buf(h->qin);
   free_buf(h->out);
+  free_buf(h->rin);
+  free_buf(h->rout);
   free_buf(h->chk);
   free_buf(h->pscr);
   h->use_sym = false;
@@ -768,9 +771,15 @@ int defmm_gemv_device(defmm_handle* h, const void* d_in, void* d_out, int64_t nr
   cudaStream_t s = stream ? (cudaStream_t)stream : h->st;
   h->launches = 0;
   const int64_t nS = (int64_t)h->plan.S.perm.size(), nT = (int64_t)h->plan.T.perm.size();
+  if (nrhs == 1) return matvec(h, (const double2*)d_in, (double2*)d_out, s);
+  // several right-hand sides: staged through the handle's own vectors so that
+  // every one replays the same captured graph (one device copy each way)
+  if ((st = ensure(h, h->rin, 16 * nS)) || (st = ensure(h, h->rout, 16 * nT))) return st;
   for (int64_t r = 0; r < nrhs; r++) {
-    st = matvec(h, (const double2*)d_in + r * nS, (double2*)d_out + r * nT, s);
+    CK(cudaMemcpyAsync(h->rin.p, (const double2*)d_in + r * nS, 16 * nS, cudaMemcpyDeviceToDevice, s));
+    st = matvec(h, (const double2*)h->rin.p, (double2*)h->rout.p, s);
     if (st) return st;
+    CK(cudaMemcpyAsync((double2*)d_out + r * nT, h->rout.p, 16 * nT, cudaMemcpyDeviceToDevice, s));
   }
   return 0;
 }
@@ -954,7 +963,7 @@ int defmm_info(const defmm_handle* h, int what, int64_t* v) {
     case DEFMM_INFO_DEVICE_BYTES:
       *v = (int64_t)(h->dev_bytes + h->M.bytes + h->Lx.bytes + h->F.bytes + h->q.bytes + h->sig.bytes +
                      h->sig2.bytes + h->ptab.bytes + h->pnear.bytes + h->pfar.bytes +
-                     h->qin.bytes + h->out.bytes);
+                     h->qin.bytes + h->out.bytes + h->rin.bytes + h->rout.bytes);
       break;
     case DEFMM_INFO_LIST_RECORDS: *v = p.keep_lists ? 1 : 0; break;
     case DEFMM_INFO_LAUNCHES: *v = h->launches; break;

@@ -878,12 +878,34 @@ __global__ void __launch_bounds__(128) k_l2p(DevPlan P, const int32_t* __restric
         lagrange_all<L, T>((T)xr[k], (T)ct.w, B[k]);
       }
       double2 acc = make_double2(0., 0.);
-      for (int64_t j = sb + warp; j < se; j += 4) {
-        const int slot = P.T_cslot[j], d = P.T_cdir[j];
+      // the next slot's expansion (and signature) is loaded into registers
+      // while the current one is contracted
+      constexpr int NV = (LL + 31) / 32;
+      C nl[NV], ns[NV];
+      int nd = 0;
+      auto fetch = [&](int64_t j) {
+        const int slot = P.T_cslot[j];
+        nd = P.T_cdir[j];
         const C* Ls = Lx + (int64_t)slot * LL;
+        const C* Ss = s2 + (int64_t)(hf ? nd : 0) * LL;
+#pragma unroll
+        for (int m = 0; m < NV; m++) {
+          const int l = lane + 32 * m;
+          nl[m] = l < LL ? Ls[l] : czero<C>();
+          ns[m] = (hf && l < LL) ? Ss[l] : czero<C>();
+        }
+      };
+      if (sb + warp < se) fetch(sb + warp);
+      for (int64_t j = sb + warp; j < se; j += 4) {
+        const int d = nd;
         __syncwarp();
-        for (int l = lane; l < LL; l += 32) buf[warp][l] = hf ? cmul(s2[(int64_t)d * LL + l], Ls[l]) : Ls[l];
+#pragma unroll
+        for (int m = 0; m < NV; m++) {
+          const int l = lane + 32 * m;
+          if (l < LL) buf[warp][l] = hf ? cmul(ns[m], nl[m]) : nl[m];
+        }
         __syncwarp();
+        if (j + 4 < se) fetch(j + 4);
         // sum_{a,b,c} B0[a] B1[b] B2[c] X[a,b,c] = sum_a B0[a] (sum_b B1[b] (sum_c B2[c] X[a,b,c]))
         C sum = czero<C>();
 #pragma unroll

@@ -88,7 +88,9 @@ int defmm_gemv(defmm_handle* h, const double* in, double* out);
 
 /* Device-resident form: d_in / d_out are device pointers to nrhs stacked
  * complex vectors (rhs-major, each in user order).  Runs on `stream`
- * (a cudaStream_t; NULL = the handle's own stream) without synchronising. */
+ * (a cudaStream_t; NULL = the handle's own stream) without synchronising.
+ * With nrhs > 1 each right-hand side is copied into and out of the handle's
+ * own device vectors, so all of them replay one captured graph. */
 int defmm_gemv_device(defmm_handle* h, const void* d_in, void* d_out,
                       int64_t nrhs, void* stream);
 
@@ -208,6 +210,41 @@ int defmm_dump_tree(const defmm_handle* h, int which, int32_t* cells_int,
  * in n[3].  Pointers may be NULL to query the counts. */
 int defmm_dump_lists(const defmm_handle* h, int32_t* far_hf, int32_t* far_lf,
                      int32_t* near_, int64_t n[3]);
+
+/* No counterpart in the reference.  Order-selection network (learned.py):
+ * a perceptron DEFMM_MLP_IN -> DEFMM_MLP_HIDDEN -> DEFMM_MLP_HIDDEN ->
+ * DEFMM_MLP_OUT (ReLU, ReLU, logits over interpolation orders 3..8) that
+ * predicts the lowest order meeting a requested accuracy from problem
+ * features.  Parameters: one flat FP32 array of DEFMM_MLP_PARAMS values,
+ * W1 (64 x 12, row-major), b1, W2 (64 x 64), b2, W3 (6 x 64), b3.  All
+ * pointers are device pointers; calls run on `stream` (a cudaStream_t, NULL
+ * the legacy default stream) without synchronising. */
+#define DEFMM_MLP_IN 12
+#define DEFMM_MLP_HIDDEN 64
+#define DEFMM_MLP_OUT 6
+#define DEFMM_MLP_PARAMS 5382
+/* FP32 forward of n samples X (n x 12): activations H1, H2 (n x 64), logits
+ * (n x 6). */
+int defmm_mlp_forward(const float* params, const float* X, int64_t n, float* H1,
+                      float* H2, float* logits, void* stream);
+/* Gradient of the weighted softmax cross-entropy
+ * sum_i w_i (-log softmax(logits_i)[y_i]) / wsum (w NULL: all 1) into grads
+ * (DEFMM_MLP_PARAMS floats) and its value into *loss (device float);
+ * scratch: n * (6 + 2 * 64) floats. */
+int defmm_mlp_backward(const float* params, const float* X, const float* H1,
+                       const float* H2, const float* logits, const int32_t* y,
+                       const float* w, float wsum, int64_t n, float* grads,
+                       float* loss, float* scratch, void* stream);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8, bias-corrected at `step` >= 1)
+ * on params with moments m, v, and decoupled weight decay wd >= 0:
+ * p -= lr (mhat / (sqrt(vhat) + eps) + wd p). */
+int defmm_mlp_adam(float* params, const float* grads, float* m, float* v,
+                   int64_t step, float lr, float wd, void* stream);
+/* BF16 copy of the parameters (round to nearest even), for inference. */
+int defmm_mlp_to_bf16(const float* params, uint16_t* out, void* stream);
+/* Inference with BF16 parameters and FP32 accumulation: logits (n x 6). */
+int defmm_mlp_infer_bf16(const uint16_t* params_bf16, const float* X, int64_t n,
+                         float* logits, void* stream);
 
 #ifdef __cplusplus
 }
