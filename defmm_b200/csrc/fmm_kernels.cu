@@ -679,10 +679,33 @@ __global__ void __launch_bounds__(256) k_m2f(int64_t n, const typename cpx_t<T>:
   C* Mi = reinterpret_cast<C*>(smem_raw) + warp * PER;
   C* A = Mi + LL;
   C* B = A + L * L * P;
-  for (int64_t e = (int64_t)blockIdx.x * NW + warp; e < n; e += (int64_t)gridDim.x * NW) {
+  // the next expansion is loaded into registers while the current one is
+  // transformed
+  constexpr int NV = (LL + 31) / 32;
+  const int64_t e0 = (int64_t)blockIdx.x * NW + warp, de = (int64_t)gridDim.x * NW;
+  C nx[NV];
+  if (e0 < n) {
+#pragma unroll
+    for (int m = 0; m < NV; m++) {
+      const int i = lane + 32 * m;
+      nx[m] = i < LL ? M[e0 * LL + i] : czero<C>();
+    }
+  }
+  for (int64_t e = e0; e < n; e += de) {
     __syncwarp();
-    for (int i = lane; i < LL; i += 32) Mi[i] = M[e * LL + i];
+#pragma unroll
+    for (int m = 0; m < NV; m++) {
+      const int i = lane + 32 * m;
+      if (i < LL) Mi[i] = nx[m];
+    }
     __syncwarp();
+    if (e + de < n) {
+#pragma unroll
+      for (int m = 0; m < NV; m++) {
+        const int i = lane + 32 * m;
+        if (i < LL) nx[m] = M[(e + de) * LL + i];
+      }
+    }
     for (int ln = lane; ln < L * L; ln += 32) {  // axis 2: (a,b) lines
       C v[L];
 #pragma unroll
