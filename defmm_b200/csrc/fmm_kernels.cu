@@ -384,6 +384,49 @@ struct Sep {
     else
       line<2 * ROLE>(v, o);
   }
+  // The same transfer with the passes in the order axis 0, 1, 2: the input
+  // lines run along axis 0 (v[q][p] = in[p, b, c] for line (b, c) = ln, so a
+  // warp reads an expansion with unit stride across lanes), res holds lines
+  // (a, b) = ln along axis 2 (res[q][k] = out[a, b, k]).
+  __device__ static __forceinline__ void run_a0(int sg0, int sg1, int sg2, const C (&v)[NLN][L], C* buf,
+                                                C (&res)[NLN][L], int lane) {
+#pragma unroll
+    for (int q = 0; q < NLN; q++) {  // axis 0: lines (b, c)
+      const int ln = lane + 32 * q;
+      if (ln < L * L) {
+        C o[L];
+        apply(sg0, v[q], o);
+#pragma unroll
+        for (int k = 0; k < L; k++) buf[k * L * L + ln] = o[k];
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < NLN; q++) {  // axis 1: lines (a, c), in place
+      const int ln = lane + 32 * q;
+      if (ln < L * L) {
+        const int a = ln / L, c = ln % L;
+        C w[L], o[L];
+#pragma unroll
+        for (int p = 0; p < L; p++) w[p] = buf[(a * L + p) * L + c];
+        apply(sg1, w, o);
+#pragma unroll
+        for (int k = 0; k < L; k++) buf[(a * L + k) * L + c] = o[k];
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < NLN; q++) {  // axis 2: lines (a, b)
+      const int ln = lane + 32 * q;
+      if (ln < L * L) {
+        C w[L];
+#pragma unroll
+        for (int p = 0; p < L; p++) w[p] = buf[ln * L + p];
+        apply(sg2, w, res[q]);
+      }
+    }
+    __syncwarp();
+  }
   __device__ static __forceinline__ void run(int sg0, int sg1, int sg2, const C (&v)[NLN][L], C* buf,
                                              C (&res)[NLN][L], int lane) {
 #pragma unroll
@@ -430,8 +473,9 @@ struct Sep {
 //   HF parent, direction d (hfM2Mblock M2M.hpp:76-105 / lf2hfM2M :108-124):
 //     M_d = conj(sig2_d) o sum_c exp(-i k d.v_c) A_{v_c}(sig_d o M_c)
 //   LF parent (lfM2M :35-41): M = sum_c A_{v_c}(M_c);   v_c = ctr_c - ctr_parent
-// A lane reads its (a, b) lines of each child's expansion straight into
-// registers (the next child's are prefetched during the current transfer).
+// A lane reads its (b, c) lines (along axis 0) of each child's expansion
+// straight into registers, lanes at unit stride (the next child's are
+// prefetched during the current transfer); the transfer runs axis 0 first.
 constexpr int kXferWarps = 4;  // warps (transfers in flight) per CTA
 
 template <typename T, int L>
@@ -467,7 +511,7 @@ __global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 4 ? 6 
 #pragma unroll
       for (int k = 0; k < L; k++) {
         acc[q][k] = czero<C>();
-        if (REG) sgr[0][k] = (hf && ln < L * L) ? sg[ln * L + k] : czero<C>();
+        if (REG) sgr[0][k] = (hf && ln < L * L) ? sg[k * L * L + ln] : czero<C>();
       }
     }
     // children metadata fetched by lane (<= 8 children), broadcast below
@@ -482,7 +526,7 @@ __global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 4 ? 6 
     if (REG) {
       const C* Mc = M + (int64_t)__shfl_sync(0xffffffffu, my_cs, 0) * LL;
 #pragma unroll
-      for (int k = 0; k < L; k++) nxt[0][k] = lane < L * L ? Mc[lane * L + k] : czero<C>();
+      for (int k = 0; k < L; k++) nxt[0][k] = lane < L * L ? Mc[k * L * L + lane] : czero<C>();
     }
     for (int e = 0; e < nch; e++) {
       const double cx = __shfl_sync(0xffffffffu, my_ct.x, e), cy = __shfl_sync(0xffffffffu, my_ct.y, e),
@@ -496,7 +540,7 @@ __global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 4 ? 6 
           const C* Mc = M + (int64_t)__shfl_sync(0xffffffffu, my_cs, e + 1) * LL;
 #pragma unroll
           for (int k = 0; k < L; k++)
-            if (lane < L * L) nxt[0][k] = Mc[lane * L + k];
+            if (lane < L * L) nxt[0][k] = Mc[k * L * L + lane];
         }
       } else {
         const C* Mc = M + (int64_t)__shfl_sync(0xffffffffu, my_cs, e) * LL;
@@ -505,13 +549,13 @@ __global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 4 ? 6 
           const int ln = lane + 32 * q;
 #pragma unroll
           for (int k = 0; k < L; k++) {
-            const C m = ln < L * L ? Mc[ln * L + k] : czero<C>();
-            in[q][k] = (hf && ln < L * L) ? cmul(sg[ln * L + k], m) : m;
+            const C m = ln < L * L ? Mc[k * L * L + ln] : czero<C>();
+            in[q][k] = (hf && ln < L * L) ? cmul(sg[k * L * L + ln], m) : m;
           }
         }
       }
       C res[NLN][L];
-      S::run(v[0] < 0. ? 0 : 1, v[1] < 0. ? 0 : 1, v[2] < 0. ? 0 : 1, in, sbuf[warp], res, lane);
+      S::run_a0(v[0] < 0. ? 0 : 1, v[1] < 0. ? 0 : 1, v[2] < 0. ? 0 : 1, in, sbuf[warp], res, lane);
       if (hf) {
         const C ph = expi<C>(-P.kappa * (dv[0] * v[0] + dv[1] * v[1] + dv[2] * v[2]));
 #pragma unroll
@@ -534,7 +578,7 @@ __global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 4 ? 6 
       if (ln < L * L)
 #pragma unroll
         for (int k = 0; k < L; k++) {
-          const int l = k * L * L + ln;
+          const int l = ln * L + k;
           M[ps * LL + l] = hf ? cmulc(sg2[l], acc[q][k]) : acc[q][k];
         }
     }

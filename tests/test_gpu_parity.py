@@ -46,6 +46,19 @@ def test_fp64_matches_oracle_and_reference_samples(name, gpu):
     assert rel(p[sample_index(trg.shape[0])], sample) <= FP64_TOL
 
 
+@pytest.mark.parametrize("order", [2, 3, 7, 8])
+def test_orders_outside_the_golden_cases_match_oracle(order, gpu):
+    # the golden cases run orders 4-6; the order-selection network also picks
+    # 3, 7 and 8, and the kernels are instantiated for 2-8
+    w = W.sphere_surface(8000, seed=21, wavelengths=6.0)
+    q = W.charges(w.n, 4)
+    A = make(w.points, w.points, order, 64, w.kappa)
+    p = A.matvec(q)
+    assert rel(p, O.OracleFMM(w.points, w.points, order, 64, w.kappa, -1).gemv(q)) <= FP64_TOL
+    A.set_precision("mixed")
+    assert rel(A.matvec(q), p) <= MIXED_TOL
+
+
 @pytest.mark.parametrize("name", ["cube20k", "cube_lf", "blobs_sphere", "cube_laplace"])
 def test_mixed_matches_fp64(name, gpu):
     src, trg, q, L, ncrit, kappa, lvmax = case_inputs(name)
