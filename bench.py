@@ -359,6 +359,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="sphere2m")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))
@@ -414,8 +415,13 @@ def main():
     dp = torch.empty(w.n, dtype=torch.complex128, device="cuda")
 
     res = {}
+    tune, tune_s = {}, 0.0
     for prec in ["fp64", "mixed"]:
         A.set_precision(prec)
+        if not args.no_autotune:  # launch choices timed on this operator (defmm_autotune)
+            t0 = time.perf_counter()
+            tune[prec] = A.autotune(reps=1)
+            tune_s += time.perf_counter() - t0
         for _ in range(args.warmup):
             A.matvec_device(dq.data_ptr(), dp.data_ptr(), 1, stream.cuda_stream)
         torch.cuda.synchronize()
@@ -526,7 +532,9 @@ def main():
             "phases_ms": phases,
             "setup_s": setup_s,
             "setup": {"prcmpt_s": setup_s, "level_walk_s": info["plan_walk_ms"] / 1e3,
-                      "level_walk_on_gpu": bool(info["plan_walk_device"]), "upload_s": upload_s},
+                      "level_walk_on_gpu": bool(info["plan_walk_device"]), "upload_s": upload_s,
+                      "autotune_s": tune_s},
+            "launch": tune,
             "plan": {k: info[k] for k in ["nlvl", "cpt", "slots_S", "slots_T", "far_hf", "far_lf", "near",
                                           "i_near", "tables", "permuted_spectra", "device_bytes"]},
         }

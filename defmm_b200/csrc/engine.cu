@@ -69,6 +69,10 @@ struct defmm_handle {
   DevBuf pscr;           // source-side partial sums (one complex per slot)
   bool use_sym = false;  // this precision runs the symmetric near field
   int nsm = 148;
+  // launch choices (defmm_autotune), per precision: M2L threads per target
+  // slot (0: the order's default) and near-field CTAs per SM
+  int m2l_nt[2] = {0, 0};
+  int p2p_bps[2] = {16, 16};
   int64_t nchunk = 0;
   size_t dev_bytes = 0;
   double phase_ms[PH_N] = {0};
@@ -444,7 +448,7 @@ int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) 
                     h->d_queue, h->nsm, sn);
     dfb::launch_p2p_sym(fp64, d, (int64_t)p.sym_order.size(), h->d_sym_order, h->d_sym_item_chunk, h->d_tfirst,
                         h->d_tn, h->d_sym_ptr, h->d_sym_sfirst, h->d_sym_sn, h->d_sym_soff, h->q.p, h->d_tpart,
-                        h->pscr.p, h->d_queue, h->nsm, sn);
+                        h->pscr.p, h->d_queue, h->nsm, h->p2p_bps[fp64 ? 0 : 1], sn);
     dfb::launch_p2p_items(h->nchunk, h->d_tfirst, h->d_tn, h->d_sym_chunk_items, h->d_tpart, (double2*)h->pnear.p,
                           h->nsm, sn);
     dfb::launch_p2p_reduce(fp64, (int64_t)p.red_first.size(), h->d_red_first, h->d_red_n, h->d_red_ptr,
@@ -487,7 +491,8 @@ int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) 
         nl_ += 2;
         rec(h, 2 * PH_M2F + 1);
         rec(h, 2 * PH_M2L);
-        ops->m2l(d, ts0, ts1, fs0, fs1, h->F.p, h->ptab.p, h->Lx.p, h->d_queue + 1, h->nsm, sf);
+        ops->m2l(d, ts0, ts1, fs0, fs1, h->F.p, h->ptab.p, h->Lx.p, h->d_queue + 1, h->nsm, h->m2l_nt[fp64 ? 0 : 1],
+                 sf);
         rec(h, 2 * PH_M2L + 1);
         if (h->events) {
           float a;
@@ -690,6 +695,72 @@ int defmm_set_graphs(defmm_handle* h, int on) {
 int defmm_set_profiling(defmm_handle* h, int on) {
   if (!h) return DEFMM_ERR_ARG;
   h->events = on != 0;
+  return 0;
+}
+
+int defmm_set_launch(defmm_handle* h, int m2l_threads, int p2p_blocks_per_sm) {
+  if (!h || (m2l_threads != 0 && m2l_threads != 128 && m2l_threads != 256) || p2p_blocks_per_sm < 0 ||
+      p2p_blocks_per_sm > 64)
+    return DEFMM_ERR_ARG;
+  const int pi = h->precision == DEFMM_PRECISION_FP64 ? 0 : 1;
+  h->m2l_nt[pi] = m2l_threads;
+  h->p2p_bps[pi] = p2p_blocks_per_sm ? p2p_blocks_per_sm : 16;
+  if (h->device >= 0) drop_graph(h);
+  return 0;
+}
+
+int defmm_autotune(defmm_handle* h, int reps, int32_t* choice) {
+  if (!h || reps < 1 || reps > 100) return DEFMM_ERR_ARG;
+  if (!h->built) return h->fail(DEFMM_ERR_ARG, "autotune before prcmpt");
+  int st = defmm_upload(h);
+  if (st) return st;
+  st = prepare_precision(h);
+  if (st) return st;
+  const int64_t nS = (int64_t)h->plan.S.perm.size(), nT = (int64_t)h->plan.T.perm.size();
+  if ((st = ensure(h, h->rin, 16 * nS)) || (st = ensure(h, h->rout, 16 * nT))) return st;
+  CK(cudaMemsetAsync(h->rin.p, 0, 16 * nS, h->st));
+  const int pi = h->precision == DEFMM_PRECISION_FP64 ? 0 : 1;
+  const bool ev = h->events;
+  h->events = true;  // phase timers, phases serialised
+  drop_graph(h);     // the captured graph holds the old launch choices
+  // fastest of `reps` profiled matvecs, for the phase `ph`
+  auto best_of = [&](int ph, double& t) -> int {
+    t = 1e300;
+    for (int r = 0; r < reps; r++) {
+      const int e = run_gemv(h, (const double2*)h->rin.p, (double2*)h->rout.p, h->st);
+      if (e) return e;
+      t = std::min(t, h->phase_ms[ph]);
+    }
+    return 0;
+  };
+  int m2l_best = 128, bps_best = 16;
+  double tb = 1e300, t = 0;
+  for (int nt : {128, 256}) {
+    h->m2l_nt[pi] = nt;
+    if ((st = best_of(PH_M2L, t))) break;
+    if (t < tb) {
+      tb = t;
+      m2l_best = nt;
+    }
+  }
+  h->m2l_nt[pi] = m2l_best;
+  tb = 1e300;
+  for (int b : {8, 16, 32}) {
+    if (st) break;
+    h->p2p_bps[pi] = b;
+    if ((st = best_of(PH_P2P, t))) break;
+    if (t < tb) {
+      tb = t;
+      bps_best = b;
+    }
+  }
+  h->p2p_bps[pi] = bps_best;
+  h->events = ev;
+  if (st) return st;
+  if (choice) {
+    choice[0] = m2l_best;
+    choice[1] = bps_best;
+  }
   return 0;
 }
 
@@ -971,6 +1042,12 @@ int defmm_info(const defmm_handle* h, int what, int64_t* v) {
     case DEFMM_INFO_PLAN_WALK_DEVICE: *v = h->walked_on_device ? 1 : 0; break;
     case DEFMM_INFO_PLAN_MS: *v = (int64_t)(1e3 * (p.t_tree + p.t_lists + p.t_tables)); break;
     case DEFMM_INFO_PLAN_WALK_MS: *v = (int64_t)(1e3 * p.t_walk); break;
+    case DEFMM_INFO_M2L_THREADS: {
+      const int pi = h->precision == DEFMM_PRECISION_FP64 ? 0 : 1;
+      *v = h->m2l_nt[pi] ? h->m2l_nt[pi] : (p.PP > 1024 ? 256 : 128);
+      break;
+    }
+    case DEFMM_INFO_P2P_BLOCKS_PER_SM: *v = h->p2p_bps[h->precision == DEFMM_PRECISION_FP64 ? 0 : 1]; break;
     case DEFMM_INFO_M2L_TARGETS: {
       int64_t n = 0;
       for (int64_t k = 0; k < p.sT.n; k++) n += p.m2l_ptr[k + 1] > p.m2l_ptr[k] ? 1 : 0;

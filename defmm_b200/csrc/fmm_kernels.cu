@@ -1681,7 +1681,11 @@ struct Launch {
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_p2m<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P2MCfg<T, L>::smem());
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_m2l<T, L, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_m2l());
+    e = cudaFuncSetAttribute(k_m2l<T, L, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_m2l());
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_m2l<T, L, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_m2l());
+    if (e != cudaSuccess) return e;
+    return cudaSuccess;
   }
   static void p2m(const DevPlan& dp, const int32_t* leaves, int n, const void* q, const void* sig2, void* M,
                   cudaStream_t s) {
@@ -1704,11 +1708,15 @@ struct Launch {
     if (n) k_m2f<T, L><<<grid_for(n, NW), 32 * NW, smem_m2f(), s>>>(n, (const C*)M, (C*)F);
   }
   static void m2l(const DevPlan& dp, int64_t t0, int64_t t1, int64_t f0, int64_t f1, const void* F,
-                  const void* ptab, void* Lx, unsigned long long* queue, int nsm, cudaStream_t s) {
+                  const void* ptab, void* Lx, unsigned long long* queue, int nsm, int nt, cudaStream_t s) {
     if (t1 <= t0) return;
     cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s);
-    const int grid = (int)std::min<int64_t>(t1 - t0, (int64_t)nsm * (2048 / NT));
-    k_m2l<T, L, NT><<<grid, NT, smem_m2l(), s>>>(dp, t0, t1, f0, f1, (const C*)F, (const C*)ptab, (C*)Lx, queue);
+    if (nt != 128 && nt != 256) nt = NT;
+    const int grid = (int)std::min<int64_t>(t1 - t0, (int64_t)nsm * (2048 / nt));
+    if (nt == 256)
+      k_m2l<T, L, 256><<<grid, 256, smem_m2l(), s>>>(dp, t0, t1, f0, f1, (const C*)F, (const C*)ptab, (C*)Lx, queue);
+    else
+      k_m2l<T, L, 128><<<grid, 128, smem_m2l(), s>>>(dp, t0, t1, f0, f1, (const C*)F, (const C*)ptab, (C*)Lx, queue);
   }
   static void permute(int64_t n, const uint32_t* key, const uint16_t* perm, const void* tables, void* out,
                       cudaStream_t s) {
@@ -1797,10 +1805,10 @@ void launch_p2p_items(int64_t nchunk, const int32_t* tfirst, const int32_t* tn, 
 void launch_p2p_sym(bool fp64, const DevPlan& dp, int64_t nwork, const int32_t* order, const int32_t* item_chunk,
                     const int32_t* tfirst, const int32_t* tn, const int64_t* ptr, const int32_t* sfirst,
                     const int32_t* sn, const int64_t* soff, const void* q, double2* tpart, void* scratch,
-                    unsigned long long* queue, int nsm, cudaStream_t s) {
+                    unsigned long long* queue, int nsm, int blocks_per_sm, cudaStream_t s) {
   if (nwork <= 0) return;
   cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s);
-  const int grid = (int)std::min<int64_t>(nwork, (int64_t)nsm * 16);
+  const int grid = (int)std::min<int64_t>(nwork, (int64_t)nsm * std::max(1, std::min(blocks_per_sm, 64)));
   if (fp64)
     k_p2p_sym<false><<<grid, 128, 0, s>>>(dp, nwork, order, item_chunk, tfirst, tn, ptr, sfirst, sn, soff, q, tpart,
                                           scratch, queue);

@@ -19,8 +19,9 @@ struct OpTable {
   void (*l2l)(const DevPlan&, int64_t s0, int64_t s1, const void* sig, const void* sig2, void* Lx, cudaStream_t);
   void (*m2f)(int64_t n, const void* M, void* F, cudaStream_t);
   // M2L with the inverse DFT fused: adds into L of target slots [t0, t1)
+  // nt: threads per target slot (128 or 256; 0 = the order's default)
   void (*m2l)(const DevPlan&, int64_t t0, int64_t t1, int64_t f0, int64_t f1, const void* F, const void* ptab,
-              void* Lx, unsigned long long* queue, int nsm, cudaStream_t);
+              void* Lx, unsigned long long* queue, int nsm, int nt, cudaStream_t);
   void (*l2p)(const DevPlan&, const int32_t* leaves, int n, const void* sig2, const void* Lx, double2* pfar,
               cudaStream_t);
   // U_k = tables[key_k >> 6][perm[key_k & 63][:]] for the permuted spectra
@@ -48,10 +49,11 @@ void launch_p2p_items(int64_t nchunk, const int32_t* tfirst, const int32_t* tn, 
 // side to tpart, the source side to scratch) and the per-leaf reduction of
 // the scratch into pnear (k_p2p_reduce).  Scratch holds double2 (fp64) or
 // float2 (mixed) partial sums.
+// blocks_per_sm: CTAs per SM of the queue-driven launch (grid nsm x it)
 void launch_p2p_sym(bool fp64, const DevPlan& dp, int64_t nwork, const int32_t* order, const int32_t* item_chunk,
                     const int32_t* tfirst, const int32_t* tn, const int64_t* ptr, const int32_t* sfirst,
                     const int32_t* sn, const int64_t* soff, const void* q, double2* tpart, void* scratch,
-                    unsigned long long* queue, int nsm, cudaStream_t s);
+                    unsigned long long* queue, int nsm, int blocks_per_sm, cudaStream_t s);
 void launch_p2p_reduce(bool fp64, int64_t nleaf, const int32_t* first, const int32_t* n, const int64_t* rptr,
                        const int64_t* roff, const void* scratch, double2* pnear, int nsm, cudaStream_t s);
 void launch_direct(int64_t ns, const double* spos, const int32_t* sperm, const double2* qin, int64_t nt,
