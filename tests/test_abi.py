@@ -4,6 +4,8 @@ import ctypes
 import os
 import re
 
+import pytest
+
 from defmm_b200 import api
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -33,3 +35,20 @@ def test_create_destroy_without_device():
     A = api.IBFMM_Mat()
     assert A.info("n_sources") == 0
     del A
+
+
+def test_argument_checks_without_device():
+    # calls that must be rejected before touching a device
+    A = api.IBFMM_Mat()
+    for nt, bps in ((64, 16), (128, -1), (256, 65)):
+        with pytest.raises(api.DefmmError):
+            A.set_launch(nt, bps)
+    A.set_launch(256, 8)  # valid choices are recorded without a device
+    with pytest.raises(api.DefmmError):
+        A.autotune(reps=0)
+    with pytest.raises(api.DefmmError):
+        A.autotune(reps=1)  # before prcmpt
+    L = api.lib()
+    assert L.defmm_mlp_forward(None, None, 1, None, None, None, None) == api.lib().defmm_mlp_forward(
+        None, None, 0, None, None, None, None) != 0
+    assert L.defmm_mlp_adam(None, None, None, None, 0, 1e-3, 0.0, None) != 0
