@@ -64,6 +64,32 @@ void pchunks(int64_t n, int K, F f) {
   for (auto& t : th) t.join();
 }
 
+// Stable counting sort of [0, n) by key(k) in [0, m): ptr gets the m + 1
+// bucket offsets and put(pos, k) places every k, ties in index order.  K
+// contiguous blocks count and place in parallel, so the result is the
+// serial one.
+template <typename Key, typename Put>
+void bucket_sort(int64_t n, int64_t m, std::vector<int64_t>& ptr, Key key, Put put) {
+  const int K = (int)std::max<int64_t>(1, std::min<int64_t>(std::min<unsigned>(hw_threads(), 32), n / 65536 + 1));
+  std::vector<std::vector<int64_t>> kc(K, std::vector<int64_t>(m, 0));
+  pchunks(n, K, [&](int k, int64_t b, int64_t e) {
+    for (int64_t i = b; i < e; i++) kc[k][key(i)]++;
+  });
+  ptr.assign(m + 1, 0);
+  for (int64_t c = 0; c < m; c++) {
+    int64_t t = ptr[c];
+    for (int k = 0; k < K; k++) {
+      const int64_t v = kc[k][c];
+      kc[k][c] = t;
+      t += v;
+    }
+    ptr[c + 1] = t;
+  }
+  pchunks(n, K, [&](int k, int64_t b, int64_t e) {
+    for (int64_t i = b; i < e; i++) put(kc[k][key(i)]++, i);
+  });
+}
+
 inline double norm3(const double* v) {
   double t = 0.;
   for (int i = 0; i < 3; i++) t += v[i] * v[i];
@@ -583,61 +609,98 @@ void build_symmetric_near(Plan& p) {
   const Tree& T = p.T;
   const int64_t nch = (int64_t)p.p2p_tfirst.size();
   std::vector<int32_t> leaf_at(T.pos.size() / 3, -1);  // particle -> leaf
-  for (int64_t c = 0; c < T.ncell; c++)
+  pfor(T.ncell, 1024, [&](int64_t c) {
     if (T.leaf(c))
       for (int32_t k = 0; k < T.nprt[c]; k++) leaf_at[T.first[c] + k] = (int32_t)c;
-  p.self_ptr.assign(1, 0);
-  p.self_sfirst.clear();
-  p.self_sn.clear();
-  p.sym_ptr.assign(1, 0);
-  p.sym_sfirst.clear();
-  p.sym_sn.clear();
-  p.sym_soff.clear();
-  int64_t tot = 0;
-  for (int64_t ch = 0; ch < nch; ch++) {
+  });
+  // per chunk: own-leaf blocks, blocks of the source leaves after the own
+  // leaf and their sources; then prefix sums and a parallel fill, in chunk
+  // order (the serial order of the lists)
+  std::vector<int64_t> nself(nch + 1, 0), nsym(nch + 1, 0), nsrc(nch + 1, 0);
+  pfor(nch, 256, [&](int64_t ch) {
     const int32_t lf = leaf_at[p.p2p_tfirst[ch]];
     const int32_t a0 = T.first[lf], a1 = a0 + T.nprt[lf];
     for (int64_t r = p.p2p_ptr[ch]; r < p.p2p_ptr[ch + 1]; r++) {
       const int32_t s0 = p.p2p_sfirst[r], s1 = s0 + p.p2p_sn[r];
+      if (s0 < a1 && s1 > a0) nself[ch + 1]++;
+      const int32_t b0 = std::max(s0, a1);
+      if (b0 < s1) {
+        nsym[ch + 1]++;
+        nsrc[ch + 1] += s1 - b0;
+      }
+    }
+  });
+  for (int64_t ch = 0; ch < nch; ch++) {
+    nself[ch + 1] += nself[ch];
+    nsym[ch + 1] += nsym[ch];
+    nsrc[ch + 1] += nsrc[ch];
+  }
+  p.self_ptr.assign(nself.begin(), nself.end());
+  p.sym_ptr.assign(nsym.begin(), nsym.end());
+  p.self_sfirst.assign(nself[nch], 0);
+  p.self_sn.assign(nself[nch], 0);
+  p.sym_sfirst.assign(nsym[nch], 0);
+  p.sym_sn.assign(nsym[nch], 0);
+  p.sym_soff.assign(nsym[nch], 0);
+  pfor(nch, 256, [&](int64_t ch) {
+    const int32_t lf = leaf_at[p.p2p_tfirst[ch]];
+    const int32_t a0 = T.first[lf], a1 = a0 + T.nprt[lf];
+    int64_t ks = nself[ch], ky = nsym[ch], tot = nsrc[ch];
+    for (int64_t r = p.p2p_ptr[ch]; r < p.p2p_ptr[ch + 1]; r++) {
+      const int32_t s0 = p.p2p_sfirst[r], s1 = s0 + p.p2p_sn[r];
       if (s0 < a1 && s1 > a0) {  // the own leaf
-        p.self_sfirst.push_back(a0);
-        p.self_sn.push_back(a1 - a0);
+        p.self_sfirst[ks] = a0;
+        p.self_sn[ks++] = a1 - a0;
       }
       const int32_t b0 = std::max(s0, a1);
       if (b0 < s1) {  // source leaves after the own leaf
-        p.sym_sfirst.push_back(b0);
-        p.sym_sn.push_back(s1 - b0);
-        p.sym_soff.push_back(tot);
+        p.sym_sfirst[ky] = b0;
+        p.sym_sn[ky] = s1 - b0;
+        p.sym_soff[ky++] = tot;
         tot += s1 - b0;
       }
     }
-    p.self_ptr.push_back((int64_t)p.self_sfirst.size());
-    p.sym_ptr.push_back((int64_t)p.sym_sfirst.size());
-  }
-  p.sym_scratch = tot;
-  // rows per source leaf, in chunk order
-  std::vector<int64_t> cnt(T.ncell + 1, 0);
-  for (size_t r = 0; r < p.sym_sfirst.size(); r++)
-    for (int32_t j = p.sym_sfirst[r]; j < p.sym_sfirst[r] + p.sym_sn[r]; j += T.nprt[leaf_at[j]]) cnt[leaf_at[j]]++;
-  std::vector<int64_t> lpos(T.ncell, -1);
+  });
+  p.sym_scratch = nsrc[nch];
+  // rows per source leaf, in row order: each of K contiguous blocks of rows
+  // counts its rows per leaf, so that its rows land after those of the
+  // blocks before it
+  const int64_t nrow = (int64_t)p.sym_sfirst.size();
+  const int K = (int)std::max<int64_t>(1, std::min<int64_t>(std::min<unsigned>(hw_threads(), 32), nrow / 4096 + 1));
+  std::vector<std::vector<int64_t>> kc(K, std::vector<int64_t>(T.ncell, 0));
+  auto each_leaf = [&](int64_t r, auto f) {
+    for (int32_t j = p.sym_sfirst[r]; j < p.sym_sfirst[r] + p.sym_sn[r]; j += T.nprt[leaf_at[j]]) f(leaf_at[j], j);
+  };
+  pchunks(nrow, K, [&](int k, int64_t b, int64_t e) {
+    for (int64_t r = b; r < e; r++) each_leaf(r, [&](int32_t c, int32_t) { kc[k][c]++; });
+  });
   p.red_first.clear();
   p.red_n.clear();
   p.red_ptr.assign(1, 0);
-  for (int64_t c = 0; c < T.ncell; c++)
-    if (cnt[c]) {
-      lpos[c] = p.red_ptr.back();
+  for (int64_t c = 0; c < T.ncell; c++) {
+    int64_t n = 0;
+    for (int k = 0; k < K; k++) {
+      const int64_t v = kc[k][c];
+      kc[k][c] = n;  // rows of the blocks before k
+      n += v;
+    }
+    if (n) {
+      for (int k = 0; k < K; k++) kc[k][c] += p.red_ptr.back();
       p.red_first.push_back(T.first[c]);
       p.red_n.push_back(T.nprt[c]);
-      p.red_ptr.push_back(p.red_ptr.back() + cnt[c]);
+      p.red_ptr.push_back(p.red_ptr.back() + n);
     }
+  }
   p.red_off.assign(p.red_ptr.back(), 0);
-  for (size_t r = 0; r < p.sym_sfirst.size(); r++)
-    for (int32_t j = p.sym_sfirst[r]; j < p.sym_sfirst[r] + p.sym_sn[r]; j += T.nprt[leaf_at[j]])
-      p.red_off[lpos[leaf_at[j]]++] = p.sym_soff[r] + (j - p.sym_sfirst[r]);
+  pchunks(nrow, K, [&](int k, int64_t b, int64_t e) {
+    for (int64_t r = b; r < e; r++)
+      each_leaf(r, [&](int32_t c, int32_t j) { p.red_off[kc[k][c]++] = p.sym_soff[r] + (j - p.sym_sfirst[r]); });
+  });
   // self blocks by decreasing work
   std::vector<int64_t> ws(nch, 0);
-  for (int64_t ch = 0; ch < nch; ch++)
+  pfor(nch, 1024, [&](int64_t ch) {
     for (int64_t r = p.self_ptr[ch]; r < p.self_ptr[ch + 1]; r++) ws[ch] += p.self_sn[r];
+  });
   p.self_order.clear();
   for (int64_t ch = 0; ch < nch; ch++)
     if (ws[ch]) p.self_order.push_back((int32_t)ch);
@@ -654,41 +717,66 @@ void split_items(const Plan& p, std::vector<int64_t>& ptr, std::vector<int32_t>&
                  std::vector<int32_t>& order, bool lanes_by_chunk) {
   constexpr int64_t SP = Plan::kItemSources;
   const int64_t nch = (int64_t)ptr.size() - 1;
-  std::vector<int64_t> nptr{0};
-  std::vector<int32_t> nsf, nsn;
-  std::vector<int64_t> nso;
-  std::vector<int64_t> work;
-  chunk.clear();
-  items.assign(1, 0);
+  // per chunk: items (ceil(sources / SP)) and range pieces (a range is cut
+  // where an item ends); then prefix sums and a parallel fill in chunk order
+  std::vector<int64_t> nit(nch + 1, 0), npc(nch + 1, 0);
+  pfor(nch, 256, [&](int64_t ch) {
+    int64_t fill = 0, pieces = 0, its = 0;
+    for (int64_t r = ptr[ch]; r < ptr[ch + 1]; r++)
+      for (int32_t o = 0; o < sn[r];) {
+        const int32_t take = (int32_t)std::min<int64_t>(sn[r] - o, SP - fill);
+        pieces++;
+        fill += take;
+        o += take;
+        if (fill == SP) {
+          its++;
+          fill = 0;
+        }
+      }
+    if (fill) its++;
+    nit[ch + 1] = its;
+    npc[ch + 1] = pieces;
+  });
   for (int64_t ch = 0; ch < nch; ch++) {
+    nit[ch + 1] += nit[ch];
+    npc[ch + 1] += npc[ch];
+  }
+  const int64_t nitem = nit[nch], npiece = npc[nch];
+  std::vector<int64_t> nptr(nitem + 1, 0);
+  std::vector<int32_t> nsf(npiece), nsn(npiece);
+  std::vector<int64_t> nso(soff ? npiece : 0);
+  std::vector<int64_t> work(nitem);
+  chunk.assign(nitem, 0);
+  pfor(nch, 256, [&](int64_t ch) {
     int tp = 32;
     if (lanes_by_chunk) {
       tp = 4;
       while (tp < p.p2p_tn[ch]) tp <<= 1;
     }
-    int64_t fill = 0;
+    int64_t fill = 0, q = npc[ch], it = nit[ch];
     for (int64_t r = ptr[ch]; r < ptr[ch + 1]; r++)
       for (int32_t o = 0; o < sn[r];) {
         const int32_t take = (int32_t)std::min<int64_t>(sn[r] - o, SP - fill);
-        nsf.push_back(sf[r] + o);
-        nsn.push_back(take);
-        if (soff) nso.push_back((*soff)[r] + o);
+        nsf[q] = sf[r] + o;
+        nsn[q] = take;
+        if (soff) nso[q] = (*soff)[r] + o;
+        q++;
         fill += take;
         o += take;
         if (fill == SP) {
-          nptr.push_back((int64_t)nsf.size());
-          chunk.push_back((int32_t)ch);
-          work.push_back(fill * tp);
+          nptr[it + 1] = q;
+          chunk[it] = (int32_t)ch;
+          work[it++] = fill * tp;
           fill = 0;
         }
       }
     if (fill) {
-      nptr.push_back((int64_t)nsf.size());
-      chunk.push_back((int32_t)ch);
-      work.push_back(fill * tp);
+      nptr[it + 1] = q;
+      chunk[it] = (int32_t)ch;
+      work[it++] = fill * tp;
     }
-    items.push_back((int64_t)chunk.size());
-  }
+  });
+  items.assign(nit.begin(), nit.end());
   ptr.swap(nptr);
   sf.swap(nsf);
   sn.swap(nsn);
@@ -1009,19 +1097,14 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
 
   // per-cell direction/slot CSR for both trees
   auto cell_csr = [&](const Tree& tr, Slots& s) {
-    s.cell_ptr.assign(tr.ncell + 1, 0);
-    for (int64_t k = 0; k < s.n; k++) s.cell_ptr[s.cell[k] + 1]++;
-    for (int64_t c = 0; c < tr.ncell; c++) s.cell_ptr[c + 1] += s.cell_ptr[c];
     s.cell_dirs.resize(s.n);
     s.cell_slots.resize(s.n);
-    std::vector<int64_t> pos(s.cell_ptr.begin(), s.cell_ptr.end() - 1);
     // slots of one cell appear in increasing direction order (cone-major)
-    for (int64_t k = 0; k < s.n; k++) {
-      const int64_t c = s.cell[k];
-      s.cell_dirs[pos[c]] = s.dir[k];
-      s.cell_slots[pos[c]] = k;
-      pos[c]++;
-    }
+    bucket_sort(s.n, tr.ncell, s.cell_ptr, [&](int64_t k) { return (int64_t)s.cell[k]; },
+                [&](int64_t pos, int64_t k) {
+                  s.cell_dirs[pos] = s.dir[k];
+                  s.cell_slots[pos] = k;
+                });
   };
   cell_csr(p.T, p.sT);
   cell_csr(p.S, p.sS);
@@ -1136,19 +1219,41 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
         p.rec_near.push_back(pr.first);
         p.rec_near.push_back(pr.second);
       }
+    // source ranges per target leaf, in pair order: K contiguous blocks of
+    // pairs count per leaf, then fill after the blocks before them
+    const int64_t npair = (int64_t)near_pairs.size();
+    const int K = (int)std::max<int64_t>(1, std::min<int64_t>(std::min<unsigned>(hw_threads(), 32), npair / 4096 + 1));
+    std::vector<std::vector<int64_t>> kc(K, std::vector<int64_t>(p.T.ncell, 0));
+    std::vector<int64_t> kin(K, 0);
+    pchunks(npair, K, [&](int k, int64_t b, int64_t e) {
+      for (int64_t i = b; i < e; i++) {
+        const auto& pr = near_pairs[i];
+        for (int64_t c = pr.first; c < p.T.sub_end[pr.first]; c++)
+          if (p.T.leaf(c)) kc[k][c]++;
+        kin[k] += (int64_t)p.T.nprt[pr.first] * p.S.nprt[pr.second];
+      }
+    });
     std::vector<int64_t> cnt(p.T.ncell + 1, 0);
-    for (auto& pr : near_pairs)
-      for (int64_t c = pr.first; c < p.T.sub_end[pr.first]; c++)
-        if (p.T.leaf(c)) cnt[c + 1]++;
-    for (int64_t c = 0; c < p.T.ncell; c++) cnt[c + 1] += cnt[c];
-    std::vector<std::pair<int32_t, int32_t>> rng(cnt[p.T.ncell]);
-    std::vector<int64_t> pos(cnt.begin(), cnt.end() - 1);
-    for (auto& pr : near_pairs) {
-      const int32_t sf = p.S.first[pr.second], sn = p.S.nprt[pr.second];
-      for (int64_t c = pr.first; c < p.T.sub_end[pr.first]; c++)
-        if (p.T.leaf(c)) rng[pos[c]++] = {sf, sn};
-      p.i_near += (int64_t)p.T.nprt[pr.first] * sn;
+    for (int64_t c = 0; c < p.T.ncell; c++) {
+      int64_t n = cnt[c];
+      for (int k = 0; k < K; k++) {
+        const int64_t v = kc[k][c];
+        kc[k][c] = n;
+        n += v;
+      }
+      cnt[c + 1] = n;
     }
+    for (int k = 0; k < K; k++) p.i_near += kin[k];
+    std::vector<std::pair<int32_t, int32_t>> rng(cnt[p.T.ncell]);
+    pchunks(npair, K, [&](int k, int64_t b, int64_t e) {
+      for (int64_t i = b; i < e; i++) {
+        const auto& pr = near_pairs[i];
+        const int32_t sf = p.S.first[pr.second], sn = p.S.nprt[pr.second];
+        for (int64_t c = pr.first; c < p.T.sub_end[pr.first]; c++)
+          if (p.T.leaf(c)) rng[kc[k][c]++] = {sf, sn};
+      }
+    });
+    std::vector<std::vector<int64_t>>().swap(kc);
     std::vector<std::pair<int32_t, int32_t>>().swap(near_pairs);
     // merge touching ranges per leaf
     std::vector<std::vector<std::pair<int32_t, int32_t>>> merged(p.T.ncell);
