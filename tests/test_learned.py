@@ -65,6 +65,17 @@ def test_features_are_deterministic_and_finite():
         assert fa.shape == (Lr.NIN,) and np.all(np.isfinite(fa))
 
 
+def test_committed_sweep_features_regenerate_from_the_seed():
+    # the sweep's inputs come from the seeded problem generator: replaying
+    # it reproduces the recorded features of the first problems exactly
+    d = np.load(Lr.SWEEP_PATH)
+    rng = np.random.default_rng(int(d["seed"]))
+    for i in range(4):
+        kind, pts, kappa, ncrit = Lr.sample_problem(rng, i)
+        assert kind == d["kind"][i] and len(pts) == d["n"][i]
+        assert np.array_equal(Lr.problem_features(pts, kappa, ncrit), d["feat"][i])
+
+
 def test_committed_sweep_and_model_load():
     d = np.load(Lr.SWEEP_PATH)
     assert d["feat"].shape[1] == Lr.NIN - 1 and d["err"].shape[1] == len(Lr.ORDERS)
