@@ -35,7 +35,7 @@ _INFO = {
     "cells_S": 6, "slots_S": 7, "slots_T": 8, "far_hf": 9, "far_lf": 10, "near": 11,
     "i_near": 12, "tables": 13, "device_bytes": 14, "list_records": 15, "launches": 16,
     "m2l_targets": 17, "leaf_slots_S": 18, "permuted_spectra": 19, "plan_walk_device": 20, "plan_ms": 21,
-    "plan_walk_ms": 22, "m2l_threads": 23, "p2p_blocks_per_sm": 24,
+    "plan_walk_ms": 22, "m2l_threads": 23, "p2p_blocks_per_sm": 24, "m2l_pairing": 25,
 }
 PHASES = ["p2m", "m2m", "m2f", "m2l", "f2l", "l2l", "l2p", "p2p", "scatter", "total"]
 
@@ -80,6 +80,7 @@ def lib():
             "defmm_set_plan_device": (ctypes.c_int, [vp, ctypes.c_int]),
             "defmm_autotune": (ctypes.c_int, [vp, ctypes.c_int, ip]),
             "defmm_set_launch": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
+            "defmm_set_m2l_pairing": (ctypes.c_int, [vp, ctypes.c_int]),
             "defmm_batch_create": (vp, [i64, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.c_int]),
             "defmm_batch_launch": (ctypes.c_int, [vp, vp]),
             "defmm_batch_destroy": (None, [vp]),
@@ -171,14 +172,19 @@ class IBFMM_Mat:
 
     def autotune(self, reps=2):
         """Pick the fastest launch choices for this operator at its current
-        precision (defmm_autotune); returns {"m2l_threads", "p2p_blocks_per_sm"}."""
+        precision (defmm_autotune); returns {"m2l_threads", "m2l_pairing",
+        "p2p_blocks_per_sm"}."""
         c = np.zeros(2, dtype=np.int32)
         self._check(lib().defmm_autotune(self._h, int(reps), _ip(c)))
-        return {"m2l_threads": int(c[0]), "p2p_blocks_per_sm": int(c[1])}
+        return {"m2l_threads": int(c[0]), "m2l_pairing": self.info("m2l_pairing"), "p2p_blocks_per_sm": int(c[1])}
 
     def set_launch(self, m2l_threads=0, p2p_blocks_per_sm=0):
         """Launch choices by hand for the current precision (0: defaults)."""
         self._check(lib().defmm_set_launch(self._h, int(m2l_threads), int(p2p_blocks_per_sm)))
+
+    def set_m2l_pairing(self, on=True):
+        """Two target slots per M2L CTA (current precision); results unchanged."""
+        self._check(lib().defmm_set_m2l_pairing(self._h, int(bool(on))))
 
     def set_profiling(self, on=True):
         self._check(lib().defmm_set_profiling(self._h, int(bool(on))))

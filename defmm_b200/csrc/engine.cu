@@ -72,6 +72,7 @@ struct defmm_handle {
   // launch choices (defmm_autotune), per precision: M2L threads per target
   // slot (0: the order's default) and near-field CTAs per SM
   int m2l_nt[2] = {0, 0};
+  int m2l_pair[2] = {0, 0};  // two target slots per M2L CTA
   int p2p_bps[2] = {16, 16};
   int64_t nchunk = 0;
   size_t dev_bytes = 0;
@@ -492,7 +493,7 @@ int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) 
         rec(h, 2 * PH_M2F + 1);
         rec(h, 2 * PH_M2L);
         ops->m2l(d, ts0, ts1, fs0, fs1, h->F.p, h->ptab.p, h->Lx.p, h->d_queue + 1, h->nsm, h->m2l_nt[fp64 ? 0 : 1],
-                 sf);
+                 h->m2l_pair[fp64 ? 0 : 1], sf);
         rec(h, 2 * PH_M2L + 1);
         if (h->events) {
           float a;
@@ -709,6 +710,13 @@ int defmm_set_launch(defmm_handle* h, int m2l_threads, int p2p_blocks_per_sm) {
   return 0;
 }
 
+int defmm_set_m2l_pairing(defmm_handle* h, int on) {
+  if (!h || (on != 0 && on != 1)) return DEFMM_ERR_ARG;
+  h->m2l_pair[h->precision == DEFMM_PRECISION_FP64 ? 0 : 1] = on;
+  if (h->device >= 0) drop_graph(h);
+  return 0;
+}
+
 int defmm_autotune(defmm_handle* h, int reps, int32_t* choice) {
   if (!h || reps < 1 || reps > 100) return DEFMM_ERR_ARG;
   if (!h->built) return h->fail(DEFMM_ERR_ARG, "autotune before prcmpt");
@@ -733,17 +741,23 @@ int defmm_autotune(defmm_handle* h, int reps, int32_t* choice) {
     }
     return 0;
   };
-  int m2l_best = 128, bps_best = 16;
+  int m2l_best = 128, pair_best = 0, bps_best = 16;
   double tb = 1e300, t = 0;
-  for (int nt : {128, 256}) {
-    h->m2l_nt[pi] = nt;
-    if ((st = best_of(PH_M2L, t))) break;
-    if (t < tb) {
-      tb = t;
-      m2l_best = nt;
+  for (int pair : {0, 1}) {
+    for (int nt : {128, 256}) {
+      if (st) break;
+      h->m2l_nt[pi] = nt;
+      h->m2l_pair[pi] = pair;
+      if ((st = best_of(PH_M2L, t))) break;
+      if (t < tb) {
+        tb = t;
+        m2l_best = nt;
+        pair_best = pair;
+      }
     }
   }
   h->m2l_nt[pi] = m2l_best;
+  h->m2l_pair[pi] = pair_best;
   tb = 1e300;
   for (int b : {8, 16, 32}) {
     if (st) break;
@@ -1048,6 +1062,7 @@ int defmm_info(const defmm_handle* h, int what, int64_t* v) {
       break;
     }
     case DEFMM_INFO_P2P_BLOCKS_PER_SM: *v = h->p2p_bps[h->precision == DEFMM_PRECISION_FP64 ? 0 : 1]; break;
+    case DEFMM_INFO_M2L_PAIRING: *v = h->m2l_pair[h->precision == DEFMM_PRECISION_FP64 ? 0 : 1]; break;
     case DEFMM_INFO_M2L_TARGETS: {
       int64_t n = 0;
       for (int64_t k = 0; k < p.sT.n; k++) n += p.m2l_ptr[k + 1] > p.m2l_ptr[k] ? 1 : 0;

@@ -807,11 +807,72 @@ __global__ void k_permute_tables(int64_t n, int PP, const uint32_t* __restrict__
 }
 
 // -------------------------------------------------------------- M2L + F2L --
+// Inverse DFT of one target slot's spectrum J (acc, K values per thread) into
+// its local expansion (fourier2geom, circulant.hpp:109-118):
+//   L_t[a,b,c] += (1/PP) sum_k J[k] conj(w)^(k0 a + k1 b + k2 c)
+// pruned to a,b,c < L, one line per thread per axis pass in shared memory.
+// Safe to call twice in a row: each pass reads only what the previous pass
+// wrote after the barrier between them.
+template <typename T, int L, int NT>
+__device__ __forceinline__ void m2l_f2l(const typename cpx_t<T>::type* acc, typename cpx_t<T>::type* Js,
+                                        typename cpx_t<T>::type* Cb, typename cpx_t<T>::type* D,
+                                        typename cpx_t<T>::type* __restrict__ Lt) {
+  typedef typename cpx_t<T>::type C;
+  constexpr int PD = 2 * L - 1, PP = PD * PD * PD, K = (PP + NT - 1) / NT;
+  const T inv = T(1) / T(PP);
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    const int i = threadIdx.x + k * NT;
+    if (i < PP) Js[i] = acc[k];
+  }
+  __syncthreads();
+  for (int ln = threadIdx.x; ln < PD * PD; ln += NT) {  // axis 0: (k1,k2) lines -> a
+    C v[PD];
+#pragma unroll
+    for (int k0 = 0; k0 < PD; k0++) v[k0] = Js[k0 * PD * PD + ln];
+#pragma unroll
+    for (int a = 0; a < L; a++) {
+      C s = v[0];
+#pragma unroll
+      for (int k0 = 1; k0 < PD; k0++) cfmac(s, v[k0], ctw<T, L>((k0 * a) % PD));
+      Cb[a * PD * PD + ln] = s;
+    }
+  }
+  __syncthreads();
+  for (int ln = threadIdx.x; ln < L * PD; ln += NT) {  // axis 1: (a,k2) lines -> b
+    const int a = ln / PD, k2 = ln % PD;
+    C v[PD];
+#pragma unroll
+    for (int k1 = 0; k1 < PD; k1++) v[k1] = Cb[(a * PD + k1) * PD + k2];
+#pragma unroll
+    for (int b = 0; b < L; b++) {
+      C s = v[0];
+#pragma unroll
+      for (int k1 = 1; k1 < PD; k1++) cfmac(s, v[k1], ctw<T, L>((k1 * b) % PD));
+      D[(a * L + b) * PD + k2] = s;
+    }
+  }
+  __syncthreads();
+  for (int ln = threadIdx.x; ln < L * L; ln += NT) {  // axis 2: (a,b) lines -> c
+    C v[PD];
+#pragma unroll
+    for (int k2 = 0; k2 < PD; k2++) v[k2] = D[ln * PD + k2];
+#pragma unroll
+    for (int c = 0; c < L; c++) {
+      C s = v[0];
+#pragma unroll
+      for (int k2 = 1; k2 < PD; k2++) cfmac(s, v[k2], ctw<T, L>((k2 * c) % PD));
+      C o = Lt[ln * L + c];
+      o.x += s.x * inv;
+      o.y += s.y * inv;
+      Lt[ln * L + c] = o;
+    }
+  }
+}
+
 // One CTA per target slot of a cone batch (M2L.hpp:115-157 target-stationary,
-// then fourier2geom circulant.hpp:109-118):
+// then the inverse DFT above):
 //   J[i] = sum_{(s, k) in list(t)} U_k[i] F_s[i]          (registers)
-//   L_t[a,b,c] += (1/PP) sum_k J[k] conj(w)^(k0 a + k1 b + k2 c)   (pruned
-//   inverse DFT in shared memory, one line per thread per axis pass)
 // J never leaves the SM.
 template <typename T, int L, int NT>
 __global__ void __launch_bounds__(NT, (sizeof(T) == 8 ? 512 : 1024) / NT) k_m2l(DevPlan P, int64_t t0, int64_t t1, int64_t f0, int64_t f1,
@@ -825,7 +886,6 @@ __global__ void __launch_bounds__(NT, (sizeof(T) == 8 ? 512 : 1024) / NT) k_m2l(
   C* Js = reinterpret_cast<C*>(smem_raw);
   C* Cb = Js + PP;
   C* D = Cb + L * PD * PD;
-  const T inv = T(1) / T(PP);
   __shared__ int64_t cur;
   // target slots are taken in order from a queue, so the slots in flight
   // stay a contiguous window of one cone (good L2 reuse of F and U)
@@ -854,55 +914,85 @@ __global__ void __launch_bounds__(NT, (sizeof(T) == 8 ? 512 : 1024) / NT) k_m2l(
         if (i < PP) cfma(acc[k], __ldg(U + i), __ldg(Fs + i));
       }
     }
-#pragma unroll
-    for (int k = 0; k < K; k++) {
-      const int i = threadIdx.x + k * NT;
-      if (i < PP) Js[i] = acc[k];
-    }
+    m2l_f2l<T, L, NT>(acc, Js, Cb, D, Lx + t * LL);
+  }
+}
+
+// Two consecutive target slots per CTA.  Each slot's list is sorted by
+// source slot, so a merge of the two lists finds their common sources
+// (about a third of the pairs at order 5), whose spectrum F_s is then read
+// once for both.  Every accumulator sees its own list in list order with the
+// same operations as k_m2l, so the results are bit-identical to it.
+template <typename T, int L, int NT>
+__global__ void __launch_bounds__(NT, (sizeof(T) == 8 ? 512 : 1024) / NT) k_m2l_pair(DevPlan P, int64_t t0, int64_t t1, int64_t f0, int64_t f1,
+                                                            const typename cpx_t<T>::type* __restrict__ F,
+                                                            const typename cpx_t<T>::type* __restrict__ ptab,
+                                                            typename cpx_t<T>::type* __restrict__ Lx,
+                                                            unsigned long long* __restrict__ queue) {
+  typedef typename cpx_t<T>::type C;
+  constexpr int PD = 2 * L - 1, LL = L * L * L, PP = PD * PD * PD, K = (PP + NT - 1) / NT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* Js = reinterpret_cast<C*>(smem_raw);
+  C* Cb = Js + PP;
+  C* D = Cb + L * PD * PD;
+  __shared__ int64_t cur;
+  for (;;) {
     __syncthreads();
-    for (int ln = threadIdx.x; ln < PD * PD; ln += NT) {  // axis 0: (k1,k2) lines -> a
-      C v[PD];
+    if (threadIdx.x == 0) cur = t0 + 2 * (int64_t)atomicAdd(queue, 1ULL);
+    __syncthreads();
+    const int64_t t = cur;
+    if (t >= t1) break;
+    const bool two = t + 1 < t1;
+    int64_t a = P.m2l_ptr[t], b = P.m2l_ptr[t + 1];
+    const int64_t ae = b, be = two ? P.m2l_ptr[t + 2] : b;
+    C acc0[K], acc1[K];
 #pragma unroll
-      for (int k0 = 0; k0 < PD; k0++) v[k0] = Js[k0 * PD * PD + ln];
+    for (int k = 0; k < K; k++) acc0[k] = acc1[k] = czero<C>();
+    while (a < ae || b < be) {
+      const int64_t sa = a < ae ? (int64_t)P.m2l_src[a] : INT64_MAX;
+      const int64_t sb = b < be ? (int64_t)P.m2l_src[b] : INT64_MAX;
+      const int64_t src = sa < sb ? sa : sb;
+      if (src < f0 || src >= f1) {  // entry outside this cone batch: a plan bug
+        if (threadIdx.x == 0) atomicExch(P.err, 1);
+        if (sa == src) a++;
+        if (sb == src) b++;
+        continue;
+      }
+      const C* Fs = F + (src - f0) * PP;
+      if (sa == sb) {
+        const C* U0 = ptab + (int64_t)P.m2l_tab[a] * PP;
+        const C* U1 = ptab + (int64_t)P.m2l_tab[b] * PP;
 #pragma unroll
-      for (int a = 0; a < L; a++) {
-        C s = v[0];
+        for (int k = 0; k < K; k++) {
+          const int i = threadIdx.x + k * NT;
+          if (i < PP) {
+            const C f = __ldg(Fs + i);
+            cfma(acc0[k], __ldg(U0 + i), f);
+            cfma(acc1[k], __ldg(U1 + i), f);
+          }
+        }
+        a++;
+        b++;
+      } else if (sa < sb) {
+        const C* U0 = ptab + (int64_t)P.m2l_tab[a] * PP;
 #pragma unroll
-        for (int k0 = 1; k0 < PD; k0++) cfmac(s, v[k0], ctw<T, L>((k0 * a) % PD));
-        Cb[a * PD * PD + ln] = s;
+        for (int k = 0; k < K; k++) {
+          const int i = threadIdx.x + k * NT;
+          if (i < PP) cfma(acc0[k], __ldg(U0 + i), __ldg(Fs + i));
+        }
+        a++;
+      } else {
+        const C* U1 = ptab + (int64_t)P.m2l_tab[b] * PP;
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+          const int i = threadIdx.x + k * NT;
+          if (i < PP) cfma(acc1[k], __ldg(U1 + i), __ldg(Fs + i));
+        }
+        b++;
       }
     }
-    __syncthreads();
-    for (int ln = threadIdx.x; ln < L * PD; ln += NT) {  // axis 1: (a,k2) lines -> b
-      const int a = ln / PD, k2 = ln % PD;
-      C v[PD];
-#pragma unroll
-      for (int k1 = 0; k1 < PD; k1++) v[k1] = Cb[(a * PD + k1) * PD + k2];
-#pragma unroll
-      for (int b = 0; b < L; b++) {
-        C s = v[0];
-#pragma unroll
-        for (int k1 = 1; k1 < PD; k1++) cfmac(s, v[k1], ctw<T, L>((k1 * b) % PD));
-        D[(a * L + b) * PD + k2] = s;
-      }
-    }
-    __syncthreads();
-    C* Lt = Lx + t * LL;
-    for (int ln = threadIdx.x; ln < L * L; ln += NT) {  // axis 2: (a,b) lines -> c
-      C v[PD];
-#pragma unroll
-      for (int k2 = 0; k2 < PD; k2++) v[k2] = D[ln * PD + k2];
-#pragma unroll
-      for (int c = 0; c < L; c++) {
-        C s = v[0];
-#pragma unroll
-        for (int k2 = 1; k2 < PD; k2++) cfmac(s, v[k2], ctw<T, L>((k2 * c) % PD));
-        C o = Lt[ln * L + c];
-        o.x += s.x * inv;
-        o.y += s.y * inv;
-        Lt[ln * L + c] = o;
-      }
-    }
+    m2l_f2l<T, L, NT>(acc0, Js, Cb, D, Lx + t * LL);
+    if (two) m2l_f2l<T, L, NT>(acc1, Js, Cb, D, Lx + (t + 1) * LL);
   }
 }
 
@@ -1685,6 +1775,10 @@ struct Launch {
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_m2l<T, L, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_m2l());
     if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_m2l_pair<T, L, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_m2l());
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_m2l_pair<T, L, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_m2l());
+    if (e != cudaSuccess) return e;
     return cudaSuccess;
   }
   static void p2m(const DevPlan& dp, const int32_t* leaves, int n, const void* q, const void* sig2, void* M,
@@ -1708,10 +1802,21 @@ struct Launch {
     if (n) k_m2f<T, L><<<grid_for(n, NW), 32 * NW, smem_m2f(), s>>>(n, (const C*)M, (C*)F);
   }
   static void m2l(const DevPlan& dp, int64_t t0, int64_t t1, int64_t f0, int64_t f1, const void* F,
-                  const void* ptab, void* Lx, unsigned long long* queue, int nsm, int nt, cudaStream_t s) {
+                  const void* ptab, void* Lx, unsigned long long* queue, int nsm, int nt, int pair,
+                  cudaStream_t s) {
     if (t1 <= t0) return;
     cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s);
     if (nt != 128 && nt != 256) nt = NT;
+    if (pair) {
+      const int grid = (int)std::min<int64_t>((t1 - t0 + 1) / 2, (int64_t)nsm * (2048 / nt));
+      if (nt == 256)
+        k_m2l_pair<T, L, 256><<<grid, 256, smem_m2l(), s>>>(dp, t0, t1, f0, f1, (const C*)F, (const C*)ptab, (C*)Lx,
+                                                            queue);
+      else
+        k_m2l_pair<T, L, 128><<<grid, 128, smem_m2l(), s>>>(dp, t0, t1, f0, f1, (const C*)F, (const C*)ptab, (C*)Lx,
+                                                            queue);
+      return;
+    }
     const int grid = (int)std::min<int64_t>(t1 - t0, (int64_t)nsm * (2048 / nt));
     if (nt == 256)
       k_m2l<T, L, 256><<<grid, 256, smem_m2l(), s>>>(dp, t0, t1, f0, f1, (const C*)F, (const C*)ptab, (C*)Lx, queue);

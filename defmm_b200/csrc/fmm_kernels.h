@@ -19,9 +19,10 @@ struct OpTable {
   void (*l2l)(const DevPlan&, int64_t s0, int64_t s1, const void* sig, const void* sig2, void* Lx, cudaStream_t);
   void (*m2f)(int64_t n, const void* M, void* F, cudaStream_t);
   // M2L with the inverse DFT fused: adds into L of target slots [t0, t1)
-  // nt: threads per target slot (128 or 256; 0 = the order's default)
+  // nt: threads per CTA (128 or 256; 0 = the order's default); pair != 0:
+  // two consecutive target slots per CTA sharing their common sources' loads
   void (*m2l)(const DevPlan&, int64_t t0, int64_t t1, int64_t f0, int64_t f1, const void* F, const void* ptab,
-              void* Lx, unsigned long long* queue, int nsm, int nt, cudaStream_t);
+              void* Lx, unsigned long long* queue, int nsm, int nt, int pair, cudaStream_t);
   void (*l2p)(const DevPlan&, const int32_t* leaves, int n, const void* sig2, const void* Lx, double2* pfar,
               cudaStream_t);
   // U_k = tables[key_k >> 6][perm[key_k & 63][:]] for the permuted spectra

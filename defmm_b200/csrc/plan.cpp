@@ -1109,7 +1109,9 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
   cell_csr(p.T, p.sT);
   cell_csr(p.S, p.sS);
 
-  // M2L grouped by target slot (stable: depth-first order within a slot)
+  // M2L grouped by target slot, each slot's entries by increasing source
+  // slot (so that consecutive target slots can be merged on their common
+  // sources; a slot meets each source slot at most once)
   if (!w.m2l_done) {
     p.m2l_ptr.assign(p.sT.n + 1, 0);
     for (int l = 0; l < nlvl; l++)
@@ -1129,6 +1131,20 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
       std::vector<int32_t>().swap(w.far_ss[l]);
       std::vector<uint32_t>().swap(w.far_tab[l]);
     }
+    pfor(p.sT.n, 1024, [&](int64_t t) {  // insertion sort: a slot has a few hundred entries at most
+      const int64_t b = p.m2l_ptr[t], e = p.m2l_ptr[t + 1];
+      for (int64_t q = b + 1; q < e; q++) {
+        const int32_t sq = p.m2l_src[q];
+        const uint32_t kq = p.m2l_tab[q];
+        int64_t r = q;
+        for (; r > b && p.m2l_src[r - 1] > sq; r--) {
+          p.m2l_src[r] = p.m2l_src[r - 1];
+          p.m2l_tab[r] = p.m2l_tab[r - 1];
+        }
+        p.m2l_src[r] = sq;
+        p.m2l_tab[r] = kq;
+      }
+    });
   }
 
   // permuted spectra: one per (spectrum, symmetry hash) pair that occurs

@@ -273,6 +273,12 @@ __global__ void k_gather_entries(int64_t n, const int32_t* __restrict__ order, c
   used[tab[o]] = 1;
 }
 
+__global__ void k_gather_i32(int64_t n, const int32_t* __restrict__ order, const int32_t* __restrict__ in,
+                             int32_t* __restrict__ out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) out[i] = in[order[i]];
+}
+
 __global__ void k_renumber(int64_t n, const int32_t* __restrict__ pid, uint32_t* __restrict__ key) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) key[i] = (uint32_t)pid[key[i]];
@@ -657,18 +663,33 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
   DW_ALLOC(keys_out, int32_t, n);
   DW_ALLOC(idx_out, int32_t, n);
   if (n) k_iota<<<nblk(n), 256>>>(n, idx);
-  int bits = 1;
-  while (bits < 31 && ((int64_t)1 << bits) <= p.sT.n) bits++;
-  {
+  // entries grouped by target slot and, within a slot, by increasing source
+  // slot: a stable sort by source, then a stable sort by target
+  auto sort_by = [&](const int32_t* keys, int64_t range, int32_t* vin, int32_t* vout) -> int {
+    int bits = 1;
+    while (bits < 31 && ((int64_t)1 << bits) <= range) bits++;
     size_t need = 0;
-    DW_CK(cub::DeviceRadixSort::SortPairs(nullptr, need, all_ts, keys_out, idx, idx_out, n, 0, bits));
+    DW_CK(cub::DeviceRadixSort::SortPairs(nullptr, need, keys, keys_out, vin, vout, n, 0, bits));
     char* t2 = A.get<char>(need);
     if (!t2) {
       err = "device plan: out of device memory";
       return -5;
     }
-    DW_CK(cub::DeviceRadixSort::SortPairs(t2, need, all_ts, keys_out, idx, idx_out, n, 0, bits));
+    DW_CK(cub::DeviceRadixSort::SortPairs(t2, need, keys, keys_out, vin, vout, n, 0, bits));
     A.drop(t2);
+    return 0;
+  };
+  if ((st = sort_by(all_ss, p.sS.n, idx, idx_out))) return st;  // idx_out: entries by source
+  {
+    int32_t* ts_by_src = A.get<int32_t>(std::max<int64_t>(1, n));
+    if (!ts_by_src) {
+      err = "device plan: out of device memory";
+      return -5;
+    }
+    if (n) k_gather_i32<<<nblk(n), 256>>>(n, idx_out, all_ts, ts_by_src);
+    if ((st = sort_by(ts_by_src, p.sT.n, idx_out, idx))) return st;  // idx: by target, then source
+    A.drop(ts_by_src);
+    std::swap(idx, idx_out);  // the gather below reads idx_out
   }
   const int64_t nslot = p.sT.n, ntab = (int64_t)walk.tab_nI.size() * 64;
   DW_ALLOC(cnt, int32_t, nslot + 1);

@@ -169,6 +169,7 @@ int defmm_direct_noalloc(defmm_handle* h, const double* d_targets, int64_t nt,
 #define DEFMM_INFO_PLAN_WALK_MS 22     /* of which the level walk, ms */
 #define DEFMM_INFO_M2L_THREADS 23      /* M2L threads per target slot (current precision) */
 #define DEFMM_INFO_P2P_BLOCKS_PER_SM 24 /* near-field CTAs per SM (current precision) */
+#define DEFMM_INFO_M2L_PAIRING 25       /* 1: two target slots per M2L CTA (current precision) */
 int defmm_info(const defmm_handle* h, int what, int64_t* value);
 
 /* Per-phase device times (ms) of the last gemv, in this order:
@@ -199,16 +200,21 @@ int defmm_set_plan_device(defmm_handle* h, int on);
 /* No counterpart in the reference.  Autotuner: on this operator and its
  * current precision, times `reps` profiled matvecs (zero charges, the
  * handle's own vectors) per candidate launch choice and keeps the fastest:
- * M2L threads per target slot (128 or 256, timed on the M2L phase) and
- * near-field CTAs per SM (8, 16 or 32, timed on the near-field phase).
- * Every choice gives bit-identical results.  The chosen pair is written to
- * choice[2] when not NULL (also DEFMM_INFO_M2L_THREADS /
- * DEFMM_INFO_P2P_BLOCKS_PER_SM); the next matvec captures a new graph. */
+ * M2L threads per CTA (128 or 256) with one or two target slots per CTA
+ * (timed on the M2L phase) and near-field CTAs per SM (8, 16 or 32, timed on
+ * the near-field phase).  Every choice gives bit-identical results.  The
+ * M2L threads and near-field CTAs per SM are written to choice[2] when not
+ * NULL (also DEFMM_INFO_M2L_THREADS / DEFMM_INFO_P2P_BLOCKS_PER_SM; the
+ * pairing: DEFMM_INFO_M2L_PAIRING); the next matvec captures a new graph. */
 int defmm_autotune(defmm_handle* h, int reps, int32_t* choice);
 /* No counterpart in the reference.  Sets the same launch choices by hand for
  * the current precision: m2l_threads 128 or 256 (0: the order's default),
  * p2p_blocks_per_sm 1..64 (0: 16). */
 int defmm_set_launch(defmm_handle* h, int m2l_threads, int p2p_blocks_per_sm);
+/* No counterpart in the reference.  on = 1: each M2L CTA takes two
+ * consecutive target slots and reads a source spectrum the two share once
+ * (current precision); 0: one slot per CTA. */
+int defmm_set_m2l_pairing(defmm_handle* h, int on);
 
 /* Tree dump in the layout of the reference's cell array (SourceRoot /
  * TargetRoot, interface.hpp:174-175; cells in depth-first pre-order):

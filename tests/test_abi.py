@@ -45,6 +45,10 @@ def test_argument_checks_without_device():
             A.set_launch(nt, bps)
     A.set_launch(256, 8)  # valid choices are recorded without a device
     with pytest.raises(api.DefmmError):
+        A._check(api.lib().defmm_set_m2l_pairing(A._h, 2))
+    A.set_m2l_pairing(True)
+    A.set_m2l_pairing(False)
+    with pytest.raises(api.DefmmError):
         A.autotune(reps=0)
     with pytest.raises(api.DefmmError):
         A.autotune(reps=1)  # before prcmpt

@@ -215,20 +215,25 @@ def test_device_multi_rhs_equals_single_calls(gpu):
 
 
 def test_launch_choices_and_autotune_keep_results_bit_identical(gpu):
-    # M2L threads per target slot and near-field CTAs per SM change only the
-    # schedule: every combination gives the same bits
+    # M2L threads per CTA, one or two target slots per M2L CTA and near-field
+    # CTAs per SM change only the schedule: every combination gives the same
+    # bits
     src, trg, q, L, ncrit, kappa, lvmax = case_inputs("sphere_l6")
     A = make(src, trg, L, ncrit, kappa, lvmax)
     for prec in ("fp64", "mixed"):
         A.set_precision(prec)
         ref = A.matvec(q)
-        for nt in (128, 256):
-            for bps in (8, 32):
-                A.set_launch(nt, bps)
-                assert A.info("m2l_threads") == nt and A.info("p2p_blocks_per_sm") == bps
-                assert np.array_equal(A.matvec(q), ref)
+        for pair in (False, True):
+            A.set_m2l_pairing(pair)
+            for nt in (128, 256):
+                for bps in (8, 32):
+                    A.set_launch(nt, bps)
+                    assert A.info("m2l_threads") == nt and A.info("p2p_blocks_per_sm") == bps
+                    assert A.info("m2l_pairing") == int(pair)
+                    assert np.array_equal(A.matvec(q), ref)
         c = A.autotune(reps=1)
         assert c["m2l_threads"] in (128, 256) and c["p2p_blocks_per_sm"] in (8, 16, 32)
+        assert c["m2l_pairing"] in (0, 1)
         assert A.info("m2l_threads") == c["m2l_threads"]
         assert np.array_equal(A.matvec(q), ref)
 
