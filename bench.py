@@ -420,8 +420,9 @@ def main():
         A.set_precision(prec)
         if not args.no_autotune:  # launch choices timed on this operator (defmm_autotune)
             t0 = time.perf_counter()
-            tune[prec] = A.autotune(reps=1)
+            A.autotune(reps=1)
             tune_s += time.perf_counter() - t0
+        tune[prec] = {k: A.info(k) for k in ("m2l_threads", "m2l_pairing", "p2p_blocks_per_sm")}
         for _ in range(args.warmup):
             A.matvec_device(dq.data_ptr(), dp.data_ptr(), 1, stream.cuda_stream)
         torch.cuda.synchronize()
@@ -481,18 +482,23 @@ def main():
                  + 2 * e * L ** 3 * info["m2l_targets"] + 8 * n_far)
     m2l_ms = phases[head]["m2l"]
     achieved = m2l_bytes / (m2l_ms * 1e-3) / 1e9
+    # the M2L kernel this run used (launch choice of the headline precision)
+    lc = tune[head]
+    kname = "%s<%s, %d, %d>" % ("k_m2l_pair" if lc["m2l_pairing"] else "k_m2l",
+                                "double" if head == "fp64" else "float", L, lc["m2l_threads"])
+    # DRAM traffic per far pair of the same kernel, measured by ncu on a
+    # smaller sphere and scaled by the far pairs of this workload
     traffic = None
     tp = os.path.join(ROOT, "profiles", "m2l_traffic.json")
     if os.path.exists(tp):
         try:
             with open(tp) as f:
-                tr = json.load(f)
-            traffic = tr.get(head, {}).get("bytes_per_pair", None)
-            if traffic is not None:
-                traffic = traffic * n_far
+                tr = json.load(f).get(head, {})
+            if tr.get("kernel") == kname and tr.get("bytes_per_pair") is not None:
+                traffic = tr["bytes_per_pair"] * n_far
         except (OSError, ValueError):
             traffic = None
-    roofline = {"bound": "hbm", "kernel": "k_m2l (M2L + inverse DFT, all cone batches)", "achieved": achieved,
+    roofline = {"bound": "hbm", "kernel": kname + " (M2L + inverse DFT, all cone batches)", "achieved": achieved,
                 "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_source": src,
                 "traffic": traffic, "algorithmic_bytes": m2l_bytes}
 

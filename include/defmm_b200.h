@@ -102,8 +102,8 @@ int defmm_gemv_device(defmm_handle* h, const void* d_in, void* d_out,
  * over `lanes` >= 1 chains (largest first, onto the chain with the fewest
  * points so far): matvecs of one chain run in turn, chains run concurrently.
  * The handles and buffers must outlive the batch; after prcmpt,
- * defmm_set_precision, defmm_autotune or defmm_set_launch on a member,
- * create the batch again (it holds a copy of the member's graph).  Returns NULL on
+ * defmm_set_precision, defmm_autotune, defmm_set_launch or
+ * defmm_set_m2l_pairing on a member, create the batch again (it holds a copy of the member's graph).  Returns NULL on
  * failure (see the members' defmm_last_error). */
 typedef struct defmm_batch defmm_batch;
 defmm_batch* defmm_batch_create(int64_t n, defmm_handle* const* hs,
