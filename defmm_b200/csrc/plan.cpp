@@ -1161,21 +1161,30 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
     pfor((int64_t)p.m2l_tab.size(), 1 << 16, [&](int64_t e) { p.m2l_tab[e] = (uint32_t)pid[p.m2l_tab[e]]; });
   }
 
-  // CSR over slots from a per-slot visitor visit(k, emit): counted, then
-  // filled, both passes in parallel over slots
+  // CSR over slots from a per-slot visitor visit(k, emit), in slot order:
+  // blocks of slots are visited in parallel once, each into its own buffer
+  // (ptr holding block-local offsets), then shifted and copied into place
   auto slot_csr = [&](int64_t n, auto visit, std::vector<int64_t>& ptr, std::vector<int32_t>& out) {
-    std::vector<int32_t> cnt(n, 0);
-    pfor(n, 4096, [&](int64_t k) {
-      int32_t c = 0;
-      visit(k, [&](int64_t) { c++; });
-      cnt[k] = c;
-    });
+    constexpr int64_t B = 1 << 15;  // slots per block
+    const int64_t nb = (n + B - 1) / B;
+    std::vector<std::vector<int32_t>> part(nb);
     ptr.assign(n + 1, 0);
-    for (int64_t k = 0; k < n; k++) ptr[k + 1] = ptr[k] + cnt[k];
-    out.resize(ptr[n]);
-    pfor(n, 4096, [&](int64_t k) {
-      int64_t o = ptr[k];
-      visit(k, [&](int64_t x) { out[o++] = (int32_t)x; });
+    pfor(nb, 1, [&](int64_t b) {
+      const int64_t k1 = std::min(n, (b + 1) * B);
+      auto& v = part[b];
+      for (int64_t k = b * B; k < k1; k++) {
+        visit(k, [&](int64_t x) { v.push_back((int32_t)x); });
+        ptr[k + 1] = (int64_t)v.size();
+      }
+    });
+    std::vector<int64_t> boff(nb + 1, 0);
+    for (int64_t b = 0; b < nb; b++) boff[b + 1] = boff[b] + (int64_t)part[b].size();
+    out.resize(boff[nb]);
+    pfor(nb, 1, [&](int64_t b) {
+      const int64_t k1 = std::min(n, (b + 1) * B);
+      for (int64_t k = b * B; k < k1; k++) ptr[k + 1] += boff[b];
+      std::copy(part[b].begin(), part[b].end(), out.begin() + boff[b]);
+      std::vector<int32_t>().swap(part[b]);
     });
   };
   // M2M: children slots of each source slot (P2M/M2M operators, M2M.hpp:35-124)
@@ -1285,19 +1294,33 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
           out.push_back(x);
       }
     });
-    p.p2p_ptr.assign(1, 0);
+    // chunks of <= 32 targets per leaf, each with the leaf's ranges: offsets
+    // per leaf in leaf order, then a parallel fill
+    std::vector<int64_t> ch_off(p.T.ncell + 1, 0), rg_off(p.T.ncell + 1, 0);
     for (int64_t c = 0; c < p.T.ncell; c++) {
-      if (merged[c].empty()) continue;
-      for (int32_t off = 0; off < p.T.nprt[c]; off += 32) {
-        p.p2p_tfirst.push_back(p.T.first[c] + off);
-        p.p2p_tn.push_back(std::min(32, p.T.nprt[c] - off));
-        for (auto& x : merged[c]) {
-          p.p2p_sfirst.push_back(x.first);
-          p.p2p_sn.push_back(x.second);
-        }
-        p.p2p_ptr.push_back((int64_t)p.p2p_sfirst.size());
-      }
+      const int64_t nch = merged[c].empty() ? 0 : (p.T.nprt[c] + 31) / 32;
+      ch_off[c + 1] = ch_off[c] + nch;
+      rg_off[c + 1] = rg_off[c] + nch * (int64_t)merged[c].size();
     }
+    p.p2p_tfirst.resize(ch_off[p.T.ncell]);
+    p.p2p_tn.resize(ch_off[p.T.ncell]);
+    p.p2p_ptr.assign(ch_off[p.T.ncell] + 1, 0);
+    p.p2p_sfirst.resize(rg_off[p.T.ncell]);
+    p.p2p_sn.resize(rg_off[p.T.ncell]);
+    pfor(p.T.ncell, 64, [&](int64_t c) {
+      if (merged[c].empty()) return;
+      int64_t q = ch_off[c], r = rg_off[c];
+      for (int32_t off = 0; off < p.T.nprt[c]; off += 32, q++) {
+        p.p2p_tfirst[q] = p.T.first[c] + off;
+        p.p2p_tn[q] = std::min(32, p.T.nprt[c] - off);
+        for (auto& x : merged[c]) {
+          p.p2p_sfirst[r] = x.first;
+          p.p2p_sn[r] = x.second;
+          r++;
+        }
+        p.p2p_ptr[q + 1] = r;
+      }
+    });
   }
   if (p.p2p_sym) {
     build_symmetric_near(p);
