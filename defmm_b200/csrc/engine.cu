@@ -79,6 +79,9 @@ struct defmm_handle {
   double phase_ms[PH_N] = {0};
   cudaEvent_t ev[2 * PH_N] = {};
   cudaEvent_t ev_ready = nullptr, ev_done = nullptr;  // cross-stream ordering
+  // recorded by defmm_direct_noalloc after its last read of qin (on the
+  // caller's stream); the next host gemv waits for it before overwriting qin
+  cudaEvent_t ev_qin_read = nullptr;
   bool events = false;
   bool has_out = false;
   int64_t launches = 0;  // kernels launched by the last gemv call
@@ -606,6 +609,7 @@ int ensure_device(defmm_handle* h) {
   for (int i = 0; i < 2 * PH_N; i++) CK(cudaEventCreate(&h->ev[i]));
   CK(cudaEventCreateWithFlags(&h->ev_ready, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&h->ev_done, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&h->ev_qin_read, cudaEventDisableTiming));
   return 0;
 }
 
@@ -641,6 +645,7 @@ void defmm_destroy(defmm_handle* h) {
       if (h->ev[i]) cudaEventDestroy(h->ev[i]);
     if (h->ev_ready) cudaEventDestroy(h->ev_ready);
     if (h->ev_done) cudaEventDestroy(h->ev_done);
+    if (h->ev_qin_read) cudaEventDestroy(h->ev_qin_read);
     if (h->st) cudaStreamDestroy(h->st);
     if (h->st2) cudaStreamDestroy(h->st2);
   }
@@ -958,6 +963,9 @@ int defmm_gemv_batched(defmm_handle* h, int64_t nrhs, const double* in, double* 
   if (st) return st;
   const int64_t nS = (int64_t)h->plan.S.perm.size(), nT = (int64_t)h->plan.T.perm.size();
   h->launches = 0;
+  // direct sums still reading the previous charges (defmm_direct_noalloc on
+  // another stream) finish before qin is overwritten
+  CK(cudaStreamWaitEvent(h->st, h->ev_qin_read, 0));
   for (int64_t r = 0; r < nrhs; r++) {
     CK(cudaMemcpyAsync(h->qin.p, in + 2 * r * nS, 16 * nS, cudaMemcpyHostToDevice, h->st));
     st = matvec(h, (const double2*)h->qin.p, (double2*)h->out.p, h->st);
@@ -1144,6 +1152,7 @@ int dfb::handle_view(defmm_handle* h, dfb::HandleView* v) {
   v->S_pos = h->dp.S_pos;
   v->S_perm = h->dp.S_perm;
   v->qin = (const double2*)h->qin.p;
+  v->qin_read = h->ev_qin_read;
   v->kappa = h->plan.kappa;
   return 0;
 }

@@ -16,6 +16,9 @@ struct HandleView {
   const double* S_pos = nullptr;  // 3 per source, tree order (device)
   const int32_t* S_perm = nullptr;  // tree position -> user index (device)
   const double2* qin = nullptr;   // charges of the last host gemv, user order (device)
+  // record on the stream that last reads qin: the handle's next host gemv
+  // waits for it before overwriting qin
+  cudaEvent_t qin_read = nullptr;
   double kappa = 0.;
 };
 

@@ -8,7 +8,10 @@
 // buffer for its samples; this entry point keeps its scratch in a file-scope
 // device array instead, so a call allocates nothing.  The first call on a
 // device looks up the array's address (cudaGetSymbolAddress, which may load
-// this file's device code); make that call before any stream capture.
+// this file's device code); make that call before any stream capture.  The
+// call reads the charges of the handle's last host gemv on the caller's
+// stream; the handle's next host gemv waits for that read (an event) before
+// it overwrites them.
 //
 // The scratch array is shared by every call on a device and keeps the last
 // call's contents.  Calls that overlap on the GPU (two streams, two threads,
@@ -30,9 +33,10 @@ constexpr int kTile = 256; // sources staged in shared memory per step
 
 // partial[s * nt + t] = sum over source chunk s of q_j G(x_t, y_j): the
 // reference's CheckFULL / P2P arithmetic (include/interface.hpp:178-221,
-// include/operators/P2P.hpp:43-79), FP64, pairs with |x - y|^2 < 1e-16
-// skipped.  Every (s, t < nt) entry is written, empty
-// chunks included, so nothing in the scratch needs clearing first.
+// include/operators/P2P.hpp:43-79), FP64; pairs with |x - y|^2 < 1e-16
+// (|x - y| < 1e-8) contribute zero, as in the reference's CheckFULL.  Every
+// (s, t < nt) entry is written, empty chunks included, so nothing in the
+// scratch needs clearing first.
 __global__ void __launch_bounds__(kTPB) k_direct_partial(int64_t ns, const double* __restrict__ spos,
                                                          const int32_t* __restrict__ sperm,
                                                          const double2* __restrict__ qin, int64_t nt,
@@ -94,18 +98,22 @@ __global__ void k_direct_reduce(int64_t nt, int S, const double2* __restrict__ p
   out[t] = a;
 }
 
-// Device address of the scratch array, looked up once per device (host code
-// may not pass the symbol itself to a kernel: it names a host-side stand-in).
+// Device address of the scratch array, per device (host code may not pass
+// the symbol itself to a kernel: it names a host-side stand-in).  Outside
+// stream capture the address is looked up on every call, which costs a table
+// lookup once the module is loaded and stays right after a device reset
+// reloads it; inside a capture the address of the last uncaptured call on
+// that device is used, so a call must precede any capture.
 std::mutex g_mu;
 void* g_addr[64] = {nullptr};
 
-int scratch_address(int dev, double2** out, std::string& err) {
+int scratch_address(int dev, bool capturing, double2** out, std::string& err) {
   if (dev < 0 || dev >= 64) {
     err = "device index out of range";
     return DEFMM_ERR_ARG;
   }
   std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_addr[dev]) {
+  if (!capturing) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_direct_scratch);
     if (e != cudaSuccess) {
@@ -114,10 +122,27 @@ int scratch_address(int dev, double2** out, std::string& err) {
       return DEFMM_ERR_CUDA;
     }
     g_addr[dev] = p;
+  } else if (!g_addr[dev]) {
+    err = "defmm_direct_noalloc: the first call on a device must come before any stream capture";
+    return DEFMM_ERR_ARG;
   }
   *out = static_cast<double2*>(g_addr[dev]);
   return 0;
 }
+
+// The calling thread's current device, put back on every return.
+struct DeviceGuard {
+  int prev = -1;
+  DeviceGuard() {
+    if (cudaGetDevice(&prev) != cudaSuccess) {
+      cudaGetLastError();
+      prev = -1;
+    }
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
 
 }  // namespace
 
@@ -130,11 +155,16 @@ extern "C" int defmm_direct_noalloc(defmm_handle* h, const double* d_targets, in
   if (nt > kScratchElems)
     return dfb::handle_fail(h, DEFMM_ERR_ARG,
                             "defmm_direct_noalloc: at most 262144 targets per call (scratch of 4 MiB)");
+  DeviceGuard guard;
   cudaError_t e = cudaSetDevice(v.device);
+  if (e != cudaSuccess) return dfb::handle_fail(h, DEFMM_ERR_CUDA, cudaGetErrorString(e));
+  cudaStream_t s = stream ? (cudaStream_t)stream : v.stream;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(s, &cap);
   if (e != cudaSuccess) return dfb::handle_fail(h, DEFMM_ERR_CUDA, cudaGetErrorString(e));
   std::string msg;
   double2* partial = nullptr;
-  st = scratch_address(v.device, &partial, msg);
+  st = scratch_address(v.device, cap != cudaStreamCaptureStatusNone, &partial, msg);
   if (st) return dfb::handle_fail(h, st, msg.c_str());
   // as many source chunks as the scratch holds (<= 64), at most one per 1024 sources
   int64_t S = kScratchElems / nt;
@@ -142,11 +172,14 @@ extern "C" int defmm_direct_noalloc(defmm_handle* h, const double* d_targets, in
   const int64_t Smax = (v.nS + 1023) / 1024;
   S = S < Smax ? S : Smax;
   if (S < 1) S = 1;
-  cudaStream_t s = stream ? (cudaStream_t)stream : v.stream;
   dim3 grid((unsigned)((nt + kTPB - 1) / kTPB), (unsigned)S);
   k_direct_partial<<<grid, kTPB, 0, s>>>(v.nS, v.S_pos, v.S_perm, v.qin, nt, d_targets, v.kappa, (int)S, partial);
   k_direct_reduce<<<(unsigned)((nt + 255) / 256), 256, 0, s>>>(nt, (int)S, partial, reinterpret_cast<double2*>(d_out));
   e = cudaGetLastError();
+  if (e != cudaSuccess) return dfb::handle_fail(h, DEFMM_ERR_CUDA, cudaGetErrorString(e));
+  // the handle's next host gemv overwrites the charges read here: it waits
+  // for this event first
+  e = cudaEventRecord(v.qin_read, s);
   if (e != cudaSuccess) return dfb::handle_fail(h, DEFMM_ERR_CUDA, cudaGetErrorString(e));
   return 0;
 }

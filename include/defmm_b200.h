@@ -128,18 +128,22 @@ int defmm_check_full(defmm_handle* h, int64_t nsamples, uint64_t seed,
 /* No counterpart in the reference.  FP64 direct sums, the arithmetic of
  * defmm_check_full, that allocate no device memory: out[t] = sum_j q_j
  * exp(i kappa |x_t - y_j|) / (4 pi |x_t - y_j|) over the handle's sources
- * y_j with the charges q_j of the last host gemv (its last right-hand side),
- * pairs closer than 1e-8 skipped.  d_targets: nt x 3 doubles, d_out: nt
- * complex doubles, both device pointers the caller owns; runs on `stream`
- * (NULL = the handle's own stream) without synchronising.
+ * y_j with the charges q_j of the last host gemv (its last right-hand side);
+ * pairs with |x_t - y_j|^2 < 1e-16 (|x_t - y_j| < 1e-8) contribute zero, as in
+ * the reference's CheckFULL.  d_targets: nt x 3 doubles, d_out: nt complex
+ * doubles, both device pointers the caller owns; runs on `stream` (NULL = the
+ * handle's own stream) without synchronising.
  *   - Scratch is a fixed 4 MiB array in the library's device image, so
  *     nt <= 262144 (DEFMM_ERR_ARG beyond, with a message).
- *   - The first call on a device looks up that array's address once (a
- *     runtime query, no allocation); make one call before any stream
- *     capture that should contain it.
+ *   - The first call on a device looks up that array's address (a runtime
+ *     query, no allocation); make one call before any stream capture that
+ *     should contain it.  Outside a capture every call looks it up again.
  *   - All calls on one device share the scratch: calls that can overlap on
  *     the GPU (different streams, threads or handles) race and must be
- *     serialised by the caller. */
+ *     serialised by the caller.
+ *   - The call reads the handle's device copy of the charges on `stream`;
+ *     the handle's next host gemv waits for that read before overwriting
+ *     them.  The calling thread's current device is left as it was. */
 int defmm_direct_noalloc(defmm_handle* h, const double* d_targets, int64_t nt,
                          double* d_out, void* stream);
 

@@ -7,6 +7,9 @@ import subprocess
 
 import pytest
 
+from oracle import refsrc
+
+REF = refsrc.reference_dir()
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIBDIR = os.path.join(ROOT, "defmm_b200")
 
@@ -23,12 +26,12 @@ def test_facade_driver_compiles(tmp_path):
                    os.path.join(ROOT, "include"))
 
 
-@pytest.mark.skipif(not os.path.isfile("/root/reference/test/testinterface.cpp"),
+@pytest.mark.skipif(not REF or not os.path.isfile(os.path.join(REF, "test", "testinterface.cpp")),
                     reason="reference checkout absent")
 def test_reference_driver_compiles_unchanged(tmp_path):
     # the reference's driver includes "../include/interface.hpp"
     (tmp_path / "test").mkdir()
-    shutil.copy("/root/reference/test/testinterface.cpp", tmp_path / "test")
+    shutil.copy(os.path.join(REF, "test", "testinterface.cpp"), tmp_path / "test")
     os.symlink(os.path.join(ROOT, "include"), tmp_path / "include")
     compile_driver(str(tmp_path / "test" / "testinterface.cpp"), str(tmp_path / "testinterface"),
                    str(tmp_path / "include"))
