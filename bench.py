@@ -128,6 +128,138 @@ def measured_peaks():
         return 6650.0, 1590.0, "fallback"
 
 
+REF_FFT = ("FFTW-API shim of the oracle (DFT by definition, oracle/shim/fftw_shim.cpp): FFTW3 is not in "
+           "the image, so the reference's M2F/F2L run slower than with FFTW")
+# nominal CUDA-core peaks (no measured figure exists in MEASURED_PEAKS.json):
+# 148 SMs x FMA lanes per SM x 2 flops x the maximum SM clock
+NOMINAL = {"fp32_tflops": 148 * 128 * 2 * 1.965e9 / 1e12, "fp64_tflops": 148 * 64 * 2 * 1.965e9 / 1e12}
+
+
+def l2_copy_bandwidth(torch):
+    """Read+write GB/s of a torch copy between two 24 MB device buffers
+    (both resident in the 126 MB L2), best of 5 runs of 200 copies: the
+    denominator of L2-bound kernels (MEASURED_PEAKS.json has HBM only)."""
+    a = torch.empty(6 << 20, dtype=torch.float32, device="cuda")
+    b = torch.empty_like(a)
+    for _ in range(20):
+        b.copy_(a)
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(200):
+            b.copy_(a)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2 * a.numel() * 4 * 200 / (e0.elapsed_time(e1) * 1e-3) / 1e9)
+    return best
+
+
+def phase_rooflines(info, L, phases, head, hn, peaks, l2_gbs, tune):
+    """Per-phase achieved rate against the resource that bounds it, for the
+    headline form (per right-hand side of a block: the phase times of one
+    profiled pass divided by its right-hand sides).
+
+      M2L: L2-to-SM bytes, 2 e P^3 per far pair in a one-right-hand-side pass
+           (source spectrum and transfer spectrum), e P^3 (1 + 1/RB) in a
+           block pass (each transfer-spectrum entry read once per RB
+           right-hand sides); against the measured L2 copy bandwidth.  The
+           same kernel's HBM figure (each spectrum once) beside it.
+      P2P: 20 flops per particle interaction (i_near) against the CUDA-core
+           FP64 (plain) or FP32 (mixed) nominal peak.
+      M2F: e (L^3 + P^3) bytes per transformed slot, against measured HBM.
+      M2M, L2L: 12 L^4 flops per transfer (three separable passes of L^4
+           real-by-complex MACs); P2M, L2P: 4 L^3 flops per (particle, slot):
+           against the CUDA-core nominal peak of the path's precision."""
+    hbm, _, src = peaks
+    fp64 = head == "fp64"
+    e = 16 if fp64 else 8
+    P3, L3 = (2 * L - 1) ** 3, L ** 3
+    ph = phases["mixed_block" if head == "mixed_block" else head]
+    per = hn if head == "mixed_block" else 1
+    n_far = info["far_hf"] + info["far_lf"]
+    rb = 8 if head == "mixed_block" else 1
+    flop_peak = NOMINAL["fp64_tflops"] if fp64 else NOMINAL["fp32_tflops"]
+    out = {}
+
+    def add(name, work, unit, peak, bound, t_ms, note):
+        t = t_ms / per
+        ach = work / (t * 1e-3) / (1e9 if unit == "GB/s" else 1e12) if t > 0 else None
+        out[name] = {"bound": bound, "achieved": ach, "peak": peak, "unit": unit,
+                     "frac": (ach / peak) if ach else None, "ms_per_rhs": t, "work_per_rhs": work, "note": note}
+    m2l_l2 = (e * P3 * (1 + 1.0 / rb) if rb > 1 else 2 * e * P3) * n_far
+    add("m2l", m2l_l2, "GB/s", l2_gbs, "l2", ph["m2l"], "L2-to-SM spectra bytes; peak: L2 copy bandwidth measured here")
+    add("p2p", 20.0 * info["i_near"], "TFLOP/s", flop_peak, "fp64" if fp64 else "fp32", ph["p2p"],
+        "20 flops per interaction; nominal CUDA-core peak")
+    add("m2f", e * (L3 + P3) * info["m2f_slots"], "GB/s", hbm, "hbm", ph["m2f"], "M read, F written once")
+    add("m2m", 12.0 * L ** 4 * info["m2m_entries"], "TFLOP/s", flop_peak, "fp64" if fp64 else "fp32", ph["m2m"],
+        "separable transfers; nominal CUDA-core peak")
+    add("l2l", 12.0 * L ** 4 * info["l2l_entries"], "TFLOP/s", flop_peak, "fp64" if fp64 else "fp32", ph["l2l"],
+        "separable transfers; nominal CUDA-core peak")
+    add("p2m", 4.0 * L3 * info["p2m_point_slots"], "TFLOP/s", flop_peak, "fp64" if fp64 else "fp32", ph["p2m"],
+        "leaf interpolation GEMM; nominal CUDA-core peak")
+    add("l2p", 4.0 * L3 * info["l2p_point_slots"], "TFLOP/s", flop_peak, "fp64" if fp64 else "fp32", ph["l2p"],
+        "leaf interpolation; nominal CUDA-core peak")
+    # the dominant kernel of the headline: M2L, against L2 (its binding
+    # resource), with the HBM view (each spectrum once) alongside
+    m2l_hbm = (e * P3 * info["slots_S"] * (1 if rb == 1 else 1) + e * P3 * info["permuted_spectra"] / rb
+               + 2 * e * L3 * info["m2l_targets"] + 8 * n_far / rb)
+    t = ph["m2l"] / per
+    lc = tune.get("mixed" if head != "fp64" else "fp64", {})
+    if head == "mixed_block":
+        kname = "k_m2l_rhs<float, %d, 256, 8>" % L
+    else:
+        kname = "%s<%s, %d, %d>" % ("k_m2l_pair" if lc.get("m2l_pairing") else "k_m2l",
+                                    "double" if fp64 else "float", L, lc.get("m2l_threads", 128))
+    head_rl = dict(out["m2l"])
+    head_rl.update({"kernel": kname + " (M2L + inverse DFT, all cone batches)", "peak_source": "measured here (L2 copy)",
+                    "traffic": None, "hbm": {"achieved": m2l_hbm / (t * 1e-3) / 1e9, "peak": hbm,
+                                             "frac": m2l_hbm / (t * 1e-3) / 1e9 / hbm, "peak_source": src,
+                                             "algorithmic_bytes_per_rhs": m2l_hbm}})
+    tp = os.path.join(ROOT, "profiles", "m2l_traffic.json")
+    if os.path.exists(tp):
+        try:
+            with open(tp) as f:
+                tr = json.load(f).get(head, {})
+            if tr.get("kernel") == kname and tr.get("bytes_per_pair") is not None:
+                head_rl["traffic"] = tr["bytes_per_pair"] * n_far
+        except (OSError, ValueError):
+            pass
+    return {"headline": head_rl, "phases": out}
+
+
+def sample_comparison(torch, ws, qs, desc, cpu_value, stream):
+    """The GPU paths on exactly the CPU baseline's sample (same points,
+    charges, wavenumber, order and leaf size): a like-for-like ratio."""
+    from defmm_b200 import IBFMM_Mat
+    B = IBFMM_Mat()
+    B.addSourceParticles(ws.points)
+    B.addTargetParticles(ws.points)
+    B.prcmpt(ws.order, ws.ncrit, ws.kappa)
+    dq = torch.from_numpy(qs).cuda()
+    dp = torch.empty(ws.n, dtype=torch.complex128, device="cuda")
+    out = {"sample": desc, "same_config": True, "cpu_points_per_s": cpu_value}
+    for prec in ("fp64", "mixed"):
+        B.set_precision(prec)
+        for _ in range(3):
+            B.matvec_device(dq.data_ptr(), dp.data_ptr(), 1, stream.cuda_stream)
+        stream.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(20):
+            B.matvec_device(dq.data_ptr(), dp.data_ptr(), 1, stream.cuda_stream)
+        e1.record(stream)
+        stream.synchronize()
+        ms = e0.elapsed_time(e1) / 20
+        t0 = time.perf_counter()
+        for _ in range(5):
+            B.matvec(qs)
+        e2e = (time.perf_counter() - t0) / 5
+        out[prec] = {"ms": ms, "points_per_s": ws.n / (ms * 1e-3), "e2e_points_per_s": ws.n / e2e,
+                     "ratio_vs_cpu": ws.n / (ms * 1e-3) / cpu_value, "e2e_ratio_vs_cpu": ws.n / e2e / cpu_value}
+    return out
+
+
 def run_reference(args, name):
     """Reference arm: the reference's own CPU matvec on the bounded sample."""
     from defmm_b200 import workloads as W
@@ -147,7 +279,7 @@ def run_reference(args, name):
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": name, "sample": desc},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "reference", "sample": desc},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "reference", "sample": desc, "fft": REF_FFT},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -270,8 +402,10 @@ def run_spheroid(args, torch):
 def run_rhs64(args, torch):
     """64 right-hand sides (complex charges with FP32-representable parts
     uniform in [-1, 1]) on the 2M-point sphere (k = 2 pi 64, order 5, leaf
-    64), mixed precision: one defmm_gemv_device call with nrhs = 64 per step
-    (each right-hand side replays the operator's captured graph)."""
+    64), mixed precision: one defmm_gemv_device call with nrhs = 64 per step,
+    run in passes of `rhs_block` right-hand sides over the grouped layout
+    (each near-field kernel value, transfer-spectrum entry and plane-wave
+    phase evaluated once per pass)."""
     from defmm_b200 import IBFMM_Mat, workloads as W
     w = W.sphere_surface(2_000_000, seed=0)
     nrhs = 64
@@ -281,6 +415,7 @@ def run_rhs64(args, torch):
     A.addSourceParticles(w.points)
     A.addTargetParticles(w.points)
     A.prcmpt(w.order, w.ncrit, w.kappa)
+    A.set_blocking(args.rhs_block, 0)
     stream = torch.cuda.Stream()
     dq = torch.from_numpy(Q).to("cuda")
     dp = torch.empty((nrhs, w.n), dtype=torch.complex128, device="cuda")
@@ -295,15 +430,24 @@ def run_rhs64(args, torch):
         e1.record(stream)
         stream.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
+    info = {k: A.info(k) for k in ("rhs_block", "groups", "device_bytes")}
+    A.set_profiling(True)
+    A.matvec_device(dq.data_ptr(), dp.data_ptr(), nrhs, stream.cuda_stream)
+    stream.synchronize()
+    phases = A.phase_times()
+    A.set_profiling(False)
+    got = dp[nrhs - 1].cpu().numpy()
+    A.set_precision("fp64")
     one = A.matvec(Q[nrhs - 1])
-    same = bool(np.array_equal(dp[nrhs - 1].cpu().numpy(), one))
+    err = float(np.linalg.norm(got - one) / np.linalg.norm(one))
     line = {"metric": "FMM matvec points/s over 64 right-hand sides, mixed precision", "impl": "ours",
             "value": nrhs * w.n / (ms * 1e-3), "unit": "points/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "ms_per_rhs": ms / nrhs, "higher_is_better": True,
             "dtype": "f32+f64", "data": "synthetic",
             "config": {"workload": "rhs64", "n_points": w.n, "nrhs": nrhs, "kappa": w.kappa, "order": w.order,
                        "leaf_size": w.ncrit, "precision": "mixed"},
-            "last_rhs_equals_single_call": same, "clocks": ck.summary()}
+            "layout": info, "phases_ms_per_pass": phases,
+            "last_rhs_rel_l2_vs_fp64_single": err, "clocks": ck.summary()}
     print(json.dumps(line), flush=True)
 
 
@@ -360,6 +504,8 @@ def main():
     ap.add_argument("--workload", default="sphere2m")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--rhs-block", type=int, default=16)
+    ap.add_argument("--nrhs", type=int, default=8, help="right-hand sides of the block form")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))
@@ -414,6 +560,29 @@ def main():
     dq = torch.from_numpy(q).to("cuda")
     dp = torch.empty(w.n, dtype=torch.complex128, device="cuda")
 
+    def timed_steps(fn, steps, clock=True):
+        """ms per step of fn() over `steps` steps (CUDA events on `stream`,
+        barriers and synchronisation on both sides), max over ranks."""
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        torch.cuda.synchronize()
+        ck = Clocks(local) if clock else None
+        if ck:
+            ck.__enter__()
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if ck:
+            ck.__exit__()
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1) / steps), (ck.summary() if ck else None)
+
+    # ---- single right-hand side: plain FP64 (the drop-in) and mixed
     res = {}
     tune, tune_s = {}, 0.0
     for prec in ["fp64", "mixed"]:
@@ -423,41 +592,66 @@ def main():
             A.autotune(reps=1)
             tune_s += time.perf_counter() - t0
         tune[prec] = {k: A.info(k) for k in ("m2l_threads", "m2l_pairing", "p2p_blocks_per_sm")}
-        for _ in range(args.warmup):
-            A.matvec_device(dq.data_ptr(), dp.data_ptr(), 1, stream.cuda_stream)
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        launches = 0
-        barrier()
-        torch.cuda.synchronize()
-        with Clocks(local) as ck:
-            e0.record(stream)
-            for _ in range(args.steps):
-                A.matvec_device(dq.data_ptr(), dp.data_ptr(), 1, stream.cuda_stream)
-                launches += A.info("launches")
-            e1.record(stream)
-            torch.cuda.synchronize()
-        barrier()
-        ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
-        res[prec] = {"ms": ms, "p": dp.cpu().numpy(), "launches": launches, "clocks": ck.summary()}
+        launches = [0]
 
+        def one():
+            A.matvec_device(dq.data_ptr(), dp.data_ptr(), 1, stream.cuda_stream)
+            launches[0] += A.info("launches")
+        ms, ck = timed_steps(one, args.steps)
+        res[prec] = {"ms": ms, "p": dp.cpu().numpy(), "launches": launches[0] // (args.steps + args.warmup),
+                     "clocks": ck}
     p64, p32 = res["fp64"]["p"], res["mixed"]["p"]
     err_mixed = float(np.linalg.norm(p32 - p64) / np.linalg.norm(p64))
-    head = "mixed" if err_mixed <= MIXED_TOL else "fp64"
-    A.set_precision(head)
-    ms = res[head]["ms"]
-    value = replicas.job_throughput(w.n, world, ms * 1e-3)
 
-    # end to end through the host-buffer C-ABI call
-    A.matvec(q)
+    # ---- a block of right-hand sides, mixed precision, grouped layout
+    nrhs = args.nrhs
+    Q = W.charges(w.n, 100 + replicas.replica_seed(rank), nrhs=nrhs).astype(np.complex64).astype(np.complex128)
+    dQ = torch.from_numpy(Q).to("cuda")
+    dP = torch.empty((nrhs, w.n), dtype=torch.complex128, device="cuda")
+    A.set_precision("mixed")
+    A.set_blocking(nrhs, 0)
+    blaunch = [0]
+
+    def block():
+        A.matvec_device(dQ.data_ptr(), dP.data_ptr(), nrhs, stream.cuda_stream)
+        blaunch[0] += A.info("launches")
+    ms_b, ck_b = timed_steps(block, args.steps)
+    blaunch = blaunch[0] // (args.steps + args.warmup)
+    layout = {k: A.info(k) for k in ("rhs_block", "groups", "device_bytes")}
+    PB = dP.cpu().numpy()
+    A.set_precision("fp64")
+    errs_b = []
+    for r in sorted({0, nrhs - 1}):
+        ref = A.matvec(Q[r])
+        errs_b.append(float(np.linalg.norm(PB[r] - ref) / np.linalg.norm(ref)))
+    err_b = max(errs_b)
+
+    # headline: the fastest form within 1e-6 of the plain FP64 path
+    forms = {"fp64": (res["fp64"]["ms"], 1, 0.0), "mixed": (res["mixed"]["ms"], 1, err_mixed),
+             "mixed_block": (ms_b, nrhs, err_b)}
+    ok = {k: v for k, v in forms.items() if v[2] <= MIXED_TOL}
+    head = max(ok, key=lambda k: ok[k][1] * w.n / ok[k][0])
+    ms, hn = ok[head][0], ok[head][1]
+    value = replicas.job_throughput(hn * w.n, world, ms * 1e-3)
+    clocks = {"fp64": res["fp64"]["clocks"], "mixed": res["mixed"]["clocks"], "mixed_block": ck_b}[head]
+    launches = {"fp64": res["fp64"]["launches"], "mixed": res["mixed"]["launches"], "mixed_block": blaunch}[head]
+
+    # ---- end to end through the host-buffer C-ABI call (defmm_gemv_batched)
+    # in the headline's form: the charges' host-to-device and the
+    # potentials' device-to-host copies inside the timed region
+    A.set_precision("fp64" if head == "fp64" else "mixed")
+    qe = q if hn == 1 else Q
+    A.matvec(qe)
     barrier()
+    e2e_steps = max(1, min(args.steps, 5))
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        A.matvec(q)
-    e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps)
+    for _ in range(e2e_steps):
+        A.matvec(qe)
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps)
+    A.matvec(q)
     chk = A.check_full(2000, seed=7)  # FP64 direct sum at 2,000 seeded targets
 
-    # per-phase device times (separate profiled runs, not part of `value`)
+    # ---- per-phase device times (separate profiled runs, phases serialised)
     phases = {}
     for prec in ["fp64", "mixed"]:
         A.set_precision(prec)
@@ -466,52 +660,29 @@ def main():
         torch.cuda.synchronize()
         phases[prec] = A.phase_times()
         A.set_profiling(False)
-    A.set_precision(head)
+    A.set_precision("mixed")
+    A.set_profiling(True)
+    A.matvec_device(dQ.data_ptr(), dP.data_ptr(), nrhs, stream.cuda_stream)
+    torch.cuda.synchronize()
+    phases["mixed_block"] = A.phase_times()
+    A.set_profiling(False)
 
-    # roofline of the dominant HBM-bound kernel, M2L (with the inverse DFT
-    # fused), on the headline path.  Algorithmic bytes per matvec: every
-    # source spectrum once (e P^3 per source slot), every permuted transfer
-    # spectrum once, the local expansion of every target slot read and
-    # written (2 e L^3), 8 B per list entry.
-    hbm, bf16, src = measured_peaks()
-    e = 16 if head == "fp64" else 8
-    L = w.order
-    PP = (2 * L - 1) ** 3
-    n_far = info["far_hf"] + info["far_lf"]
-    m2l_bytes = (e * PP * info["slots_S"] + e * PP * info["permuted_spectra"]
-                 + 2 * e * L ** 3 * info["m2l_targets"] + 8 * n_far)
-    m2l_ms = phases[head]["m2l"]
-    achieved = m2l_bytes / (m2l_ms * 1e-3) / 1e9
-    # the M2L kernel this run used (launch choice of the headline precision)
-    lc = tune[head]
-    kname = "%s<%s, %d, %d>" % ("k_m2l_pair" if lc["m2l_pairing"] else "k_m2l",
-                                "double" if head == "fp64" else "float", L, lc["m2l_threads"])
-    # DRAM traffic per far pair of the same kernel, measured by ncu on a
-    # smaller sphere and scaled by the far pairs of this workload
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "m2l_traffic.json")
-    if os.path.exists(tp):
-        try:
-            with open(tp) as f:
-                tr = json.load(f).get(head, {})
-            if tr.get("kernel") == kname and tr.get("bytes_per_pair") is not None:
-                traffic = tr["bytes_per_pair"] * n_far
-        except (OSError, ValueError):
-            traffic = None
-    roofline = {"bound": "hbm", "kernel": kname + " (M2L + inverse DFT, all cone batches)", "achieved": achieved,
-                "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_source": src,
-                "traffic": traffic, "algorithmic_bytes": m2l_bytes}
+    peaks = measured_peaks()
+    l2_gbs = l2_copy_bandwidth(torch)
+    rl = phase_rooflines(info, w.order, phases, head, hn, peaks, l2_gbs, tune)
+    roofline = rl["headline"]
 
-    cpu = None
+    cpu, sample = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             from oracle import refrun
             ws, desc = cpu_sample(args.workload)
+            qs = W.charges(ws.n, 1)
             if refrun.available(fast=True):
-                r = refrun.run(ws.points, ws.points, W.charges(ws.n, 1), ws.order, ws.ncrit, ws.kappa,
-                               lists=False, fast=True)
+                r = refrun.run(ws.points, ws.points, qs, ws.order, ws.ncrit, ws.kappa, lists=False, fast=True)
                 cpu = {"value": ws.n / r.summary["gemv_s"], "unit": UNIT, "cores": 1, "kind": "reference",
-                       "sample": desc, "gemv_s": r.summary["gemv_s"]}
+                       "sample": desc, "gemv_s": r.summary["gemv_s"], "fft": REF_FFT}
+                sample = sample_comparison(torch, ws, qs, desc, cpu["value"], stream)
         except Exception as ex:  # the baseline must not sink the GPU result
             cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"failed: {ex}"}
 
@@ -519,22 +690,29 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32+f64" if head == "mixed" else "f64", "data": "synthetic",
+            "vs_baseline": None, "dtype": "f64" if head == "fp64" else "f32+f64", "data": "synthetic",
             "config": {"workload": args.workload, "n_points": w.n, "kappa": w.kappa, "order": w.order,
-                       "leaf_size": w.ncrit, "precision": head, "parallelism": f"replicas{world}",
+                       "leaf_size": w.ncrit, "precision": "fp64" if head == "fp64" else "mixed",
+                       "right_hand_sides_per_step": hn, "form": head, "parallelism": f"replicas{world}",
                        "l2": "working set per step >> L2 (126 MB): expansions and spectra are GBs"},
-            "matvecs_per_s": world / (ms * 1e-3),
+            "matvecs_per_s": world * hn / (ms * 1e-3),
             "fp64": {"ms_per_step": res["fp64"]["ms"], "points_per_s": world * w.n / (res["fp64"]["ms"] * 1e-3)},
             "mixed": {"ms_per_step": res["mixed"]["ms"], "points_per_s": world * w.n / (res["mixed"]["ms"] * 1e-3),
                       "rel_l2_vs_fp64": err_mixed},
-            "speedup_mixed_vs_fp64": res["fp64"]["ms"] / res["mixed"]["ms"],
-            "accuracy": {"direct_sum_2000_targets": chk, "precision": head},
-            "e2e": {"value": world * w.n / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 16 * w.n,
-                    "d2h_bytes_per_step": 16 * w.n},
+            "mixed_block": {"right_hand_sides": nrhs, "ms_per_step": ms_b, "ms_per_rhs": ms_b / nrhs,
+                            "points_per_s": world * nrhs * w.n / (ms_b * 1e-3), "rel_l2_vs_fp64": err_b,
+                            "layout": layout},
+            "speedup_vs_fp64": {"mixed": res["fp64"]["ms"] / res["mixed"]["ms"],
+                                "mixed_block": res["fp64"]["ms"] * nrhs / ms_b},
+            "accuracy": {"direct_sum_2000_targets": chk, "precision": "mixed" if head != "fp64" else "fp64"},
+            "e2e": {"value": world * hn * w.n / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 16 * w.n * hn,
+                    "d2h_bytes_per_step": 16 * w.n * hn},
             "roofline": roofline,
+            "phase_rooflines": rl["phases"],
             "cpu_baseline": cpu,
-            "clocks": res[head]["clocks"],
-            "gpu_launches": res[head]["launches"],
+            "sample_comparison": sample,
+            "clocks": clocks,
+            "gpu_launches": launches,
             "phases_ms": phases,
             "setup_s": setup_s,
             "setup": {"prcmpt_s": setup_s, "level_walk_s": info["plan_walk_ms"] / 1e3,

@@ -36,6 +36,8 @@ _INFO = {
     "i_near": 12, "tables": 13, "device_bytes": 14, "list_records": 15, "launches": 16,
     "m2l_targets": 17, "leaf_slots_S": 18, "permuted_spectra": 19, "plan_walk_device": 20, "plan_ms": 21,
     "plan_walk_ms": 22, "m2l_threads": 23, "p2p_blocks_per_sm": 24, "m2l_pairing": 25,
+    "layout": 26, "rhs_block": 27, "groups": 28, "m2m_entries": 29, "l2l_entries": 30,
+    "p2m_point_slots": 31, "l2p_point_slots": 32, "m2f_slots": 33,
 }
 PHASES = ["p2m", "m2m", "m2f", "m2l", "f2l", "l2l", "l2p", "p2p", "scatter", "total"]
 
@@ -81,6 +83,9 @@ def lib():
             "defmm_autotune": (ctypes.c_int, [vp, ctypes.c_int, ip]),
             "defmm_set_launch": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
             "defmm_set_m2l_pairing": (ctypes.c_int, [vp, ctypes.c_int]),
+            "defmm_set_blocking": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
+            "defmm_dump_m2l": (ctypes.c_int, [vp, vp, vp, vp, ctypes.POINTER(i64)]),
+            "defmm_set_rhs_per_cta": (ctypes.c_int, [vp, ctypes.c_int]),
             "defmm_batch_create": (vp, [i64, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.c_int]),
             "defmm_batch_launch": (ctypes.c_int, [vp, vp]),
             "defmm_batch_destroy": (None, [vp]),
@@ -186,6 +191,16 @@ class IBFMM_Mat:
         """Two target slots per M2L CTA (current precision); results unchanged."""
         self._check(lib().defmm_set_m2l_pairing(self._h, int(bool(on))))
 
+    def set_blocking(self, rhs_block=16, groups=0):
+        """Right-hand sides per pass of multi-RHS calls (1..32) and the number
+        of direction groups of the grouped layout (0: as memory needs; >= 1:
+        about that many, also for single right-hand sides)."""
+        self._check(lib().defmm_set_blocking(self._h, int(rhs_block), int(groups)))
+
+    def set_rhs_per_cta(self, rb=8):
+        """Right-hand sides per M2L CTA of the grouped layout (1, 2, 4, 8)."""
+        self._check(lib().defmm_set_rhs_per_cta(self._h, int(rb)))
+
     def set_profiling(self, on=True):
         self._check(lib().defmm_set_profiling(self._h, int(bool(on))))
 
@@ -258,6 +273,17 @@ class IBFMM_Mat:
         nr = np.zeros((n[2], 2), np.int32)
         self._check(lib().defmm_dump_lists(self._h, _ip(fh), _ip(fl), _ip(nr), n))
         return nr, fh, fl
+
+    def m2l_entries(self):
+        """(ptr, src, tab): the M2L work per target slot as the matvec runs
+        it (defmm_dump_m2l)."""
+        n = (ctypes.c_int64 * 2)()
+        self._check(lib().defmm_dump_m2l(self._h, None, None, None, n))
+        ptr = np.zeros(n[0], np.int64)
+        src = np.zeros(n[1], np.int32)
+        tab = np.zeros(n[1], np.uint32)
+        self._check(lib().defmm_dump_m2l(self._h, ptr.ctypes.data, src.ctypes.data, tab.ctypes.data, n))
+        return ptr, src, tab
 
 
 class Batch:

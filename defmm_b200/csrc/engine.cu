@@ -1,6 +1,7 @@
 // Operator handle: host plan -> device arrays, matvec orchestration, C ABI.
 #include <algorithm>
 #include <chrono>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -15,6 +16,7 @@
 
 using dfb::DevPlan;
 using dfb::Plan;
+using dfb::Levels;
 
 namespace {
 
@@ -26,6 +28,25 @@ struct DevBuf {
 };
 
 }  // namespace
+
+// Direction-streamed layout with right-hand-side blocks (no counterpart in
+// the reference, whose expansions are all resident).  The HF levels' slots
+// are split into groups by direction at the deepest HF level (the pivot):
+// direction c there owns directions [c f, (c + 1) f) at a level with f times
+// more directions, and M2M, M2L and L2L never leave a group.  One group's M
+// and L (R right-hand sides per slot) are on the device at a time; LF levels
+// (below the pivot, one slot per cell) stay resident.
+struct GroupedLayout {
+  int R = 0;                        // right-hand sides per slot
+  std::vector<int> hl;              // HF levels holding slots, coarse to fine
+  int lh = -1;                      // pivot (deepest HF level), -1: none
+  std::vector<int64_t> fl;          // per level of hl: directions per pivot direction
+  std::vector<std::pair<int, int>> groups;  // pivot direction ranges [c0, c1)
+  int64_t gS_max = 0, gT_max = 0;   // slots of the largest group (S, T)
+  int64_t lfS0 = 0, lfS1 = 0, lfT0 = 0, lfT1 = 0;  // LF slot ranges
+  int64_t f_cap = 0;                // source slots per F batch
+  DevBuf Mg, Lg, Mlf, Llf, F, q, pnear, pfar, tpart;
+};
 
 struct defmm_handle {
   std::vector<double> src, trg;  // user-order coordinates
@@ -76,6 +97,17 @@ struct defmm_handle {
   int p2p_bps[2] = {16, 16};
   int64_t nchunk = 0;
   size_t dev_bytes = 0;
+  // layout of the expansions: 0 none, 1 resident (every slot's M and L),
+  // 2 grouped (GroupedLayout)
+  int layout = 0;
+  GroupedLayout gl;
+  int rhs_block = 16;     // right-hand sides per pass of multi-RHS calls
+  int rhs_block_m2l = 8;  // right-hand sides per M2L CTA (capped by the order)
+  int groups_forced = 0;  // > 0: direction groups requested (also for one RHS)
+  int groups_used = 0;    // groups of the last grouped pass
+  // leaves at precomputed levels sorted by level (P2M: sources, L2P: targets)
+  const int32_t *d_p2m_bylvl = nullptr, *d_l2p_bylvl = nullptr;
+  std::vector<int64_t> p2m_lvl_off, l2p_lvl_off;  // nlvl + 1 offsets
   double phase_ms[PH_N] = {0};
   cudaEvent_t ev[2 * PH_N] = {};
   cudaEvent_t ev_ready = nullptr, ev_done = nullptr;  // cross-stream ordering
@@ -164,6 +196,12 @@ void drop_graph(defmm_handle* h) {
   h->g_prec = -1;
 }
 
+void free_grouped(defmm_handle* h) {
+  GroupedLayout& g = h->gl;
+  for (DevBuf* b : {&g.Mg, &g.Lg, &g.Mlf, &g.Llf, &g.F, &g.q, &g.pnear, &g.pfar, &g.tpart}) free_buf(*b);
+  g = GroupedLayout();
+}
+
 void free_plan_device(defmm_handle* h) {
   drop_graph(h);
   for (void* p : h->plan_allocs) cudaFree(p);
@@ -183,6 +221,8 @@ void free_plan_device(defmm_handle* h) {
   free_buf(h->rout);
   free_buf(h->chk);
   free_buf(h->pscr);
+  free_grouped(h);
+  h->layout = 0;
   h->use_sym = false;
   h->ops_prec = -1;
   h->dev_bytes = 0;
@@ -263,6 +303,22 @@ int upload_plan(defmm_handle* h) {
   d.nlvl = p.lv.nlvl;
   UP(p.p2m_leaf, h->d_p2m_leaf);
   UP(p.l2p_leaf, h->d_l2p_leaf);
+  {  // the same leaves grouped by level (stable), for per-level launches
+    auto bylvl = [&](const std::vector<int32_t>& lv, const std::vector<int32_t>& leaves, std::vector<int32_t>& out,
+                     std::vector<int64_t>& off) {
+      off.assign(p.lv.nlvl + 1, 0);
+      for (int32_t c : leaves) off[lv[c] + 1]++;
+      for (int l = 0; l < p.lv.nlvl; l++) off[l + 1] += off[l];
+      out.assign(leaves.size(), 0);
+      std::vector<int64_t> pos(off.begin(), off.end() - 1);
+      for (int32_t c : leaves) out[pos[lv[c]]++] = c;
+    };
+    std::vector<int32_t> tmp;
+    bylvl(p.S.lvl, p.p2m_leaf, tmp, h->p2m_lvl_off);
+    UP(tmp, h->d_p2m_bylvl);
+    bylvl(p.T.lvl, p.l2p_leaf, tmp, h->l2p_lvl_off);
+    UP(tmp, h->d_l2p_bylvl);
+  }
   UP(p.p2p_tfirst, h->d_tfirst);
   UP(p.p2p_tn, h->d_tn);
   UP(p.p2p_ptr, h->d_p2p_ptr);
@@ -317,8 +373,10 @@ int upload_plan(defmm_handle* h) {
   return 0;
 }
 
-// Allocate / convert the arrays whose element type follows the precision.
-int prepare_precision(defmm_handle* h) {
+// Tables whose element type follows the precision: the order's kernels and
+// constant tables, signatures, permuted transfer spectra.  Releases the
+// expansion layout of the previous precision.
+int prepare_tables(defmm_handle* h) {
   if (h->ops_prec == h->precision) return 0;
   drop_graph(h);
   Plan& p = h->plan;
@@ -331,12 +389,17 @@ int prepare_precision(defmm_handle* h) {
   free_buf(h->sig);
   free_buf(h->sig2);
   free_buf(h->ptab);
+  free_buf(h->pscr);
+  free_grouped(h);
+  h->layout = 0;
+  h->use_sym = false;
   h->ops = dfb::op_table(p.L, fp64);
   if (!h->ops) return h->fail(DEFMM_ERR_ARG, "unsupported order");
   std::vector<double> mats;
   for (int k = 0; k < 2; k++) mats.insert(mats.end(), p.m2m[k].begin(), p.m2m[k].end());
   for (int k = 0; k < 2; k++) mats.insert(mats.end(), p.l2l[k].begin(), p.l2l[k].end());
   CK(h->ops->setup(mats.data()));
+  CK(dfb::setup_rhs_kernels());
   auto put = [&](DevBuf& b, const dfb::cplx* src, size_t n) -> int {
     int st = ensure(h, b, std::max<size_t>(1, n) * cs);
     if (st) return st;
@@ -373,6 +436,38 @@ int prepare_precision(defmm_handle* h) {
     CK(cudaStreamSynchronize(h->st));
     free_buf(base);
   }
+  h->ops_prec = h->precision;
+  return 0;
+}
+
+// Largest cone (source slots) of any precomputed level: the smallest F batch.
+int64_t largest_cone(const Plan& p) {
+  int64_t need = 1;
+  for (int l = 0; l < p.lv.nlvl; l++) {
+    const auto& cS = p.sS.cone_begin[l];
+    for (size_t c = 0; c + 1 < cS.size(); c++) need = std::max(need, cS[c + 1] - cS[c]);
+  }
+  return need;
+}
+
+// Device bytes of the resident layout: every slot's M and L, charges, the
+// smallest F batch.
+size_t resident_bytes(const defmm_handle* h) {
+  const Plan& p = h->plan;
+  const size_t cs = h->precision == DEFMM_PRECISION_FP64 ? 16 : 8;
+  return (size_t)(p.sS.n + p.sT.n) * p.LL * cs + p.S.perm.size() * cs + (size_t)largest_cone(p) * p.PP * cs;
+}
+
+// Resident layout: M and L of every slot.  Releases a grouped layout first.
+int prepare_resident(defmm_handle* h) {
+  if (h->layout == 1) return 0;
+  drop_graph(h);
+  free_grouped(h);
+  h->layout = 0;
+  Plan& p = h->plan;
+  const bool fp64 = h->precision == DEFMM_PRECISION_FP64;
+  const size_t cs = fp64 ? 16 : 8;
+  int st;
   const int64_t nS = (int64_t)p.S.perm.size();
   if ((st = ensure(h, h->M, std::max<int64_t>(1, p.sS.n) * p.LL * cs)) ||
       (st = ensure(h, h->Lx, std::max<int64_t>(1, p.sT.n) * p.LL * cs)) || (st = ensure(h, h->q, nS * cs)))
@@ -399,10 +494,9 @@ int prepare_precision(defmm_handle* h) {
   }
   // F batch buffer: at least the largest cone of any level, at most about
   // half of the free memory
-  int64_t need = 1, want = 0;
+  int64_t need = largest_cone(p), want = 0;
   for (int l = 0; l < p.lv.nlvl; l++) {
     const auto& cS = p.sS.cone_begin[l];
-    for (size_t c = 0; c + 1 < cS.size(); c++) need = std::max(need, cS[c + 1] - cS[c]);
     want = std::max(want, cS.back() - cS.front());
   }
   size_t fr = 0, tot = 0;
@@ -414,7 +508,123 @@ int prepare_precision(defmm_handle* h) {
   if (cap < need) return h->fail(DEFMM_ERR_MEMORY, "not enough device memory for one cone of spectra");
   h->f_cap = cap;
   if ((st = ensure(h, h->F, cap * per))) return st;
-  h->ops_prec = h->precision;
+  h->layout = 1;
+  return 0;
+}
+
+int prepare_precision(defmm_handle* h) {
+  int st = prepare_tables(h);
+  if (st) return st;
+  return prepare_resident(h);
+}
+
+// Slot ranges of one direction group at HF level hl[i]: S [*s0, *s1),
+// T [*t0, *t1).
+void group_range(const Plan& p, const GroupedLayout& g, size_t i, int c0, int c1, int64_t* s0, int64_t* s1,
+                 int64_t* t0, int64_t* t1) {
+  const int l = g.hl[i];
+  const int64_t f = g.fl[i];
+  *s0 = p.sS.cone_begin[l][c0 * f];
+  *s1 = p.sS.cone_begin[l][c1 * f];
+  *t0 = p.sT.cone_begin[l][c0 * f];
+  *t1 = p.sT.cone_begin[l][c1 * f];
+}
+
+// Grouped layout for R right-hand sides per pass: the HF levels split into
+// direction groups that fit the device memory (or `groups_forced` groups),
+// one group's M and L at a time, LF levels resident.
+int prepare_grouped(defmm_handle* h, int R) {
+  if (h->layout == 2 && h->gl.R == R) return 0;
+  drop_graph(h);
+  free_buf(h->M);
+  free_buf(h->Lx);
+  free_buf(h->F);
+  free_buf(h->q);
+  free_buf(h->pscr);
+  h->use_sym = false;
+  free_grouped(h);
+  h->layout = 0;
+  Plan& p = h->plan;
+  GroupedLayout& g = h->gl;
+  g.R = R;
+  const bool fp64 = h->precision == DEFMM_PRECISION_FP64;
+  const size_t cs = fp64 ? 16 : 8;
+  const Levels& v = p.lv;
+  // HF levels with slots (contiguous, coarse to fine) and the pivot
+  for (int l = 0; l < v.nlvl; l++)
+    if (v.prec[l] && v.isHF[l] && p.sS.lvl_begin[l + 1] + p.sT.lvl_begin[l + 1] > p.sS.lvl_begin[l] + p.sT.lvl_begin[l])
+      g.hl.push_back(l);
+  for (size_t i = 1; i < g.hl.size(); i++)
+    if (g.hl[i] != g.hl[i - 1] + 1) return h->fail(DEFMM_ERR_ARG, "grouped layout: HF levels are not contiguous");
+  g.lh = g.hl.empty() ? -1 : g.hl.back();
+  for (int l : g.hl) g.fl.push_back((int64_t)1 << (2 * (v.HFStage[l] - v.HFStage[g.lh])));
+  // LF slots: every level below the pivot (or every level without HF slots)
+  const int lf = g.lh < 0 ? 0 : g.lh + 1;
+  g.lfS0 = p.sS.lvl_begin[lf];
+  g.lfS1 = p.sS.n;
+  g.lfT0 = p.sT.lvl_begin[lf];
+  g.lfT1 = p.sT.n;
+  const int64_t nS = (int64_t)p.S.perm.size(), nT = (int64_t)p.T.perm.size();
+  const size_t slot_b = (size_t)R * p.LL * cs;
+  const size_t nitem = std::max<size_t>(1, p.p2p_item_chunk.size());
+  int st;
+  if ((st = ensure(h, g.q, (size_t)nS * R * cs)) || (st = ensure(h, g.pnear, (size_t)nT * R * 16)) ||
+      (st = ensure(h, g.pfar, (size_t)nT * R * 16)) || (st = ensure(h, g.tpart, nitem * 32 * R * 16)) ||
+      (st = ensure(h, g.Mlf, std::max<int64_t>(1, g.lfS1 - g.lfS0) * slot_b)) ||
+      (st = ensure(h, g.Llf, std::max<int64_t>(1, g.lfT1 - g.lfT0) * slot_b)))
+    return st;
+  size_t fr = 0, tot = 0;
+  CK(cudaMemGetInfo(&fr, &tot));
+  // F batch: at least the largest cone, at most a quarter of the free memory
+  // (and 32 GB)
+  const size_t fper = (size_t)R * p.PP * cs;
+  const int64_t need = largest_cone(p);
+  int64_t cap = (int64_t)(std::min<size_t>(fr / 4, (size_t)32 << 30) / fper);
+  int64_t want = 0;
+  for (int l = 0; l < v.nlvl; l++) want = std::max(want, p.sS.cone_begin[l].back() - p.sS.cone_begin[l].front());
+  cap = std::min(cap, std::max(want, need));
+  if (cap < need) return h->fail(DEFMM_ERR_MEMORY, "not enough device memory for one cone of spectra");
+  g.f_cap = cap;
+  if ((st = ensure(h, g.F, (size_t)cap * fper))) return st;
+  // direction groups: consecutive pivot directions while the group's M and L
+  // fit in 70% of what is left (or about 1 / groups_forced of all HF slots)
+  if (g.lh >= 0) {
+    CK(cudaMemGetInfo(&fr, &tot));
+    const int nd = v.nDir[g.lh];
+    std::vector<int64_t> cost(nd, 0), cS(nd, 0), cT(nd, 0);
+    int64_t total = 0;
+    for (int c = 0; c < nd; c++) {
+      for (size_t i = 0; i < g.hl.size(); i++) {
+        int64_t s0, s1, t0, t1;
+        group_range(p, g, i, c, c + 1, &s0, &s1, &t0, &t1);
+        cS[c] += s1 - s0;
+        cT[c] += t1 - t0;
+      }
+      cost[c] = cS[c] + cT[c];
+      total += cost[c];
+    }
+    int64_t budget = (int64_t)(0.7 * (double)fr / (double)slot_b);
+    if (h->groups_forced > 0) budget = std::max<int64_t>(1, (total + h->groups_forced - 1) / h->groups_forced);
+    int c0 = 0;
+    while (c0 < nd) {
+      int c1 = c0 + 1;
+      int64_t acc = cost[c0];
+      while (c1 < nd && acc + cost[c1] <= budget) acc += cost[c1++];
+      int64_t gs = 0, gt = 0;
+      for (int c = c0; c < c1; c++) {
+        gs += cS[c];
+        gt += cT[c];
+      }
+      g.gS_max = std::max(g.gS_max, gs);
+      g.gT_max = std::max(g.gT_max, gt);
+      g.groups.push_back({c0, c1});
+      c0 = c1;
+    }
+    if ((st = ensure(h, g.Mg, std::max<int64_t>(1, g.gS_max) * slot_b)) ||
+        (st = ensure(h, g.Lg, std::max<int64_t>(1, g.gT_max) * slot_b)))
+      return st;
+  }
+  h->layout = 2;
   return 0;
 }
 
@@ -469,11 +679,11 @@ int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) 
   if (h->events) cudaEventRecord(h->ev[2 * PH_P2P + 1], sn);
   // upward pass
   rec(h, 2 * PH_P2M);
-  ops->p2m(d, h->d_p2m_leaf, (int)p.p2m_leaf.size(), h->q.p, h->sig2.p, h->M.p, sf);
+  ops->p2m(d, h->d_p2m_leaf, (int)p.p2m_leaf.size(), h->q.p, h->sig2.p, h->M.p, 1, INT_MIN, INT_MAX, sf);
   rec(h, 2 * PH_P2M + 1);
   rec(h, 2 * PH_M2M);
   for (int l = nl - 2; l >= p.lv.max_stage; l--) {
-    ops->m2m(d, p.sS.lvl_begin[l], p.sS.lvl_begin[l + 1], h->sig.p, h->sig2.p, h->M.p, sf);
+    ops->m2m(d, p.sS.lvl_begin[l], p.sS.lvl_begin[l + 1], h->sig.p, h->sig2.p, h->M.p, h->M.p, 1, sf);
     nl_ += p.sS.lvl_begin[l + 1] > p.sS.lvl_begin[l] ? 1 : 0;
   }
   rec(h, 2 * PH_M2M + 1);
@@ -511,7 +721,8 @@ int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) 
     }
     if (l + 1 < nl) {
       rec(h, 2 * PH_L2L);
-      ops->l2l(d, p.sT.lvl_begin[l + 1], p.sT.lvl_begin[l + 2], h->sig.p, h->sig2.p, h->Lx.p, sf);
+      ops->l2l(d, p.sT.lvl_begin[l + 1], p.sT.lvl_begin[l + 2], h->sig.p, h->sig2.p, h->Lx.p, h->Lx.p, 1, INT64_MIN,
+               INT64_MAX, sf);
       nl_ += p.sT.lvl_begin[l + 2] > p.sT.lvl_begin[l + 1] ? 1 : 0;
       rec(h, 2 * PH_L2L + 1);
       if (h->events) {
@@ -523,7 +734,8 @@ int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) 
     }
   }
   rec(h, 2 * PH_L2P);
-  ops->l2p(d, h->d_l2p_leaf, (int)p.l2p_leaf.size(), h->sig2.p, h->Lx.p, (double2*)h->pfar.p, sf);
+  ops->l2p(d, h->d_l2p_leaf, (int)p.l2p_leaf.size(), h->sig2.p, h->Lx.p, (double2*)h->pfar.p, 1, INT_MIN, INT_MAX,
+           false, sf);
   rec(h, 2 * PH_L2P + 1);
   CK(cudaEventRecord(h->ev_done, sn));
   CK(cudaStreamWaitEvent(s, h->ev_done, 0));
@@ -551,6 +763,270 @@ int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) 
     h->phase_ms[PH_P2P] = el(PH_P2P);
     h->phase_ms[PH_SCATTER] = el(PH_SCATTER);
     h->phase_ms[PH_TOTAL] = el(PH_TOTAL);
+  }
+  return 0;
+}
+
+// Address of global slot `slot` (right-hand side 0) in a buffer that holds
+// the slots [first, ...) with slot_b bytes per slot, as a base for the
+// kernels (base + slot * R * LL elements); computed in integers because the
+// base itself may lie before the buffer.
+void* slot_base(void* buf, int64_t first, size_t slot_b) {
+  return reinterpret_cast<void*>(reinterpret_cast<uintptr_t>(buf) - (uintptr_t)((size_t)first * slot_b));
+}
+
+// Up to R matvecs in one pass over the grouped layout: qin holds nvec <= R
+// user-order charge vectors (vector r at qin + r * stride_in), out receives
+// nvec potential vectors (at out + r * stride_out).
+int run_gemv_grouped(defmm_handle* h, const double2* qin, int64_t stride_in, double2* out, int64_t stride_out,
+                     int nvec, cudaStream_t s) {
+  Plan& p = h->plan;
+  GroupedLayout& g = h->gl;
+  const int R = g.R;
+  const bool fp64 = h->precision == DEFMM_PRECISION_FP64;
+  const DevPlan& d = h->dp;
+  const dfb::OpTable* ops = h->ops;
+  const Levels& v = p.lv;
+  const int64_t nS = (int64_t)p.S.perm.size(), nT = (int64_t)p.T.perm.size();
+  const int nl = v.nlvl;
+  const size_t cs = fp64 ? 16 : 8;
+  const size_t slot_b = (size_t)R * p.LL * cs;
+  const int pi = fp64 ? 0 : 1;
+  h->cur = s;
+  int64_t nk = 0;  // kernels launched
+  for (int i = 0; i < PH_N; i++) h->phase_ms[i] = 0;
+  // profiling: each phase segment timed with events on the main stream
+  cudaEvent_t e0 = h->ev[0], e1 = h->ev[1];
+  auto timed = [&](int ph, auto&& fn) -> int {
+    if (h->events) CK(cudaEventRecord(e0, s));
+    fn();
+    if (h->events) {
+      CK(cudaEventRecord(e1, s));
+      CK(cudaEventSynchronize(e1));
+      float a = 0;
+      cudaEventElapsedTime(&a, e0, e1);
+      h->phase_ms[ph] += a;
+    }
+    return 0;
+  };
+  cudaEvent_t t_all0 = h->ev[2], t_all1 = h->ev[3];
+  if (h->events) CK(cudaEventRecord(t_all0, s));
+  dfb::launch_gather_rhs(fp64, qin, d.S_perm, g.q.p, nS, stride_in, R, nvec, s);
+  nk++;
+  CK(cudaMemsetAsync(g.pfar.p, 0, (size_t)nT * R * 16, s));
+  CK(cudaMemsetAsync(g.pnear.p, 0, (size_t)nT * R * 16, s));
+  if (g.lfT1 > g.lfT0) CK(cudaMemsetAsync(g.Llf.p, 0, (size_t)(g.lfT1 - g.lfT0) * slot_b, s));
+  // near field on the second stream (the main one when profiling)
+  cudaStream_t sn = h->events ? s : h->st2;
+  CK(cudaEventRecord(h->ev_ready, s));
+  CK(cudaStreamWaitEvent(sn, h->ev_ready, 0));
+  {
+    float a = 0;
+    if (h->events) CK(cudaEventRecord(e0, sn));
+    dfb::launch_p2p_rhs(fp64, d, (int64_t)p.p2p_order.size(), h->d_p2p_order, h->d_p2p_item_chunk, h->d_tfirst,
+                        h->d_tn, h->d_p2p_ptr, h->d_sfirst, h->d_sn, g.q.p, R, (double2*)g.pnear.p,
+                        (double2*)g.tpart.p, h->d_queue, h->nsm, h->p2p_bps[pi], sn);
+    dfb::launch_p2p_items_rhs(h->nchunk, h->d_tfirst, h->d_tn, h->d_p2p_chunk_items, (const double2*)g.tpart.p, R,
+                              (double2*)g.pnear.p, h->nsm, sn);
+    nk += p.p2p_order.empty() ? 0 : (R + 7) / 8 + 1;
+    if (h->events) {
+      CK(cudaEventRecord(e1, sn));
+      CK(cudaEventSynchronize(e1));
+      cudaEventElapsedTime(&a, e0, e1);
+      h->phase_ms[PH_P2P] += a;
+    }
+  }
+  void* Mlf = slot_base(g.Mlf.p, g.lfS0, slot_b);
+  void* Llf = slot_base(g.Llf.p, g.lfT0, slot_b);
+  const int lf = g.lh < 0 ? 0 : g.lh + 1;  // first LF level
+  // M2F + M2L of source cones [c0, c1) at level l: targets into Lbase
+  auto far_cones = [&](int l, int64_t c0, int64_t c1, void* Mbase, void* Lbase) -> int {
+    const auto& cS = p.sS.cone_begin[l];
+    const auto& cT = p.sT.cone_begin[l];
+    int64_t a = c0;
+    while (a < c1) {
+      int64_t b = a + 1;
+      while (b < c1 && cS[b + 1] - cS[a] <= g.f_cap) b++;
+      const int64_t fs0 = cS[a], fs1 = cS[b], ts0 = cT[a], ts1 = cT[b];
+      if (ts1 > ts0 && fs1 > fs0) {
+        timed(PH_M2F, [&] {
+          ops->m2f((fs1 - fs0) * R, (const char*)Mbase + (size_t)fs0 * slot_b, g.F.p, s);
+        });
+        timed(PH_M2L, [&] {
+          if (R == 1)
+            ops->m2l(d, ts0, ts1, fs0, fs1, g.F.p, h->ptab.p, Lbase, h->d_queue + 1, h->nsm, h->m2l_nt[pi],
+                     h->m2l_pair[pi], s);
+          else
+            ops->m2l_rhs(d, ts0, ts1, fs0, fs1, R, h->rhs_block_m2l, g.F.p, h->ptab.p, Lbase, h->d_queue + 1,
+                         h->nsm, s);
+        });
+        nk += 2;
+      }
+      a = b;
+    }
+    return 0;
+  };
+  // ---- LF levels (resident): upward pass and their far field
+  if (g.lfS1 > g.lfS0 || g.lfT1 > g.lfT0) {
+    timed(PH_P2M, [&] {
+      for (int l = lf; l < nl; l++) {
+        const int64_t b = h->p2m_lvl_off[l], e = h->p2m_lvl_off[l + 1];
+        if (e > b) {
+          ops->p2m(d, h->d_p2m_bylvl + b, (int)(e - b), g.q.p, h->sig2.p, Mlf, R, INT_MIN, INT_MAX, s);
+          nk++;
+        }
+      }
+    });
+    timed(PH_M2M, [&] {
+      for (int l = nl - 2; l >= lf; l--)
+        if (p.sS.lvl_begin[l + 1] > p.sS.lvl_begin[l]) {
+          ops->m2m(d, p.sS.lvl_begin[l], p.sS.lvl_begin[l + 1], h->sig.p, h->sig2.p, Mlf, Mlf, R, s);
+          nk++;
+        }
+    });
+    for (int l = lf; l < nl; l++)
+      if (v.prec[l]) far_cones(l, 0, (int64_t)p.sS.cone_begin[l].size() - 1, Mlf, Llf);
+  }
+  // ---- HF levels, one direction group at a time
+  h->groups_used = (int)g.groups.size();
+  for (const auto& gr : g.groups) {
+    const int c0 = gr.first, c1 = gr.second;
+    const size_t nh = g.hl.size();
+    std::vector<int64_t> s0(nh), s1(nh), t0(nh), t1(nh);
+    std::vector<void*> Mb(nh), Lb(nh);
+    int64_t so = 0, to = 0;
+    for (size_t i = 0; i < nh; i++) {
+      group_range(p, g, i, c0, c1, &s0[i], &s1[i], &t0[i], &t1[i]);
+      Mb[i] = slot_base((char*)g.Mg.p + (size_t)so * slot_b, s0[i], slot_b);
+      Lb[i] = slot_base((char*)g.Lg.p + (size_t)to * slot_b, t0[i], slot_b);
+      so += s1[i] - s0[i];
+      to += t1[i] - t0[i];
+    }
+    if (to > 0) CK(cudaMemsetAsync(g.Lg.p, 0, (size_t)to * slot_b, s));
+    // upward: P2M of the group's leaf slots, M2M level by level
+    timed(PH_P2M, [&] {
+      for (size_t i = 0; i < nh; i++) {
+        const int l = g.hl[i];
+        const int64_t b = h->p2m_lvl_off[l], e = h->p2m_lvl_off[l + 1];
+        if (e > b && s1[i] > s0[i]) {
+          ops->p2m(d, h->d_p2m_bylvl + b, (int)(e - b), g.q.p, h->sig2.p, Mb[i], R, (int)(c0 * g.fl[i]),
+                   (int)(c1 * g.fl[i]), s);
+          nk++;
+        }
+      }
+    });
+    timed(PH_M2M, [&] {
+      for (int i = (int)nh - 1; i >= 0; i--) {
+        if (s1[i] <= s0[i]) continue;
+        const void* Mc = (size_t)i + 1 < nh ? Mb[i + 1] : Mlf;  // children: next HF level or the LF level below
+        ops->m2m(d, s0[i], s1[i], h->sig.p, h->sig2.p, Mb[i], Mc, R, s);
+        nk++;
+      }
+    });
+    // far field top-down, then the downward transfer
+    for (size_t i = 0; i < nh; i++) {
+      far_cones(g.hl[i], (int64_t)c0 * g.fl[i], (int64_t)c1 * g.fl[i], Mb[i], Lb[i]);
+      timed(PH_L2L, [&] {
+        if (i + 1 < nh) {
+          if (t1[i + 1] > t0[i + 1]) {
+            ops->l2l(d, t0[i + 1], t1[i + 1], h->sig.p, h->sig2.p, Lb[i + 1], Lb[i], R, t0[i], t1[i], s);
+            nk++;
+          }
+        } else if (g.hl[i] + 1 < nl) {  // into the LF level below, from this group's parents only
+          const int l = g.hl[i] + 1;
+          if (p.sT.lvl_begin[l + 1] > p.sT.lvl_begin[l]) {
+            ops->l2l(d, p.sT.lvl_begin[l], p.sT.lvl_begin[l + 1], h->sig.p, h->sig2.p, Llf, Lb[i], R, t0[i], t1[i],
+                     s);
+            nk++;
+          }
+        }
+      });
+    }
+    timed(PH_L2P, [&] {
+      for (size_t i = 0; i < nh; i++) {
+        const int l = g.hl[i];
+        const int64_t b = h->l2p_lvl_off[l], e = h->l2p_lvl_off[l + 1];
+        if (e > b && t1[i] > t0[i]) {
+          ops->l2p(d, h->d_l2p_bylvl + b, (int)(e - b), h->sig2.p, Lb[i], (double2*)g.pfar.p, R,
+                   (int)(c0 * g.fl[i]), (int)(c1 * g.fl[i]), true, s);
+          nk++;
+        }
+      }
+    });
+  }
+  // ---- LF levels: downward pass and L2P
+  if (g.lfT1 > g.lfT0) {
+    timed(PH_L2L, [&] {
+      for (int l = lf; l + 1 < nl; l++)
+        if (p.sT.lvl_begin[l + 2] > p.sT.lvl_begin[l + 1]) {
+          ops->l2l(d, p.sT.lvl_begin[l + 1], p.sT.lvl_begin[l + 2], h->sig.p, h->sig2.p, Llf, Llf, R, INT64_MIN,
+                   INT64_MAX, s);
+          nk++;
+        }
+    });
+    timed(PH_L2P, [&] {
+      for (int l = lf; l < nl; l++) {
+        const int64_t b = h->l2p_lvl_off[l], e = h->l2p_lvl_off[l + 1];
+        if (e > b) {
+          ops->l2p(d, h->d_l2p_bylvl + b, (int)(e - b), h->sig2.p, Llf, (double2*)g.pfar.p, R, INT_MIN, INT_MAX,
+                   true, s);
+          nk++;
+        }
+      }
+    });
+  }
+  CK(cudaEventRecord(h->ev_done, sn));
+  CK(cudaStreamWaitEvent(s, h->ev_done, 0));
+  timed(PH_SCATTER, [&] {
+    dfb::launch_scatter_rhs((const double2*)g.pnear.p, (const double2*)g.pfar.p, d.T_perm, out, nT, stride_out, R,
+                            nvec, s);
+  });
+  nk++;
+  if (h->events) {
+    CK(cudaEventRecord(t_all1, s));
+    CK(cudaEventSynchronize(t_all1));
+    float a = 0;
+    cudaEventElapsedTime(&a, t_all0, t_all1);
+    h->phase_ms[PH_TOTAL] = a;
+  }
+  h->launches += nk;
+  CK(cudaGetLastError());
+  return 0;
+}
+
+// Device bytes held by the expansion layout of the current precision.
+size_t layout_bytes(const defmm_handle* h) {
+  const GroupedLayout& g = h->gl;
+  size_t b = h->M.bytes + h->Lx.bytes + h->F.bytes + h->q.bytes + h->pscr.bytes;
+  for (const DevBuf* x : {&g.Mg, &g.Lg, &g.Mlf, &g.Llf, &g.F, &g.q, &g.pnear, &g.pfar, &g.tpart}) b += x->bytes;
+  return b;
+}
+
+// Right-hand sides per pass of the grouped layout for a call with nrhs
+// right-hand sides, or 0 for the resident layout (one right-hand side whose
+// M and L of every slot fit in 85% of the memory this handle can use).
+int choose_rhs_block(defmm_handle* h, int64_t nrhs) {
+  if (nrhs > 1) return (int)std::min<int64_t>(std::max(1, h->rhs_block), nrhs);
+  if (h->groups_forced > 0) return 1;
+  if (h->layout == 1) return 0;
+  size_t fr = 0, tot = 0;
+  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return (double)resident_bytes(h) <= 0.85 * (double)(fr + layout_bytes(h)) ? 0 : 1;
+}
+
+// nrhs matvecs on device vectors (rhs-major, user order) through the grouped
+// layout with R right-hand sides per pass.
+int gemv_grouped(defmm_handle* h, const double2* in, double2* out, int64_t nrhs, int R, cudaStream_t s) {
+  int st = prepare_grouped(h, R);
+  if (st) return st;
+  const int64_t nS = (int64_t)h->plan.S.perm.size(), nT = (int64_t)h->plan.T.perm.size();
+  for (int64_t b = 0; b < nrhs; b += R) {
+    const int nvec = (int)std::min<int64_t>(R, nrhs - b);
+    st = run_gemv_grouped(h, in + b * nS, nS, out + b * nT, nT, nvec, s);
+    if (st) return st;
   }
   return 0;
 }
@@ -856,21 +1332,33 @@ int defmm_gemv_device(defmm_handle* h, const void* d_in, void* d_out, int64_t nr
   if (!h->built) return h->fail(DEFMM_ERR_ARG, "gemv before prcmpt");
   int st = defmm_upload(h);
   if (st) return st;
-  st = prepare_precision(h);
+  st = prepare_tables(h);
   if (st) return st;
   cudaStream_t s = stream ? (cudaStream_t)stream : h->st;
   h->launches = 0;
-  const int64_t nS = (int64_t)h->plan.S.perm.size(), nT = (int64_t)h->plan.T.perm.size();
-  if (nrhs == 1) return matvec(h, (const double2*)d_in, (double2*)d_out, s);
-  // several right-hand sides: staged through the handle's own vectors so that
-  // every one replays the same captured graph (one device copy each way)
-  if ((st = ensure(h, h->rin, 16 * nS)) || (st = ensure(h, h->rout, 16 * nT))) return st;
-  for (int64_t r = 0; r < nrhs; r++) {
-    CK(cudaMemcpyAsync(h->rin.p, (const double2*)d_in + r * nS, 16 * nS, cudaMemcpyDeviceToDevice, s));
-    st = matvec(h, (const double2*)h->rin.p, (double2*)h->rout.p, s);
-    if (st) return st;
-    CK(cudaMemcpyAsync((double2*)d_out + r * nT, h->rout.p, 16 * nT, cudaMemcpyDeviceToDevice, s));
+  const int R = choose_rhs_block(h, nrhs);
+  if (R > 0) return gemv_grouped(h, (const double2*)d_in, (double2*)d_out, nrhs, R, s);
+  st = prepare_resident(h);
+  if (st) return st;
+  return matvec(h, (const double2*)d_in, (double2*)d_out, s);
+}
+
+int defmm_set_blocking(defmm_handle* h, int rhs_block, int groups) {
+  if (!h || rhs_block < 1 || rhs_block > dfb::kMaxRhsBlock || groups < 0) return DEFMM_ERR_ARG;
+  if (h->rhs_block != rhs_block || h->groups_forced != groups) {
+    h->rhs_block = rhs_block;
+    h->groups_forced = groups;
+    if (h->layout == 2) {  // planned for the old choice
+      free_grouped(h);
+      h->layout = 0;
+    }
   }
+  return 0;
+}
+
+int defmm_set_rhs_per_cta(defmm_handle* h, int rb) {
+  if (!h || (rb != 1 && rb != 2 && rb != 4 && rb != 8)) return DEFMM_ERR_ARG;
+  h->rhs_block_m2l = rb;
   return 0;
 }
 
@@ -959,18 +1447,39 @@ int defmm_gemv_batched(defmm_handle* h, int64_t nrhs, const double* in, double* 
   if (!h->built) return h->fail(DEFMM_ERR_ARG, "gemv before prcmpt");
   int st = defmm_upload(h);
   if (st) return st;
-  st = prepare_precision(h);
+  st = prepare_tables(h);
   if (st) return st;
   const int64_t nS = (int64_t)h->plan.S.perm.size(), nT = (int64_t)h->plan.T.perm.size();
   h->launches = 0;
   // direct sums still reading the previous charges (defmm_direct_noalloc on
   // another stream) finish before qin is overwritten
   CK(cudaStreamWaitEvent(h->st, h->ev_qin_read, 0));
-  for (int64_t r = 0; r < nrhs; r++) {
-    CK(cudaMemcpyAsync(h->qin.p, in + 2 * r * nS, 16 * nS, cudaMemcpyHostToDevice, h->st));
-    st = matvec(h, (const double2*)h->qin.p, (double2*)h->out.p, h->st);
-    if (st) return st;
-    CK(cudaMemcpyAsync(out + 2 * r * nT, h->out.p, 16 * nT, cudaMemcpyDeviceToHost, h->st));
+  const int R = choose_rhs_block(h, nrhs);
+  if (R == 0) {
+    if ((st = prepare_resident(h))) return st;
+    for (int64_t r = 0; r < nrhs; r++) {
+      CK(cudaMemcpyAsync(h->qin.p, in + 2 * r * nS, 16 * nS, cudaMemcpyHostToDevice, h->st));
+      st = matvec(h, (const double2*)h->qin.p, (double2*)h->out.p, h->st);
+      if (st) return st;
+      CK(cudaMemcpyAsync(out + 2 * r * nT, h->out.p, 16 * nT, cudaMemcpyDeviceToHost, h->st));
+    }
+  } else {
+    // blocks of R right-hand sides staged through the handle's device vectors
+    if ((st = prepare_grouped(h, R))) return st;
+    if ((st = ensure(h, h->rin, (size_t)16 * nS * R)) || (st = ensure(h, h->rout, (size_t)16 * nT * R))) return st;
+    for (int64_t b = 0; b < nrhs; b += R) {
+      const int nvec = (int)std::min<int64_t>(R, nrhs - b);
+      CK(cudaMemcpyAsync(h->rin.p, in + 2 * b * nS, (size_t)16 * nS * nvec, cudaMemcpyHostToDevice, h->st));
+      st = run_gemv_grouped(h, (const double2*)h->rin.p, nS, (double2*)h->rout.p, nT, nvec, h->st);
+      if (st) return st;
+      CK(cudaMemcpyAsync(out + 2 * b * nT, h->rout.p, (size_t)16 * nT * nvec, cudaMemcpyDeviceToHost, h->st));
+    }
+    // the last right-hand side's charges and potentials, for the direct-sum checks
+    const int last = (int)((nrhs - 1) % R);
+    CK(cudaMemcpyAsync(h->qin.p, (const double2*)h->rin.p + (size_t)last * nS, 16 * nS, cudaMemcpyDeviceToDevice,
+                       h->st));
+    CK(cudaMemcpyAsync(h->out.p, (const double2*)h->rout.p + (size_t)last * nT, 16 * nT, cudaMemcpyDeviceToDevice,
+                       h->st));
   }
   CK(cudaStreamSynchronize(h->st));
   int flag = 0;
@@ -1054,10 +1563,12 @@ int defmm_info(const defmm_handle* h, int what, int64_t* v) {
     case DEFMM_INFO_I_NEAR: *v = p.i_near; break;
     case DEFMM_INFO_TABLES: *v = (int64_t)p.tab_lvl.size(); break;
     case DEFMM_INFO_DEVICE_BYTES:
-      *v = (int64_t)(h->dev_bytes + h->M.bytes + h->Lx.bytes + h->F.bytes + h->q.bytes + h->sig.bytes +
-                     h->sig2.bytes + h->ptab.bytes + h->pnear.bytes + h->pfar.bytes +
-                     h->qin.bytes + h->out.bytes + h->rin.bytes + h->rout.bytes);
+      *v = (int64_t)(h->dev_bytes + layout_bytes(h) + h->sig.bytes + h->sig2.bytes + h->ptab.bytes +
+                     h->pnear.bytes + h->pfar.bytes + h->qin.bytes + h->out.bytes + h->rin.bytes + h->rout.bytes);
       break;
+    case DEFMM_INFO_LAYOUT: *v = h->layout; break;
+    case DEFMM_INFO_RHS_BLOCK: *v = h->layout == 2 ? h->gl.R : 0; break;
+    case DEFMM_INFO_GROUPS: *v = h->layout == 2 ? (int64_t)h->gl.groups.size() : 0; break;
     case DEFMM_INFO_LIST_RECORDS: *v = p.keep_lists ? 1 : 0; break;
     case DEFMM_INFO_LAUNCHES: *v = h->launches; break;
     case DEFMM_INFO_PERMUTED_SPECTRA: *v = (int64_t)p.ptab_key.size(); break;
@@ -1080,6 +1591,31 @@ int defmm_info(const defmm_handle* h, int what, int64_t* v) {
     case DEFMM_INFO_LEAF_SLOTS_S: {
       int64_t n = 0;
       for (int32_t c : p.p2m_leaf) n += p.sS.cell_ptr[c + 1] - p.sS.cell_ptr[c];
+      *v = n;
+      break;
+    }
+    case DEFMM_INFO_M2M_ENTRIES: *v = p.m2m_ptr.empty() ? 0 : p.m2m_ptr.back(); break;
+    case DEFMM_INFO_L2L_ENTRIES: *v = p.l2l_ptr.empty() ? 0 : p.l2l_ptr.back(); break;
+    case DEFMM_INFO_P2M_POINT_SLOTS: {
+      int64_t n = 0;
+      for (int32_t c : p.p2m_leaf) n += (int64_t)p.S.nprt[c] * (p.sS.cell_ptr[c + 1] - p.sS.cell_ptr[c]);
+      *v = n;
+      break;
+    }
+    case DEFMM_INFO_L2P_POINT_SLOTS: {
+      int64_t n = 0;
+      for (int32_t c : p.l2p_leaf) n += (int64_t)p.T.nprt[c] * (p.sT.cell_ptr[c + 1] - p.sT.cell_ptr[c]);
+      *v = n;
+      break;
+    }
+    case DEFMM_INFO_M2F_SLOTS: {  // source slots at precomputed levels that have target slots in their cone
+      int64_t n = 0;
+      for (int l = 0; l < p.lv.nlvl; l++) {
+        const auto& cS = p.sS.cone_begin[l];
+        const auto& cT = p.sT.cone_begin[l];
+        for (size_t c = 0; c + 1 < cS.size() && c + 1 < cT.size(); c++)
+          if (cT[c + 1] > cT[c]) n += cS[c + 1] - cS[c];
+      }
       *v = n;
       break;
     }
@@ -1138,6 +1674,29 @@ int defmm_dump_lists(const defmm_handle* h, int32_t* far_hf, int32_t* far_lf, in
   if (far_hf) std::memcpy(far_hf, p.rec_far_hf.data(), p.rec_far_hf.size() * 4);
   if (far_lf) std::memcpy(far_lf, p.rec_far_lf.data(), p.rec_far_lf.size() * 4);
   if (near_) std::memcpy(near_, p.rec_near.data(), p.rec_near.size() * 4);
+  return 0;
+}
+
+int defmm_dump_m2l(const defmm_handle* h, int64_t* ptr, int32_t* src, uint32_t* tab, int64_t n[2]) {
+  if (!h || !h->built || !n) return DEFMM_ERR_ARG;
+  const Plan& p = h->plan;
+  n[0] = (int64_t)p.m2l_ptr.size();
+  n[1] = p.m2l_ptr.empty() ? 0 : p.m2l_ptr.back();
+  if (ptr) std::memcpy(ptr, p.m2l_ptr.data(), p.m2l_ptr.size() * 8);
+  if (!src && !tab) return 0;
+  if (p.dev_m2l_src) {  // entries left on the device by the level walk
+    if (h->device >= 0 && cudaSetDevice(h->device) != cudaSuccess) return DEFMM_ERR_CUDA;
+    if ((src && cudaMemcpy(src, p.dev_m2l_src, (size_t)n[1] * 4, cudaMemcpyDeviceToHost) != cudaSuccess) ||
+        (tab && cudaMemcpy(tab, p.dev_m2l_tab, (size_t)n[1] * 4, cudaMemcpyDeviceToHost) != cudaSuccess)) {
+      cudaGetLastError();
+      return DEFMM_ERR_CUDA;
+    }
+  } else {
+    if (src) std::memcpy(src, p.m2l_src.data(), p.m2l_src.size() * 4);
+    if (tab) std::memcpy(tab, p.m2l_tab.data(), p.m2l_tab.size() * 4);
+  }
+  if (tab)  // ids -> (table << 6) | hash keys
+    for (int64_t i = 0; i < n[1]; i++) tab[i] = p.ptab_key[tab[i]];
   return 0;
 }
 

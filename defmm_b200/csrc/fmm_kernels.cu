@@ -217,10 +217,11 @@ struct P2MCfg {
   static constexpr int NPB0 = 65536 / (LLP * (int)sizeof(T));
   static constexpr int NPB = NPB0 > 64 ? 64 : NPB0;  // points per chunk
   typedef typename cpx_t<T>::type C;
-  // shared memory: Z, basis values, point offsets, charges, W blocks of 4 warps
-  static constexpr size_t smem() {
-    return sizeof(T) * (size_t)NPB * LLP + sizeof(double) * NPB * 3 + sizeof(T) * NPB * 3 * L + sizeof(C) * NPB +
-           sizeof(C) * 4 * NPB * S;
+  // shared memory: Z, point offsets, basis values, W blocks of 4 warps,
+  // (with R > 1 right-hand sides) phase blocks of 4 warps, charges (R per point)
+  static constexpr size_t smem(int R = 1) {
+    return sizeof(T) * (size_t)NPB * LLP + sizeof(double) * NPB * 3 + sizeof(T) * NPB * 3 * L +
+           sizeof(C) * 4 * NPB * S * (R > 1 ? 2 : 1) + sizeof(C) * (size_t)NPB * R;
   }
 };
 
@@ -228,62 +229,80 @@ template <typename T, int L, int SS>
 __device__ __forceinline__ void p2m_group(const DevPlan& P, int64_t j0, int ns, bool hf, bool first, int np,
                                           const T* __restrict__ Zs, const double* __restrict__ yc,
                                           const typename cpx_t<T>::type* __restrict__ qs,
-                                          typename cpx_t<T>::type* __restrict__ Ws, const double* dirs,
+                                          typename cpx_t<T>::type* __restrict__ Ws,
+                                          typename cpx_t<T>::type* __restrict__ Es, const double* dirs,
                                           const typename cpx_t<T>::type* __restrict__ s2,
-                                          typename cpx_t<T>::type* __restrict__ M, int lane) {
+                                          typename cpx_t<T>::type* __restrict__ M, int R, int lane) {
   typedef typename cpx_t<T>::type C;
   typedef P2MCfg<T, L> G;
-  constexpr int R = G::R, LLP = G::LLP, LL = G::LL;
+  constexpr int RE = G::R, LLP = G::LLP, LL = G::LL;
   __syncwarp();
+  // phases exp(-i k d_s.(y_j - c)) of the group's slots, shared by the
+  // right-hand sides (with one right-hand side the charge is folded in here)
   for (int idx = lane; idx < np * SS; idx += 32) {
     const int j = idx / SS, s = idx % SS;
-    C w = qs[j];
+    C w;
     if (s >= ns) {
       w = czero<C>();
     } else if (hf) {
       const double* dv = dirs + 3 * P.S_cdir[j0 + s];
       double dp = 0.;
       for (int k = 0; k < 3; k++) dp += dv[k] * yc[3 * j + k];
-      w = cmul(w, expi<C>(-P.kappa * dp));
+      w = expi<C>(-P.kappa * dp);
+    } else {
+      w.x = T(1);
+      w.y = T(0);
     }
-    Ws[j * SS + s] = w;
+    if (R == 1)
+      Ws[j * SS + s] = cmul(w, qs[j]);
+    else
+      Es[j * SS + s] = w;
   }
-  __syncwarp();
-  C acc[R][SS];
+  for (int r = 0; r < R; r++) {
+    __syncwarp();
+    if (R > 1) {
+      for (int idx = lane; idx < np * SS; idx += 32) {
+        const int j = idx / SS;
+        Ws[idx] = cmul(Es[idx], qs[j * R + r]);
+      }
+      __syncwarp();
+    }
+    C acc[RE][SS];
 #pragma unroll
-  for (int r = 0; r < R; r++)
+    for (int e = 0; e < RE; e++)
 #pragma unroll
-    for (int s = 0; s < SS; s++) acc[r][s] = czero<C>();
-  const T* zl = Zs + lane * R;
-  for (int j = 0; j < np; j++) {
-    T z[R];
-    C w[SS];
+      for (int s = 0; s < SS; s++) acc[e][s] = czero<C>();
+    const T* zl = Zs + lane * RE;
+    for (int j = 0; j < np; j++) {
+      T z[RE];
+      C w[SS];
 #pragma unroll
-    for (int r = 0; r < R; r++) z[r] = zl[j * LLP + r];
+      for (int e = 0; e < RE; e++) z[e] = zl[j * LLP + e];
 #pragma unroll
-    for (int s = 0; s < SS; s++) w[s] = Ws[j * SS + s];
+      for (int s = 0; s < SS; s++) w[s] = Ws[j * SS + s];
 #pragma unroll
-    for (int r = 0; r < R; r++)
+      for (int e = 0; e < RE; e++)
 #pragma unroll
-      for (int s = 0; s < SS; s++) rfma(acc[r][s], z[r], w[s]);
-  }
+        for (int s = 0; s < SS; s++) rfma(acc[e][s], z[e], w[s]);
+    }
 #pragma unroll
-  for (int s = 0; s < SS; s++) {
-    if (s < ns) {
-      const int slot = P.S_cslot[j0 + s], d = P.S_cdir[j0 + s];
+    for (int s = 0; s < SS; s++) {
+      if (s < ns) {
+        const int slot = P.S_cslot[j0 + s], d = P.S_cdir[j0 + s];
 #pragma unroll
-      for (int r = 0; r < R; r++) {
-        const int l = lane * R + r;
-        if (l < LL) {
-          const C a = hf ? cmulc(s2[(int64_t)d * LL + l], acc[r][s]) : acc[r][s];
-          C* out = M + (int64_t)slot * LL + l;
-          if (first) {
-            *out = a;
-          } else {
-            C o = *out;
-            o.x += a.x;
-            o.y += a.y;
-            *out = o;
+        for (int e = 0; e < RE; e++) {
+          const int l = lane * RE + e;
+          if (l < LL) {
+            const C a = hf ? cmulc(s2[(int64_t)d * LL + l], acc[e][s]) : acc[e][s];
+            C* out = M + ((int64_t)slot * R + r) * LL + l;
+            if (first) {
+              *out = a;
+            } else {
+              C o = *out;
+              o.x += a.x;
+              o.y += a.y;
+              *out = o;
+            }
           }
         }
       }
@@ -291,11 +310,33 @@ __device__ __forceinline__ void p2m_group(const DevPlan& P, int64_t j0, int ns, 
   }
 }
 
+// Leaf slots of cell c (CSR of the slot lists, directions increasing) whose
+// direction lies in [d0, d1): a contiguous sub-range [*b, *e).
+__device__ __forceinline__ void dir_range(const int64_t* __restrict__ cptr, const int32_t* __restrict__ cdir,
+                                          int64_t c, int d0, int d1, int64_t* b, int64_t* e) {
+  int64_t lo = cptr[c], hi = cptr[c + 1];
+  int64_t a = lo, z = hi;
+  while (a < z) {  // first entry with dir >= d0
+    const int64_t m = (a + z) >> 1;
+    if (cdir[m] < d0) a = m + 1; else z = m;
+  }
+  int64_t a2 = a, z2 = hi;
+  while (a2 < z2) {  // first entry with dir >= d1
+    const int64_t m = (a2 + z2) >> 1;
+    if (cdir[m] < d1) a2 = m + 1; else z2 = m;
+  }
+  *b = a;
+  *e = a2;
+}
+
+// M: base of the expansions written here (slot s, right-hand side r at
+// M + (s R + r) LL); q: tree-order charges, R per particle (q[j R + r]);
+// only the leaf slots with a direction in [d0, d1) are computed.
 template <typename T, int L>
 __global__ void __launch_bounds__(128) k_p2m(DevPlan P, const int32_t* __restrict__ leaves, int nleaves,
                                              const typename cpx_t<T>::type* __restrict__ q,
                                              const typename cpx_t<T>::type* __restrict__ sig2,
-                                             typename cpx_t<T>::type* __restrict__ M) {
+                                             typename cpx_t<T>::type* __restrict__ M, int R, int d0, int d1) {
   typedef typename cpx_t<T>::type C;
   typedef P2MCfg<T, L> G;
   constexpr int LL = G::LL, LLP = G::LLP, NPB = G::NPB, S = G::S;
@@ -303,10 +344,12 @@ __global__ void __launch_bounds__(128) k_p2m(DevPlan P, const int32_t* __restric
   T* Zs = reinterpret_cast<T*>(smem_raw);
   double* yc = reinterpret_cast<double*>(Zs + (size_t)NPB * LLP);
   T* Bs = reinterpret_cast<T*>(yc + NPB * 3);
-  C* qs = reinterpret_cast<C*>(Bs + NPB * 3 * L);
-  C* Wall = qs + NPB;
+  C* Wall = reinterpret_cast<C*>(Bs + NPB * 3 * L);
+  C* Eall = Wall + 4 * NPB * S;
+  C* qs = Eall + (R > 1 ? 4 * NPB * S : 0);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   C* Ws = Wall + warp * NPB * S;
+  C* Es = Eall + warp * NPB * S;
   for (int li = blockIdx.x; li < nleaves; li += gridDim.x) {
     const int c = leaves[li];
     const int n = P.S_nprt[c], f = P.S_first[c];
@@ -314,8 +357,10 @@ __global__ void __launch_bounds__(128) k_p2m(DevPlan P, const int32_t* __restric
     const int lv = P.S_lvl[c];
     const bool hf = P.ishf[lv] != 0;
     const int h = P.hfstage[lv];
-    const int64_t sb = P.S_cptr[c], se = P.S_cptr[c + 1];
+    int64_t sb, se;
+    dir_range(P.S_cptr, P.S_cdir, c, d0, d1, &sb, &se);
     const int nslots = (int)(se - sb);
+    if (nslots == 0) continue;
     const double* dirs = P.dirs + P.dir_off[h] * 3;
     const C* s2 = sig2 + P.sig_off[h];
     for (int p0 = 0; p0 < n; p0 += NPB) {
@@ -330,7 +375,7 @@ __global__ void __launch_bounds__(128) k_p2m(DevPlan P, const int32_t* __restric
 #pragma unroll
         for (int l = 0; l < L; l++) Bs[(p * 3 + k) * L + l] = b[l];
       }
-      for (int p = threadIdx.x; p < np; p += blockDim.x) qs[p] = q[f + p0 + p];
+      for (int p = threadIdx.x; p < np * R; p += blockDim.x) qs[p] = q[(int64_t)(f + p0) * R + p];
       __syncthreads();
       for (int o = threadIdx.x; o < np * LLP; o += blockDim.x) {
         const int p = o / LLP, l = o % LLP;
@@ -345,9 +390,9 @@ __global__ void __launch_bounds__(128) k_p2m(DevPlan P, const int32_t* __restric
       for (int g0 = warp * S; g0 < nslots; g0 += 4 * S) {
         const int ns = min(S, nslots - g0);
         if (ns == 1)
-          p2m_group<T, L, 1>(P, sb + g0, 1, hf, p0 == 0, np, Zs, yc, qs, Ws, dirs, s2, M, lane);
+          p2m_group<T, L, 1>(P, sb + g0, 1, hf, p0 == 0, np, Zs, yc, qs, Ws, Es, dirs, s2, M, R, lane);
         else
-          p2m_group<T, L, S>(P, sb + g0, ns, hf, p0 == 0, np, Zs, yc, qs, Ws, dirs, s2, M, lane);
+          p2m_group<T, L, S>(P, sb + g0, ns, hf, p0 == 0, np, Zs, yc, qs, Ws, Es, dirs, s2, M, R, lane);
       }
     }
   }
@@ -476,19 +521,26 @@ struct Sep {
 // A lane reads its (b, c) lines (along axis 0) of each child's expansion
 // straight into registers, lanes at unit stride (the next child's are
 // prefetched during the current transfer); the transfer runs axis 0 first.
+// With R right-hand sides a warp takes one (parent slot, right-hand side);
+// the parent's expansions live at Mp + (slot R + r) LL, the children's at
+// Mc0 + (slot R + r) LL (both bases may be the same array).
 constexpr int kXferWarps = 4;  // warps (transfers in flight) per CTA
 
 template <typename T, int L>
 __global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 4 ? 6 : (L == 5 ? 5 : 3)) : (L <= 5 ? 3 : 1)) k_m2m(DevPlan P, int64_t s0, int64_t s1,
                                                          const typename cpx_t<T>::type* __restrict__ sig,
                                                          const typename cpx_t<T>::type* __restrict__ sig2,
-                                                         typename cpx_t<T>::type* __restrict__ M) {
+                                                         typename cpx_t<T>::type* __restrict__ Mp,
+                                                         const typename cpx_t<T>::type* __restrict__ Mc0, int R) {
   typedef typename cpx_t<T>::type C;
   typedef Sep<T, L, 0> S;
   constexpr int LL = L * L * L, NW = kXferWarps, NLN = S::NLN;
   __shared__ C sbuf[NW][LL];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int64_t ps = s0 + blockIdx.x * NW + warp; ps < s1; ps += (int64_t)gridDim.x * NW) {
+  const int64_t nw = (s1 - s0) * R;
+  for (int64_t w = blockIdx.x * NW + warp; w < nw; w += (int64_t)gridDim.x * NW) {
+    const int64_t ps = s0 + w / R;
+    const int rr = (int)(w % R);
     const int64_t eb = P.m2m_ptr[ps], ee = P.m2m_ptr[ps + 1];
     if (eb == ee) continue;  // leaf slot: written by P2M
     const int pc = P.sS_cell[ps], d = P.sS_dir[ps];
@@ -524,7 +576,7 @@ __global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 4 ? 6 
     }
     C nxt[REG ? NLN : 1][L];  // next child's (a, b) lines, prefetched
     if (REG) {
-      const C* Mc = M + (int64_t)__shfl_sync(0xffffffffu, my_cs, 0) * LL;
+      const C* Mc = Mc0 + ((int64_t)__shfl_sync(0xffffffffu, my_cs, 0) * R + rr) * LL;
 #pragma unroll
       for (int k = 0; k < L; k++) nxt[0][k] = lane < L * L ? Mc[k * L * L + lane] : czero<C>();
     }
@@ -537,13 +589,13 @@ __global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 4 ? 6 
 #pragma unroll
         for (int k = 0; k < L; k++) in[0][k] = hf ? cmul(sgr[0][k], nxt[0][k]) : nxt[0][k];
         if (e + 1 < nch) {
-          const C* Mc = M + (int64_t)__shfl_sync(0xffffffffu, my_cs, e + 1) * LL;
+          const C* Mc = Mc0 + ((int64_t)__shfl_sync(0xffffffffu, my_cs, e + 1) * R + rr) * LL;
 #pragma unroll
           for (int k = 0; k < L; k++)
             if (lane < L * L) nxt[0][k] = Mc[k * L * L + lane];
         }
       } else {
-        const C* Mc = M + (int64_t)__shfl_sync(0xffffffffu, my_cs, e) * LL;
+        const C* Mc = Mc0 + ((int64_t)__shfl_sync(0xffffffffu, my_cs, e) * R + rr) * LL;
 #pragma unroll
         for (int q = 0; q < NLN; q++) {
           const int ln = lane + 32 * q;
@@ -579,7 +631,7 @@ __global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 4 ? 6 
 #pragma unroll
         for (int k = 0; k < L; k++) {
           const int l = ln * L + k;
-          M[ps * LL + l] = hf ? cmulc(sg2[l], acc[q][k]) : acc[q][k];
+          Mp[(ps * R + rr) * LL + l] = hf ? cmulc(sg2[l], acc[q][k]) : acc[q][k];
         }
     }
   }
@@ -590,17 +642,25 @@ __global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 4 ? 6 
 //   HF parent direction d (hfL2Lblock L2L.hpp:78-108 / hf2lfL2L :111-127):
 //     L_c += sum_d exp(i k v.d) conj(sig_d) o B_v(sig2_d o L_d)
 //   LF parent (lfL2L :35-41): L_c += B_v(L_p);   v = ctr_child - ctr_parent
+// With R right-hand sides a warp takes one (child slot, right-hand side);
+// children at Lc + (slot R + r) LL, parents at Lp0 + (slot R + r) LL.  Only
+// parent slots in [p0, p1) contribute (a pass over part of the directions).
 template <typename T, int L>
 __global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 5 ? 6 : 3) : (L <= 5 ? 3 : 1)) k_l2l(DevPlan P, int64_t s0, int64_t s1,
                                                          const typename cpx_t<T>::type* __restrict__ sig,
                                                          const typename cpx_t<T>::type* __restrict__ sig2,
-                                                         typename cpx_t<T>::type* __restrict__ Lx) {
+                                                         typename cpx_t<T>::type* __restrict__ Lc,
+                                                         const typename cpx_t<T>::type* __restrict__ Lp0, int R,
+                                                         int64_t p0, int64_t p1) {
   typedef typename cpx_t<T>::type C;
   typedef Sep<T, L, 1> S;
   constexpr int LL = L * L * L, NW = kXferWarps, NLN = S::NLN;
   __shared__ C sbuf[NW][LL];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int64_t cs = s0 + blockIdx.x * NW + warp; cs < s1; cs += (int64_t)gridDim.x * NW) {
+  const int64_t nw = (s1 - s0) * R;
+  for (int64_t w = blockIdx.x * NW + warp; w < nw; w += (int64_t)gridDim.x * NW) {
+    const int64_t cs = s0 + w / R;
+    const int rr = (int)(w % R);
     const int64_t eb = P.l2l_ptr[cs], ee = P.l2l_ptr[cs + 1];
     if (eb == ee) continue;
     const int cc = P.sT_cell[cs];
@@ -616,19 +676,33 @@ __global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 5 ? 6 
     for (int q = 0; q < NLN; q++)
 #pragma unroll
       for (int k = 0; k < L; k++) acc[q][k] = czero<C>();
-    // parents' slots and directions fetched by lane (<= 6 per child slot)
-    const int npa = (int)(ee - eb);
-    int my_ps = 0, my_d = 0;
-    if (lane < npa) {
-      my_ps = P.l2l_parent[eb + lane];
-      my_d = P.sT_dir[my_ps];
+    // parents' slots and directions fetched by lane (<= 6 per child slot),
+    // only those in [p0, p1), compacted to the first lanes
+    const int nall = (int)(ee - eb);
+    int all_ps = 0, all_d = 0;
+    if (lane < nall) {
+      all_ps = P.l2l_parent[eb + lane];
+      all_d = P.sT_dir[all_ps];
     }
+    int my_ps = 0, my_d = 0, npa = 0;
+    for (int e = 0; e < nall; e++) {  // warp-uniform: keep the parents in range, in order
+      const int ps_e = __shfl_sync(0xffffffffu, all_ps, e);
+      const int d_e = __shfl_sync(0xffffffffu, all_d, e);
+      if (ps_e >= p0 && ps_e < p1) {
+        if (lane == npa) {
+          my_ps = ps_e;
+          my_d = d_e;
+        }
+        npa++;
+      }
+    }
+    if (npa == 0) continue;
     // with one line per lane (L <= 5) the next parent's lines are
     // prefetched into registers; larger orders load them when used
     constexpr bool REG = NLN == 1;
     C nxt[REG ? NLN : 1][L];
     if (REG) {
-      const C* Lp = Lx + (int64_t)__shfl_sync(0xffffffffu, my_ps, 0) * LL;
+      const C* Lp = Lp0 + ((int64_t)__shfl_sync(0xffffffffu, my_ps, 0) * R + rr) * LL;
 #pragma unroll
       for (int k = 0; k < L; k++) nxt[0][k] = lane < L * L ? Lp[lane * L + k] : czero<C>();
     }
@@ -641,13 +715,13 @@ __global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 5 ? 6 
 #pragma unroll
         for (int k = 0; k < L; k++) in[0][k] = (hf && lane < L * L) ? cmul(sgq[lane * L + k], nxt[0][k]) : nxt[0][k];
         if (e + 1 < npa) {
-          const C* Lp = Lx + (int64_t)__shfl_sync(0xffffffffu, my_ps, e + 1) * LL;
+          const C* Lp = Lp0 + ((int64_t)__shfl_sync(0xffffffffu, my_ps, e + 1) * R + rr) * LL;
 #pragma unroll
           for (int k = 0; k < L; k++)
             if (lane < L * L) nxt[0][k] = Lp[lane * L + k];
         }
       } else {
-        const C* Lp = Lx + (int64_t)__shfl_sync(0xffffffffu, my_ps, e) * LL;
+        const C* Lp = Lp0 + ((int64_t)__shfl_sync(0xffffffffu, my_ps, e) * R + rr) * LL;
 #pragma unroll
         for (int q = 0; q < NLN; q++) {
           const int ln = lane + 32 * q;
@@ -686,11 +760,11 @@ __global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 5 ? 6 
       if (ln < L * L)
 #pragma unroll
         for (int k = 0; k < L; k++) {
-          const int64_t l = cs * LL + k * L * L + ln;
-          C o = Lx[l];
+          const int64_t l = (cs * R + rr) * LL + k * L * L + ln;
+          C o = Lc[l];
           o.x += acc[q][k].x;
           o.y += acc[q][k].y;
-          Lx[l] = o;
+          Lc[l] = o;
         }
     }
   }
@@ -996,6 +1070,75 @@ __global__ void __launch_bounds__(NT, (sizeof(T) == 8 ? 512 : 1024) / NT) k_m2l_
   }
 }
 
+// Right-hand-side blocks: R charge vectors per pass, F and L holding R
+// expansions per slot (F + ((s - f0) R + r) PP, Lx + (t R + r) LL).  A CTA
+// takes one (target slot, block of RB right-hand sides) at a time; each
+// transfer spectrum entry U_k[i] is loaded once and multiplied into the RB
+// spectra of its source slot, so the spectra traffic per right-hand side is
+// e P^3 (1 + 1/RB) per far pair instead of 2 e P^3.
+// CTAs per SM of k_m2l_rhs: room for K x RB complex accumulators per thread
+template <typename T, int NT, int RB>
+constexpr int m2l_rhs_ctas() {
+  return (sizeof(T) == 8 ? (RB >= 8 ? 512 : (RB >= 2 ? 768 : 1024)) : (RB >= 8 ? 768 : 1024)) / NT;
+}
+
+template <typename T, int L, int NT, int RB>
+__global__ void __launch_bounds__(NT, m2l_rhs_ctas<T, NT, RB>()) k_m2l_rhs(DevPlan P, int64_t t0, int64_t t1, int64_t f0, int64_t f1, int R,
+                                                             const typename cpx_t<T>::type* __restrict__ F,
+                                                             const typename cpx_t<T>::type* __restrict__ ptab,
+                                                             typename cpx_t<T>::type* __restrict__ Lx,
+                                                             unsigned long long* __restrict__ queue) {
+  typedef typename cpx_t<T>::type C;
+  constexpr int PD = 2 * L - 1, LL = L * L * L, PP = PD * PD * PD, K = (PP + NT - 1) / NT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* Js = reinterpret_cast<C*>(smem_raw);
+  C* Cb = Js + PP;
+  C* D = Cb + L * PD * PD;
+  __shared__ int64_t cur;
+  const int nb = R / RB;
+  const int64_t nwork = (t1 - t0) * nb;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) cur = (int64_t)atomicAdd(queue, 1ULL);
+    __syncthreads();
+    const int64_t w = cur;
+    if (w >= nwork) break;
+    const int64_t t = t0 + w / nb;
+    const int r0 = (int)(w % nb) * RB;
+    const int64_t eb = P.m2l_ptr[t], ee = P.m2l_ptr[t + 1];
+    C acc[K][RB];
+#pragma unroll
+    for (int k = 0; k < K; k++)
+#pragma unroll
+      for (int b = 0; b < RB; b++) acc[k][b] = czero<C>();
+    for (int64_t e = eb; e < ee; e++) {
+      const int64_t src = P.m2l_src[e];
+      if (src < f0 || src >= f1) {  // entry outside this cone batch: a plan bug
+        if (threadIdx.x == 0) atomicExch(P.err, 1);
+        continue;
+      }
+      const C* Fs = F + ((src - f0) * R + r0) * PP;
+      const C* U = ptab + (int64_t)P.m2l_tab[e] * PP;
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        const int i = threadIdx.x + k * NT;
+        if (i < PP) {
+          const C u = __ldg(U + i);
+#pragma unroll
+          for (int b = 0; b < RB; b++) cfma(acc[k][b], u, __ldg(Fs + b * PP + i));
+        }
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < RB; b++) {
+      C a[K];
+#pragma unroll
+      for (int k = 0; k < K; k++) a[k] = acc[k][b];
+      m2l_f2l<T, L, NT>(a, Js, Cb, D, Lx + (t * R + r0 + b) * LL);
+    }
+  }
+}
+
 // -------------------------------------------------------------------- L2P --
 // One CTA (4 warps) per target leaf at a precomputed level
 // (dwnpass.hpp:39-47): HF (phfL2P, L2P.hpp:122-142)
@@ -1004,24 +1147,31 @@ __global__ void __launch_bounds__(NT, (sizeof(T) == 8 ? 512 : 1024) / NT) k_m2l_
 // Warps take the leaf's slots in turn, lanes its particles; each lane keeps
 // its particle's 3 L basis values in registers and accumulates over the
 // warp's slots in registers; the 4 warps are summed at the end.
-template <typename T, int L>
+// Lx: base of the local expansions read here (slot s, right-hand side r at
+// Lx + (s R + r) LL); only the leaf slots with a direction in [d0, d1)
+// contribute; pfar holds R potentials per particle (pfar[j R + r]), written
+// (acc = false) or added to (acc = true).  RC right-hand sides per pass over
+// the slots (the phase of a slot is computed once per pass).
+template <typename T, int L, int RC>
 __global__ void __launch_bounds__(128) k_l2p(DevPlan P, const int32_t* __restrict__ leaves, int nleaves,
                                              const typename cpx_t<T>::type* __restrict__ sig2,
                                              const typename cpx_t<T>::type* __restrict__ Lx,
-                                             double2* __restrict__ pfar) {
+                                             double2* __restrict__ pfar, int R, int d0, int d1, bool accum) {
   typedef typename cpx_t<T>::type C;
   constexpr int LL = L * L * L;
   __shared__ C buf[4][LL];
-  __shared__ double2 part[4][32];
+  __shared__ double2 part[4][RC][32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int li = blockIdx.x; li < nleaves; li += gridDim.x) {
     const int c = leaves[li];
+    int64_t sb, se;
+    dir_range(P.T_cptr, P.T_cdir, c, d0, d1, &sb, &se);
+    if (sb == se) continue;
     const int n = P.T_nprt[c], f = P.T_first[c];
     const double4 ct = P.T_ctr[c];
     const int lv = P.T_lvl[c];
     const bool hf = P.ishf[lv] != 0;
     const int h = P.hfstage[lv];
-    const int64_t sb = P.T_cptr[c], se = P.T_cptr[c + 1];
     const double* dirs = P.dirs + P.dir_off[h] * 3;
     const C* s2 = sig2 + P.sig_off[h];
     for (int p0 = 0; p0 < n; p0 += 32) {
@@ -1034,67 +1184,97 @@ __global__ void __launch_bounds__(128) k_l2p(DevPlan P, const int32_t* __restric
         xr[k] = P.T_pos[3 * (int64_t)pi + k] - (&ct.x)[k];
         lagrange_all<L, T>((T)xr[k], (T)ct.w, B[k]);
       }
-      double2 acc = make_double2(0., 0.);
-      // the next slot's expansion (and signature) is loaded into registers
-      // while the current one is contracted
-      constexpr int NV = (LL + 31) / 32;
-      C nl[NV], ns[NV];
-      int nd = 0;
-      auto fetch = [&](int64_t j) {
-        const int slot = P.T_cslot[j];
-        nd = P.T_cdir[j];
-        const C* Ls = Lx + (int64_t)slot * LL;
-        const C* Ss = s2 + (int64_t)(hf ? nd : 0) * LL;
+      for (int r0 = 0; r0 < R; r0 += RC) {
+        const int nr = min(RC, R - r0);
+        double2 acc[RC];
 #pragma unroll
-        for (int m = 0; m < NV; m++) {
-          const int l = lane + 32 * m;
-          nl[m] = l < LL ? Ls[l] : czero<C>();
-          ns[m] = (hf && l < LL) ? Ss[l] : czero<C>();
-        }
-      };
-      if (sb + warp < se) fetch(sb + warp);
-      for (int64_t j = sb + warp; j < se; j += 4) {
-        const int d = nd;
-        __syncwarp();
+        for (int u = 0; u < RC; u++) acc[u] = make_double2(0., 0.);
+        // units (slot of this warp, right-hand side); the next unit's
+        // expansion (and, on a new slot, signature) is loaded into registers
+        // while the current one is contracted
+        constexpr int NV = (LL + 31) / 32;
+        const int64_t nunit = ((se - sb - warp + 3) / 4) * nr;
+        C nl[NV], ns[NV];
+        int nd = 0;
+        auto fetch = [&](int64_t k) {
+          const int64_t j = sb + warp + 4 * (k / nr);
+          const int u = (int)(k % nr);
+          const int slot = P.T_cslot[j];
+          const C* Ls = Lx + ((int64_t)slot * R + r0 + u) * LL;
 #pragma unroll
-        for (int m = 0; m < NV; m++) {
-          const int l = lane + 32 * m;
-          if (l < LL) buf[warp][l] = hf ? cmul(ns[m], nl[m]) : nl[m];
-        }
-        __syncwarp();
-        if (j + 4 < se) fetch(j + 4);
-        // sum_{a,b,c} B0[a] B1[b] B2[c] X[a,b,c] = sum_a B0[a] (sum_b B1[b] (sum_c B2[c] X[a,b,c]))
-        C sum = czero<C>();
-#pragma unroll
-        for (int a = 0; a < L; a++) {
-          C sa = czero<C>();
-#pragma unroll
-          for (int b = 0; b < L; b++) {
-            C sb = czero<C>();
-#pragma unroll
-            for (int cc = 0; cc < L; cc++) rfma(sb, B[2][cc], buf[warp][(a * L + b) * L + cc]);
-            rfma(sa, B[1][b], sb);
+          for (int m = 0; m < NV; m++) {
+            const int l = lane + 32 * m;
+            nl[m] = l < LL ? Ls[l] : czero<C>();
           }
-          rfma(sum, B[0][a], sa);
+          if (u == 0) {
+            nd = P.T_cdir[j];
+            const C* Ss = s2 + (int64_t)(hf ? nd : 0) * LL;
+#pragma unroll
+            for (int m = 0; m < NV; m++) {
+              const int l = lane + 32 * m;
+              ns[m] = (hf && l < LL) ? Ss[l] : czero<C>();
+            }
+          }
+        };
+        if (nunit > 0) fetch(0);
+        C ph = czero<C>();
+        for (int64_t k = 0; k < nunit; k++) {
+          const int u = (int)(k % nr);
+          if (u == 0 && hf) {
+            const double* dv = dirs + 3 * nd;
+            ph = expi<C>(P.kappa * (dv[0] * xr[0] + dv[1] * xr[1] + dv[2] * xr[2]));
+          }
+          __syncwarp();
+#pragma unroll
+          for (int m = 0; m < NV; m++) {
+            const int l = lane + 32 * m;
+            if (l < LL) buf[warp][l] = hf ? cmul(ns[m], nl[m]) : nl[m];
+          }
+          __syncwarp();
+          if (k + 1 < nunit) fetch(k + 1);
+          // sum_{a,b,c} B0[a] B1[b] B2[c] X[a,b,c] = sum_a B0[a] (sum_b B1[b] (sum_c B2[c] X[a,b,c]))
+          C sum = czero<C>();
+#pragma unroll
+          for (int a = 0; a < L; a++) {
+            C sa = czero<C>();
+#pragma unroll
+            for (int b = 0; b < L; b++) {
+              C sbb = czero<C>();
+#pragma unroll
+              for (int cc = 0; cc < L; cc++) rfma(sbb, B[2][cc], buf[warp][(a * L + b) * L + cc]);
+              rfma(sa, B[1][b], sbb);
+            }
+            rfma(sum, B[0][a], sa);
+          }
+          if (hf) sum = cmul(sum, ph);
+#pragma unroll
+          for (int v = 0; v < RC; v++)
+            if (v == u) {
+              acc[v].x += (double)sum.x;
+              acc[v].y += (double)sum.y;
+            }
         }
-        if (hf) {
-          const double* dv = dirs + 3 * d;
-          sum = cmul(sum, expi<C>(P.kappa * (dv[0] * xr[0] + dv[1] * xr[1] + dv[2] * xr[2])));
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < RC; u++) part[warp][u][lane] = acc[u];
+        __syncthreads();
+        if (threadIdx.x < np) {
+#pragma unroll
+          for (int u = 0; u < RC; u++) {
+            if (r0 + u >= R) break;
+            double2 t = part[0][u][threadIdx.x];
+            for (int w = 1; w < 4; w++) {
+              t.x += part[w][u][threadIdx.x].x;
+              t.y += part[w][u][threadIdx.x].y;
+            }
+            double2* o = pfar + (int64_t)(f + p0 + threadIdx.x) * R + r0 + u;
+            if (accum) {
+              t.x += o->x;
+              t.y += o->y;
+            }
+            *o = t;
+          }
         }
-        const double2 v = make_double2((double)sum.x, (double)sum.y);
-        acc.x += v.x;
-        acc.y += v.y;
-      }
-      __syncthreads();
-      part[warp][lane] = acc;
-      __syncthreads();
-      if (threadIdx.x < np) {
-        double2 t = part[0][threadIdx.x];
-        for (int w = 1; w < 4; w++) {
-          t.x += part[w][threadIdx.x].x;
-          t.y += part[w][threadIdx.x].y;
-        }
-        pfar[f + p0 + threadIdx.x] = t;
       }
     }
   }
@@ -1399,6 +1579,202 @@ __device__ __forceinline__ float2 green32(double dx, double dy, double dz, doubl
   const float K0 = odd ? -0.0795774715459476679f * y : 0.0795774715459476679f * y;
   const float K = skip ? 0.f : K0;
   return make_float2(pc * K, x * ps * K);
+}
+
+// Near field for a block of right-hand sides (the target-side form of
+// k_p2p_tiled): per work item, the chunk's targets in lanes (groups of
+// tp >= nt lanes), sources streamed through shared memory with RB charges
+// each; one evaluation of G(x, y) (green64 / green32) is multiplied into the
+// RB right-hand sides r0 .. r0 + RB - 1 of the R in q (q[j R + r]).  Mixed:
+// FP32 products in compensated FP32 sums per tile, added into FP64 per tile.
+// Sums go to pnear[(t) R + r] (item_chunk == nullptr: items are chunks) or
+// to tpart[(item 32 + t) R + r] for k_p2p_items_rhs.
+template <bool MIXED, int RB>
+struct P2PRhsCfg {
+  static constexpr int TS = 256;  // sources per tile
+  typedef typename std::conditional<MIXED, float2, double2>::type Q;
+  static constexpr size_t smem() { return sizeof(double2) * 2 * TS + sizeof(Q) * TS * RB + sizeof(double2) * 4 * 32 * RB; }
+};
+
+template <bool MIXED, int RB>
+__global__ void __launch_bounds__(128) k_p2p_rhs(DevPlan P, int64_t nitem, const int32_t* __restrict__ order,
+                                                 const int32_t* __restrict__ item_chunk,
+                                                 const int32_t* __restrict__ tfirst, const int32_t* __restrict__ tn,
+                                                 const int64_t* __restrict__ ptr, const int32_t* __restrict__ sfirst,
+                                                 const int32_t* __restrict__ sn, const void* __restrict__ qv, int R,
+                                                 int r0, double2* __restrict__ pnear, double2* __restrict__ tpart,
+                                                 unsigned long long* __restrict__ queue) {
+  typedef P2PRhsCfg<MIXED, RB> G;
+  constexpr int TS = G::TS;
+  typedef typename G::Q Q;
+  const Q* q = static_cast<const Q*>(qv);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* sa = reinterpret_cast<double2*>(smem_raw);
+  double2* sb = sa + TS;
+  Q* sq = reinterpret_cast<Q*>(sb + TS);
+  double2* red = reinterpret_cast<double2*>(sq + TS * RB);  // [4][32][RB]
+  __shared__ int64_t cur;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) cur = (int64_t)atomicAdd(queue, 1ULL);
+    __syncthreads();
+    const int64_t k = cur;
+    if (k >= nitem) break;
+    const int64_t it = order[k];
+    const int64_t ch = item_chunk ? item_chunk[it] : it;
+    const int f = tfirst[ch], nt = tn[ch];
+    int tp = 1;
+    while (tp < nt) tp <<= 1;
+    const int groups = 32 / tp, GS = 4 * groups;
+    const int mt = lane & (tp - 1), gid = warp * groups + lane / tp;
+    const int ti = f + min(mt, nt - 1);
+    const double x0 = P.T_pos[3 * (int64_t)ti], x1 = P.T_pos[3 * (int64_t)ti + 1], x2 = P.T_pos[3 * (int64_t)ti + 2];
+    double2 acc[RB];
+    float2 fs[RB], fc[RB];  // mixed: compensated FP32 sums of the current tile
+#pragma unroll
+    for (int b = 0; b < RB; b++) {
+      acc[b] = make_double2(0., 0.);
+      fs[b] = make_float2(0.f, 0.f);
+      fc[b] = make_float2(0.f, 0.f);
+    }
+    const int64_t rb = ptr[it], re = ptr[it + 1];
+    int64_t r = rb;
+    int off = 0;
+    while (r < re) {
+      int fill = 0;
+      __syncthreads();
+      while (r < re && fill < TS) {
+        const int s0 = sfirst[r], ns = sn[r];
+        const int take = min(ns - off, TS - fill);
+        for (int t = threadIdx.x; t < take; t += blockDim.x) {
+          const int64_t sj = (int64_t)s0 + off + t;
+          const double* y = P.S_pos + 3 * sj;
+          sa[fill + t] = make_double2(y[0], y[1]);
+          sb[fill + t] = make_double2(y[2], 0.);
+        }
+        for (int t = threadIdx.x; t < take * RB; t += blockDim.x) {
+          const int64_t sj = (int64_t)s0 + off + t / RB;
+          sq[fill * RB + t] = q[sj * R + r0 + t % RB];
+        }
+        fill += take;
+        off += take;
+        if (off == ns) {
+          r++;
+          off = 0;
+        }
+      }
+      __syncthreads();
+      for (int j = gid; j < fill; j += GS) {
+        const double2 a = sa[j], bz = sb[j];
+        const Q* qj = sq + j * RB;
+        if constexpr (MIXED) {
+          const float2 g = green32(x0 - a.x, x1 - a.y, x2 - bz.x, P.kappa);
+#pragma unroll
+          for (int b = 0; b < RB; b++) {
+            const float2 qq = qj[b];
+            kahan_add(fs[b].x, fc[b].x, fmaf(g.x, qq.x, -g.y * qq.y));
+            kahan_add(fs[b].y, fc[b].y, fmaf(g.x, qq.y, g.y * qq.x));
+          }
+        } else {
+          const double2 g = green64(x0 - a.x, x1 - a.y, x2 - bz.x, P.kappa);
+#pragma unroll
+          for (int b = 0; b < RB; b++) {
+            const double2 qq = qj[b];
+            acc[b].x = fma(g.x, qq.x, fma(-g.y, qq.y, acc[b].x));
+            acc[b].y = fma(g.x, qq.y, fma(g.y, qq.x, acc[b].y));
+          }
+        }
+      }
+      if constexpr (MIXED) {
+#pragma unroll
+        for (int b = 0; b < RB; b++) {
+          acc[b].x += (double)fs[b].x - (double)fc[b].x;
+          acc[b].y += (double)fs[b].y - (double)fc[b].y;
+          fs[b] = make_float2(0.f, 0.f);
+          fc[b] = make_float2(0.f, 0.f);
+        }
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < RB; b++) {
+      for (int o = tp; o < 32; o <<= 1) {
+        acc[b].x += __shfl_xor_sync(0xffffffffu, acc[b].x, o);
+        acc[b].y += __shfl_xor_sync(0xffffffffu, acc[b].y, o);
+      }
+      if (lane < tp) red[(warp * 32 + lane) * RB + b] = acc[b];
+    }
+    __syncthreads();
+    for (int o = threadIdx.x; o < nt * RB; o += blockDim.x) {
+      const int t = o / RB, b = o % RB;
+      double2 a = red[t * RB + b];
+      for (int w = 1; w < 4; w++) {
+        a.x += red[(w * 32 + t) * RB + b].x;
+        a.y += red[(w * 32 + t) * RB + b].y;
+      }
+      if (tpart)
+        tpart[(it * 32 + t) * R + r0 + b] = a;
+      else
+        pnear[(int64_t)(f + t) * R + r0 + b] = a;
+    }
+  }
+}
+
+// Item partial sums of the near field into p for R right-hand sides, per
+// chunk in item order (k_p2p_items with R sums per target).
+__global__ void k_p2p_items_rhs(int64_t nchunk, const int32_t* __restrict__ tfirst, const int32_t* __restrict__ tn,
+                                const int64_t* __restrict__ chunk_items, const double2* __restrict__ tpart, int R,
+                                double2* __restrict__ pnear) {
+  const int64_t per = 32 * (int64_t)R;
+  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nchunk * per;
+       w += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t ch = w / per;
+    const int t = (int)((w % per) / R), rr = (int)(w % R);
+    if (t >= tn[ch]) continue;
+    double ar = 0., ai = 0.;
+    for (int64_t it = chunk_items[ch]; it < chunk_items[ch + 1]; it++) {
+      const double2 v = tpart[(it * 32 + t) * R + rr];
+      ar += v.x;
+      ai += v.y;
+    }
+    double2* o = pnear + (int64_t)(tfirst[ch] + t) * R + rr;
+    double2 v = *o;
+    v.x += ar;
+    v.y += ai;
+    *o = v;
+  }
+}
+
+// Tree-order R-wide charges from R stacked user-order vectors:
+// q[i R + r] = qin[r stride + perm[i]].
+// Vectors r >= nvec of a partly filled block get zero charges.
+template <typename T>
+__global__ void k_gather_rhs(const double2* __restrict__ qin, const int32_t* __restrict__ perm,
+                             typename cpx_t<T>::type* __restrict__ q, int64_t n, int64_t stride, int R, int nvec) {
+  const int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (w >= n * R) return;
+  const int64_t i = w / R;
+  const int r = (int)(w % R);
+  const double2 v = r < nvec ? qin[r * stride + perm[i]] : make_double2(0., 0.);
+  typename cpx_t<T>::type o;
+  o.x = (T)v.x;
+  o.y = (T)v.y;
+  q[w] = o;
+}
+
+// out[r stride + perm[i]] = pnear[i R + r] + pfar[i R + r].
+__global__ void k_scatter_rhs(const double2* __restrict__ pnear, const double2* __restrict__ pfar,
+                              const int32_t* __restrict__ perm, double2* __restrict__ out, int64_t n, int64_t stride,
+                              int R, int nvec) {
+  const int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (w >= n * R) return;
+  const int64_t i = w / R;
+  const int r = (int)(w % R);
+  if (r >= nvec) return;
+  double2 a = pnear[w], b = pfar[w];
+  a.x += b.x;
+  a.y += b.y;
+  out[r * stride + perm[i]] = a;
 }
 
 // tp steps of a symmetric block: lane ls owns one source (y, qj) and meets
@@ -1769,8 +2145,6 @@ struct Launch {
     if (e0 != cudaSuccess) return e0;
     cudaError_t e = cudaFuncSetAttribute(k_m2f<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_m2f());
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_p2m<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P2MCfg<T, L>::smem());
-    if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_m2l<T, L, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_m2l());
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_m2l<T, L, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_m2l());
@@ -1779,23 +2153,69 @@ struct Launch {
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_m2l_pair<T, L, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_m2l());
     if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_p2m<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)P2MCfg<T, L>::smem(kMaxRhsBlock));
+    if (e != cudaSuccess) return e;
+    if ((e = rhs_attr<1, 128>()) != cudaSuccess || (e = rhs_attr<2, 128>()) != cudaSuccess ||
+        (e = rhs_attr<4, 256>()) != cudaSuccess || (e = rhs_attr<8, 256>()) != cudaSuccess)
+      return e;
     return cudaSuccess;
   }
-  static void p2m(const DevPlan& dp, const int32_t* leaves, int n, const void* q, const void* sig2, void* M,
-                  cudaStream_t s) {
+  // largest block of right-hand sides per M2L CTA: K x RB <= 24 complex
+  // accumulators per thread at 256 threads
+  static constexpr int kMaxRB = (PP + 255) / 256 <= 3 ? 8 : ((PP + 255) / 256 <= 6 ? 4 : ((PP + 255) / 256 <= 12 ? 2 : 1));
+  template <int RB, int NT>
+  static cudaError_t rhs_attr() {
+    if (RB > kMaxRB) return cudaSuccess;
+    return cudaFuncSetAttribute(k_m2l_rhs<T, L, NT, (RB <= kMaxRB ? RB : 1)>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_m2l());
+  }
+  template <int RB, int NT>
+  static void m2l_rhs_go(const DevPlan& dp, int64_t t0, int64_t t1, int64_t f0, int64_t f1, int R, const void* F,
+                         const void* ptab, void* Lx, unsigned long long* queue, int nsm, cudaStream_t s) {
+    constexpr int RBE = RB <= kMaxRB ? RB : 1;
+    const int64_t nwork = (t1 - t0) * (R / RBE);
+    const int grid = (int)std::min<int64_t>(nwork, (int64_t)nsm * m2l_rhs_ctas<T, NT, RBE>());
+    k_m2l_rhs<T, L, NT, RBE><<<grid, NT, smem_m2l(), s>>>(dp, t0, t1, f0, f1, R, (const C*)F, (const C*)ptab,
+                                                          (C*)Lx, queue);
+  }
+  // M2L for R right-hand sides in blocks of rb (1, 2, 4 or 8; a divisor of
+  // R, capped by the order's kMaxRB)
+  static void m2l_rhs(const DevPlan& dp, int64_t t0, int64_t t1, int64_t f0, int64_t f1, int R, int rb,
+                      const void* F, const void* ptab, void* Lx, unsigned long long* queue, int nsm,
+                      cudaStream_t s) {
+    if (t1 <= t0) return;
+    cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s);
+    if (rb > kMaxRB) rb = kMaxRB;
+    while (rb > 1 && R % rb) rb >>= 1;
+    if (rb >= 8)
+      m2l_rhs_go<8, 256>(dp, t0, t1, f0, f1, R, F, ptab, Lx, queue, nsm, s);
+    else if (rb >= 4)
+      m2l_rhs_go<4, 256>(dp, t0, t1, f0, f1, R, F, ptab, Lx, queue, nsm, s);
+    else if (rb >= 2)
+      m2l_rhs_go<2, 128>(dp, t0, t1, f0, f1, R, F, ptab, Lx, queue, nsm, s);
+    else
+      m2l_rhs_go<1, 128>(dp, t0, t1, f0, f1, R, F, ptab, Lx, queue, nsm, s);
+  }
+  static void p2m(const DevPlan& dp, const int32_t* leaves, int n, const void* q, const void* sig2, void* M, int R,
+                  int d0, int d1, cudaStream_t s) {
     if (n)
-      k_p2m<T, L><<<grid_for(n, 1), 128, P2MCfg<T, L>::smem(), s>>>(dp, leaves, n, (const C*)q, (const C*)sig2,
-                                                                    (C*)M);
+      k_p2m<T, L><<<grid_for(n, 1), 128, P2MCfg<T, L>::smem(R), s>>>(dp, leaves, n, (const C*)q, (const C*)sig2,
+                                                                     (C*)M, R, d0, d1);
   }
-  static void m2m(const DevPlan& dp, int64_t s0, int64_t s1, const void* sig, const void* sig2, void* M,
-                  cudaStream_t s) {
+  static void m2m(const DevPlan& dp, int64_t s0, int64_t s1, const void* sig, const void* sig2, void* Mp,
+                  const void* Mc, int R, cudaStream_t s) {
     constexpr int NW = kXferWarps;
-    if (s1 > s0) k_m2m<T, L><<<grid_for(s1 - s0, NW), 32 * NW, 0, s>>>(dp, s0, s1, (const C*)sig, (const C*)sig2, (C*)M);
+    if (s1 > s0)
+      k_m2m<T, L><<<grid_for((s1 - s0) * R, NW), 32 * NW, 0, s>>>(dp, s0, s1, (const C*)sig, (const C*)sig2, (C*)Mp,
+                                                                  (const C*)Mc, R);
   }
-  static void l2l(const DevPlan& dp, int64_t s0, int64_t s1, const void* sig, const void* sig2, void* Lx,
-                  cudaStream_t s) {
+  static void l2l(const DevPlan& dp, int64_t s0, int64_t s1, const void* sig, const void* sig2, void* Lc,
+                  const void* Lp, int R, int64_t p0, int64_t p1, cudaStream_t s) {
     constexpr int NW = kXferWarps;
-    if (s1 > s0) k_l2l<T, L><<<grid_for(s1 - s0, NW), 32 * NW, 0, s>>>(dp, s0, s1, (const C*)sig, (const C*)sig2, (C*)Lx);
+    if (s1 > s0)
+      k_l2l<T, L><<<grid_for((s1 - s0) * R, NW), 32 * NW, 0, s>>>(dp, s0, s1, (const C*)sig, (const C*)sig2, (C*)Lc,
+                                                                  (const C*)Lp, R, p0, p1);
   }
   static void m2f(int64_t n, const void* M, void* F, cudaStream_t s) {
     constexpr int NW = M2FCfg<T, L>::NW;
@@ -1828,8 +2248,14 @@ struct Launch {
     if (n) k_permute_tables<T><<<grid_for(n, 1), 256, 0, s>>>(n, PP, key, perm, (const C*)tables, (C*)out);
   }
   static void l2p(const DevPlan& dp, const int32_t* leaves, int n, const void* sig2, const void* Lx, double2* pfar,
-                  cudaStream_t s) {
-    if (n) k_l2p<T, L><<<grid_for(n, 1), 128, 0, s>>>(dp, leaves, n, (const C*)sig2, (const C*)Lx, pfar);
+                  int R, int d0, int d1, bool accum, cudaStream_t s) {
+    if (!n) return;
+    if (R == 1)
+      k_l2p<T, L, 1><<<grid_for(n, 1), 128, 0, s>>>(dp, leaves, n, (const C*)sig2, (const C*)Lx, pfar, R, d0, d1,
+                                                    accum);
+    else
+      k_l2p<T, L, 4><<<grid_for(n, 1), 128, 0, s>>>(dp, leaves, n, (const C*)sig2, (const C*)Lx, pfar, R, d0, d1,
+                                                    accum);
   }
 };
 
@@ -1839,7 +2265,8 @@ const OpTable* op_table_for(int L);
 #define DFB_OPS(T, L)                                                                                     \
   {                                                                                                       \
     Launch<T, L>::setup, Launch<T, L>::p2m, Launch<T, L>::m2m, Launch<T, L>::l2l, Launch<T, L>::m2f,       \
-        Launch<T, L>::m2l, Launch<T, L>::l2p, Launch<T, L>::permute                                       \
+        Launch<T, L>::m2l, Launch<T, L>::m2l_rhs, Launch<T, L>::l2p, Launch<T, L>::permute,                 \
+        Launch<T, L>::kMaxRB                                                                              \
   }
 
 template <>
@@ -1930,6 +2357,74 @@ void launch_p2p_reduce(bool fp64, int64_t nleaf, const int32_t* first, const int
     k_p2p_reduce<false><<<grid, 256, 0, s>>>(nleaf, first, n, rptr, roff, scratch, pnear);
   else
     k_p2p_reduce<true><<<grid, 256, 0, s>>>(nleaf, first, n, rptr, roff, scratch, pnear);
+}
+
+cudaError_t setup_rhs_kernels() {
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(k_p2p_rhs<true, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)P2PRhsCfg<true, 8>::smem())) != cudaSuccess ||
+      (e = cudaFuncSetAttribute(k_p2p_rhs<false, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)P2PRhsCfg<false, 8>::smem())) != cudaSuccess ||
+      (e = cudaFuncSetAttribute(k_p2p_rhs<true, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)P2PRhsCfg<true, 4>::smem())) != cudaSuccess ||
+      (e = cudaFuncSetAttribute(k_p2p_rhs<false, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)P2PRhsCfg<false, 4>::smem())) != cudaSuccess)
+    return e;
+  return cudaSuccess;
+}
+
+template <bool MIXED, int RB>
+static void p2p_rhs_go(const DevPlan& dp, int64_t nitem, const int32_t* order, const int32_t* item_chunk,
+                       const int32_t* tfirst, const int32_t* tn, const int64_t* ptr, const int32_t* sfirst,
+                       const int32_t* sn, const void* q, int R, int r0, double2* pnear, double2* tpart,
+                       unsigned long long* queue, int grid, cudaStream_t s) {
+  k_p2p_rhs<MIXED, RB><<<grid, 128, P2PRhsCfg<MIXED, RB>::smem(), s>>>(dp, nitem, order, item_chunk, tfirst, tn, ptr,
+                                                                       sfirst, sn, q, R, r0, pnear, tpart, queue);
+}
+
+void launch_p2p_rhs(bool fp64, const DevPlan& dp, int64_t nitem, const int32_t* order, const int32_t* item_chunk,
+                    const int32_t* tfirst, const int32_t* tn, const int64_t* ptr, const int32_t* sfirst,
+                    const int32_t* sn, const void* q, int R, double2* pnear, double2* tpart,
+                    unsigned long long* queue, int nsm, int blocks_per_sm, cudaStream_t s) {
+  if (!nitem) return;
+  const int grid = (int)std::min<int64_t>(nitem, (int64_t)nsm * std::max(1, std::min(blocks_per_sm, 64)));
+  for (int r0 = 0; r0 < R;) {
+    const int left = R - r0;
+    const int rb = left >= 8 ? 8 : (left >= 4 ? 4 : 1);
+    cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s);
+    if (rb == 8) {
+      if (fp64) p2p_rhs_go<false, 8>(dp, nitem, order, item_chunk, tfirst, tn, ptr, sfirst, sn, q, R, r0, pnear, tpart, queue, grid, s);
+      else p2p_rhs_go<true, 8>(dp, nitem, order, item_chunk, tfirst, tn, ptr, sfirst, sn, q, R, r0, pnear, tpart, queue, grid, s);
+    } else if (rb == 4) {
+      if (fp64) p2p_rhs_go<false, 4>(dp, nitem, order, item_chunk, tfirst, tn, ptr, sfirst, sn, q, R, r0, pnear, tpart, queue, grid, s);
+      else p2p_rhs_go<true, 4>(dp, nitem, order, item_chunk, tfirst, tn, ptr, sfirst, sn, q, R, r0, pnear, tpart, queue, grid, s);
+    } else {
+      if (fp64) p2p_rhs_go<false, 1>(dp, nitem, order, item_chunk, tfirst, tn, ptr, sfirst, sn, q, R, r0, pnear, tpart, queue, grid, s);
+      else p2p_rhs_go<true, 1>(dp, nitem, order, item_chunk, tfirst, tn, ptr, sfirst, sn, q, R, r0, pnear, tpart, queue, grid, s);
+    }
+    r0 += rb;
+  }
+}
+
+void launch_p2p_items_rhs(int64_t nchunk, const int32_t* tfirst, const int32_t* tn, const int64_t* chunk_items,
+                          const double2* tpart, int R, double2* pnear, int nsm, cudaStream_t s) {
+  if (nchunk <= 0) return;
+  const int grid = (int)std::min<int64_t>((nchunk * 32 * R + 255) / 256, (int64_t)nsm * 16);
+  k_p2p_items_rhs<<<grid, 256, 0, s>>>(nchunk, tfirst, tn, chunk_items, tpart, R, pnear);
+}
+
+void launch_gather_rhs(bool fp64, const double2* qin, const int32_t* perm, void* q, int64_t n, int64_t stride, int R,
+                       int nvec, cudaStream_t s) {
+  const int g = (int)((n * R + 255) / 256);
+  if (fp64)
+    k_gather_rhs<double><<<g, 256, 0, s>>>(qin, perm, (double2*)q, n, stride, R, nvec);
+  else
+    k_gather_rhs<float><<<g, 256, 0, s>>>(qin, perm, (float2*)q, n, stride, R, nvec);
+}
+
+void launch_scatter_rhs(const double2* pnear, const double2* pfar, const int32_t* perm, double2* out, int64_t n,
+                        int64_t stride, int R, int nvec, cudaStream_t s) {
+  k_scatter_rhs<<<(int)((n * R + 255) / 256), 256, 0, s>>>(pnear, pfar, perm, out, n, stride, R, nvec);
 }
 
 void launch_direct(int64_t ns, const double* spos, const int32_t* sperm, const double2* qin, int64_t nt,

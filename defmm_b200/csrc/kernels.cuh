@@ -13,6 +13,10 @@
 
 namespace dfb {
 
+// Most right-hand sides carried through one pass of the far and near field
+// (expansions hold R = 1 .. kMaxRhsBlock vectors per slot).
+constexpr int kMaxRhsBlock = 32;
+
 template <typename T> struct cpx_t;
 template <> struct cpx_t<double> { typedef double2 type; };
 template <> struct cpx_t<float> { typedef float2 type; };

@@ -89,10 +89,26 @@ int defmm_gemv(defmm_handle* h, const double* in, double* out);
 /* Device-resident form: d_in / d_out are device pointers to nrhs stacked
  * complex vectors (rhs-major, each in user order).  Runs on `stream`
  * (a cudaStream_t; NULL = the handle's own stream) without synchronising.
- * With nrhs > 1 each right-hand side is copied into and out of the handle's
- * own device vectors, so all of them replay one captured graph. */
+ * One right-hand side runs on the resident layout (every expansion on the
+ * device, the matvec replayed from a captured graph) when it fits, else on
+ * the grouped layout below.  nrhs > 1 runs in passes of up to
+ * defmm_set_blocking's rhs_block right-hand sides over the grouped layout:
+ * the HF levels' expansions split into direction groups (one group's M and
+ * L on the device at a time), and every pass evaluates each near-field
+ * kernel value, transfer-spectrum entry and plane-wave phase once for all
+ * its right-hand sides. */
 int defmm_gemv_device(defmm_handle* h, const void* d_in, void* d_out,
                       int64_t nrhs, void* stream);
+
+/* No counterpart in the reference.  rhs_block: right-hand sides per pass of
+ * calls with nrhs > 1 (1 .. 32, default 16); groups: 0 = as many direction
+ * groups as the device memory needs, >= 1 = about that many, and the grouped
+ * layout also for single right-hand sides (for tests and memory limits). */
+int defmm_set_blocking(defmm_handle* h, int rhs_block, int groups);
+/* No counterpart in the reference.  Right-hand sides per M2L CTA of the
+ * grouped layout (1, 2, 4, 8; capped by the order's register budget): each
+ * transfer-spectrum entry is read once for them. */
+int defmm_set_rhs_per_cta(defmm_handle* h, int rb);
 
 /* No counterpart in the reference.  Independent operators (handles of
  * problems of any sizes, orders and wavenumbers) applied together: each
@@ -114,7 +130,8 @@ defmm_batch* defmm_batch_create(int64_t n, defmm_handle* const* hs,
 int defmm_batch_launch(defmm_batch* b, void* stream);
 void defmm_batch_destroy(defmm_batch* b);
 
-/* Many right-hand sides at once (host vectors, rhs-major). */
+/* Many right-hand sides at once (host vectors, rhs-major), in passes as in
+ * defmm_gemv_device. */
 int defmm_gemv_batched(defmm_handle* h, int64_t nrhs, const double* in,
                        double* out);
 
@@ -174,6 +191,14 @@ int defmm_direct_noalloc(defmm_handle* h, const double* d_targets, int64_t nt,
 #define DEFMM_INFO_M2L_THREADS 23      /* M2L threads per target slot (current precision) */
 #define DEFMM_INFO_P2P_BLOCKS_PER_SM 24 /* near-field CTAs per SM (current precision) */
 #define DEFMM_INFO_M2L_PAIRING 25       /* 1: two target slots per M2L CTA (current precision) */
+#define DEFMM_INFO_LAYOUT 26            /* 0 none yet, 1 resident, 2 grouped */
+#define DEFMM_INFO_RHS_BLOCK 27         /* right-hand sides per pass of the grouped layout */
+#define DEFMM_INFO_GROUPS 28            /* direction groups of the grouped layout */
+#define DEFMM_INFO_M2M_ENTRIES 29       /* (parent slot, child slot) transfers of M2M */
+#define DEFMM_INFO_L2L_ENTRIES 30       /* (child slot, parent slot) transfers of L2L */
+#define DEFMM_INFO_P2M_POINT_SLOTS 31   /* sum over source leaves of particles x slots */
+#define DEFMM_INFO_L2P_POINT_SLOTS 32   /* sum over target leaves of particles x slots */
+#define DEFMM_INFO_M2F_SLOTS 33         /* source slots transformed by M2F */
 int defmm_info(const defmm_handle* h, int what, int64_t* value);
 
 /* Per-phase device times (ms) of the last gemv, in this order:
@@ -237,6 +262,16 @@ int defmm_dump_tree(const defmm_handle* h, int which, int32_t* cells_int,
  * in n[3].  Pointers may be NULL to query the counts. */
 int defmm_dump_lists(const defmm_handle* h, int32_t* far_hf, int32_t* far_lf,
                      int32_t* near_, int64_t n[3]);
+
+/* No counterpart in the reference (its M2L tables are per-cell pointers,
+ * M2L.hpp:41-83).  The far-field work as the matvec runs it: per target
+ * slot (CSR ptr, n[0] = target slots + 1 entries) the source slots and the
+ * transfer spectra as (table index << 6) | symmetry hash, n[1] entries each,
+ * sorted by source slot within a target slot.  Identical whether prcmpt's
+ * level walk ran on the GPU or on the host.  Pointers may be NULL to query
+ * the counts. */
+int defmm_dump_m2l(const defmm_handle* h, int64_t* ptr, int32_t* src,
+                   uint32_t* tab, int64_t n[2]);
 
 /* No counterpart in the reference.  Order-selection network (learned.py):
  * a perceptron DEFMM_MLP_IN -> DEFMM_MLP_HIDDEN -> DEFMM_MLP_HIDDEN ->

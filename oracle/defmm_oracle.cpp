@@ -862,7 +862,8 @@ void downward(Oracle& o, int ci, cplx* p) {
   }
 }
 
-int prcmpt(Oracle& o) {
+int prcmpt(Oracle& o, bool lists_only = false);
+int prcmpt(Oracle& o, bool lists_only) {
   init_circulant(o);
   int st = init_frequency(o);
   if (st) return st;
@@ -882,6 +883,10 @@ int prcmpt(Oracle& o) {
   }
   o.nsrc_exp = assign_slots(o, o.S, seff);
   o.ntrg_exp = assign_slots(o, o.T, teff);
+  if (lists_only) {  // trees, cones, effective directions and lists only
+    hrz_lists(o, 0, 0);
+    return 0;
+  }
   // LF spectra (precompute.hpp:38-76): every sorted fundamental index with
   // max >= 2 inside the level bound
   for (int l = 2; l < o.nlvl; l++) {
@@ -1011,8 +1016,18 @@ void gemv(Oracle& o, const cplx* q_user, cplx* p_user) {
 // =================================================================== C ABI ==
 extern "C" {
 
+void* oracle_create_opt(const double* src, int64_t ns, const double* trg, int64_t nt,
+                        int L, int ncrit, double kappa, int lvmax, int lists_only);
 void* oracle_create(const double* src, int64_t ns, const double* trg, int64_t nt,
                     int L, int ncrit, double kappa, int lvmax) {
+  return oracle_create_opt(src, ns, trg, nt, L, ncrit, kappa, lvmax, 0);
+}
+
+// lists_only != 0: prcmpt stops after the trees, cones, effective directions
+// and interaction lists (no leaf matrices, no LF spectra): enough to pin
+// those at sizes whose full precomputation does not fit in host memory.
+void* oracle_create_opt(const double* src, int64_t ns, const double* trg, int64_t nt,
+                        int L, int ncrit, double kappa, int lvmax, int lists_only) {
   Oracle* o = new Oracle;
   o->L = L;
   o->P = 2 * L - 1;
@@ -1045,8 +1060,51 @@ void* oracle_create(const double* src, int64_t ns, const double* trg, int64_t nt
       return o;
     }
   }
-  o->status = prcmpt(*o);
+  o->status = prcmpt(*o, lists_only != 0);
   return o;
+}
+
+// Order-independent digest of n records of w int32 fields: out = {n,
+// sum of h1(record), sum of h2(record)} mod 2^64, h1 / h2 two seeded
+// splitmix64 chains over the fields.  Equal multisets of records give equal
+// digests; a changed, missing or extra record changes both sums.
+static uint64_t mix64(uint64_t z) {
+  z += 0x9e3779b97f4a7c15ULL;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+  return z ^ (z >> 31);
+}
+void oracle_digest_records(const int32_t* rec, int64_t n, int w, uint64_t* out) {
+  std::atomic<uint64_t> a1(0), a2(0);
+  const long nb = (long)((n + 65535) / 65536);
+  parallel_for(nb, 1, [&](long b) {
+    uint64_t s1 = 0, s2 = 0;
+    const int64_t e = std::min<int64_t>(n, (int64_t)(b + 1) * 65536);
+    for (int64_t i = (int64_t)b * 65536; i < e; i++) {
+      uint64_t h1 = 0x243f6a8885a308d3ULL, h2 = 0x13198a2e03707344ULL;
+      for (int k = 0; k < w; k++) {
+        const uint64_t v = (uint64_t)(uint32_t)rec[i * w + k];
+        h1 = mix64(h1 ^ v);
+        h2 = mix64(h2 + v * 0xa4093822299f31d0ULL);
+      }
+      s1 += h1;
+      s2 += h2;
+    }
+    a1 += s1;
+    a2 += s2;
+  });
+  out[0] = (uint64_t)n;
+  out[1] = a1.load();
+  out[2] = a2.load();
+}
+
+// The same digest of the oracle's own lists: which 0 near (2 fields),
+// 1 far HF (6 fields), 2 far LF (5 fields).
+void oracle_lists_digest(void* h, int which, uint64_t* out) {
+  Oracle* o = static_cast<Oracle*>(h);
+  const std::vector<int32_t>& v = which == 0 ? o->near : which == 1 ? o->far_hf : o->far_lf;
+  const int w = which == 0 ? 2 : which == 1 ? 6 : 5;
+  oracle_digest_records(v.data(), (int64_t)v.size() / w, w, out);
 }
 
 int oracle_status(void* h) { return static_cast<Oracle*>(h)->status; }

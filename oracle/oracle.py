@@ -47,6 +47,12 @@ def lib():
         L.oracle_direction.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, dp]
         L.oracle_direct.argtypes = [dp, ctypes.c_int64, dp, dp, ctypes.c_int64,
                                     ctypes.c_double, dp]
+        L.oracle_create_opt.restype = ctypes.c_void_p
+        L.oracle_create_opt.argtypes = [dp, ctypes.c_int64, dp, ctypes.c_int64, ctypes.c_int,
+                                        ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int]
+        u64p = ctypes.POINTER(ctypes.c_uint64)
+        L.oracle_digest_records.argtypes = [ip, ctypes.c_int64, ctypes.c_int, u64p]
+        L.oracle_lists_digest.argtypes = [ctypes.c_void_p, ctypes.c_int, u64p]
         _lib = L
     return _lib
 
@@ -62,13 +68,25 @@ def _ip(a):
 class OracleFMM:
     """CPU restatement of IBFMM_Mat<3>: build (prcmpt) at construction."""
 
-    def __init__(self, src, trg, L, ncrit, kappa, lvmax=-1):
+    def __init__(self, src, trg, L, ncrit, kappa, lvmax=-1, lists_only=False):
+        """lists_only: build the trees, cones, effective directions and
+        interaction lists only (no matvec possible)."""
         self.src = np.ascontiguousarray(src, dtype=np.float64)
         self.trg = np.ascontiguousarray(trg, dtype=np.float64)
         self.L, self.ncrit, self.kappa = L, ncrit, kappa
-        self._h = lib().oracle_create(_dp(self.src), self.src.shape[0], _dp(self.trg),
-                                      self.trg.shape[0], L, ncrit, kappa, lvmax)
+        self._h = lib().oracle_create_opt(_dp(self.src), self.src.shape[0], _dp(self.trg),
+                                          self.trg.shape[0], L, ncrit, kappa, lvmax, int(bool(lists_only)))
         self.status = lib().oracle_status(self._h)
+
+    def lists_digest(self):
+        """Order-independent digests {near, far_hf, far_lf} of the lists
+        (see records_digest)."""
+        out = {}
+        for w, name in enumerate(["near", "far_hf", "far_lf"]):
+            d = np.zeros(3, np.uint64)
+            lib().oracle_lists_digest(self._h, w, d.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)))
+            out[name] = [int(x) for x in d]
+        return out
 
     def __del__(self):
         if getattr(self, "_h", None):
@@ -119,6 +137,18 @@ class OracleFMM:
         out = np.zeros(3)
         lib().oracle_direction(self._h, stage, d, _dp(out))
         return out
+
+
+def records_digest(rec):
+    """[count, sum h1, sum h2] (mod 2^64) of the rows of an int32 record
+    array: equal for equal multisets of rows, whatever their order."""
+    rec = np.ascontiguousarray(rec, dtype=np.int32)
+    d = np.zeros(3, np.uint64)
+    n = rec.shape[0]
+    w = rec.shape[1] if rec.ndim == 2 else 1
+    lib().oracle_digest_records(_ip(rec.reshape(-1)) if n else None, n, w,
+                                d.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)))
+    return [int(x) for x in d]
 
 
 def direct(src, q, trg, kappa):

@@ -48,6 +48,14 @@ def test_argument_checks_without_device():
         A._check(api.lib().defmm_set_m2l_pairing(A._h, 2))
     A.set_m2l_pairing(True)
     A.set_m2l_pairing(False)
+    for rb, g in ((0, 0), (33, 0), (4, -1)):
+        with pytest.raises(api.DefmmError):
+            A.set_blocking(rb, g)
+    A.set_blocking(8, 3)
+    for rb in (0, 3, 16):
+        with pytest.raises(api.DefmmError):
+            A.set_rhs_per_cta(rb)
+    A.set_rhs_per_cta(4)
     with pytest.raises(api.DefmmError):
         A.autotune(reps=0)
     with pytest.raises(api.DefmmError):
