@@ -135,27 +135,16 @@ REF_FFT = ("FFTW-API shim of the oracle (DFT by definition, oracle/shim/fftw_shi
 NOMINAL = {"fp32_tflops": 148 * 128 * 2 * 1.965e9 / 1e12, "fp64_tflops": 148 * 64 * 2 * 1.965e9 / 1e12}
 
 
-def l2_copy_bandwidth(torch):
-    """Read+write GB/s of a torch copy between two 24 MB device buffers
-    (both resident in the 126 MB L2), best of 5 runs of 200 copies: the
-    denominator of L2-bound kernels (MEASURED_PEAKS.json has HBM only)."""
-    a = torch.empty(6 << 20, dtype=torch.float32, device="cuda")
-    b = torch.empty_like(a)
-    for _ in range(20):
-        b.copy_(a)
-    best = 0.0
-    for _ in range(5):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(200):
-            b.copy_(a)
-        e1.record()
-        torch.cuda.synchronize()
-        best = max(best, 2 * a.numel() * 4 * 200 / (e0.elapsed_time(e1) * 1e-3) / 1e9)
-    return best
+def l2_read_bandwidth():
+    """L2-to-SM read GB/s measured here by the library's probe kernel
+    (defmm_probe_l2_read: every SM streams an L2-resident buffer with 16-byte
+    loads cached in L2 only), best of 32 and 64 MB buffers: the denominator
+    of the L2-bound M2L kernel (MEASURED_PEAKS.json has HBM only)."""
+    from defmm_b200 import api
+    return max(api.probe_l2_read(mb << 20, 200) for mb in (32, 64))
 
 
-def phase_rooflines(info, L, phases, head, hn, peaks, l2_gbs, tune):
+def phase_rooflines(info, L, phases, head, hn, peaks, l2_gbs, tune, rb_block=4):
     """Per-phase achieved rate against the resource that bounds it, for the
     headline form (per right-hand side of a block: the phase times of one
     profiled pass divided by its right-hand sides).
@@ -178,7 +167,7 @@ def phase_rooflines(info, L, phases, head, hn, peaks, l2_gbs, tune):
     ph = phases["mixed_block" if head == "mixed_block" else head]
     per = hn if head == "mixed_block" else 1
     n_far = info["far_hf"] + info["far_lf"]
-    rb = 8 if head == "mixed_block" else 1
+    rb = rb_block if head == "mixed_block" else 1
     flop_peak = NOMINAL["fp64_tflops"] if fp64 else NOMINAL["fp32_tflops"]
     out = {}
 
@@ -188,7 +177,7 @@ def phase_rooflines(info, L, phases, head, hn, peaks, l2_gbs, tune):
         out[name] = {"bound": bound, "achieved": ach, "peak": peak, "unit": unit,
                      "frac": (ach / peak) if ach else None, "ms_per_rhs": t, "work_per_rhs": work, "note": note}
     m2l_l2 = (e * P3 * (1 + 1.0 / rb) if rb > 1 else 2 * e * P3) * n_far
-    add("m2l", m2l_l2, "GB/s", l2_gbs, "l2", ph["m2l"], "L2-to-SM spectra bytes; peak: L2 copy bandwidth measured here")
+    add("m2l", m2l_l2, "GB/s", l2_gbs, "l2", ph["m2l"], "L2-to-SM spectra bytes; peak: L2 read bandwidth measured here")
     add("p2p", 20.0 * info["i_near"], "TFLOP/s", flop_peak, "fp64" if fp64 else "fp32", ph["p2p"],
         "20 flops per interaction; nominal CUDA-core peak")
     add("m2f", e * (L3 + P3) * info["m2f_slots"], "GB/s", hbm, "hbm", ph["m2f"], "M read, F written once")
@@ -207,12 +196,13 @@ def phase_rooflines(info, L, phases, head, hn, peaks, l2_gbs, tune):
     t = ph["m2l"] / per
     lc = tune.get("mixed" if head != "fp64" else "fp64", {})
     if head == "mixed_block":
-        kname = "k_m2l_rhs<float, %d, 256, 8>" % L
+        kname = "k_m2l_rhs<float, %d, %d, %d>" % (L, 256 if rb >= 4 else 128, rb)
     else:
         kname = "%s<%s, %d, %d>" % ("k_m2l_pair" if lc.get("m2l_pairing") else "k_m2l",
                                     "double" if fp64 else "float", L, lc.get("m2l_threads", 128))
     head_rl = dict(out["m2l"])
-    head_rl.update({"kernel": kname + " (M2L + inverse DFT, all cone batches)", "peak_source": "measured here (L2 copy)",
+    head_rl.update({"kernel": kname + " (M2L + inverse DFT, all cone batches)",
+                    "peak_source": "measured here (L2 read probe, defmm_probe_l2_read)",
                     "traffic": None, "hbm": {"achieved": m2l_hbm / (t * 1e-3) / 1e9, "peak": hbm,
                                              "frac": m2l_hbm / (t * 1e-3) / 1e9 / hbm, "peak_source": src,
                                              "algorithmic_bytes_per_rhs": m2l_hbm}})
@@ -617,7 +607,7 @@ def main():
         blaunch[0] += A.info("launches")
     ms_b, ck_b = timed_steps(block, args.steps)
     blaunch = blaunch[0] // (args.steps + args.warmup)
-    layout = {k: A.info(k) for k in ("rhs_block", "groups", "device_bytes")}
+    layout = {k: A.info(k) for k in ("rhs_block", "groups", "device_bytes", "rhs_per_cta")}
     PB = dP.cpu().numpy()
     A.set_precision("fp64")
     errs_b = []
@@ -668,8 +658,8 @@ def main():
     A.set_profiling(False)
 
     peaks = measured_peaks()
-    l2_gbs = l2_copy_bandwidth(torch)
-    rl = phase_rooflines(info, w.order, phases, head, hn, peaks, l2_gbs, tune)
+    l2_gbs = l2_read_bandwidth()
+    rl = phase_rooflines(info, w.order, phases, head, hn, peaks, l2_gbs, tune, layout["rhs_per_cta"])
     roofline = rl["headline"]
 
     cpu, sample = None, None

@@ -37,7 +37,8 @@ _INFO = {
     "m2l_targets": 17, "leaf_slots_S": 18, "permuted_spectra": 19, "plan_walk_device": 20, "plan_ms": 21,
     "plan_walk_ms": 22, "m2l_threads": 23, "p2p_blocks_per_sm": 24, "m2l_pairing": 25,
     "layout": 26, "rhs_block": 27, "groups": 28, "m2m_entries": 29, "l2l_entries": 30,
-    "p2m_point_slots": 31, "l2p_point_slots": 32, "m2f_slots": 33,
+    "p2m_point_slots": 31, "l2p_point_slots": 32, "m2f_slots": 33, "tensor_cores": 34,
+    "tree_device": 35, "tree_ms": 36, "rhs_per_cta": 37,
 }
 PHASES = ["p2m", "m2m", "m2f", "m2l", "f2l", "l2l", "l2p", "p2p", "scatter", "total"]
 
@@ -85,7 +86,9 @@ def lib():
             "defmm_set_m2l_pairing": (ctypes.c_int, [vp, ctypes.c_int]),
             "defmm_set_blocking": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
             "defmm_dump_m2l": (ctypes.c_int, [vp, vp, vp, vp, ctypes.POINTER(i64)]),
+            "defmm_probe_l2_read": (ctypes.c_int, [i64, ctypes.c_int, dp]),
             "defmm_set_rhs_per_cta": (ctypes.c_int, [vp, ctypes.c_int]),
+            "defmm_set_tensor_cores": (ctypes.c_int, [vp, ctypes.c_int]),
             "defmm_batch_create": (vp, [i64, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.c_int]),
             "defmm_batch_launch": (ctypes.c_int, [vp, vp]),
             "defmm_batch_destroy": (None, [vp]),
@@ -112,6 +115,15 @@ def _dp(a):
 
 def _ip(a):
     return None if a is None else a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+
+
+def probe_l2_read(nbytes=64 << 20, reps=200) -> float:
+    """L2-to-SM read bandwidth of the current device, GB/s (defmm_probe_l2_read)."""
+    g = ctypes.c_double(0.0)
+    st = lib().defmm_probe_l2_read(int(nbytes), int(reps), ctypes.byref(g))
+    if st:
+        raise DefmmError(st, "L2 bandwidth probe failed")
+    return float(g.value)
 
 
 def device_count() -> int:
@@ -197,8 +209,13 @@ class IBFMM_Mat:
         about that many, also for single right-hand sides)."""
         self._check(lib().defmm_set_blocking(self._h, int(rhs_block), int(groups)))
 
+    def set_tensor_cores(self, on=True):
+        """Mixed precision: P2M on the tensor cores (tcgen05, split TF32)."""
+        self._check(lib().defmm_set_tensor_cores(self._h, int(bool(on))))
+
     def set_rhs_per_cta(self, rb=8):
-        """Right-hand sides per M2L CTA of the grouped layout (1, 2, 4, 8)."""
+        """Right-hand sides per M2L CTA of the grouped layout (1, 2, 4, 8;
+        negative: the same, work ordered block by block)."""
         self._check(lib().defmm_set_rhs_per_cta(self._h, int(rb)))
 
     def set_profiling(self, on=True):

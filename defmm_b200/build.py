@@ -16,12 +16,12 @@ LIB = os.path.join(HERE, "libdefmm_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU = ["fmm_kernels.cu", "engine.cu", "noalloc.cu", "plan_device.cu", "mlp.cu"]
+CU = ["fmm_kernels.cu", "tc_interp.cu", "engine.cu", "noalloc.cu", "plan_device.cu", "mlp.cu", "measure.cu"]
 # the device level walk reproduces the host plan's floating-point decisions:
 # no FMA contraction there
 CU_FLAGS = {"plan_device.cu": ["--fmad=false"]}
 CPP = ["plan.cpp"]
-HEADERS = ["plan.hpp", "kernels.cuh", "fmm_kernels.h", "engine_internal.h", "plan_device.hpp"]
+HEADERS = ["plan.hpp", "kernels.cuh", "device_math.cuh", "fmm_kernels.h", "engine_internal.h", "plan_device.hpp"]
 
 
 def _newer(target, deps):

@@ -1,7 +1,11 @@
 // Operator handle: host plan -> device arrays, matvec orchestration, C ABI.
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <climits>
+#include <map>
+#include <memory>
+#include <mutex>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -102,12 +106,15 @@ struct defmm_handle {
   int layout = 0;
   GroupedLayout gl;
   int rhs_block = 16;     // right-hand sides per pass of multi-RHS calls
-  int rhs_block_m2l = 8;  // right-hand sides per M2L CTA (capped by the order)
+  int rhs_block_m2l = 4;  // right-hand sides per M2L CTA (capped by the order)
+  bool use_tc = false;    // mixed precision: P2M on the tensor cores (tcgen05)
+  bool m2l_chunk_major = false;  // grouped M2L: target slots inner, right-hand-side blocks outer
   int groups_forced = 0;  // > 0: direction groups requested (also for one RHS)
   int groups_used = 0;    // groups of the last grouped pass
   // leaves at precomputed levels sorted by level (P2M: sources, L2P: targets)
   const int32_t *d_p2m_bylvl = nullptr, *d_l2p_bylvl = nullptr;
   std::vector<int64_t> p2m_lvl_off, l2p_lvl_off;  // nlvl + 1 offsets
+  int l2p_max_points = 0;  // largest target leaf at a precomputed level
   double phase_ms[PH_N] = {0};
   cudaEvent_t ev[2 * PH_N] = {};
   cudaEvent_t ev_ready = nullptr, ev_done = nullptr;  // cross-stream ordering
@@ -313,6 +320,8 @@ int upload_plan(defmm_handle* h) {
       std::vector<int64_t> pos(off.begin(), off.end() - 1);
       for (int32_t c : leaves) out[pos[lv[c]]++] = c;
     };
+    h->l2p_max_points = 0;
+    for (int32_t c : p.l2p_leaf) h->l2p_max_points = std::max(h->l2p_max_points, (int)p.T.nprt[c]);
     std::vector<int32_t> tmp;
     bylvl(p.S.lvl, p.p2m_leaf, tmp, h->p2m_lvl_off);
     UP(tmp, h->d_p2m_bylvl);
@@ -400,6 +409,7 @@ int prepare_tables(defmm_handle* h) {
   for (int k = 0; k < 2; k++) mats.insert(mats.end(), p.l2l[k].begin(), p.l2l[k].end());
   CK(h->ops->setup(mats.data()));
   CK(dfb::setup_rhs_kernels());
+  if (!fp64) CK(dfb::setup_tc_kernels());
   auto put = [&](DevBuf& b, const dfb::cplx* src, size_t n) -> int {
     int st = ensure(h, b, std::max<size_t>(1, n) * cs);
     if (st) return st;
@@ -679,7 +689,11 @@ int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) 
   if (h->events) cudaEventRecord(h->ev[2 * PH_P2P + 1], sn);
   // upward pass
   rec(h, 2 * PH_P2M);
-  ops->p2m(d, h->d_p2m_leaf, (int)p.p2m_leaf.size(), h->q.p, h->sig2.p, h->M.p, 1, INT_MIN, INT_MAX, sf);
+  if (!fp64 && h->use_tc)
+    dfb::launch_p2m_tc(p.L, d, h->d_p2m_leaf, (int)p.p2m_leaf.size(), h->q.p, h->sig2.p, h->M.p, 1, INT_MIN,
+                       INT_MAX, h->nsm, sf);
+  else
+    ops->p2m(d, h->d_p2m_leaf, (int)p.p2m_leaf.size(), h->q.p, h->sig2.p, h->M.p, 1, INT_MIN, INT_MAX, sf);
   rec(h, 2 * PH_P2M + 1);
   rec(h, 2 * PH_M2M);
   for (int l = nl - 2; l >= p.lv.max_stage; l--) {
@@ -734,8 +748,12 @@ int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) 
     }
   }
   rec(h, 2 * PH_L2P);
-  ops->l2p(d, h->d_l2p_leaf, (int)p.l2p_leaf.size(), h->sig2.p, h->Lx.p, (double2*)h->pfar.p, 1, INT_MIN, INT_MAX,
-           false, sf);
+  if (!fp64 && h->use_tc && h->l2p_max_points <= 128)
+    dfb::launch_l2p_tc(p.L, d, h->d_l2p_leaf, (int)p.l2p_leaf.size(), h->sig2.p, h->Lx.p, (double2*)h->pfar.p, 1,
+                       INT_MIN, INT_MAX, false, h->nsm, sf);
+  else
+    ops->l2p(d, h->d_l2p_leaf, (int)p.l2p_leaf.size(), h->sig2.p, h->Lx.p, (double2*)h->pfar.p, 1, INT_MIN, INT_MAX,
+             false, sf);
   rec(h, 2 * PH_L2P + 1);
   CK(cudaEventRecord(h->ev_done, sn));
   CK(cudaStreamWaitEvent(s, h->ev_done, 0));
@@ -836,6 +854,20 @@ int run_gemv_grouped(defmm_handle* h, const double2* qin, int64_t stride_in, dou
       h->phase_ms[PH_P2P] += a;
     }
   }
+  // P2M of the given leaves' slots with directions in [d0, d1) into Mbase
+  auto p2m = [&](const int32_t* leaves, int n, void* Mbase, int d0, int d1) {
+    if (!fp64 && h->use_tc)
+      dfb::launch_p2m_tc(p.L, d, leaves, n, g.q.p, h->sig2.p, Mbase, R, d0, d1, h->nsm, s);
+    else
+      ops->p2m(d, leaves, n, g.q.p, h->sig2.p, Mbase, R, d0, d1, s);
+  };
+  // L2P of the given leaves' slots with directions in [d0, d1) from Lbase
+  auto l2p = [&](const int32_t* leaves, int n, const void* Lbase, int d0, int d1) {
+    if (!fp64 && h->use_tc && h->l2p_max_points <= 128)
+      dfb::launch_l2p_tc(p.L, d, leaves, n, h->sig2.p, Lbase, (double2*)g.pfar.p, R, d0, d1, true, h->nsm, s);
+    else
+      ops->l2p(d, leaves, n, h->sig2.p, Lbase, (double2*)g.pfar.p, R, d0, d1, true, s);
+  };
   void* Mlf = slot_base(g.Mlf.p, g.lfS0, slot_b);
   void* Llf = slot_base(g.Llf.p, g.lfT0, slot_b);
   const int lf = g.lh < 0 ? 0 : g.lh + 1;  // first LF level
@@ -857,8 +889,8 @@ int run_gemv_grouped(defmm_handle* h, const double2* qin, int64_t stride_in, dou
             ops->m2l(d, ts0, ts1, fs0, fs1, g.F.p, h->ptab.p, Lbase, h->d_queue + 1, h->nsm, h->m2l_nt[pi],
                      h->m2l_pair[pi], s);
           else
-            ops->m2l_rhs(d, ts0, ts1, fs0, fs1, R, h->rhs_block_m2l, g.F.p, h->ptab.p, Lbase, h->d_queue + 1,
-                         h->nsm, s);
+            ops->m2l_rhs(d, ts0, ts1, fs0, fs1, R, h->rhs_block_m2l, h->m2l_chunk_major, g.F.p, h->ptab.p, Lbase,
+                         h->d_queue + 1, h->nsm, s);
         });
         nk += 2;
       }
@@ -872,7 +904,7 @@ int run_gemv_grouped(defmm_handle* h, const double2* qin, int64_t stride_in, dou
       for (int l = lf; l < nl; l++) {
         const int64_t b = h->p2m_lvl_off[l], e = h->p2m_lvl_off[l + 1];
         if (e > b) {
-          ops->p2m(d, h->d_p2m_bylvl + b, (int)(e - b), g.q.p, h->sig2.p, Mlf, R, INT_MIN, INT_MAX, s);
+          p2m(h->d_p2m_bylvl + b, (int)(e - b), Mlf, INT_MIN, INT_MAX);
           nk++;
         }
       }
@@ -909,8 +941,7 @@ int run_gemv_grouped(defmm_handle* h, const double2* qin, int64_t stride_in, dou
         const int l = g.hl[i];
         const int64_t b = h->p2m_lvl_off[l], e = h->p2m_lvl_off[l + 1];
         if (e > b && s1[i] > s0[i]) {
-          ops->p2m(d, h->d_p2m_bylvl + b, (int)(e - b), g.q.p, h->sig2.p, Mb[i], R, (int)(c0 * g.fl[i]),
-                   (int)(c1 * g.fl[i]), s);
+          p2m(h->d_p2m_bylvl + b, (int)(e - b), Mb[i], (int)(c0 * g.fl[i]), (int)(c1 * g.fl[i]));
           nk++;
         }
       }
@@ -947,8 +978,7 @@ int run_gemv_grouped(defmm_handle* h, const double2* qin, int64_t stride_in, dou
         const int l = g.hl[i];
         const int64_t b = h->l2p_lvl_off[l], e = h->l2p_lvl_off[l + 1];
         if (e > b && t1[i] > t0[i]) {
-          ops->l2p(d, h->d_l2p_bylvl + b, (int)(e - b), h->sig2.p, Lb[i], (double2*)g.pfar.p, R,
-                   (int)(c0 * g.fl[i]), (int)(c1 * g.fl[i]), true, s);
+          l2p(h->d_l2p_bylvl + b, (int)(e - b), Lb[i], (int)(c0 * g.fl[i]), (int)(c1 * g.fl[i]));
           nk++;
         }
       }
@@ -968,8 +998,7 @@ int run_gemv_grouped(defmm_handle* h, const double2* qin, int64_t stride_in, dou
       for (int l = lf; l < nl; l++) {
         const int64_t b = h->l2p_lvl_off[l], e = h->l2p_lvl_off[l + 1];
         if (e > b) {
-          ops->l2p(d, h->d_l2p_bylvl + b, (int)(e - b), h->sig2.p, Llf, (double2*)g.pfar.p, R, INT_MIN, INT_MAX,
-                   true, s);
+          l2p(h->d_l2p_bylvl + b, (int)(e - b), Llf, INT_MIN, INT_MAX);
           nk++;
         }
       }
@@ -1089,6 +1118,11 @@ int ensure_device(defmm_handle* h) {
   return 0;
 }
 
+// Launch choices of defmm_autotune per operator shape (order, precision,
+// levels, slots, far pairs, particle interactions, device) in this process.
+std::mutex g_tune_mu;
+std::map<std::array<int64_t, 9>, std::array<int, 3>> g_tune;
+
 uint64_t splitmix(uint64_t& s) {
   uint64_t z = (s += 0x9e3779b97f4a7c15ULL);
   z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
@@ -1203,6 +1237,26 @@ int defmm_autotune(defmm_handle* h, int reps, int32_t* choice) {
   if (!h->built) return h->fail(DEFMM_ERR_ARG, "autotune before prcmpt");
   int st = defmm_upload(h);
   if (st) return st;
+  // choices already timed on an operator of the same shape in this process
+  const Plan& pl = h->plan;
+  const std::array<int64_t, 9> key = {pl.L, h->precision, pl.lv.nlvl, pl.sS.n, pl.sT.n, pl.n_far_hf,
+                                      pl.n_far_lf, pl.i_near, h->device};
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) {
+      const int pi = h->precision == DEFMM_PRECISION_FP64 ? 0 : 1;
+      h->m2l_nt[pi] = it->second[0];
+      h->m2l_pair[pi] = it->second[1];
+      h->p2p_bps[pi] = it->second[2];
+      drop_graph(h);
+      if (choice) {
+        choice[0] = it->second[0];
+        choice[1] = it->second[2];
+      }
+      return 0;
+    }
+  }
   st = prepare_precision(h);
   if (st) return st;
   const int64_t nS = (int64_t)h->plan.S.perm.size(), nT = (int64_t)h->plan.T.perm.size();
@@ -1212,46 +1266,43 @@ int defmm_autotune(defmm_handle* h, int reps, int32_t* choice) {
   const bool ev = h->events;
   h->events = true;  // phase timers, phases serialised
   drop_graph(h);     // the captured graph holds the old launch choices
-  // fastest of `reps` profiled matvecs, for the phase `ph`
-  auto best_of = [&](int ph, double& t) -> int {
-    t = 1e300;
-    for (int r = 0; r < reps; r++) {
-      const int e = run_gemv(h, (const double2*)h->rin.p, (double2*)h->rout.p, h->st);
-      if (e) return e;
-      t = std::min(t, h->phase_ms[ph]);
-    }
-    return 0;
-  };
+  // phases are serialised and timed separately in profiled matvecs, so one
+  // matvec times one M2L candidate and one near-field candidate together:
+  // four matvecs (the M2L candidates) cover the three near-field candidates
   int m2l_best = 128, pair_best = 0, bps_best = 16;
-  double tb = 1e300, t = 0;
-  for (int pair : {0, 1}) {
-    for (int nt : {128, 256}) {
-      if (st) break;
-      h->m2l_nt[pi] = nt;
-      h->m2l_pair[pi] = pair;
-      if ((st = best_of(PH_M2L, t))) break;
-      if (t < tb) {
-        tb = t;
-        m2l_best = nt;
-        pair_best = pair;
-      }
+  double tb_m2l = 1e300, tb_p2p = 1e300;
+  const int m2l_cand[4][2] = {{0, 128}, {0, 256}, {1, 128}, {1, 256}};
+  const int bps_cand[3] = {8, 16, 32};
+  for (int i = 0; i < 4 && !st; i++) {
+    h->m2l_pair[pi] = m2l_cand[i][0];
+    h->m2l_nt[pi] = m2l_cand[i][1];
+    const int b = bps_cand[i < 3 ? i : 2];
+    h->p2p_bps[pi] = b;
+    double tm = 1e300, tp = 1e300;
+    for (int r = 0; r < reps && !st; r++) {
+      st = run_gemv(h, (const double2*)h->rin.p, (double2*)h->rout.p, h->st);
+      tm = std::min(tm, h->phase_ms[PH_M2L]);
+      tp = std::min(tp, h->phase_ms[PH_P2P]);
+    }
+    if (tm < tb_m2l) {
+      tb_m2l = tm;
+      pair_best = m2l_cand[i][0];
+      m2l_best = m2l_cand[i][1];
+    }
+    if (i < 3 && tp < tb_p2p) {
+      tb_p2p = tp;
+      bps_best = b;
     }
   }
   h->m2l_nt[pi] = m2l_best;
   h->m2l_pair[pi] = pair_best;
-  tb = 1e300;
-  for (int b : {8, 16, 32}) {
-    if (st) break;
-    h->p2p_bps[pi] = b;
-    if ((st = best_of(PH_P2P, t))) break;
-    if (t < tb) {
-      tb = t;
-      bps_best = b;
-    }
-  }
   h->p2p_bps[pi] = bps_best;
   h->events = ev;
   if (st) return st;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune[key] = {m2l_best, pair_best, bps_best};
+  }
   if (choice) {
     choice[0] = m2l_best;
     choice[1] = bps_best;
@@ -1287,17 +1338,20 @@ int defmm_prcmpt(defmm_handle* h, int L, int Ncrit, double kappa, int lvMAX) {
   // the level walk on the GPU when there is one (list records for parity
   // checks come from the host walk)
   dfb::LevelWalker* walker = nullptr;
+  std::unique_ptr<dfb::TreeSorter> sorter;
   h->walked_on_device = false;
-  if (h->plan_device && !h->keep_lists) {
+  if (h->plan_device) {
     int n = 0;
     if (cudaGetDeviceCount(&n) == cudaSuccess && n > 0 && ensure_device(h) == 0 &&
-        cudaSetDevice(h->device) == cudaSuccess)
-      walker = dfb::device_level_walker();
+        cudaSetDevice(h->device) == cudaSuccess) {
+      sorter = dfb::make_device_tree_sorter();
+      if (!h->keep_lists) walker = dfb::device_level_walker();
+    }
     cudaGetLastError();
     h->err.clear();
   }
   int st = dfb::build_plan(h->plan, h->src.data(), (int64_t)h->src.size() / 3, h->trg.data(),
-                           (int64_t)h->trg.size() / 3, L, Ncrit, kappa, lvMAX, e, walker);
+                           (int64_t)h->trg.size() / 3, L, Ncrit, kappa, lvMAX, e, walker, sorter.get());
   if (st) return h->fail(st == -4 ? DEFMM_ERR_CUDA : st == -5 ? DEFMM_ERR_MEMORY : st, e);
   h->walked_on_device = walker != nullptr;
   // M2L entries the walk left on the device belong to this handle's plan
@@ -1356,9 +1410,20 @@ int defmm_set_blocking(defmm_handle* h, int rhs_block, int groups) {
   return 0;
 }
 
+int defmm_set_tensor_cores(defmm_handle* h, int on) {
+  if (!h || (on != 0 && on != 1)) return DEFMM_ERR_ARG;
+  if (h->use_tc != (on != 0)) {
+    h->use_tc = on != 0;
+    if (h->device >= 0) drop_graph(h);
+  }
+  return 0;
+}
+
 int defmm_set_rhs_per_cta(defmm_handle* h, int rb) {
-  if (!h || (rb != 1 && rb != 2 && rb != 4 && rb != 8)) return DEFMM_ERR_ARG;
-  h->rhs_block_m2l = rb;
+  if (!h || (rb != 1 && rb != 2 && rb != 4 && rb != 8 && rb != -1 && rb != -2 && rb != -4 && rb != -8))
+    return DEFMM_ERR_ARG;
+  h->rhs_block_m2l = rb < 0 ? -rb : rb;
+  h->m2l_chunk_major = rb < 0;
   return 0;
 }
 
@@ -1484,6 +1549,7 @@ int defmm_gemv_batched(defmm_handle* h, int64_t nrhs, const double* in, double* 
   CK(cudaStreamSynchronize(h->st));
   int flag = 0;
   CK(cudaMemcpy(&flag, h->dp.err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (flag == 3) return h->fail(DEFMM_ERR_CUDA, "a tensor-core kernel's wait for its MMAs timed out");
   if (flag) return h->fail(DEFMM_ERR_ARG, "inconsistent interaction list detected on the device");
   h->has_out = true;
   return 0;
@@ -1569,6 +1635,16 @@ int defmm_info(const defmm_handle* h, int what, int64_t* v) {
     case DEFMM_INFO_LAYOUT: *v = h->layout; break;
     case DEFMM_INFO_RHS_BLOCK: *v = h->layout == 2 ? h->gl.R : 0; break;
     case DEFMM_INFO_GROUPS: *v = h->layout == 2 ? (int64_t)h->gl.groups.size() : 0; break;
+    case DEFMM_INFO_TENSOR_CORES: *v = h->use_tc ? 1 : 0; break;
+    case DEFMM_INFO_TREE_DEVICE: *v = p.tree_on_device ? 1 : 0; break;
+    case DEFMM_INFO_RHS_PER_CTA: {  // the block the M2L launcher uses for the grouped layout's R
+      const int R = h->layout == 2 ? h->gl.R : 1;
+      int rb = std::min(h->rhs_block_m2l, h->ops ? h->ops->max_rb : 1);
+      while (rb > 1 && R % rb) rb >>= 1;
+      *v = rb;
+      break;
+    }
+    case DEFMM_INFO_TREE_MS: *v = (int64_t)(1e3 * p.t_tree); break;
     case DEFMM_INFO_LIST_RECORDS: *v = p.keep_lists ? 1 : 0; break;
     case DEFMM_INFO_LAUNCHES: *v = h->launches; break;
     case DEFMM_INFO_PERMUTED_SPECTRA: *v = (int64_t)p.ptab_key.size(); break;

@@ -1,6 +1,7 @@
 // Matvec kernels.  One template per phase, instantiated per precision (T)
 // and interpolation order (L).  See kernels.cuh for the memory layout.
 #include "kernels.cuh"
+#include "device_math.cuh"
 #include "fmm_kernels.h"
 
 #include <algorithm>
@@ -11,106 +12,6 @@
 #include <vector>
 
 namespace dfb {
-
-// ----------------------------------------------------------------- basics --
-// equispaced Lagrange basis of order L on [-rad, rad] at x
-// (thetis_polynomials.hpp:81-94): b[l] = prod_{j != l} (x/rad - p_j)/(p_l - p_j),
-// p_j = -1 + 2 j/(L-1)
-template <int L, typename T>
-__device__ __forceinline__ void lagrange_all(T x, T rad, T* b) {
-  const T nx = x / rad;
-#pragma unroll
-  for (int l = 0; l < L; l++) {
-    T r = 1;
-    const T pl = T(-1) + T(2) * (T(l) / T(L - 1));
-#pragma unroll
-    for (int j = 0; j < L; j++) {
-      if (j == l) continue;
-      const T pj = T(-1) + T(2) * (T(j) / T(L - 1));
-      r *= (nx - pj) / (pl - pj);
-    }
-    b[l] = r;
-  }
-}
-
-// FP64 sin and cos of x: Cody-Waite reduction by pi/2 in two FMA steps
-// (pi/2 split into its double and the remainder), then the Taylor series of
-// sin to degree 15 and of cos to degree 16 on [-pi/4, pi/4] (truncation
-// below 7e-17 relative), quadrant by n mod 4.
-__device__ __forceinline__ void sincos_cw(double x, double& s, double& c) {
-  const double n = rint(x * 0.6366197723675814);
-  double r = fma(-n, 1.5707963267948966, x);
-  r = fma(-n, 6.123233995736766e-17, r);
-  const double r2 = r * r;
-  double ps = fma(r2, -7.647163731819816e-13, 1.6059043836821613e-10);
-  ps = fma(r2, ps, -2.505210838544172e-08);
-  ps = fma(r2, ps, 2.7557319223985893e-06);
-  ps = fma(r2, ps, -1.984126984126984e-04);
-  ps = fma(r2, ps, 8.333333333333333e-03);
-  ps = fma(r2, ps, -1.6666666666666666e-01);
-  const double sr = fma(r * r2, ps, r);
-  double pc = fma(r2, 4.779477332387385e-14, -1.1470745597729725e-11);
-  pc = fma(r2, pc, 2.08767569878681e-09);
-  pc = fma(r2, pc, -2.755731922398589e-07);
-  pc = fma(r2, pc, 2.48015873015873e-05);
-  pc = fma(r2, pc, -1.388888888888889e-03);
-  pc = fma(r2, pc, 4.1666666666666664e-02);
-  pc = fma(r2, pc, -0.5);
-  const double cr = fma(r2, pc, 1.0);
-  const int q = __double2int_rn(n) & 3;
-  const double ss = (q & 1) ? cr : sr, cc = (q & 1) ? sr : cr;
-  s = (q & 2) ? -ss : ss;
-  c = ((q + 1) & 2) ? -cc : cc;
-}
-
-// exp(i a) with a in FP64
-template <typename C>
-__device__ __forceinline__ C expi64(double a) {
-  double s, c;
-  sincos_cw(a, s, c);
-  C r;
-  r.x = c;
-  r.y = s;
-  return r;
-}
-
-// exp(i a) for the FP32 path: a = n pi + x reduced in FP64 (n from the low
-// mantissa bits of a / pi + 1.5 * 2^52, exact for |a / pi| < 2^51, any sign),
-// sin/cos of x in FP32 by Taylor polynomials of degree 13/12 on
-// [-pi/2, pi/2] (truncation < 7e-10), (-1)^n applied to both.
-__device__ __forceinline__ float2 expi_reduced(double a) {
-  const double t = fma(a, 0.31830988618379067154, 6755399441055744.0);
-  const double n = t - 6755399441055744.0;
-  const int odd = __double2loint(t) & 1;
-  const float x = (float)fma(-n, 3.14159265358979323846, a);
-  const float xx = x * x;
-  float ps = fmaf(xx, 1.6059043836821613e-10f, -2.5052108385441720e-08f);
-  ps = fmaf(xx, ps, 2.7557319223985893e-06f);
-  ps = fmaf(xx, ps, -1.9841269841269841e-04f);
-  ps = fmaf(xx, ps, 8.3333333333333333e-03f);
-  ps = fmaf(xx, ps, -1.6666666666666667e-01f);
-  ps = fmaf(xx, ps, 1.0f);
-  float pc = fmaf(xx, 2.0876756987868099e-09f, -2.7557319223985891e-07f);
-  pc = fmaf(xx, pc, 2.4801587301587302e-05f);
-  pc = fmaf(xx, pc, -1.3888888888888889e-03f);
-  pc = fmaf(xx, pc, 4.1666666666666667e-02f);
-  pc = fmaf(xx, pc, -0.5f);
-  pc = fmaf(xx, pc, 1.0f);
-  const float sg = odd ? -1.0f : 1.0f;
-  return make_float2(sg * pc, sg * x * ps);
-}
-
-// Plane-wave phase exp(i a) at the precision of the complex type.
-template <typename C>
-__device__ __forceinline__ C expi(double a);
-template <>
-__device__ __forceinline__ double2 expi<double2>(double a) {
-  return expi64<double2>(a);
-}
-template <>
-__device__ __forceinline__ float2 expi<float2>(double a) {
-  return expi_reduced(a);
-}
 
 // --------------------------------------------------------- constant tables --
 // Per order L = 2..8: the four L x L interpolation matrices (m2m[0], m2m[1],
@@ -308,25 +209,6 @@ __device__ __forceinline__ void p2m_group(const DevPlan& P, int64_t j0, int ns, 
       }
     }
   }
-}
-
-// Leaf slots of cell c (CSR of the slot lists, directions increasing) whose
-// direction lies in [d0, d1): a contiguous sub-range [*b, *e).
-__device__ __forceinline__ void dir_range(const int64_t* __restrict__ cptr, const int32_t* __restrict__ cdir,
-                                          int64_t c, int d0, int d1, int64_t* b, int64_t* e) {
-  int64_t lo = cptr[c], hi = cptr[c + 1];
-  int64_t a = lo, z = hi;
-  while (a < z) {  // first entry with dir >= d0
-    const int64_t m = (a + z) >> 1;
-    if (cdir[m] < d0) a = m + 1; else z = m;
-  }
-  int64_t a2 = a, z2 = hi;
-  while (a2 < z2) {  // first entry with dir >= d1
-    const int64_t m = (a2 + z2) >> 1;
-    if (cdir[m] < d1) a2 = m + 1; else z2 = m;
-  }
-  *b = a;
-  *e = a2;
 }
 
 // M: base of the expansions written here (slot s, right-hand side r at
@@ -1087,7 +969,8 @@ __global__ void __launch_bounds__(NT, m2l_rhs_ctas<T, NT, RB>()) k_m2l_rhs(DevPl
                                                              const typename cpx_t<T>::type* __restrict__ F,
                                                              const typename cpx_t<T>::type* __restrict__ ptab,
                                                              typename cpx_t<T>::type* __restrict__ Lx,
-                                                             unsigned long long* __restrict__ queue) {
+                                                             unsigned long long* __restrict__ queue,
+                                                             bool chunk_major) {
   typedef typename cpx_t<T>::type C;
   constexpr int PD = 2 * L - 1, LL = L * L * L, PP = PD * PD * PD, K = (PP + NT - 1) / NT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1103,8 +986,10 @@ __global__ void __launch_bounds__(NT, m2l_rhs_ctas<T, NT, RB>()) k_m2l_rhs(DevPl
     __syncthreads();
     const int64_t w = cur;
     if (w >= nwork) break;
-    const int64_t t = t0 + w / nb;
-    const int r0 = (int)(w % nb) * RB;
+    // chunk_major: all target slots for one block of right-hand sides, then
+    // the next block (the spectra in flight are RB of the R per source slot)
+    const int64_t t = chunk_major ? t0 + w % (t1 - t0) : t0 + w / nb;
+    const int r0 = (int)(chunk_major ? w / (t1 - t0) : w % nb) * RB;
     const int64_t eb = P.m2l_ptr[t], ee = P.m2l_ptr[t + 1];
     C acc[K][RB];
 #pragma unroll
@@ -1586,7 +1471,8 @@ __device__ __forceinline__ float2 green32(double dx, double dy, double dz, doubl
 // tp >= nt lanes), sources streamed through shared memory with RB charges
 // each; one evaluation of G(x, y) (green64 / green32) is multiplied into the
 // RB right-hand sides r0 .. r0 + RB - 1 of the R in q (q[j R + r]).  Mixed:
-// FP32 products in compensated FP32 sums per tile, added into FP64 per tile.
+// FP32 products summed in FP32 over at most 16 sources per lane, those
+// partial sums added in FP64.
 // Sums go to pnear[(t) R + r] (item_chunk == nullptr: items are chunks) or
 // to tpart[(item 32 + t) R + r] for k_p2p_items_rhs.
 template <bool MIXED, int RB>
@@ -1631,13 +1517,8 @@ __global__ void __launch_bounds__(128) k_p2p_rhs(DevPlan P, int64_t nitem, const
     const int ti = f + min(mt, nt - 1);
     const double x0 = P.T_pos[3 * (int64_t)ti], x1 = P.T_pos[3 * (int64_t)ti + 1], x2 = P.T_pos[3 * (int64_t)ti + 2];
     double2 acc[RB];
-    float2 fs[RB], fc[RB];  // mixed: compensated FP32 sums of the current tile
 #pragma unroll
-    for (int b = 0; b < RB; b++) {
-      acc[b] = make_double2(0., 0.);
-      fs[b] = make_float2(0.f, 0.f);
-      fc[b] = make_float2(0.f, 0.f);
-    }
+    for (int b = 0; b < RB; b++) acc[b] = make_double2(0., 0.);
     const int64_t rb = ptr[it], re = ptr[it + 1];
     int64_t r = rb;
     int off = 0;
@@ -1665,18 +1546,36 @@ __global__ void __launch_bounds__(128) k_p2p_rhs(DevPlan P, int64_t nitem, const
         }
       }
       __syncthreads();
-      for (int j = gid; j < fill; j += GS) {
-        const double2 a = sa[j], bz = sb[j];
-        const Q* qj = sq + j * RB;
-        if constexpr (MIXED) {
-          const float2 g = green32(x0 - a.x, x1 - a.y, x2 - bz.x, P.kappa);
+      if constexpr (MIXED) {
+        // FP32 products summed in FP32 over at most kFlush sources of this
+        // lane, then added into the FP64 sums
+        constexpr int kFlush = 16;
+        for (int j0 = gid; j0 < fill; j0 += kFlush * GS) {
+          const int j1 = min(fill, j0 + kFlush * GS);
+          float2 fs[RB];
+#pragma unroll
+          for (int b = 0; b < RB; b++) fs[b] = make_float2(0.f, 0.f);
+          for (int j = j0; j < j1; j += GS) {
+            const double2 a = sa[j], bz = sb[j];
+            const Q* qj = sq + j * RB;
+            const float2 g = green32(x0 - a.x, x1 - a.y, x2 - bz.x, P.kappa);
+#pragma unroll
+            for (int b = 0; b < RB; b++) {
+              const float2 qq = qj[b];
+              fs[b].x = fmaf(g.x, qq.x, fmaf(-g.y, qq.y, fs[b].x));
+              fs[b].y = fmaf(g.x, qq.y, fmaf(g.y, qq.x, fs[b].y));
+            }
+          }
 #pragma unroll
           for (int b = 0; b < RB; b++) {
-            const float2 qq = qj[b];
-            kahan_add(fs[b].x, fc[b].x, fmaf(g.x, qq.x, -g.y * qq.y));
-            kahan_add(fs[b].y, fc[b].y, fmaf(g.x, qq.y, g.y * qq.x));
+            acc[b].x += (double)fs[b].x;
+            acc[b].y += (double)fs[b].y;
           }
-        } else {
+        }
+      } else {
+        for (int j = gid; j < fill; j += GS) {
+          const double2 a = sa[j], bz = sb[j];
+          const Q* qj = sq + j * RB;
           const double2 g = green64(x0 - a.x, x1 - a.y, x2 - bz.x, P.kappa);
 #pragma unroll
           for (int b = 0; b < RB; b++) {
@@ -1684,15 +1583,6 @@ __global__ void __launch_bounds__(128) k_p2p_rhs(DevPlan P, int64_t nitem, const
             acc[b].x = fma(g.x, qq.x, fma(-g.y, qq.y, acc[b].x));
             acc[b].y = fma(g.x, qq.y, fma(g.y, qq.x, acc[b].y));
           }
-        }
-      }
-      if constexpr (MIXED) {
-#pragma unroll
-        for (int b = 0; b < RB; b++) {
-          acc[b].x += (double)fs[b].x - (double)fc[b].x;
-          acc[b].y += (double)fs[b].y - (double)fc[b].y;
-          fs[b] = make_float2(0.f, 0.f);
-          fc[b] = make_float2(0.f, 0.f);
         }
       }
     }
@@ -2172,30 +2062,31 @@ struct Launch {
   }
   template <int RB, int NT>
   static void m2l_rhs_go(const DevPlan& dp, int64_t t0, int64_t t1, int64_t f0, int64_t f1, int R, const void* F,
-                         const void* ptab, void* Lx, unsigned long long* queue, int nsm, cudaStream_t s) {
+                         const void* ptab, void* Lx, unsigned long long* queue, int nsm, bool chunk_major,
+                         cudaStream_t s) {
     constexpr int RBE = RB <= kMaxRB ? RB : 1;
     const int64_t nwork = (t1 - t0) * (R / RBE);
     const int grid = (int)std::min<int64_t>(nwork, (int64_t)nsm * m2l_rhs_ctas<T, NT, RBE>());
     k_m2l_rhs<T, L, NT, RBE><<<grid, NT, smem_m2l(), s>>>(dp, t0, t1, f0, f1, R, (const C*)F, (const C*)ptab,
-                                                          (C*)Lx, queue);
+                                                          (C*)Lx, queue, chunk_major);
   }
   // M2L for R right-hand sides in blocks of rb (1, 2, 4 or 8; a divisor of
-  // R, capped by the order's kMaxRB)
+  // R, capped by the order's kMaxRB); chunk_major: target slots inner
   static void m2l_rhs(const DevPlan& dp, int64_t t0, int64_t t1, int64_t f0, int64_t f1, int R, int rb,
-                      const void* F, const void* ptab, void* Lx, unsigned long long* queue, int nsm,
-                      cudaStream_t s) {
+                      bool chunk_major, const void* F, const void* ptab, void* Lx, unsigned long long* queue,
+                      int nsm, cudaStream_t s) {
     if (t1 <= t0) return;
     cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s);
     if (rb > kMaxRB) rb = kMaxRB;
     while (rb > 1 && R % rb) rb >>= 1;
     if (rb >= 8)
-      m2l_rhs_go<8, 256>(dp, t0, t1, f0, f1, R, F, ptab, Lx, queue, nsm, s);
+      m2l_rhs_go<8, 256>(dp, t0, t1, f0, f1, R, F, ptab, Lx, queue, nsm, chunk_major, s);
     else if (rb >= 4)
-      m2l_rhs_go<4, 256>(dp, t0, t1, f0, f1, R, F, ptab, Lx, queue, nsm, s);
+      m2l_rhs_go<4, 256>(dp, t0, t1, f0, f1, R, F, ptab, Lx, queue, nsm, chunk_major, s);
     else if (rb >= 2)
-      m2l_rhs_go<2, 128>(dp, t0, t1, f0, f1, R, F, ptab, Lx, queue, nsm, s);
+      m2l_rhs_go<2, 128>(dp, t0, t1, f0, f1, R, F, ptab, Lx, queue, nsm, chunk_major, s);
     else
-      m2l_rhs_go<1, 128>(dp, t0, t1, f0, f1, R, F, ptab, Lx, queue, nsm, s);
+      m2l_rhs_go<1, 128>(dp, t0, t1, f0, f1, R, F, ptab, Lx, queue, nsm, chunk_major, s);
   }
   static void p2m(const DevPlan& dp, const int32_t* leaves, int n, const void* q, const void* sig2, void* M, int R,
                   int d0, int d1, cudaStream_t s) {

@@ -36,8 +36,9 @@ struct OpTable {
               void* Lx, unsigned long long* queue, int nsm, int nt, int pair, cudaStream_t);
   // The same for R right-hand sides (F: R spectra per source slot of the
   // batch, Lx: base as above), rb of them per CTA sharing each spectrum load
-  void (*m2l_rhs)(const DevPlan&, int64_t t0, int64_t t1, int64_t f0, int64_t f1, int R, int rb, const void* F,
-                  const void* ptab, void* Lx, unsigned long long* queue, int nsm, cudaStream_t);
+  // (chunk_major: every target slot for one block, then the next block)
+  void (*m2l_rhs)(const DevPlan&, int64_t t0, int64_t t1, int64_t f0, int64_t f1, int R, int rb, bool chunk_major,
+                  const void* F, const void* ptab, void* Lx, unsigned long long* queue, int nsm, cudaStream_t);
   // L2P of the leaves' slots with a direction in [d0, d1) into pfar (R per
   // particle), written (accum = false) or added
   void (*l2p)(const DevPlan&, const int32_t* leaves, int n, const void* sig2, const void* Lx, double2* pfar, int R,
@@ -78,6 +79,15 @@ void launch_p2p_reduce(bool fp64, int64_t nleaf, const int32_t* first, const int
 // Kernel attributes of the right-hand-side block kernels (call once per
 // device, outside stream capture).
 cudaError_t setup_rhs_kernels();
+// Tensor-core (tcgen05, 3-pass split-TF32) P2M of the mixed-precision path
+// (tc_interp.cu): same arguments and results as OpTable::p2m for FP32 data,
+// order L.  setup_tc_kernels sets their attributes (once per device).
+cudaError_t setup_tc_kernels();
+void launch_p2m_tc(int L, const DevPlan& dp, const int32_t* leaves, int n, const void* q, const void* sig2, void* M,
+                   int R, int d0, int d1, int nsm, cudaStream_t s);
+// The same for L2P (OpTable::l2p arguments); leaves of at most 128 points.
+void launch_l2p_tc(int L, const DevPlan& dp, const int32_t* leaves, int n, const void* sig2, const void* Lx,
+                   double2* pfar, int R, int d0, int d1, bool accum, int nsm, cudaStream_t s);
 // Near field of R right-hand sides (q: R charges per particle, tree order),
 // target-side, in passes of up to 8 right-hand sides; sums to pnear[i R + r]
 // (item_chunk == nullptr) or to tpart[(item 32 + t) R + r], added per chunk

@@ -80,4 +80,23 @@ struct DevPlan {
   int nlvl;
 };
 
+// Leaf slots of cell c (CSR of the slot lists, directions increasing) whose
+// direction lies in [d0, d1): a contiguous sub-range [*b, *e).
+__device__ __forceinline__ void dir_range(const int64_t* __restrict__ cptr, const int32_t* __restrict__ cdir,
+                                          int64_t c, int d0, int d1, int64_t* b, int64_t* e) {
+  int64_t lo = cptr[c], hi = cptr[c + 1];
+  int64_t a = lo, z = hi;
+  while (a < z) {  // first entry with dir >= d0
+    const int64_t m = (a + z) >> 1;
+    if (cdir[m] < d0) a = m + 1; else z = m;
+  }
+  int64_t a2 = a, z2 = hi;
+  while (a2 < z2) {  // first entry with dir >= d1
+    const int64_t m = (a2 + z2) >> 1;
+    if (cdir[m] < d1) a2 = m + 1; else z2 = m;
+  }
+  *b = a;
+  *e = a2;
+}
+
 }  // namespace dfb

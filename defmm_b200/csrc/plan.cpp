@@ -114,10 +114,14 @@ struct Node {
 // lvmax >= 0, sort.hpp:51); child centres c + (r/2)(2 b_k - 1); particles are
 // split stably, so a leaf keeps the input order of its particles.
 int build_tree(Tree& t, const double* pts, int64_t n, const double* bctr,
-               double brad, int ncrit, int lvmax, std::string& err) {
-  std::vector<int32_t> order(n);
-  for (int64_t i = 0; i < n; i++) order[i] = (int32_t)i;
-  std::vector<int32_t> tmp(n);
+               double brad, int ncrit, int lvmax, std::string& err, TreeSorter* sorter) {
+  std::vector<int32_t> order(sorter ? 0 : n);
+  for (int64_t i = 0; i < (int64_t)order.size(); i++) order[i] = (int32_t)i;
+  std::vector<int32_t> tmp(sorter ? 0 : n);
+  if (sorter) {
+    const int st = sorter->begin(pts, n, err);
+    if (st) return st;
+  }
   std::vector<Node> nodes(1);
   Node& r = nodes[0];
   r.first = 0;
@@ -135,6 +139,28 @@ int build_tree(Tree& t, const double* pts, int64_t n, const double* bctr,
     const int64_t cnt = le - lb;
     std::vector<std::array<int64_t, 8>> hist(cnt);
     std::atomic<int> bad(0);
+    if (sorter) {  // octant counts on the sorter's side
+      std::vector<int64_t> first(cnt);
+      std::vector<double> ctr(3 * cnt);
+      std::vector<uint8_t> split(cnt);
+      for (int64_t ii = 0; ii < cnt; ii++) {
+        const Node& c = nodes[lb + ii];
+        first[ii] = c.first;
+        for (int k = 0; k < 3; k++) ctr[3 * ii + k] = c.ctr[k];
+        const bool stop = lvmax >= 0 ? c.lvl >= lvmax : c.n < ncrit;
+        split[ii] = stop ? 0 : 1;
+        if (!stop && c.lvl >= 60) bad = 1;
+      }
+      if (bad) {
+        err = "coincident points keep a cell at or above the leaf size beyond level 60";
+        return -2;
+      }
+      std::vector<int64_t> hflat(8 * cnt, 0);
+      const int st = sorter->histogram(cnt, first.data(), ctr.data(), split.data(), hflat.data(), err);
+      if (st) return st;
+      for (int64_t ii = 0; ii < cnt; ii++)
+        for (int b = 0; b < 8; b++) hist[ii][b] = hflat[8 * ii + b];
+    } else
     pfor(cnt, 1, [&](int64_t ii) {
       Node& c = nodes[lb + ii];
       auto& h = hist[ii];
@@ -198,9 +224,25 @@ int build_tree(Tree& t, const double* pts, int64_t n, const double* bctr,
         off += h;
       }
     });
+    if (sorter && total) {  // children's ranges: the sorter moves the particles
+      std::vector<int64_t> cf(8 * cnt, -1);
+      for (int64_t ii = 0; ii < cnt; ii++) {
+        const Node& c = nodes[lb + ii];
+        int64_t ch = c.child0;
+        for (int b = 0; b < 8; b++)
+          if (hist[ii][b]) cf[8 * ii + b] = nodes[ch++].first;
+      }
+      const int st = sorter->reorder(cf.data(), err);
+      if (st) return st;
+    }
     lb = le;
     le = le + total;
     lvl++;
+  }
+  if (sorter) {
+    order.resize(n);
+    const int st = sorter->finish(order.data(), err);
+    if (st) return st;
   }
   const int64_t nc = (int64_t)nodes.size();
   // subtree sizes bottom-up (children always follow their parent in BFS order)
@@ -1025,7 +1067,7 @@ int walk_levels_host(Plan& p, LevelWalk& walk) {
 
 int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
                int64_t nt, int L, int ncrit, double kappa, int lvmax,
-               std::string& err, LevelWalker* walker) {
+               std::string& err, LevelWalker* walker, TreeSorter* sorter) {
   if (ns <= 0 || nt <= 0) {
     err = "empty source or target set";
     return -1;
@@ -1073,10 +1115,11 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
     }
     p.box_rad = std::max(a, b);
   }
-  int st = build_tree(p.T, trg, nt, p.box_ctr, p.box_rad, ncrit, lvmax, err);
+  int st = build_tree(p.T, trg, nt, p.box_ctr, p.box_rad, ncrit, lvmax, err, sorter);
   if (st) return st;
-  st = build_tree(p.S, src, ns, p.box_ctr, p.box_rad, ncrit, lvmax, err);
+  st = build_tree(p.S, src, ns, p.box_ctr, p.box_rad, ncrit, lvmax, err, sorter);
   if (st) return st;
+  p.tree_on_device = sorter != nullptr;
   p.t_tree = now_s() - t0;
   t0 = now_s();
   st = init_levels(p, err);

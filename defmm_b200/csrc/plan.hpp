@@ -145,6 +145,7 @@ struct Plan {
   bool keep_lists = false;
   std::vector<int32_t> rec_far_hf, rec_far_lf, rec_near;
   double t_tree = 0, t_lists = 0, t_tables = 0, t_walk = 0;  // t_walk: part of t_lists
+  bool tree_on_device = false;  // the octrees' particle ordering ran on the device
 };
 
 // Result of the level-by-level dual traversal (hrzpass.hpp:62-143 with the
@@ -170,14 +171,34 @@ struct LevelWalker {
   virtual int walk(Plan& p, LevelWalk& w, std::string& err) = 0;
 };
 
+// The particle ordering of the octree build on another processor (the
+// device one, plan_device.cu).  The host keeps the cells and decides which
+// split; per level the sorter returns the octant counts of the splitting
+// cells' particles (bit code sum_k (x_k > c_k) << k, the cell centres given
+// by the host) and then moves every particle of a splitting cell to its
+// child's range, stably; at the end it returns the final order.  The cells
+// and the order are then exactly the host build's.
+struct TreeSorter {
+  virtual ~TreeSorter() = default;
+  virtual int begin(const double* pts, int64_t n, std::string& err) = 0;
+  // m cells of the level: first particle position, centre (3 per cell),
+  // split flag; hist: m x 8 octant counts (zero for cells that stay)
+  virtual int histogram(int64_t m, const int64_t* first, const double* ctr, const uint8_t* split, int64_t* hist,
+                        std::string& err) = 0;
+  // first position of each (cell, octant) child, -1 where there is none
+  virtual int reorder(const int64_t* child_first, std::string& err) = 0;
+  virtual int finish(int32_t* order, std::string& err) = 0;
+};
+
 // Build the plan; returns 0 or a negative status with `err` set.  With a
-// walker (and no list records requested) the level walk runs there.
+// walker (and no list records requested) the level walk runs there; with a
+// sorter the octrees' particle ordering runs there.
 //   -2: coincident points keep a cell above ncrit (the reference recurses
 //       without end, sort.hpp:98-162)
 //   -3: the tree is too shallow for any M2L level (frequency.hpp:114-120)
 //   -1: invalid arguments
 int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
                int64_t nt, int L, int ncrit, double kappa, int lvmax,
-               std::string& err, LevelWalker* walker = nullptr);
+               std::string& err, LevelWalker* walker = nullptr, TreeSorter* sorter = nullptr);
 
 }  // namespace dfb

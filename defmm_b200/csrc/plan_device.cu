@@ -10,6 +10,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <memory>
 #include <cstring>
 
 #include "plan.hpp"
@@ -745,9 +746,172 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
 
 }  // namespace
 
+// ------------------------------------------------------ octree on the device --
+// The particle side of the octree build (TreeSorter): per level, each
+// particle of a splitting cell gets its bit code sum_k (x_k > c_k) << k
+// against the cell centre the host computed, the codes are counted per
+// (cell, octant), and every particle is keyed by the first position of its
+// new cell (its child's, or its own cell's when the cell stays); a stable
+// radix sort by that key moves the particles of every splitting cell into
+// its children's ranges in octant order, keeping their order within a child
+// (sort.hpp:98-170).  cf[i] is the first position of the cell of the
+// particle at position i; at[cf] maps a cell of the current level to its
+// index (-1 for cells that stay).
+__global__ void k_tree_mark(int64_t m, const int64_t* __restrict__ first, const uint8_t* __restrict__ split,
+                            int32_t* __restrict__ at) {
+  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j < m) at[first[j]] = split[j] ? (int32_t)j : -1;
+}
+
+__global__ void k_tree_codes(int64_t n, const double* __restrict__ pts, const int32_t* __restrict__ order,
+                             const int32_t* __restrict__ cf, const int32_t* __restrict__ at,
+                             const double* __restrict__ ctr, uint8_t* __restrict__ code, int32_t* __restrict__ cnt) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int32_t s = at[cf[i]];
+  if (s < 0) {
+    code[i] = 255;
+    return;
+  }
+  const double* x = pts + 3 * (int64_t)order[i];
+  const double* c = ctr + 3 * (int64_t)s;
+  const int b = (x[0] > c[0] ? 1 : 0) | (x[1] > c[1] ? 2 : 0) | (x[2] > c[2] ? 4 : 0);
+  code[i] = (uint8_t)b;
+  atomicAdd(&cnt[8 * s + b], 1);
+}
+
+__global__ void k_tree_keys(int64_t n, const int32_t* __restrict__ cf, const int32_t* __restrict__ at,
+                            const uint8_t* __restrict__ code, const int64_t* __restrict__ child_first,
+                            int32_t* __restrict__ key) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint8_t b = code[i];
+  key[i] = b == 255 ? cf[i] : (int32_t)child_first[8 * (int64_t)at[cf[i]] + b];
+}
+
+struct DeviceSorter final : TreeSorter {
+  int64_t n = 0;
+  int bits = 1;
+  double* pts = nullptr;
+  int32_t *order = nullptr, *order2 = nullptr, *cf = nullptr, *key = nullptr, *at = nullptr, *cnt = nullptr;
+  uint8_t* code = nullptr;
+  int64_t *first = nullptr, *childf = nullptr;
+  double* ctr = nullptr;
+  uint8_t* split = nullptr;
+  int64_t cap = 0;  // cells per level the level arrays hold
+  void* tmp = nullptr;
+  size_t tmp_bytes = 0;
+  cudaStream_t st = nullptr;
+  void release() {
+    for (void* p : {(void*)pts, (void*)order, (void*)order2, (void*)cf, (void*)key, (void*)at, (void*)cnt,
+                    (void*)code, (void*)first, (void*)childf, (void*)ctr, (void*)split, tmp})
+      if (p) cudaFree(p);
+    pts = nullptr;
+    order = order2 = cf = key = at = cnt = nullptr;
+    code = nullptr;
+    first = childf = nullptr;
+    ctr = nullptr;
+    split = nullptr;
+    tmp = nullptr;
+    tmp_bytes = 0;
+    cap = 0;
+    if (st) cudaStreamDestroy(st);
+    st = nullptr;
+  }
+  ~DeviceSorter() override { release(); }
+  int fail(std::string& err, const char* what, cudaError_t e) {
+    err = std::string("device tree: ") + what + ": " + cudaGetErrorString(e);
+    cudaGetLastError();
+    release();
+    return e == cudaErrorMemoryAllocation ? -5 : -4;
+  }
+  int begin(const double* p, int64_t np, std::string& err) override {
+    release();
+    n = np;
+    bits = 1;
+    while (bits < 31 && ((int64_t)1 << bits) <= n) bits++;
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaMalloc(&pts, 24 * (size_t)n)) != cudaSuccess ||
+        (e = cudaMalloc(&order, 4 * (size_t)n)) != cudaSuccess ||
+        (e = cudaMalloc(&order2, 4 * (size_t)n)) != cudaSuccess || (e = cudaMalloc(&cf, 4 * (size_t)n)) != cudaSuccess ||
+        (e = cudaMalloc(&key, 4 * (size_t)n)) != cudaSuccess || (e = cudaMalloc(&at, 4 * (size_t)n)) != cudaSuccess ||
+        (e = cudaMalloc(&code, (size_t)n)) != cudaSuccess)
+      return fail(err, "allocation", e);
+    if ((e = cudaMemcpyAsync(pts, p, 24 * (size_t)n, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+        (e = cudaMemsetAsync(cf, 0, 4 * (size_t)n, st)) != cudaSuccess ||
+        (e = cudaMemsetAsync(at, 0xff, 4 * (size_t)n, st)) != cudaSuccess)
+      return fail(err, "upload", e);
+    k_iota<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, order);
+    size_t need = 0;
+    if ((e = cub::DeviceRadixSort::SortPairs(nullptr, need, key, cf, order, order2, (int)n, 0, bits, st)) !=
+        cudaSuccess)
+      return fail(err, "sort size", e);
+    if ((e = cudaMalloc(&tmp, need)) != cudaSuccess) return fail(err, "allocation", e);
+    tmp_bytes = need;
+    return 0;
+  }
+  int histogram(int64_t m, const int64_t* f, const double* c, const uint8_t* sp, int64_t* hist,
+                std::string& err) override {
+    cudaError_t e;
+    if (m > cap) {
+      for (void* q : {(void*)first, (void*)childf, (void*)ctr, (void*)split, (void*)cnt})
+        if (q) cudaFree(q);
+      first = childf = nullptr;
+      ctr = nullptr;
+      split = nullptr;
+      cnt = nullptr;
+      cap = std::max<int64_t>(m, 1024);
+      if ((e = cudaMalloc(&first, 8 * cap)) != cudaSuccess || (e = cudaMalloc(&childf, 64 * cap)) != cudaSuccess ||
+          (e = cudaMalloc(&ctr, 24 * cap)) != cudaSuccess || (e = cudaMalloc(&split, cap)) != cudaSuccess ||
+          (e = cudaMalloc(&cnt, 32 * cap)) != cudaSuccess)
+        return fail(err, "allocation", e);
+    }
+    if ((e = cudaMemcpyAsync(first, f, 8 * m, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(ctr, c, 24 * m, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(split, sp, m, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+        (e = cudaMemsetAsync(cnt, 0, 32 * m, st)) != cudaSuccess)
+      return fail(err, "level upload", e);
+    k_tree_mark<<<(unsigned)((m + 255) / 256), 256, 0, st>>>(m, first, split, at);
+    k_tree_codes<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, pts, order, cf, at, ctr, code, cnt);
+    std::vector<int32_t> h(8 * m);
+    if ((e = cudaMemcpyAsync(h.data(), cnt, 32 * m, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+      return fail(err, "level histogram", e);
+    for (int64_t i = 0; i < 8 * m; i++) hist[i] = h[i];
+    last_m = m;
+    return 0;
+  }
+  int reorder(const int64_t* child_first, std::string& err) override {
+    // the level's cells are those of the last histogram call
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(childf, child_first, 64 * last_m, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+      return fail(err, "level upload", e);
+    k_tree_keys<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, cf, at, code, childf, key);
+    size_t tb = tmp_bytes;
+    if ((e = cub::DeviceRadixSort::SortPairs(tmp, tb, key, cf, order, order2, (int)n, 0, bits, st)) !=
+        cudaSuccess)
+      return fail(err, "sort", e);
+    std::swap(order, order2);
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return fail(err, "sort", e);
+    return 0;
+  }
+  int finish(int32_t* out, std::string& err) override {
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(out, order, 4 * (size_t)n, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+      return fail(err, "download", e);
+    release();
+    return 0;
+  }
+  int64_t last_m = 0;
+};
+
 LevelWalker* device_level_walker() {
   static DeviceWalker w;
   return &w;
 }
+
+std::unique_ptr<TreeSorter> make_device_tree_sorter() { return std::unique_ptr<TreeSorter>(new DeviceSorter()); }
 
 }  // namespace dfb

@@ -16,6 +16,9 @@ the workloads the matvec is measured on:
   density proportional to 1 + 4|z| (rejection sampling); k such that the long
   axis (2) spans 256 wavelengths.
 * ``gaussian_blobs`` -- isotropic Gaussian blobs inside the unit cube.
+* ``mixture``       -- 40 % cube surface, 30 % sphere surface of radius 0.4,
+  30 % Gaussian blobs with sigma in [0.01, 0.1]; k such that the cube
+  diagonal (sqrt 3) spans 512 wavelengths; order 6, leaf size 96.
 
 Charges are complex with real and imaginary parts uniform in [-1, 1].
 """
@@ -125,6 +128,28 @@ def gaussian_blobs(n: int, seed: int = 0, nblobs: int = 8, sigma: float = 0.05,
     pts = np.clip(pts, -0.5, 0.5)
     return Workload("gaussian_blobs", np.ascontiguousarray(pts),
                     2.0 * math.pi * wavelengths / math.sqrt(3.0), order, ncrit)
+
+
+def mixture(n: int = 8_000_000, seed: int = 0, wavelengths: float = 512.0, order: int = 6,
+            ncrit: int = 96, nblobs: int = 16) -> Workload:
+    """40 % of the points uniform on the surface of [-0.5, 0.5]^3, 30 % uniform
+    on the sphere of radius 0.4 about the origin, 30 % in `nblobs` isotropic
+    Gaussian blobs (centres uniform in [-0.3, 0.3]^3, sigma log-uniform in
+    [0.01, 0.1], clipped to the cube); the diagonal sqrt(3) spans
+    `wavelengths` wavelengths."""
+    rng = np.random.default_rng(seed)
+    n_cube = int(round(0.4 * n))
+    n_sph = int(round(0.3 * n))
+    n_blob = n - n_cube - n_sph
+    cube = _face_points(rng, n_cube)
+    g = rng.standard_normal(size=(n_sph, 3))
+    sph = 0.4 * g / np.linalg.norm(g, axis=1, keepdims=True)
+    centres = rng.uniform(-0.3, 0.3, size=(nblobs, 3))
+    sig = np.exp(rng.uniform(math.log(0.01), math.log(0.1), size=nblobs))
+    which = rng.integers(0, nblobs, size=n_blob)
+    blob = np.clip(centres[which] + sig[which, None] * rng.standard_normal(size=(n_blob, 3)), -0.5, 0.5)
+    pts = np.concatenate([cube, sph, blob])[rng.permutation(n)]
+    return Workload("mixture", np.ascontiguousarray(pts), 2.0 * math.pi * wavelengths / math.sqrt(3.0), order, ncrit)
 
 
 def ragged_problems(count: int = 48, seed: int = 0) -> list:

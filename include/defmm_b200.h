@@ -66,10 +66,12 @@ int defmm_load_inp(defmm_handle* h, const char* path, int64_t nparts, int which)
 /* IBFMM_Mat<3>::prcmpt(int L, int Ncrit, flt kappa, int lvMAX = -1)
  * (interface.hpp:100-151): build both octrees (leaf = fewer than Ncrit
  * particles, or fixed depth lvMAX when lvMAX >= 0), the frequency regime,
- * cones, interaction lists, expansion slots and transfer spectra; the level
- * walk (dual traversal, cones, effective directions, slots, far entries) runs
- * on the GPU when one is present (defmm_set_plan_device), the rest on the
- * host (multi-threaded).  2 <= L <= 8. */
+ * cones, interaction lists, expansion slots and transfer spectra.  With a
+ * GPU present (defmm_set_plan_device) the octrees' particle ordering (octant
+ * codes, counts and a stable radix sort per level) and the level walk (dual
+ * traversal, cones, effective directions, slots, far entries) run there, the
+ * rest on the host (multi-threaded); the results are the host build's, bit
+ * for bit.  2 <= L <= 8. */
 int defmm_prcmpt(defmm_handle* h, int L, int Ncrit, double kappa, int lvMAX);
 
 /* Copy the plan to the current CUDA device (done by the first gemv when not
@@ -105,9 +107,20 @@ int defmm_gemv_device(defmm_handle* h, const void* d_in, void* d_out,
  * groups as the device memory needs, >= 1 = about that many, and the grouped
  * layout also for single right-hand sides (for tests and memory limits). */
 int defmm_set_blocking(defmm_handle* h, int rhs_block, int groups);
+/* No counterpart in the reference.  on = 1: the mixed-precision path runs
+ * the leaf interpolation GEMMs on the tensor cores (tcgen05 MMAs, 3-pass
+ * split TF32, FP32 accumulation in tensor memory): P2M, M = Z W
+ * (P2M.hpp:114-136), and L2P, p = Z^T X (L2P.hpp:122-173; target leaves of
+ * at most 128 points); 0: CUDA-core FP32 FMAs.  The FP64 path always uses
+ * FP64 FMAs. */
+int defmm_set_tensor_cores(defmm_handle* h, int on);
 /* No counterpart in the reference.  Right-hand sides per M2L CTA of the
- * grouped layout (1, 2, 4, 8; capped by the order's register budget): each
- * transfer-spectrum entry is read once for them. */
+ * grouped layout (1, 2, 4, 8, default 4; capped by the order's register
+ * budget and a divisor of the pass's right-hand sides): each
+ * transfer-spectrum entry is read once for them.  A negative value (-1, -2,
+ * -4, -8) sets the same block and orders the CTAs' work by block first
+ * (every target slot for one block of right-hand sides, then the next), so
+ * fewer source spectra are in flight at a time. */
 int defmm_set_rhs_per_cta(defmm_handle* h, int rb);
 
 /* No counterpart in the reference.  Independent operators (handles of
@@ -164,6 +177,12 @@ int defmm_check_full(defmm_handle* h, int64_t nsamples, uint64_t seed,
 int defmm_direct_noalloc(defmm_handle* h, const double* d_targets, int64_t nt,
                          double* d_out, void* stream);
 
+/* No counterpart in the reference.  Measurement helper: L2-to-SM read
+ * bandwidth of the current device in GB/s (every SM streaming a buffer of
+ * `bytes`, 1..96 MiB, that stays in L2, `reps` times; allocates and frees
+ * the buffer).  The roofline denominator of the L2-bound M2L kernels. */
+int defmm_probe_l2_read(int64_t bytes, int reps, double* gbs);
+
 /* Sizes and statistics.  what: see DEFMM_INFO_* below. */
 #define DEFMM_INFO_N_SOURCES 0
 #define DEFMM_INFO_N_TARGETS 1
@@ -199,6 +218,10 @@ int defmm_direct_noalloc(defmm_handle* h, const double* d_targets, int64_t nt,
 #define DEFMM_INFO_P2M_POINT_SLOTS 31   /* sum over source leaves of particles x slots */
 #define DEFMM_INFO_L2P_POINT_SLOTS 32   /* sum over target leaves of particles x slots */
 #define DEFMM_INFO_M2F_SLOTS 33         /* source slots transformed by M2F */
+#define DEFMM_INFO_TENSOR_CORES 34      /* 1: mixed-precision P2M and L2P on the tensor cores */
+#define DEFMM_INFO_TREE_DEVICE 35       /* 1 if prcmpt ordered the octrees' particles on the GPU */
+#define DEFMM_INFO_TREE_MS 36           /* prcmpt's octree build, ms */
+#define DEFMM_INFO_RHS_PER_CTA 37       /* right-hand sides per M2L CTA of the grouped layout */
 int defmm_info(const defmm_handle* h, int what, int64_t* value);
 
 /* Per-phase device times (ms) of the last gemv, in this order:

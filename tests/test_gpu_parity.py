@@ -289,3 +289,40 @@ def test_launch_choices_and_autotune_keep_results_bit_identical(gpu):
         assert A.info("m2l_threads") == c["m2l_threads"]
         assert np.array_equal(A.matvec(q), ref)
 
+
+
+@pytest.mark.parametrize("order", [3, 5, 6, 8])
+def test_tensor_core_p2m_matches_fp64(order, gpu):
+    # P2M on the tensor cores (tcgen05, 3-pass split TF32): one M tile
+    # (orders <= 5), two (6) and four (8) tiles of 128 expansion entries; the
+    # sphere's leaves hold up to 63 points (two K chunks of 32)
+    w = W.sphere_surface(20000, seed=23, wavelengths=8.0)
+    q = W.charges(w.n, 6)
+    A = make(w.points, w.points, order, 64, w.kappa)
+    p64 = A.matvec(q)
+    A.set_precision("mixed")
+    p_cc = A.matvec(q)
+    A.set_tensor_cores(True)
+    p_tc = A.matvec(q)
+    assert A.info("tensor_cores") == 1
+    assert rel(p_tc, p64) <= MIXED_TOL
+    assert rel(p_tc, p_cc) <= MIXED_TOL
+    # a block of right-hand sides over the grouped layout
+    rng = np.random.default_rng(8)
+    Q = (rng.uniform(-1, 1, (3, w.n)) + 1j * rng.uniform(-1, 1, (3, w.n))).astype(np.complex128)
+    A.set_blocking(3, 2)
+    P = A.matvec(Q)
+    A.set_precision("fp64")
+    for r in range(3):
+        assert rel(P[r], A.matvec(Q[r])) <= MIXED_TOL
+
+
+@pytest.mark.parametrize("name", ["cube_lf", "blobs_sphere", "cube_laplace"])
+def test_tensor_core_p2m_low_frequency_and_distinct_sets(name, gpu):
+    # LF leaves (no plane-wave phases) and distinct source / target trees
+    src, trg, q, L, ncrit, kappa, lvmax = case_inputs(name)
+    A = make(src, trg, L, ncrit, kappa, lvmax)
+    p64 = A.matvec(q)
+    A.set_precision("mixed")
+    A.set_tensor_cores(True)
+    assert rel(A.matvec(q), p64) <= MIXED_TOL

@@ -1,4 +1,6 @@
-"""The plan's level walk on the GPU (plan_device.cu) against the host walk
+"""The plan's octree build and level walk on the GPU (plan_device.cu: the
+particles ordered level by level with octant codes, counts and a stable
+radix sort; the dual traversal) against the host build and walk
 (plan.cpp, itself pinned to the reference's trees, cones and lists by
 tests/test_plan.py): same statistics, same effective directions per cell
 (the cell-array dump, which carries the slots' directions), and a
@@ -30,6 +32,7 @@ def compare(src, trg, q, L, ncrit, kappa, lvmax):
     H = build(src, trg, L, ncrit, kappa, lvmax, False)
     D = build(src, trg, L, ncrit, kappa, lvmax, True)
     assert H.info("plan_walk_device") == 0 and D.info("plan_walk_device") == 1
+    assert H.info("tree_device") == 0 and D.info("tree_device") == 1
     for k in STATS:
         assert H.info(k) == D.info(k), k
     for which in ("T", "S"):

@@ -64,7 +64,7 @@ def test_sphere2m_host_plan_is_bit_exact_with_oracle():
 def test_sphere2m_device_walk_is_bit_exact(gpu):
     m = meta()
     D = build(True, False)
-    assert D.info("plan_walk_device") == 1
+    assert D.info("plan_walk_device") == 1 and D.info("tree_device") == 1
     check_counts(D, m)
     for tag in "TS":
         assert digest(*D.tree(tag)) == m[f"tree_{tag}"], tag
