@@ -337,15 +337,15 @@ def run_ragged(args, torch):
 
 def run_spheroid(args, torch):
     """Spheroid with semi-axes (1, 0.5, 0.25), N = 4,000,000, density
-    1 + 4|z|, 256 wavelengths along the long axis, order 6, leaf 96, mixed
-    precision only: the FP64 path would hold M and L for 2 x 33.3M
-    expansion slots of 216 entries (230 GB), beyond the 180 GB of one B200.
-    Accuracy: FP64 direct sums at 2,000 seeded targets."""
+    1 + 4|z|, 256 wavelengths along the long axis, order 6, leaf 96: the
+    plain FP64 path and the mixed path (each on whichever layout fits: the
+    FP64 path's M and L for 2 x 33.3M slots of 216 entries, 230 GB, do not,
+    so it runs on the grouped layout).  Accuracy: FP64 direct sums at 2,000
+    seeded targets, and mixed against FP64."""
     from defmm_b200 import IBFMM_Mat, workloads as W
     w = W.spheroid(4_000_000, seed=0)
     q = W.charges(w.n, 1)
     A = IBFMM_Mat()
-    A.set_precision("mixed")
     A.addSourceParticles(w.points)
     A.addTargetParticles(w.points)
     t0 = time.perf_counter()
@@ -357,35 +357,113 @@ def run_spheroid(args, torch):
     torch.cuda.set_stream(stream)
     dq = torch.from_numpy(q).to("cuda")
     dp = torch.empty(w.n, dtype=torch.complex128, device="cuda")
-    for _ in range(args.warmup):
-        A.matvec_device(dq.data_ptr(), dp.data_ptr(), 1, stream.cuda_stream)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with Clocks(0) as ck:
-        e0.record(stream)
-        for _ in range(args.steps):
+    res = {}
+    for prec in ("fp64", "mixed"):
+        A.set_precision(prec)
+        for _ in range(args.warmup):
             A.matvec_device(dq.data_ptr(), dp.data_ptr(), 1, stream.cuda_stream)
-        e1.record(stream)
         torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
-    A.matvec(q)
-    chk = A.check_full(2000, seed=7)
-    A.set_profiling(True)
-    A.matvec_device(dq.data_ptr(), dp.data_ptr(), 1, stream.cuda_stream)
-    torch.cuda.synchronize()
-    phases = A.phase_times()
-    A.set_profiling(False)
-    line = {"metric": "FMM matvec points/s, mixed precision, spheroid", "impl": "ours",
-            "value": w.n / (ms * 1e-3), "unit": "points/s", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "dtype": "f32+f64",
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with Clocks(0) as ck:
+            e0.record(stream)
+            for _ in range(args.steps):
+                A.matvec_device(dq.data_ptr(), dp.data_ptr(), 1, stream.cuda_stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        p = A.matvec(q)
+        res[prec] = {"ms": ms, "points_per_s": w.n / (ms * 1e-3), "layout": A.info("layout"),
+                     "groups": A.info("groups"), "device_bytes": A.info("device_bytes"),
+                     "vs_direct_sum": A.check_full(2000, seed=7), "clocks": ck.summary(), "p": p}
+        A.set_profiling(True)
+        A.matvec_device(dq.data_ptr(), dp.data_ptr(), 1, stream.cuda_stream)
+        torch.cuda.synchronize()
+        res[prec]["phases_ms"] = A.phase_times()
+        A.set_profiling(False)
+    err = float(np.linalg.norm(res["mixed"]["p"] - res["fp64"]["p"]) / np.linalg.norm(res["fp64"]["p"]))
+    for r in res.values():
+        r.pop("p")
+    line = {"metric": "FMM matvec points/s, spheroid", "impl": "ours",
+            "value": res["mixed"]["points_per_s"], "unit": "points/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": res["mixed"]["ms"], "higher_is_better": True, "dtype": "f32+f64",
             "data": "synthetic",
             "config": {"workload": "spheroid4m", "n_points": w.n, "kappa": w.kappa, "order": w.order,
-                       "leaf_size": w.ncrit, "precision": "mixed",
-                       "fp64": "not run: M and L would need 230 GB"},
-            "accuracy": {"direct_sum_2000_targets": chk}, "clocks": ck.summary(), "phases_ms": phases,
-            "setup_s": setup_s, "device_bytes": A.info("device_bytes"),
+                       "leaf_size": w.ncrit},
+            "fp64": res["fp64"], "mixed": res["mixed"], "mixed_rel_l2_vs_fp64": err,
+            "speedup_mixed_vs_fp64": res["fp64"]["ms"] / res["mixed"]["ms"], "setup_s": setup_s,
             "plan": {k: info[k] for k in ["nlvl", "cpt", "slots_S", "slots_T", "far_hf", "near", "i_near",
                                           "tables", "permuted_spectra"]}}
+    print(json.dumps(line), flush=True)
+
+
+def run_mixture(args, torch):
+    """Mixture workload, N = 8,000,000: 40 % cube surface, 30 % sphere of
+    radius 0.4, 30 % Gaussian blobs (sigma 0.01-0.1), 512 wavelengths across
+    the cube diagonal, leaf size 96, FP32-representable charges.  For each
+    requested tolerance (1e-4, 1e-6, 1e-8) the order-selection network picks
+    the interpolation order (falling back to the fixed order 6 when it is not
+    confident below order 8); the mixed-precision matvec at that order runs
+    on whichever layout fits (the grouped layout when every expansion does
+    not), and FP64 direct sums at 2,000 seeded targets judge every result.
+    The plain FP64 path at the fixed order 6 is timed beside it."""
+    from defmm_b200 import DefmmError, IBFMM_Mat, workloads as W
+    from defmm_b200.learned import OrderModel
+    w = W.mixture(8_000_000, seed=0)
+    q = W.charges(w.n, 1).astype(np.complex64).astype(np.complex128)
+    model = OrderModel.load()
+    stream = torch.cuda.Stream()
+    dq = torch.from_numpy(q).to("cuda")
+    dp = torch.empty(w.n, dtype=torch.complex128, device="cuda")
+    runs = {}
+
+    def run(order, prec):
+        key = (order, prec)
+        if key in runs:
+            return runs[key]
+        A = IBFMM_Mat()
+        A.set_precision(prec)
+        A.addSourceParticles(w.points)
+        A.addTargetParticles(w.points)
+        t0 = time.perf_counter()
+        try:
+            A.prcmpt(order, w.ncrit, w.kappa)
+            setup = time.perf_counter() - t0
+            A.matvec_device(dq.data_ptr(), dp.data_ptr(), 1, stream.cuda_stream)
+            stream.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            steps = max(1, min(args.steps, 2))
+            e0.record(stream)
+            for _ in range(steps):
+                A.matvec_device(dq.data_ptr(), dp.data_ptr(), 1, stream.cuda_stream)
+            e1.record(stream)
+            stream.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+            A.matvec(q)
+            chk = A.check_full(2000, seed=7)
+            r = {"order": order, "precision": prec, "ms": ms, "points_per_s": w.n / (ms * 1e-3),
+                 "vs_direct_sum": chk, "prcmpt_s": setup, "layout": A.info("layout"), "groups": A.info("groups"),
+                 "device_bytes": A.info("device_bytes"),
+                 "plan": {k: A.info(k) for k in ("nlvl", "cpt", "slots_S", "far_hf", "far_lf", "near", "i_near",
+                                                  "permuted_spectra")}}
+        except DefmmError as ex:
+            r = {"order": order, "precision": prec, "not_run": str(ex)}
+        runs[key] = r
+        del A
+        torch.cuda.empty_cache()
+        return r
+
+    rows = []
+    for tol in (1e-4, 1e-6, 1e-8):
+        order, learned = model.choose(w.points, w.kappa, w.ncrit, tol)
+        r = run(order, "mixed")
+        rows.append({"tolerance": tol, "order": order, "learned": bool(learned),
+                     "met": bool("vs_direct_sum" in r and r["vs_direct_sum"]["l2"] <= tol), **r})
+    base = run(6, "fp64")
+    line = {"metric": "FMM matvec points/s, mixture, learned orders per tolerance", "impl": "ours",
+            "unit": "points/s", "n_gpus": 1, "data": "synthetic",
+            "config": {"workload": "mixture8m", "n_points": w.n, "kappa": w.kappa, "leaf_size": w.ncrit,
+                       "charges": "complex, FP32-representable"},
+            "tolerances": rows, "fp64_fixed_order6": base}
     print(json.dumps(line), flush=True)
 
 
@@ -520,7 +598,7 @@ def main():
             dist.barrier()
 
     extra = {"ragged48": run_ragged, "spheroid4m": run_spheroid, "spheroid_orders": run_orders,
-             "rhs64": run_rhs64}
+             "rhs64": run_rhs64, "mixture8m": run_mixture}
     if args.workload in extra:
         if rank == 0:
             extra[args.workload](args, torch)

@@ -200,8 +200,10 @@ class IBFMM_Mat:
         self._check(lib().defmm_set_launch(self._h, int(m2l_threads), int(p2p_blocks_per_sm)))
 
     def set_m2l_pairing(self, on=True):
-        """Two target slots per M2L CTA (current precision); results unchanged."""
-        self._check(lib().defmm_set_m2l_pairing(self._h, int(bool(on))))
+        """Target slots per M2L CTA (current precision): True / 1 two, 4 a
+        group of four walking their union list, False / 0 one; results
+        unchanged."""
+        self._check(lib().defmm_set_m2l_pairing(self._h, 4 if on == 4 else int(bool(on))))
 
     def set_blocking(self, rhs_block=16, groups=0):
         """Right-hand sides per pass of multi-RHS calls (1..32) and the number
@@ -301,6 +303,43 @@ class IBFMM_Mat:
         tab = np.zeros(n[1], np.uint32)
         self._check(lib().defmm_dump_m2l(self._h, ptr.ctypes.data, src.ctypes.data, tab.ctypes.data, n))
         return ptr, src, tab
+
+
+class MultiFreqMat:
+    """The reference's multi-frequency kernel (thetis_kernels.hpp:36)
+        G(R) = sum_{a in (1, 3.6, 2, 8)} exp(i (kappa / a) R) / (4 pi R),
+    applied as the sum of four Helmholtz operators, one per wavenumber, each
+    with the tree, cones and lists of its own wavenumber (the reference
+    defines the kernel but builds its transfer spectra and cones for one
+    Helmholtz wavenumber only, interface.hpp:127, M2L.hpp:181).  Same calls
+    as IBFMM_Mat for building and applying."""
+
+    DIVISORS = (1.0, 3.6, 2.0, 8.0)
+
+    def __init__(self):
+        self.parts = [IBFMM_Mat() for _ in self.DIVISORS]
+
+    def addSourceParticles(self, pts):
+        for A in self.parts:
+            A.addSourceParticles(pts)
+
+    def addTargetParticles(self, pts):
+        for A in self.parts:
+            A.addTargetParticles(pts)
+
+    def set_precision(self, mode):
+        for A in self.parts:
+            A.set_precision(mode)
+
+    def prcmpt(self, L, Ncrit, kappa, lvMAX=-1):
+        for A, a in zip(self.parts, self.DIVISORS):
+            A.prcmpt(L, Ncrit, kappa / a, lvMAX)
+
+    def matvec(self, q):
+        out = self.parts[0].matvec(q)
+        for A in self.parts[1:]:
+            out = out + A.matvec(q)
+        return out
 
 
 class Batch:
