@@ -200,10 +200,8 @@ class IBFMM_Mat:
         self._check(lib().defmm_set_launch(self._h, int(m2l_threads), int(p2p_blocks_per_sm)))
 
     def set_m2l_pairing(self, on=True):
-        """Target slots per M2L CTA (current precision): True / 1 two, 4 a
-        group of four walking their union list, False / 0 one; results
-        unchanged."""
-        self._check(lib().defmm_set_m2l_pairing(self._h, 4 if on == 4 else int(bool(on))))
+        """Two target slots per M2L CTA (current precision); results unchanged."""
+        self._check(lib().defmm_set_m2l_pairing(self._h, int(bool(on))))
 
     def set_blocking(self, rhs_block=16, groups=0):
         """Right-hand sides per pass of multi-RHS calls (1..32) and the number

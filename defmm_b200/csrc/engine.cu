@@ -115,15 +115,6 @@ struct defmm_handle {
   const int32_t *d_p2m_bylvl = nullptr, *d_l2p_bylvl = nullptr;
   std::vector<int64_t> p2m_lvl_off, l2p_lvl_off;  // nlvl + 1 offsets
   int l2p_max_points = 0;  // largest target leaf at a precomputed level
-  // M2L target groups (up to 4 consecutive target slots of a cone) with
-  // the union of their lists, built on the device when first used
-  bool grp_ready = false;
-  std::vector<int64_t> grp_t0_host;
-  const int64_t *d_grp_t0 = nullptr, *d_grp_ptr = nullptr;
-  const int32_t *d_grp_n = nullptr, *d_ent_src = nullptr;
-  const uint8_t* d_ent_mask = nullptr;
-  const uint4* d_ent_tab = nullptr;
-  int64_t grp_entries = 0;
   double phase_ms[PH_N] = {0};
   cudaEvent_t ev[2 * PH_N] = {};
   cudaEvent_t ev_ready = nullptr, ev_done = nullptr;  // cross-stream ordering
@@ -220,9 +211,6 @@ void free_grouped(defmm_handle* h) {
 
 void free_plan_device(defmm_handle* h) {
   drop_graph(h);
-  h->grp_ready = false;
-  h->grp_t0_host.clear();
-  h->grp_entries = 0;
   for (void* p : h->plan_allocs) cudaFree(p);
   h->plan_allocs.clear();
   free_buf(h->M);
@@ -660,70 +648,6 @@ void rec(defmm_handle* h, int i) {
   if (h->events) cudaEventRecord(h->ev[i], h->cur);
 }
 
-// Target groups of the M2L for the group kernel: every cone of every
-// precomputed level cut into runs of 4 consecutive target slots, with the
-// union of the runs' lists (source slot, target mask, 4 spectrum ids) built
-// on the device from the M2L CSR.  Allocates: call outside stream capture.
-int ensure_m2l_groups(defmm_handle* h) {
-  if (h->grp_ready) return 0;
-  Plan& p = h->plan;
-  std::vector<int64_t> t0;
-  std::vector<int32_t> gn;
-  for (int l = 0; l < p.lv.nlvl; l++) {
-    const auto& cT = p.sT.cone_begin[l];
-    for (size_t c = 0; c + 1 < cT.size(); c++)
-      for (int64_t a = cT[c]; a < cT[c + 1]; a += 4) {
-        t0.push_back(a);
-        gn.push_back((int32_t)std::min<int64_t>(4, cT[c + 1] - a));
-      }
-  }
-  const int64_t ng = (int64_t)t0.size();
-  int st;
-  if ((st = upload(h, t0, &h->d_grp_t0)) || (st = upload(h, gn, &h->d_grp_n))) return st;
-  std::vector<int64_t> ptr(ng + 1, 0);
-  if (ng) {
-    void* cnt = nullptr;
-    CK(cudaMalloc(&cnt, 8 * (size_t)ng));
-    dfb::launch_grp_lists(ng, h->d_grp_t0, h->d_grp_n, h->dp.m2l_ptr, h->dp.m2l_src, h->dp.m2l_tab, nullptr,
-                          (int64_t*)cnt, nullptr, nullptr, nullptr, h->st);
-    cudaError_t e = cudaMemcpyAsync(ptr.data() + 1, cnt, 8 * (size_t)ng, cudaMemcpyDeviceToHost, h->st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
-    cudaFree(cnt);
-    CK(e);
-    for (int64_t g = 0; g < ng; g++) ptr[g + 1] += ptr[g];
-  }
-  const int64_t ne = ptr[ng];
-  if ((st = upload(h, ptr, &h->d_grp_ptr))) return st;
-  void *src = nullptr, *mask = nullptr, *tab = nullptr;
-  CK(cudaMalloc(&src, 4 * (size_t)std::max<int64_t>(1, ne)));
-  h->plan_allocs.push_back(src);
-  CK(cudaMalloc(&mask, (size_t)std::max<int64_t>(1, ne)));
-  h->plan_allocs.push_back(mask);
-  CK(cudaMalloc(&tab, 16 * (size_t)std::max<int64_t>(1, ne)));
-  h->plan_allocs.push_back(tab);
-  h->dev_bytes += (size_t)ne * 21;
-  dfb::launch_grp_lists(ng, h->d_grp_t0, h->d_grp_n, h->dp.m2l_ptr, h->dp.m2l_src, h->dp.m2l_tab, h->d_grp_ptr,
-                        nullptr, (int32_t*)src, (uint8_t*)mask, (uint4*)tab, h->st);
-  CK(cudaStreamSynchronize(h->st));
-  h->d_ent_src = (const int32_t*)src;
-  h->d_ent_mask = (const uint8_t*)mask;
-  h->d_ent_tab = (const uint4*)tab;
-  h->grp_t0_host.swap(t0);
-  h->grp_entries = ne;
-  h->grp_ready = true;
-  return 0;
-}
-
-// M2L of target slots [ts0, ts1) (whole cones) through the group kernel.
-void m2l_groups(defmm_handle* h, int64_t ts0, int64_t ts1, int64_t fs0, int64_t fs1, int R, const void* F,
-                void* Lbase, cudaStream_t s) {
-  const auto& t0 = h->grp_t0_host;
-  const int64_t g0 = std::lower_bound(t0.begin(), t0.end(), ts0) - t0.begin();
-  const int64_t g1 = std::lower_bound(t0.begin(), t0.end(), ts1) - t0.begin();
-  h->ops->m2l_grp(h->dp, g0, g1, h->d_grp_t0, h->d_grp_n, h->d_grp_ptr, h->d_ent_src, h->d_ent_mask, h->d_ent_tab,
-                  fs0, fs1, R, R % 2 == 0 ? 2 : 1, F, h->ptab.p, Lbase, h->d_queue + 1, h->nsm, s);
-}
-
 // One matvec, everything on the device: qin (user order) -> out (user order).
 int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) {
   Plan& p = h->plan;
@@ -801,11 +725,8 @@ int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) 
         nl_ += 2;
         rec(h, 2 * PH_M2F + 1);
         rec(h, 2 * PH_M2L);
-        if (h->m2l_pair[fp64 ? 0 : 1] == 4 && h->grp_ready)
-          m2l_groups(h, ts0, ts1, fs0, fs1, 1, h->F.p, h->Lx.p, sf);
-        else
-          ops->m2l(d, ts0, ts1, fs0, fs1, h->F.p, h->ptab.p, h->Lx.p, h->d_queue + 1, h->nsm,
-                   h->m2l_nt[fp64 ? 0 : 1], h->m2l_pair[fp64 ? 0 : 1] == 1, sf);
+        ops->m2l(d, ts0, ts1, fs0, fs1, h->F.p, h->ptab.p, h->Lx.p, h->d_queue + 1, h->nsm, h->m2l_nt[fp64 ? 0 : 1],
+                 h->m2l_pair[fp64 ? 0 : 1], sf);
         rec(h, 2 * PH_M2L + 1);
         if (h->events) {
           float a;
@@ -970,11 +891,9 @@ int run_gemv_grouped(defmm_handle* h, const double2* qin, int64_t stride_in, dou
           ops->m2f((fs1 - fs0) * R, (const char*)Mbase + (size_t)fs0 * slot_b, g.F.p, s);
         });
         timed(PH_M2L, [&] {
-          if (h->m2l_pair[pi] == 4 && h->grp_ready)
-            m2l_groups(h, ts0, ts1, fs0, fs1, R, g.F.p, Lbase, s);
-          else if (R == 1)
+          if (R == 1)
             ops->m2l(d, ts0, ts1, fs0, fs1, g.F.p, h->ptab.p, Lbase, h->d_queue + 1, h->nsm, h->m2l_nt[pi],
-                     h->m2l_pair[pi] == 1, s);
+                     h->m2l_pair[pi], s);
           else
             ops->m2l_rhs(d, ts0, ts1, fs0, fs1, R, h->rhs_block_m2l, h->m2l_chunk_major, g.F.p, h->ptab.p, Lbase,
                          h->d_queue + 1, h->nsm, s);
@@ -1313,7 +1232,7 @@ int defmm_set_launch(defmm_handle* h, int m2l_threads, int p2p_blocks_per_sm) {
 }
 
 int defmm_set_m2l_pairing(defmm_handle* h, int on) {
-  if (!h || (on != 0 && on != 1 && on != 4)) return DEFMM_ERR_ARG;
+  if (!h || (on != 0 && on != 1)) return DEFMM_ERR_ARG;
   h->m2l_pair[h->precision == DEFMM_PRECISION_FP64 ? 0 : 1] = on;
   if (h->device >= 0) drop_graph(h);
   return 0;
@@ -1355,14 +1274,13 @@ int defmm_autotune(defmm_handle* h, int reps, int32_t* choice) {
   drop_graph(h);     // the captured graph holds the old launch choices
   // phases are serialised and timed separately in profiled matvecs, so one
   // matvec times one M2L candidate and one near-field candidate together:
-  // five matvecs (the M2L candidates: one or two target slots per CTA at 128
-  // or 256 threads, target groups of four) cover the three near-field ones
+  // four matvecs (the M2L candidates: one or two target slots per CTA at 128
+  // or 256 threads) cover the three near-field ones
   int m2l_best = 128, pair_best = 0, bps_best = 16;
   double tb_m2l = 1e300, tb_p2p = 1e300;
-  const int m2l_cand[5][2] = {{0, 128}, {0, 256}, {1, 128}, {1, 256}, {4, 0}};
+  const int m2l_cand[4][2] = {{0, 128}, {0, 256}, {1, 128}, {1, 256}};
   const int bps_cand[3] = {8, 16, 32};
-  if ((st = ensure_m2l_groups(h))) return st;
-  for (int i = 0; i < 5 && !st; i++) {
+  for (int i = 0; i < 4 && !st; i++) {
     h->m2l_pair[pi] = m2l_cand[i][0];
     h->m2l_nt[pi] = m2l_cand[i][1];
     const int b = bps_cand[i < 3 ? i : 2];
@@ -1479,7 +1397,6 @@ int defmm_gemv_device(defmm_handle* h, const void* d_in, void* d_out, int64_t nr
   if (st) return st;
   cudaStream_t s = stream ? (cudaStream_t)stream : h->st;
   h->launches = 0;
-  if (h->m2l_pair[h->precision == DEFMM_PRECISION_FP64 ? 0 : 1] == 4 && (st = ensure_m2l_groups(h))) return st;
   const int R = choose_rhs_block(h, nrhs);
   if (R > 0) return gemv_grouped(h, (const double2*)d_in, (double2*)d_out, nrhs, R, s);
   st = prepare_resident(h);
@@ -1609,7 +1526,6 @@ int defmm_gemv_batched(defmm_handle* h, int64_t nrhs, const double* in, double* 
   // direct sums still reading the previous charges (defmm_direct_noalloc on
   // another stream) finish before qin is overwritten
   CK(cudaStreamWaitEvent(h->st, h->ev_qin_read, 0));
-  if (h->m2l_pair[h->precision == DEFMM_PRECISION_FP64 ? 0 : 1] == 4 && (st = ensure_m2l_groups(h))) return st;
   const int R = choose_rhs_block(h, nrhs);
   if (R == 0) {
     if ((st = prepare_resident(h))) return st;

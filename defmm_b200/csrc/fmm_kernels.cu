@@ -1024,143 +1024,6 @@ __global__ void __launch_bounds__(NT, m2l_rhs_ctas<T, NT, RB>()) k_m2l_rhs(DevPl
   }
 }
 
-// Target groups: up to four consecutive target slots of one cone (grp_t0,
-// grp_n) with the union of their lists, sorted by source slot: entry e has
-// source slot ent_src[e], the targets that meet it as bits of ent_mask[e]
-// and their permuted-spectrum ids ent_tab[e] (4 ids, 0 where unused).  The
-// CTA loads each source spectrum once for the whole group and every
-// right-hand side block; each thread owns K frequency entries.  A target's
-// accumulator sees its own list in list order with the operations of
-// k_m2l / k_m2l_rhs, so the results are bit-identical to those kernels.
-template <typename T, int L, int NT, int K, int RB>
-__global__ void __launch_bounds__(NT, 1) k_m2l_grp(DevPlan P, int64_t g0, int64_t g1, const int64_t* __restrict__ grp_t0,
-                                                   const int32_t* __restrict__ grp_n,
-                                                   const int64_t* __restrict__ grp_ptr,
-                                                   const int32_t* __restrict__ ent_src,
-                                                   const uint8_t* __restrict__ ent_mask,
-                                                   const uint4* __restrict__ ent_tab, int64_t f0, int64_t f1, int R,
-                                                   const typename cpx_t<T>::type* __restrict__ F,
-                                                   const typename cpx_t<T>::type* __restrict__ ptab,
-                                                   typename cpx_t<T>::type* __restrict__ Lx,
-                                                   unsigned long long* __restrict__ queue) {
-  typedef typename cpx_t<T>::type C;
-  constexpr int PD = 2 * L - 1, LL = L * L * L, PP = PD * PD * PD;
-  static_assert(K * NT >= PP, "threads x entries must cover the spectrum");
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* Js = reinterpret_cast<C*>(smem_raw);
-  C* Cb = Js + PP;
-  C* D = Cb + L * PD * PD;
-  __shared__ int64_t cur;
-  const int nb = R / RB;
-  const int64_t nwork = (g1 - g0) * nb;
-  for (;;) {
-    __syncthreads();
-    if (threadIdx.x == 0) cur = (int64_t)atomicAdd(queue, 1ULL);
-    __syncthreads();
-    const int64_t w = cur;
-    if (w >= nwork) break;
-    const int64_t g = g0 + w / nb;
-    const int r0 = (int)(w % nb) * RB;
-    const int64_t t0 = grp_t0[g];
-    const int gn = grp_n[g];
-    C acc[4][RB][K];
-#pragma unroll
-    for (int a = 0; a < 4; a++)
-#pragma unroll
-      for (int b = 0; b < RB; b++)
-#pragma unroll
-        for (int k = 0; k < K; k++) acc[a][b][k] = czero<C>();
-    const int64_t eb = grp_ptr[g], ee = grp_ptr[g + 1];
-    for (int64_t e = eb; e < ee; e++) {
-      const int64_t src = ent_src[e];
-      const unsigned m = ent_mask[e];
-      const uint4 tb = ent_tab[e];
-      if (src < f0 || src >= f1) {  // entry outside this cone batch: a plan bug
-        if (threadIdx.x == 0) atomicExch(P.err, 1);
-        continue;
-      }
-      const C* Fs = F + ((src - f0) * R + r0) * PP;
-      C f[RB][K];
-#pragma unroll
-      for (int b = 0; b < RB; b++)
-#pragma unroll
-        for (int k = 0; k < K; k++) {
-          const int i = threadIdx.x + k * NT;
-          f[b][k] = i < PP ? __ldg(Fs + b * PP + i) : czero<C>();
-        }
-      const uint32_t tabs[4] = {tb.x, tb.y, tb.z, tb.w};
-#pragma unroll
-      for (int a = 0; a < 4; a++) {
-        if (!((m >> a) & 1u)) continue;  // uniform across the CTA
-        const C* U = ptab + (int64_t)tabs[a] * PP;
-#pragma unroll
-        for (int k = 0; k < K; k++) {
-          const int i = threadIdx.x + k * NT;
-          if (i < PP) {
-            const C u = __ldg(U + i);
-#pragma unroll
-            for (int b = 0; b < RB; b++) cfma(acc[a][b][k], u, f[b][k]);
-          }
-        }
-      }
-    }
-#pragma unroll
-    for (int a = 0; a < 4; a++) {
-      if (a >= gn) break;
-#pragma unroll
-      for (int b = 0; b < RB; b++) {
-        C v[K];
-#pragma unroll
-        for (int k = 0; k < K; k++) v[k] = acc[a][b][k];
-        m2l_f2l<T, L, NT>(v, Js, Cb, D, Lx + ((t0 + a) * R + r0 + b) * LL);
-      }
-    }
-  }
-}
-
-// Union lists of the target groups (one thread per group, merging the
-// groups' sorted lists): count pass (out_src == nullptr: cnt[g] = entries)
-// and fill pass (entries at ptr[g]).
-__global__ void k_grp_lists(int64_t ng, const int64_t* __restrict__ grp_t0, const int32_t* __restrict__ grp_n,
-                            const int64_t* __restrict__ m2l_ptr, const int32_t* __restrict__ m2l_src,
-                            const uint32_t* __restrict__ m2l_tab, const int64_t* __restrict__ ptr,
-                            int64_t* __restrict__ cnt, int32_t* __restrict__ out_src, uint8_t* __restrict__ out_mask,
-                            uint4* __restrict__ out_tab) {
-  const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (g >= ng) return;
-  const int64_t t0 = grp_t0[g];
-  const int n = grp_n[g];
-  int64_t pos[4], end[4];
-  for (int a = 0; a < 4; a++) {
-    pos[a] = a < n ? m2l_ptr[t0 + a] : 0;
-    end[a] = a < n ? m2l_ptr[t0 + a + 1] : 0;
-  }
-  int64_t k = out_src ? ptr[g] : 0, c = 0;
-  for (;;) {
-    int64_t s = INT64_MAX;
-    for (int a = 0; a < 4; a++)
-      if (pos[a] < end[a]) s = min(s, (int64_t)m2l_src[pos[a]]);
-    if (s == INT64_MAX) break;
-    unsigned m = 0;
-    uint32_t tb[4] = {0, 0, 0, 0};
-    for (int a = 0; a < 4; a++)
-      if (pos[a] < end[a] && (int64_t)m2l_src[pos[a]] == s) {
-        m |= 1u << a;
-        tb[a] = m2l_tab[pos[a]];
-        pos[a]++;
-      }
-    if (out_src) {
-      out_src[k] = (int32_t)s;
-      out_mask[k] = (uint8_t)m;
-      out_tab[k] = make_uint4(tb[0], tb[1], tb[2], tb[3]);
-      k++;
-    } else {
-      c++;
-    }
-  }
-  if (!out_src) cnt[g] = c;
-}
-
 // -------------------------------------------------------------------- L2P --
 // One CTA (4 warps) per target leaf at a precomputed level
 // (dwnpass.hpp:39-47): HF (phfL2P, L2P.hpp:122-142)
@@ -2186,11 +2049,6 @@ struct Launch {
     if ((e = rhs_attr<1, 128>()) != cudaSuccess || (e = rhs_attr<2, 128>()) != cudaSuccess ||
         (e = rhs_attr<4, 256>()) != cudaSuccess || (e = rhs_attr<8, 256>()) != cudaSuccess)
       return e;
-    if ((e = cudaFuncSetAttribute(k_m2l_grp<T, L, GNT, GK, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem_m2l())) != cudaSuccess ||
-        (e = cudaFuncSetAttribute(k_m2l_grp<T, L, GNT, GK, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem_m2l())) != cudaSuccess)
-      return e;
     return cudaSuccess;
   }
   // largest block of right-hand sides per M2L CTA: K x RB <= 24 complex
@@ -2276,31 +2134,6 @@ struct Launch {
     else
       k_m2l<T, L, 128><<<grid, 128, smem_m2l(), s>>>(dp, t0, t1, f0, f1, (const C*)F, (const C*)ptab, (C*)Lx, queue);
   }
-  // target-group M2L: K entries per thread at NT threads (K * NT >= PP)
-  static constexpr int GK = PP <= 1024 ? 1 : (PP + 767) / 768;
-  static constexpr int GNT = PP <= 1024 ? ((PP + 31) / 32) * 32 : 768;
-  template <int RB>
-  static void m2l_grp_go(const DevPlan& dp, int64_t g0, int64_t g1, const int64_t* t0, const int32_t* gn,
-                         const int64_t* gp, const int32_t* es, const uint8_t* em, const uint4* et, int64_t f0,
-                         int64_t f1, int R, const void* F, const void* ptab, void* Lx, unsigned long long* queue,
-                         int nsm, cudaStream_t s) {
-    const int64_t nwork = (g1 - g0) * (R / RB);
-    const int grid = (int)std::min<int64_t>(nwork, (int64_t)nsm);
-    k_m2l_grp<T, L, GNT, GK, RB><<<grid, GNT, smem_m2l(), s>>>(dp, g0, g1, t0, gn, gp, es, em, et, f0, f1, R,
-                                                                 (const C*)F, (const C*)ptab, (C*)Lx, queue);
-  }
-  // rb: right-hand sides per CTA (1 or 2; a divisor of R)
-  static void m2l_grp(const DevPlan& dp, int64_t g0, int64_t g1, const int64_t* t0, const int32_t* gn,
-                      const int64_t* gp, const int32_t* es, const uint8_t* em, const uint4* et, int64_t f0,
-                      int64_t f1, int R, int rb, const void* F, const void* ptab, void* Lx,
-                      unsigned long long* queue, int nsm, cudaStream_t s) {
-    if (g1 <= g0) return;
-    cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s);
-    if (rb >= 2 && R % 2 == 0 && GK == 1)
-      m2l_grp_go<2>(dp, g0, g1, t0, gn, gp, es, em, et, f0, f1, R, F, ptab, Lx, queue, nsm, s);
-    else
-      m2l_grp_go<1>(dp, g0, g1, t0, gn, gp, es, em, et, f0, f1, R, F, ptab, Lx, queue, nsm, s);
-  }
   static void permute(int64_t n, const uint32_t* key, const uint16_t* perm, const void* tables, void* out,
                       cudaStream_t s) {
     if (n) k_permute_tables<T><<<grid_for(n, 1), 256, 0, s>>>(n, PP, key, perm, (const C*)tables, (C*)out);
@@ -2323,8 +2156,7 @@ const OpTable* op_table_for(int L);
 #define DFB_OPS(T, L)                                                                                     \
   {                                                                                                       \
     Launch<T, L>::setup, Launch<T, L>::p2m, Launch<T, L>::m2m, Launch<T, L>::l2l, Launch<T, L>::m2f,       \
-        Launch<T, L>::m2l, Launch<T, L>::m2l_rhs, Launch<T, L>::m2l_grp, Launch<T, L>::l2p,                 \
-        Launch<T, L>::permute,                                                                            \
+        Launch<T, L>::m2l, Launch<T, L>::m2l_rhs, Launch<T, L>::l2p, Launch<T, L>::permute,                 \
         Launch<T, L>::kMaxRB                                                                              \
   }
 
@@ -2484,14 +2316,6 @@ void launch_gather_rhs(bool fp64, const double2* qin, const int32_t* perm, void*
 void launch_scatter_rhs(const double2* pnear, const double2* pfar, const int32_t* perm, double2* out, int64_t n,
                         int64_t stride, int R, int nvec, cudaStream_t s) {
   k_scatter_rhs<<<(int)((n * R + 255) / 256), 256, 0, s>>>(pnear, pfar, perm, out, n, stride, R, nvec);
-}
-
-void launch_grp_lists(int64_t ng, const int64_t* grp_t0, const int32_t* grp_n, const int64_t* m2l_ptr,
-                      const int32_t* m2l_src, const uint32_t* m2l_tab, const int64_t* ptr, int64_t* cnt,
-                      int32_t* out_src, uint8_t* out_mask, uint4* out_tab, cudaStream_t s) {
-  if (ng <= 0) return;
-  k_grp_lists<<<(unsigned)((ng + 127) / 128), 128, 0, s>>>(ng, grp_t0, grp_n, m2l_ptr, m2l_src, m2l_tab, ptr, cnt,
-                                                           out_src, out_mask, out_tab);
 }
 
 void launch_direct(int64_t ns, const double* spos, const int32_t* sperm, const double2* qin, int64_t nt,

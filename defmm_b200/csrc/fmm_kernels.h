@@ -39,14 +39,6 @@ struct OpTable {
   // (chunk_major: every target slot for one block, then the next block)
   void (*m2l_rhs)(const DevPlan&, int64_t t0, int64_t t1, int64_t f0, int64_t f1, int R, int rb, bool chunk_major,
                   const void* F, const void* ptab, void* Lx, unsigned long long* queue, int nsm, cudaStream_t);
-  // M2L over target groups [g0, g1) (up to 4 consecutive target slots of a
-  // cone each, with the union of their lists; see launch_grp_lists), R
-  // right-hand sides, rb (1 or 2) per CTA; each source spectrum load serves
-  // every target of the group that meets it
-  void (*m2l_grp)(const DevPlan&, int64_t g0, int64_t g1, const int64_t* grp_t0, const int32_t* grp_n,
-                  const int64_t* grp_ptr, const int32_t* ent_src, const uint8_t* ent_mask, const uint4* ent_tab,
-                  int64_t f0, int64_t f1, int R, int rb, const void* F, const void* ptab, void* Lx,
-                  unsigned long long* queue, int nsm, cudaStream_t);
   // L2P of the leaves' slots with a direction in [d0, d1) into pfar (R per
   // particle), written (accum = false) or added
   void (*l2p)(const DevPlan&, const int32_t* leaves, int n, const void* sig2, const void* Lx, double2* pfar, int R,
@@ -112,12 +104,6 @@ void launch_gather_rhs(bool fp64, const double2* qin, const int32_t* perm, void*
                        int nvec, cudaStream_t s);
 void launch_scatter_rhs(const double2* pnear, const double2* pfar, const int32_t* perm, double2* out, int64_t n,
                         int64_t stride, int R, int nvec, cudaStream_t s);
-// Union lists of target groups from the M2L CSR: with out_src == nullptr,
-// cnt[g] = the group's distinct source slots; else the entries (source slot,
-// target mask, 4 permuted-spectrum ids) are written from ptr[g] on.
-void launch_grp_lists(int64_t ng, const int64_t* grp_t0, const int32_t* grp_n, const int64_t* m2l_ptr,
-                      const int32_t* m2l_src, const uint32_t* m2l_tab, const int64_t* ptr, int64_t* cnt,
-                      int32_t* out_src, uint8_t* out_mask, uint4* out_tab, cudaStream_t s);
 void launch_direct(int64_t ns, const double* spos, const int32_t* sperm, const double2* qin, int64_t nt,
                    const double* tpos, double kappa, double2* out, cudaStream_t s);
 

@@ -210,7 +210,7 @@ int defmm_probe_l2_read(int64_t bytes, int reps, double* gbs);
 #define DEFMM_INFO_PLAN_WALK_MS 22     /* of which the level walk, ms */
 #define DEFMM_INFO_M2L_THREADS 23      /* M2L threads per target slot (current precision) */
 #define DEFMM_INFO_P2P_BLOCKS_PER_SM 24 /* near-field CTAs per SM (current precision) */
-#define DEFMM_INFO_M2L_PAIRING 25       /* target slots per M2L CTA: 0 one, 1 two, 4 groups of four */
+#define DEFMM_INFO_M2L_PAIRING 25       /* 1: two target slots per M2L CTA (current precision) */
 #define DEFMM_INFO_LAYOUT 26            /* 0 none yet, 1 resident, 2 grouped */
 #define DEFMM_INFO_RHS_BLOCK 27         /* right-hand sides per pass of the grouped layout */
 #define DEFMM_INFO_GROUPS 28            /* direction groups of the grouped layout */
@@ -253,9 +253,9 @@ int defmm_set_plan_device(defmm_handle* h, int on);
 /* No counterpart in the reference.  Autotuner: on this operator and its
  * current precision, times `reps` profiled matvecs (zero charges, the
  * handle's own vectors) per candidate launch choice and keeps the fastest:
- * M2L threads per CTA (128 or 256) with one or two target slots per CTA, or
- * target groups of four (timed on the M2L phase) and near-field CTAs per SM
- * (8, 16 or 32, timed on the near-field phase).  Every choice gives bit-identical results.  The
+ * M2L threads per CTA (128 or 256) with one or two target slots per CTA
+ * (timed on the M2L phase) and near-field CTAs per SM (8, 16 or 32, timed on
+ * the near-field phase).  Every choice gives bit-identical results.  The
  * M2L threads and near-field CTAs per SM are written to choice[2] when not
  * NULL (also DEFMM_INFO_M2L_THREADS / DEFMM_INFO_P2P_BLOCKS_PER_SM; the
  * pairing: DEFMM_INFO_M2L_PAIRING); the next matvec captures a new graph. */
@@ -266,10 +266,7 @@ int defmm_autotune(defmm_handle* h, int reps, int32_t* choice);
 int defmm_set_launch(defmm_handle* h, int m2l_threads, int p2p_blocks_per_sm);
 /* No counterpart in the reference.  on = 1: each M2L CTA takes two
  * consecutive target slots and reads a source spectrum the two share once
- * (current precision); 4: each CTA takes a group of up to four consecutive
- * target slots of one cone and walks the union of their lists (built on the
- * device at the first use), loading every source spectrum once for the
- * group; 0: one slot per CTA.  Results are bit-identical for every choice. */
+ * (current precision); 0: one slot per CTA. */
 int defmm_set_m2l_pairing(defmm_handle* h, int on);
 
 /* Tree dump in the layout of the reference's cell array (SourceRoot /
