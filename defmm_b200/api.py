@@ -213,9 +213,9 @@ class IBFMM_Mat:
         """Mixed precision: P2M on the tensor cores (tcgen05, split TF32)."""
         self._check(lib().defmm_set_tensor_cores(self._h, int(bool(on))))
 
-    def set_rhs_per_cta(self, rb=8):
+    def set_rhs_per_cta(self, rb=4):
         """Right-hand sides per M2L CTA of the grouped layout (1, 2, 4, 8;
-        negative: the same, work ordered block by block)."""
+        -1, -2, -4: two target slots per CTA sharing source loads)."""
         self._check(lib().defmm_set_rhs_per_cta(self._h, int(rb)))
 
     def set_profiling(self, on=True):

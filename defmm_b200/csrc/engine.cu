@@ -108,7 +108,6 @@ struct defmm_handle {
   int rhs_block = 16;     // right-hand sides per pass of multi-RHS calls
   int rhs_block_m2l = 4;  // right-hand sides per M2L CTA (capped by the order)
   bool use_tc = false;    // mixed precision: P2M on the tensor cores (tcgen05)
-  bool m2l_chunk_major = false;  // grouped M2L: target slots inner, right-hand-side blocks outer
   int groups_forced = 0;  // > 0: direction groups requested (also for one RHS)
   int groups_used = 0;    // groups of the last grouped pass
   // leaves at precomputed levels sorted by level (P2M: sources, L2P: targets)
@@ -895,8 +894,8 @@ int run_gemv_grouped(defmm_handle* h, const double2* qin, int64_t stride_in, dou
             ops->m2l(d, ts0, ts1, fs0, fs1, g.F.p, h->ptab.p, Lbase, h->d_queue + 1, h->nsm, h->m2l_nt[pi],
                      h->m2l_pair[pi], s);
           else
-            ops->m2l_rhs(d, ts0, ts1, fs0, fs1, R, h->rhs_block_m2l, h->m2l_chunk_major, g.F.p, h->ptab.p, Lbase,
-                         h->d_queue + 1, h->nsm, s);
+            ops->m2l_rhs(d, ts0, ts1, fs0, fs1, R, h->rhs_block_m2l, g.F.p, h->ptab.p, Lbase, h->d_queue + 1,
+                         h->nsm, s);
         });
         nk += 2;
       }
@@ -1427,10 +1426,8 @@ int defmm_set_tensor_cores(defmm_handle* h, int on) {
 }
 
 int defmm_set_rhs_per_cta(defmm_handle* h, int rb) {
-  if (!h || (rb != 1 && rb != 2 && rb != 4 && rb != 8 && rb != -1 && rb != -2 && rb != -4 && rb != -8))
-    return DEFMM_ERR_ARG;
-  h->rhs_block_m2l = rb < 0 ? -rb : rb;
-  h->m2l_chunk_major = rb < 0;
+  if (!h || (rb != 1 && rb != 2 && rb != 4 && rb != 8 && rb != -1 && rb != -2 && rb != -4)) return DEFMM_ERR_ARG;
+  h->rhs_block_m2l = rb;
   return 0;
 }
 
@@ -1646,9 +1643,17 @@ int defmm_info(const defmm_handle* h, int what, int64_t* v) {
     case DEFMM_INFO_TREE_DEVICE: *v = p.tree_on_device ? 1 : 0; break;
     case DEFMM_INFO_RHS_PER_CTA: {  // the block the M2L launcher uses for the grouped layout's R
       const int R = h->layout == 2 ? h->gl.R : 1;
-      int rb = std::min(h->rhs_block_m2l, h->ops ? h->ops->max_rb : 1);
-      while (rb > 1 && R % rb) rb >>= 1;
-      *v = rb;
+      const int mx = h->ops ? h->ops->max_rb : 1;
+      int rb = h->rhs_block_m2l;
+      if (rb < 0) {  // two target slots per work item
+        rb = -rb;
+        while (rb > 1 && (R % rb || 2 * rb > mx)) rb >>= 1;
+        *v = -rb;
+      } else {
+        rb = std::min(rb, mx);
+        while (rb > 1 && R % rb) rb >>= 1;
+        *v = rb;
+      }
       break;
     }
     case DEFMM_INFO_TREE_MS: *v = (int64_t)(1e3 * p.t_tree); break;
