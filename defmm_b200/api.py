@@ -214,8 +214,7 @@ class IBFMM_Mat:
         self._check(lib().defmm_set_tensor_cores(self._h, int(bool(on))))
 
     def set_rhs_per_cta(self, rb=4):
-        """Right-hand sides per M2L CTA of the grouped layout (1, 2, 4, 8;
-        -1, -2, -4: two target slots per CTA sharing source loads)."""
+        """Right-hand sides per M2L CTA of the grouped layout (1, 2, 4, 8)."""
         self._check(lib().defmm_set_rhs_per_cta(self._h, int(rb)))
 
     def set_profiling(self, on=True):

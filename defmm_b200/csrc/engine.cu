@@ -1426,7 +1426,7 @@ int defmm_set_tensor_cores(defmm_handle* h, int on) {
 }
 
 int defmm_set_rhs_per_cta(defmm_handle* h, int rb) {
-  if (!h || (rb != 1 && rb != 2 && rb != 4 && rb != 8 && rb != -1 && rb != -2 && rb != -4)) return DEFMM_ERR_ARG;
+  if (!h || (rb != 1 && rb != 2 && rb != 4 && rb != 8)) return DEFMM_ERR_ARG;
   h->rhs_block_m2l = rb;
   return 0;
 }
@@ -1643,17 +1643,9 @@ int defmm_info(const defmm_handle* h, int what, int64_t* v) {
     case DEFMM_INFO_TREE_DEVICE: *v = p.tree_on_device ? 1 : 0; break;
     case DEFMM_INFO_RHS_PER_CTA: {  // the block the M2L launcher uses for the grouped layout's R
       const int R = h->layout == 2 ? h->gl.R : 1;
-      const int mx = h->ops ? h->ops->max_rb : 1;
-      int rb = h->rhs_block_m2l;
-      if (rb < 0) {  // two target slots per work item
-        rb = -rb;
-        while (rb > 1 && (R % rb || 2 * rb > mx)) rb >>= 1;
-        *v = -rb;
-      } else {
-        rb = std::min(rb, mx);
-        while (rb > 1 && R % rb) rb >>= 1;
-        *v = rb;
-      }
+      int rb = std::min(h->rhs_block_m2l, h->ops ? h->ops->max_rb : 1);
+      while (rb > 1 && R % rb) rb >>= 1;
+      *v = rb;
       break;
     }
     case DEFMM_INFO_TREE_MS: *v = (int64_t)(1e3 * p.t_tree); break;

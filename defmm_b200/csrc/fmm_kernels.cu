@@ -1021,95 +1021,6 @@ __global__ void __launch_bounds__(NT, m2l_rhs_ctas<T, NT, RB>()) k_m2l_rhs(DevPl
   }
 }
 
-// The block kernel with two consecutive target slots per work item (as
-// k_m2l_pair): a source spectrum block the two slots share is loaded once
-// for both.  Same operations per accumulator as k_m2l_rhs: bit-identical.
-template <typename T, int L, int NT, int RB>
-__global__ void __launch_bounds__(NT, m2l_rhs_ctas<T, NT, 2 * RB>()) k_m2l_rhs_pair(
-    DevPlan P, int64_t t0, int64_t t1, int64_t f0, int64_t f1, int R, const typename cpx_t<T>::type* __restrict__ F,
-    const typename cpx_t<T>::type* __restrict__ ptab, typename cpx_t<T>::type* __restrict__ Lx,
-    unsigned long long* __restrict__ queue) {
-  typedef typename cpx_t<T>::type C;
-  constexpr int PD = 2 * L - 1, LL = L * L * L, PP = PD * PD * PD, K = (PP + NT - 1) / NT;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* Js = reinterpret_cast<C*>(smem_raw);
-  C* Cb = Js + PP;
-  C* D = Cb + L * PD * PD;
-  __shared__ int64_t cur;
-  const int nb = R / RB;
-  const int64_t npair = (t1 - t0 + 1) / 2;
-  const int64_t nwork = npair * nb;
-  for (;;) {
-    __syncthreads();
-    if (threadIdx.x == 0) cur = (int64_t)atomicAdd(queue, 1ULL);
-    __syncthreads();
-    const int64_t w = cur;
-    if (w >= nwork) break;
-    const int64_t t = t0 + 2 * (w / nb);
-    const int r0 = (int)(w % nb) * RB;
-    const bool two = t + 1 < t1;
-    int64_t a = P.m2l_ptr[t], b = P.m2l_ptr[t + 1];
-    const int64_t ae = b, be = two ? P.m2l_ptr[t + 2] : b;
-    C acc0[K][RB], acc1[K][RB];
-#pragma unroll
-    for (int k = 0; k < K; k++)
-#pragma unroll
-      for (int r = 0; r < RB; r++) acc0[k][r] = acc1[k][r] = czero<C>();
-    while (a < ae || b < be) {
-      const int64_t sa = a < ae ? (int64_t)P.m2l_src[a] : INT64_MAX;
-      const int64_t sb = b < be ? (int64_t)P.m2l_src[b] : INT64_MAX;
-      const int64_t src = sa < sb ? sa : sb;
-      if (src < f0 || src >= f1) {  // entry outside this cone batch: a plan bug
-        if (threadIdx.x == 0) atomicExch(P.err, 1);
-        if (sa == src) a++;
-        if (sb == src) b++;
-        continue;
-      }
-      const C* Fs = F + ((src - f0) * R + r0) * PP;
-      const bool use0 = sa == src, use1 = sb == src;
-      const C* U0 = ptab + (int64_t)P.m2l_tab[use0 ? a : b] * PP;
-      const C* U1 = ptab + (int64_t)P.m2l_tab[use1 ? b : a] * PP;
-#pragma unroll
-      for (int k = 0; k < K; k++) {
-        const int i = threadIdx.x + k * NT;
-        if (i < PP) {
-          C f[RB];
-#pragma unroll
-          for (int r = 0; r < RB; r++) f[r] = __ldg(Fs + r * PP + i);
-          if (use0) {
-            const C u = __ldg(U0 + i);
-#pragma unroll
-            for (int r = 0; r < RB; r++) cfma(acc0[k][r], u, f[r]);
-          }
-          if (use1) {
-            const C u = __ldg(U1 + i);
-#pragma unroll
-            for (int r = 0; r < RB; r++) cfma(acc1[k][r], u, f[r]);
-          }
-        }
-      }
-      if (use0) a++;
-      if (use1) b++;
-    }
-#pragma unroll
-    for (int r = 0; r < RB; r++) {
-      C v[K];
-#pragma unroll
-      for (int k = 0; k < K; k++) v[k] = acc0[k][r];
-      m2l_f2l<T, L, NT>(v, Js, Cb, D, Lx + (t * R + r0 + r) * LL);
-    }
-    if (two) {
-#pragma unroll
-      for (int r = 0; r < RB; r++) {
-        C v[K];
-#pragma unroll
-        for (int k = 0; k < K; k++) v[k] = acc1[k][r];
-        m2l_f2l<T, L, NT>(v, Js, Cb, D, Lx + ((t + 1) * R + r0 + r) * LL);
-      }
-    }
-  }
-}
-
 // -------------------------------------------------------------------- L2P --
 // One CTA (4 warps) per target leaf at a precomputed level
 // (dwnpass.hpp:39-47): HF (phfL2P, L2P.hpp:122-142)
@@ -2133,9 +2044,7 @@ struct Launch {
                              (int)P2MCfg<T, L>::smem(kMaxRhsBlock));
     if (e != cudaSuccess) return e;
     if ((e = rhs_attr<1, 128>()) != cudaSuccess || (e = rhs_attr<2, 128>()) != cudaSuccess ||
-        (e = rhs_attr<4, 256>()) != cudaSuccess || (e = rhs_attr<8, 256>()) != cudaSuccess ||
-        (e = rhs_pair_attr<1, 128>()) != cudaSuccess || (e = rhs_pair_attr<2, 256>()) != cudaSuccess ||
-        (e = rhs_pair_attr<4, 256>()) != cudaSuccess)
+        (e = rhs_attr<4, 256>()) != cudaSuccess || (e = rhs_attr<8, 256>()) != cudaSuccess)
       return e;
     return cudaSuccess;
   }
@@ -2157,41 +2066,13 @@ struct Launch {
     k_m2l_rhs<T, L, NT, RBE><<<grid, NT, smem_m2l(), s>>>(dp, t0, t1, f0, f1, R, (const C*)F, (const C*)ptab,
                                                           (C*)Lx, queue);
   }
-  template <int RB, int NT>
-  static void m2l_rhs_pair_go(const DevPlan& dp, int64_t t0, int64_t t1, int64_t f0, int64_t f1, int R,
-                              const void* F, const void* ptab, void* Lx, unsigned long long* queue, int nsm,
-                              cudaStream_t s) {
-    constexpr int RBE = 2 * RB <= kMaxRB ? RB : 1;
-    const int64_t nwork = (t1 - t0 + 1) / 2 * (R / RBE);
-    const int grid = (int)std::min<int64_t>(nwork, (int64_t)nsm * m2l_rhs_ctas<T, NT, 2 * RBE>());
-    k_m2l_rhs_pair<T, L, NT, RBE><<<grid, NT, smem_m2l(), s>>>(dp, t0, t1, f0, f1, R, (const C*)F, (const C*)ptab,
-                                                               (C*)Lx, queue);
-  }
-  template <int RB, int NT>
-  static cudaError_t rhs_pair_attr() {
-    constexpr int RBE = 2 * RB <= kMaxRB ? RB : 1;
-    return cudaFuncSetAttribute(k_m2l_rhs_pair<T, L, NT, RBE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem_m2l());
-  }
   // M2L for R right-hand sides in blocks of rb (1, 2, 4 or 8; a divisor of
-  // R, capped by the order's kMaxRB); rb < 0: two target slots per work
-  // item and -rb right-hand sides, sharing the source loads
+  // R, capped by the order's kMaxRB)
   static void m2l_rhs(const DevPlan& dp, int64_t t0, int64_t t1, int64_t f0, int64_t f1, int R, int rb,
                       const void* F, const void* ptab, void* Lx, unsigned long long* queue, int nsm,
                       cudaStream_t s) {
     if (t1 <= t0) return;
     cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s);
-    if (rb < 0) {  // two target slots per work item, -rb right-hand sides
-      int pr = -rb;
-      while (pr > 1 && (R % pr || 2 * pr > kMaxRB)) pr >>= 1;
-      if (pr >= 4)
-        m2l_rhs_pair_go<4, 256>(dp, t0, t1, f0, f1, R, F, ptab, Lx, queue, nsm, s);
-      else if (pr >= 2)
-        m2l_rhs_pair_go<2, 256>(dp, t0, t1, f0, f1, R, F, ptab, Lx, queue, nsm, s);
-      else
-        m2l_rhs_pair_go<1, 128>(dp, t0, t1, f0, f1, R, F, ptab, Lx, queue, nsm, s);
-      return;
-    }
     if (rb > kMaxRB) rb = kMaxRB;
     while (rb > 1 && R % rb) rb >>= 1;
     if (rb >= 8)
@@ -2367,11 +2248,7 @@ void launch_p2p_reduce(bool fp64, int64_t nleaf, const int32_t* first, const int
 
 cudaError_t setup_rhs_kernels() {
   cudaError_t e;
-  if ((e = cudaFuncSetAttribute(k_p2p_rhs<true, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)P2PRhsCfg<true, 16>::smem())) != cudaSuccess ||
-      (e = cudaFuncSetAttribute(k_p2p_rhs<false, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)P2PRhsCfg<false, 16>::smem())) != cudaSuccess ||
-      (e = cudaFuncSetAttribute(k_p2p_rhs<true, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  if ((e = cudaFuncSetAttribute(k_p2p_rhs<true, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)P2PRhsCfg<true, 8>::smem())) != cudaSuccess ||
       (e = cudaFuncSetAttribute(k_p2p_rhs<false, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)P2PRhsCfg<false, 8>::smem())) != cudaSuccess ||
@@ -2400,12 +2277,9 @@ void launch_p2p_rhs(bool fp64, const DevPlan& dp, int64_t nitem, const int32_t* 
   const int grid = (int)std::min<int64_t>(nitem, (int64_t)nsm * std::max(1, std::min(blocks_per_sm, 64)));
   for (int r0 = 0; r0 < R;) {
     const int left = R - r0;
-    const int rb = left >= 16 ? 16 : (left >= 8 ? 8 : (left >= 4 ? 4 : 1));
+    const int rb = left >= 8 ? 8 : (left >= 4 ? 4 : 1);
     cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s);
-    if (rb == 16) {
-      if (fp64) p2p_rhs_go<false, 16>(dp, nitem, order, item_chunk, tfirst, tn, ptr, sfirst, sn, q, R, r0, pnear, tpart, queue, grid, s);
-      else p2p_rhs_go<true, 16>(dp, nitem, order, item_chunk, tfirst, tn, ptr, sfirst, sn, q, R, r0, pnear, tpart, queue, grid, s);
-    } else if (rb == 8) {
+    if (rb == 8) {
       if (fp64) p2p_rhs_go<false, 8>(dp, nitem, order, item_chunk, tfirst, tn, ptr, sfirst, sn, q, R, r0, pnear, tpart, queue, grid, s);
       else p2p_rhs_go<true, 8>(dp, nitem, order, item_chunk, tfirst, tn, ptr, sfirst, sn, q, R, r0, pnear, tpart, queue, grid, s);
     } else if (rb == 4) {

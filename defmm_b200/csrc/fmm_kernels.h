@@ -36,7 +36,6 @@ struct OpTable {
               void* Lx, unsigned long long* queue, int nsm, int nt, int pair, cudaStream_t);
   // The same for R right-hand sides (F: R spectra per source slot of the
   // batch, Lx: base as above), rb of them per CTA sharing each spectrum load
-  // (rb < 0: two target slots per CTA, -rb right-hand sides)
   void (*m2l_rhs)(const DevPlan&, int64_t t0, int64_t t1, int64_t f0, int64_t f1, int R, int rb, const void* F,
                   const void* ptab, void* Lx, unsigned long long* queue, int nsm, cudaStream_t);
   // L2P of the leaves' slots with a direction in [d0, d1) into pfar (R per

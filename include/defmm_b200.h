@@ -118,10 +118,8 @@ int defmm_set_tensor_cores(defmm_handle* h, int on);
 /* No counterpart in the reference.  Right-hand sides per M2L CTA of the
  * grouped layout (1, 2, 4, 8, default 4; capped by the order's register
  * budget and a divisor of the pass's right-hand sides): each
- * transfer-spectrum entry is read once for them.  A negative value (-1, -2,
- * -4) gives each CTA two consecutive target slots and -rb right-hand sides,
- * loading a source spectrum block the two slots share once.  Results are
- * bit-identical for every choice. */
+ * transfer-spectrum entry is read once for them.  Results are bit-identical
+ * for every choice. */
 int defmm_set_rhs_per_cta(defmm_handle* h, int rb);
 
 /* No counterpart in the reference.  Independent operators (handles of
@@ -222,7 +220,7 @@ int defmm_probe_l2_read(int64_t bytes, int reps, double* gbs);
 #define DEFMM_INFO_TENSOR_CORES 34      /* 1: mixed-precision P2M and L2P run on the tensor cores */
 #define DEFMM_INFO_TREE_DEVICE 35       /* 1 if prcmpt ordered the octrees' particles on the GPU */
 #define DEFMM_INFO_TREE_MS 36           /* prcmpt's octree build, ms */
-#define DEFMM_INFO_RHS_PER_CTA 37       /* right-hand sides per M2L CTA of the grouped layout (< 0: two target slots) */
+#define DEFMM_INFO_RHS_PER_CTA 37       /* right-hand sides per M2L CTA of the grouped layout */
 int defmm_info(const defmm_handle* h, int what, int64_t* value);
 
 /* Per-phase device times (ms) of the last gemv, in this order:

@@ -52,7 +52,7 @@ def test_argument_checks_without_device():
         with pytest.raises(api.DefmmError):
             A.set_blocking(rb, g)
     A.set_blocking(8, 3)
-    for rb in (0, 3, 16, -8):
+    for rb in (0, 3, 16, -4):
         with pytest.raises(api.DefmmError):
             A.set_rhs_per_cta(rb)
     A.set_rhs_per_cta(4)

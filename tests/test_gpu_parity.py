@@ -255,7 +255,7 @@ def test_rhs_blocks_do_not_change_any_right_hand_side(gpu):
         ref = np.stack([A.matvec(Q[r]) for r in range(5)])
         assert A.info("groups") >= 3
         for rb in (2, 4):
-            for per_cta in (1, 2, 4, 8, -1, -2, -4):
+            for per_cta in (1, 2, 4, 8):
                 A.set_blocking(rb, 4)
                 A.set_rhs_per_cta(per_cta)
                 P = A.matvec(Q)
