@@ -53,6 +53,8 @@ def workload(name, rank=0):
         return W.sphere_surface(100_000, seed=0, wavelengths=32)
     if name == "sphere200k":  # config-2 points per wavelength^2, for profiling
         return W.sphere_surface(200_000, seed=0, wavelengths=40)
+    if name == "sphere31k":  # the CPU sample of sphere2m; a few GB on the device, for ncu captures
+        return W.sphere_surface(2_000_000 // 64, seed=0, wavelengths=128 / 8)
     if name == "cube20k":
         return W.cube_surface(20_000, seed=0)
     raise KeyError(name)
@@ -396,10 +398,15 @@ def run_spheroid(args, torch):
     print(json.dumps(line), flush=True)
 
 
+MIXTURES = {"mixture8m": 8_000_000, "mixture2m": 2_000_000, "mixture1m": 1_000_000}
+
+
 def run_mixture(args, torch):
     """Mixture workload, N = 8,000,000: 40 % cube surface, 30 % sphere of
     radius 0.4, 30 % Gaussian blobs (sigma 0.01-0.1), 512 wavelengths across
-    the cube diagonal, leaf size 96, FP32-representable charges.  For each
+    the cube diagonal, leaf size 96, FP32-representable charges
+    (mixture2m / mixture1m: 2,000,000 / 1,000,000 points at the same points
+    per wavelength squared, 256 / 181 wavelengths).  For each
     requested tolerance (1e-4, 1e-6, 1e-8) the order-selection network picks
     the interpolation order (falling back to the fixed order 6 when it is not
     confident below order 8); the mixed-precision matvec at that order runs
@@ -408,7 +415,8 @@ def run_mixture(args, torch):
     The plain FP64 path at the fixed order 6 is timed beside it."""
     from defmm_b200 import DefmmError, IBFMM_Mat, workloads as W
     from defmm_b200.learned import OrderModel
-    w = W.mixture(8_000_000, seed=0)
+    n = MIXTURES[args.workload]
+    w = W.mixture(n, seed=0, wavelengths=512.0 * math.sqrt(n / 8_000_000))
     q = W.charges(w.n, 1).astype(np.complex64).astype(np.complex128)
     model = OrderModel.load()
     stream = torch.cuda.Stream()
@@ -461,7 +469,7 @@ def run_mixture(args, torch):
     base = run(6, "fp64")
     line = {"metric": "FMM matvec points/s, mixture, learned orders per tolerance", "impl": "ours",
             "unit": "points/s", "n_gpus": 1, "data": "synthetic",
-            "config": {"workload": "mixture8m", "n_points": w.n, "kappa": w.kappa, "leaf_size": w.ncrit,
+            "config": {"workload": args.workload, "n_points": w.n, "kappa": w.kappa, "leaf_size": w.ncrit,
                        "charges": "complex, FP32-representable"},
             "tolerances": rows, "fp64_fixed_order6": base}
     print(json.dumps(line), flush=True)
@@ -574,6 +582,10 @@ def main():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--rhs-block", type=int, default=16)
     ap.add_argument("--nrhs", type=int, default=8, help="right-hand sides of the block form")
+    ap.add_argument("--groups", type=int, default=0,
+                    help="direction groups of the block form's grouped layout (0: as memory needs)")
+    ap.add_argument("--tensor-cores", action="store_true",
+                    help="mixed forms: leaf interpolation (P2M, L2P) on the tensor cores")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))
@@ -598,7 +610,7 @@ def main():
             dist.barrier()
 
     extra = {"ragged48": run_ragged, "spheroid4m": run_spheroid, "spheroid_orders": run_orders,
-             "rhs64": run_rhs64, "mixture8m": run_mixture}
+             "rhs64": run_rhs64, **{m: run_mixture for m in MIXTURES}}
     if args.workload in extra:
         if rank == 0:
             extra[args.workload](args, torch)
@@ -617,6 +629,8 @@ def main():
     t0 = time.perf_counter()
     A.prcmpt(w.order, w.ncrit, w.kappa)
     setup_s = time.perf_counter() - t0
+    if args.tensor_cores:
+        A.set_tensor_cores(True)
     t0 = time.perf_counter()
     A.upload()
     upload_s = time.perf_counter() - t0
@@ -677,7 +691,7 @@ def main():
     dQ = torch.from_numpy(Q).to("cuda")
     dP = torch.empty((nrhs, w.n), dtype=torch.complex128, device="cuda")
     A.set_precision("mixed")
-    A.set_blocking(nrhs, 0)
+    A.set_blocking(nrhs, args.groups)
     blaunch = [0]
 
     def block():
@@ -762,6 +776,7 @@ def main():
             "config": {"workload": args.workload, "n_points": w.n, "kappa": w.kappa, "order": w.order,
                        "leaf_size": w.ncrit, "precision": "fp64" if head == "fp64" else "mixed",
                        "right_hand_sides_per_step": hn, "form": head, "parallelism": f"replicas{world}",
+                       "tensor_cores": bool(args.tensor_cores),
                        "l2": "working set per step >> L2 (126 MB): expansions and spectra are GBs"},
             "matvecs_per_s": world * hn / (ms * 1e-3),
             "fp64": {"ms_per_step": res["fp64"]["ms"], "points_per_s": world * w.n / (res["fp64"]["ms"] * 1e-3)},

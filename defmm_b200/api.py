@@ -38,7 +38,7 @@ _INFO = {
     "plan_walk_ms": 22, "m2l_threads": 23, "p2p_blocks_per_sm": 24, "m2l_pairing": 25,
     "layout": 26, "rhs_block": 27, "groups": 28, "m2m_entries": 29, "l2l_entries": 30,
     "p2m_point_slots": 31, "l2p_point_slots": 32, "m2f_slots": 33, "tensor_cores": 34,
-    "tree_device": 35, "tree_ms": 36, "rhs_per_cta": 37,
+    "tree_device": 35, "tree_ms": 36, "rhs_per_cta": 37, "m2l_staging": 38, "m2l_group_list": 39,
 }
 PHASES = ["p2m", "m2m", "m2f", "m2l", "f2l", "l2l", "l2p", "p2p", "scatter", "total"]
 
@@ -89,6 +89,7 @@ def lib():
             "defmm_probe_l2_read": (ctypes.c_int, [i64, ctypes.c_int, dp]),
             "defmm_set_rhs_per_cta": (ctypes.c_int, [vp, ctypes.c_int]),
             "defmm_set_tensor_cores": (ctypes.c_int, [vp, ctypes.c_int]),
+            "defmm_set_m2l_staging": (ctypes.c_int, [vp, ctypes.c_int]),
             "defmm_batch_create": (vp, [i64, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.c_int]),
             "defmm_batch_launch": (ctypes.c_int, [vp, vp]),
             "defmm_batch_destroy": (None, [vp]),
@@ -212,6 +213,12 @@ class IBFMM_Mat:
     def set_tensor_cores(self, on=True):
         """Mixed precision: P2M on the tensor cores (tcgen05, split TF32)."""
         self._check(lib().defmm_set_tensor_cores(self._h, int(bool(on))))
+
+    def set_m2l_staging(self, on=True):
+        """Grouped layout, mixed precision, orders 3-6: M2L staged through
+        shared memory by bulk copies with four target slots per CTA, or one
+        target slot per CTA (default, faster); bit-identical results."""
+        self._check(lib().defmm_set_m2l_staging(self._h, int(bool(on))))
 
     def set_rhs_per_cta(self, rb=4):
         """Right-hand sides per M2L CTA of the grouped layout (1, 2, 4, 8)."""

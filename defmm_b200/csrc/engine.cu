@@ -107,6 +107,8 @@ struct defmm_handle {
   GroupedLayout gl;
   int rhs_block = 16;     // right-hand sides per pass of multi-RHS calls
   int rhs_block_m2l = 4;  // right-hand sides per M2L CTA (capped by the order)
+  bool m2l_staging = false;  // grouped layout, FP32: shared-memory-staged M2L with target groups
+  int64_t m2l_lgroup = 0;   // longest list total of kM2LGroup consecutive target slots
   bool use_tc = false;    // mixed precision: P2M on the tensor cores (tcgen05)
   int groups_forced = 0;  // > 0: direction groups requested (also for one RHS)
   int groups_used = 0;    // groups of the last grouped pass
@@ -437,7 +439,7 @@ int prepare_tables(defmm_handle* h) {
     DevBuf base;
     if ((st = put(base, p.tables.data(), p.tables.size()))) return st;
     const int64_t np = (int64_t)p.ptab_key.size();
-    if ((st = ensure(h, h->ptab, std::max<int64_t>(1, np) * p.PP * cs))) {
+    if ((st = ensure(h, h->ptab, std::max<int64_t>(1, np) * p.PP * cs + 16))) {  // + slack as for F
       free_buf(base);
       return st;
     }
@@ -594,7 +596,7 @@ int prepare_grouped(defmm_handle* h, int R) {
   cap = std::min(cap, std::max(want, need));
   if (cap < need) return h->fail(DEFMM_ERR_MEMORY, "not enough device memory for one cone of spectra");
   g.f_cap = cap;
-  if ((st = ensure(h, g.F, (size_t)cap * fper))) return st;
+  if ((st = ensure(h, g.F, (size_t)cap * fper + 16))) return st;  // slack for 16-byte-rounded bulk copies
   // direction groups: consecutive pivot directions while the group's M and L
   // fit in 70% of what is left (or about 1 / groups_forced of all HF slots)
   if (g.lh >= 0) {
@@ -895,7 +897,7 @@ int run_gemv_grouped(defmm_handle* h, const double2* qin, int64_t stride_in, dou
                      h->m2l_pair[pi], s);
           else
             ops->m2l_rhs(d, ts0, ts1, fs0, fs1, R, h->rhs_block_m2l, g.F.p, h->ptab.p, Lbase, h->d_queue + 1,
-                         h->nsm, s);
+                         h->nsm, h->m2l_staging ? h->m2l_lgroup : 0, s);
         });
         nk += 2;
       }
@@ -1364,6 +1366,13 @@ int defmm_prcmpt(defmm_handle* h, int L, int Ncrit, double kappa, int lvMAX) {
   if (h->plan.dev_m2l_src) h->plan_allocs.push_back(h->plan.dev_m2l_src);
   if (h->plan.dev_m2l_tab) h->plan_allocs.push_back(h->plan.dev_m2l_tab);
   if (h->plan.lv.nlvl > 32) return h->fail(DEFMM_ERR_DEPTH, "more than 32 tree levels");
+  {
+    const std::vector<int64_t>& ptr = h->plan.m2l_ptr;
+    int64_t lg = 0;
+    for (size_t t = 0; t + 1 < ptr.size(); t++)
+      lg = std::max(lg, ptr[std::min(ptr.size() - 1, t + dfb::kM2LGroup)] - ptr[t]);
+    h->m2l_lgroup = lg;
+  }
   h->built = true;
   return 0;
 }
@@ -1428,6 +1437,12 @@ int defmm_set_tensor_cores(defmm_handle* h, int on) {
 int defmm_set_rhs_per_cta(defmm_handle* h, int rb) {
   if (!h || (rb != 1 && rb != 2 && rb != 4 && rb != 8)) return DEFMM_ERR_ARG;
   h->rhs_block_m2l = rb;
+  return 0;
+}
+
+int defmm_set_m2l_staging(defmm_handle* h, int on) {
+  if (!h || (on != 0 && on != 1)) return DEFMM_ERR_ARG;
+  h->m2l_staging = on != 0;
   return 0;
 }
 
@@ -1648,6 +1663,8 @@ int defmm_info(const defmm_handle* h, int what, int64_t* v) {
       *v = rb;
       break;
     }
+    case DEFMM_INFO_M2L_STAGING: *v = h->m2l_staging ? 1 : 0; break;
+    case DEFMM_INFO_M2L_GROUP_LIST: *v = h->m2l_lgroup; break;
     case DEFMM_INFO_TREE_MS: *v = (int64_t)(1e3 * p.t_tree); break;
     case DEFMM_INFO_LIST_RECORDS: *v = p.keep_lists ? 1 : 0; break;
     case DEFMM_INFO_LAUNCHES: *v = h->launches; break;

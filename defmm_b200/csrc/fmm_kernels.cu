@@ -3,6 +3,7 @@
 #include "kernels.cuh"
 #include "device_math.cuh"
 #include "fmm_kernels.h"
+#include "ptx.cuh"
 
 #include <algorithm>
 #include <mutex>
@@ -1018,6 +1019,369 @@ __global__ void __launch_bounds__(NT, m2l_rhs_ctas<T, NT, RB>()) k_m2l_rhs(DevPl
       for (int k = 0; k < K; k++) a[k] = acc[k][b];
       m2l_f2l<T, L, NT>(a, Js, Cb, D, Lx + (t * R + r0 + b) * LL);
     }
+  }
+}
+
+// Right-hand-side blocks with target groups, fed through shared memory by
+// bulk copies (FP32 spectra).  A work item is (G consecutive target slots of
+// a cone batch, RB right-hand sides).  Their lists are sorted by source slot;
+// merged, every source slot met by any of the G lists is one entry, and its
+// RB spectra F_s are loaded once for all the targets that meet it (a group of
+// 4 consecutive slots meets 0.45 distinct sources per far pair on a sphere
+// at 40 points per wavelength squared, order 5), with the transfer spectrum
+// U_k of each such pair.
+//
+// Warp roles: the last warp produces, the others consume.  The producer
+// takes work items from the queue, loads the G lists into shared memory,
+// merges them and, per entry, copies the RB spectra of the source and the
+// entry's transfer spectra into one of NS stages with 1-D bulk copies
+// (cp.async.bulk global -> shared, completing on the stage's "full"
+// mbarrier).  Consumer thread c owns spectrum entries c + k NC and keeps the
+// G x RB accumulators of its entries in registers; after a stage it arrives
+// on the stage's "empty" mbarrier, and after the last entry of an item it
+// runs the inverse DFT of every (target, right-hand side) with an entry,
+// NSPEC spectra per round, and adds the results into L.  The producer keeps
+// filling stages meanwhile.
+//
+// Every accumulator sees its list in list order with the operations of
+// k_m2l_rhs, and the inverse DFT sums in the order of m2l_f2l, so the
+// results are bit-identical to k_m2l_rhs (and to the one-right-hand-side
+// kernels).  A copy starts at the 16-byte boundary at or below its first
+// byte and ends at the one at or above its last (both buffers carry 16 bytes
+// of slack at the end); consumers index from the remainder.
+//
+// Every wait is bounded.  A thread that gives up sets a shared stop flag
+// (the other waits then return at once) and the error code 3; the producer
+// then waits (bounded) for the copies it issued before it returns.
+template <int L>
+struct M2LBulk {
+  static constexpr int PD = 2 * L - 1, PP = PD * PD * PD, LL = L * L * L;
+  static constexpr int G = kM2LGroup;                                   // target slots per work item
+  static constexpr int RB = L <= 5 ? 4 : 2;                             // right-hand sides per work item
+  static constexpr int K = (PP + 767) / 768;                            // entries per consumer thread
+  static constexpr int NC = 32 * ((PP + 32 * K - 1) / (32 * K));        // consumer threads
+  static constexpr int NT = NC + 32;                                    // + the producer warp
+  static constexpr int NSPEC = L <= 5 ? 4 : 1;                          // spectra per inverse-DFT round
+  static constexpr int FB = (RB * PP * 8 + 16 + 15) / 16 * 16;          // stage bytes of the F block
+  static constexpr int UB = (PP * 8 + 16 + 15) / 16 * 16;               // stage bytes of one U
+  static constexpr int SB = FB + G * UB;
+  static constexpr int XB = NSPEC * (PP + L * PD * PD + L * L * PD) * 8;  // inverse-DFT scratch
+  static constexpr int LCAP = L <= 4 ? 1024 : 2048;                     // list entries of one work item
+  static constexpr int HDR = 1024;                                      // barriers, entry records, twiddles
+  static constexpr int NS0 = (232448 - XB - LCAP * 8 - HDR) / SB;
+  static constexpr int NS = NS0 > 4 ? 4 : NS0;                          // stages
+  static constexpr int CTAS = L <= 3 ? 4 : (L == 4 ? 2 : 1);           // CTAs per SM
+  static constexpr size_t smem() { return (size_t)NS * SB + XB + (size_t)LCAP * 8 + HDR; }
+};
+
+struct BulkEntry {  // one stage's record, written by the producer
+  int64_t tb;       // first target slot of the item
+  int mask;         // targets of the item that meet this source
+  int flags;        // 1: last entry of the item; 2: no more work
+  int nt, r0;       // targets in the item, first right-hand side
+  int foff;         // F block: offset (complex entries) from the stage start
+  int uoff[kM2LGroup];
+};
+
+constexpr uint32_t kBulkWait = 1u << 22;  // polls before a wait counts as failed
+
+template <int L>
+__global__ void __launch_bounds__(M2LBulk<L>::NT, M2LBulk<L>::CTAS) k_m2l_bulk(
+    DevPlan P, int64_t t0, int64_t t1, int64_t f0, int64_t f1, int R, const float2* __restrict__ F,
+    const float2* __restrict__ ptab, float2* __restrict__ Lx, unsigned long long* __restrict__ queue) {
+  typedef M2LBulk<L> B;
+  constexpr int PD = B::PD, PP = B::PP, LL = B::LL, G = B::G, RB = B::RB, K = B::K, NC = B::NC, NS = B::NS,
+                NSPEC = B::NSPEC, FB = B::FB, UB = B::UB, SB = B::SB;
+  static_assert(NS >= 2, "at least two stages");
+  static_assert((G * RB) % NSPEC == 0, "whole inverse-DFT rounds");
+  static_assert(NSPEC * LL <= NC, "one output of the last inverse-DFT pass per thread");
+  static_assert(NS * 16 + 8 + NS * sizeof(BulkEntry) + PD * 8 + 8 <= B::HDR, "header");
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  unsigned char* stages = smem_raw;
+  float2* Js = reinterpret_cast<float2*>(smem_raw + NS * SB);
+  float2* Cb = Js + NSPEC * PP;
+  float2* D = Cb + NSPEC * L * PD * PD;
+  int32_t* ls_src = reinterpret_cast<int32_t*>(D + NSPEC * L * L * PD);
+  uint32_t* ls_tab = reinterpret_cast<uint32_t*>(ls_src + B::LCAP);
+  uint64_t* full = reinterpret_cast<uint64_t*>(ls_tab + B::LCAP);
+  uint64_t* empty = full + NS;
+  uint64_t* cbar = empty + NS;
+  BulkEntry* rec = reinterpret_cast<BulkEntry*>(cbar + 1);
+  float2* tw = reinterpret_cast<float2*>(rec + NS);
+  volatile int* stop = reinterpret_cast<volatile int*>(tw + PD);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  constexpr unsigned kAll = 0xffffffffu;
+  if (tid == 0) {
+    for (int i = 0; i < NS; i++) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], NC / 32);
+    }
+    mbar_init(cbar, NC / 32);
+    *stop = 0;
+  }
+  if (tid < PD) tw[tid] = ctw<float, L>(tid);
+  __syncthreads();
+
+  if (warp == NC / 32) {
+    // ---------------------------------------------------------- producer
+    const int nb = R / RB;
+    const int64_t nwork = (t1 - t0 + G - 1) / G * nb;
+    uint32_t it = 0;  // stages issued
+    bool ok = true;
+    for (;;) {
+      unsigned long long w = 0;
+      if (lane == 0) w = atomicAdd(queue, 1ULL);
+      w = __shfl_sync(kAll, w, 0);
+      if ((int64_t)w >= nwork) break;
+      const int64_t tb = t0 + (int64_t)(w / nb) * G;
+      const int r0 = (int)(w % nb) * RB;
+      const int nt = (int)(t1 - tb < G ? t1 - tb : G);
+      const int64_t eb = P.m2l_ptr[tb], ee = P.m2l_ptr[tb + nt];
+      const int64_t n = ee - eb;
+      if (n == 0) continue;
+      if (n > B::LCAP) {  // the launcher checks the plan's largest group: a plan bug
+        if (lane == 0) atomicExch(P.err, 1);
+        continue;
+      }
+      __syncwarp();  // lane 0 is done with the previous item's lists
+      for (int64_t i = lane; i < n; i += 32) {
+        ls_src[i] = P.m2l_src[eb + i];
+        ls_tab[i] = P.m2l_tab[eb + i];
+      }
+      __syncwarp();
+      if (lane == 0) {
+        int hd[G], he[G];
+#pragma unroll
+        for (int j = 0; j < G; j++) {
+          hd[j] = j < nt ? (int)(P.m2l_ptr[tb + j] - eb) : 0;
+          he[j] = j < nt ? (int)(P.m2l_ptr[tb + j + 1] - eb) : 0;
+        }
+        // one entry of look-ahead, so the item's last entry is known when issued
+        bool have = false;
+        int pmask = 0, psrc = 0;
+        uint32_t ptabs[G];
+        auto issue = [&](bool last) -> bool {
+          const int s = (int)(it % NS);
+          const uint32_t ph = (it / NS) & 1u;
+          if (!mbar_wait_or_stop(&empty[s], ph ^ 1u, kBulkWait, stop)) return false;
+          unsigned char* st = stages + (size_t)s * SB;
+          BulkEntry& e = rec[s];
+          const uintptr_t a = (uintptr_t)(F + ((int64_t)(psrc - f0) * R + r0) * PP);
+          const uintptr_t a0 = a & ~(uintptr_t)15, a1 = (a + (uintptr_t)RB * PP * 8 + 15) & ~(uintptr_t)15;
+          uint32_t total = (uint32_t)(a1 - a0);
+          e.tb = tb;
+          e.mask = pmask;
+          e.flags = last ? 1 : 0;
+          e.nt = nt;
+          e.r0 = r0;
+          e.foff = (int)((a - a0) >> 3);
+          uintptr_t u0[G];
+          uint32_t ub[G];
+#pragma unroll
+          for (int j = 0; j < G; j++) {
+            u0[j] = 0;
+            ub[j] = 0;
+            if ((pmask >> j) & 1) {
+              const uintptr_t u = (uintptr_t)(ptab + (int64_t)ptabs[j] * PP);
+              u0[j] = u & ~(uintptr_t)15;
+              ub[j] = (uint32_t)(((u + (uintptr_t)PP * 8 + 15) & ~(uintptr_t)15) - u0[j]);
+              e.uoff[j] = (int)((u - u0[j]) >> 3);
+              total += ub[j];
+            }
+          }
+          mbar_arrive_expect_tx(&full[s], total);
+          bulk_g2s(st, (const void*)a0, (uint32_t)(a1 - a0), &full[s]);
+#pragma unroll
+          for (int j = 0; j < G; j++)
+            if ((pmask >> j) & 1) bulk_g2s(st + FB + j * UB, (const void*)u0[j], ub[j], &full[s]);
+          it++;
+          return true;
+        };
+        for (;;) {
+          int src = INT_MAX;
+#pragma unroll
+          for (int j = 0; j < G; j++)
+            if (hd[j] < he[j] && ls_src[hd[j]] < src) src = ls_src[hd[j]];
+          if (src == INT_MAX) break;
+          int mask = 0;
+          uint32_t tabs[G];
+#pragma unroll
+          for (int j = 0; j < G; j++) {
+            tabs[j] = 0;
+            if (hd[j] < he[j] && ls_src[hd[j]] == src) {
+              mask |= 1 << j;
+              tabs[j] = ls_tab[hd[j]];
+              hd[j]++;
+            }
+          }
+          if (src < f0 || src >= f1) {  // entry outside this cone batch: a plan bug
+            atomicExch(P.err, 1);
+            continue;
+          }
+          if (have && !issue(false)) {
+            ok = false;
+            break;
+          }
+          have = true;
+          psrc = src;
+          pmask = mask;
+#pragma unroll
+          for (int j = 0; j < G; j++) ptabs[j] = tabs[j];
+        }
+        if (ok && have && !issue(true)) ok = false;
+      }
+      ok = __shfl_sync(kAll, ok, 0);
+      if (!ok) break;
+    }
+    if (lane == 0) {
+      if (ok) {  // no more work
+        const int s = (int)(it % NS);
+        if (mbar_wait_or_stop(&empty[s], ((it / NS) & 1u) ^ 1u, kBulkWait, stop)) {
+          rec[s].flags = 2;
+          mbar_arrive(&full[s]);
+        } else {
+          ok = false;
+        }
+      }
+      if (!ok) {
+        *stop = 1;
+        atomicExch(P.err, 3);
+        // the copies issued into the last NS stages land before the CTA ends
+        for (uint32_t k = it > (uint32_t)NS ? it - NS : 0; k < it; k++) mbar_wait(&full[k % NS], (k / NS) & 1u, kBulkWait);
+      }
+    }
+    return;
+  }
+
+  // ------------------------------------------------------------ consumers
+  float2 acc[G][RB][K];
+#pragma unroll
+  for (int j = 0; j < G; j++)
+#pragma unroll
+    for (int r = 0; r < RB; r++)
+#pragma unroll
+      for (int k = 0; k < K; k++) acc[j][r][k] = czero<float2>();
+  int seen = 0;
+  uint32_t cph = 0;
+  const float inv = 1.0f / (float)PP;
+  // barrier of the consumer warps (bounded; false once any thread gave up)
+  auto cbarrier = [&]() -> bool {
+    __syncwarp();
+    if (lane == 0) mbar_arrive(cbar);
+    const bool ok = __all_sync(kAll, mbar_wait_or_stop(cbar, cph, kBulkWait, stop));
+    cph ^= 1u;
+    if (!ok && lane == 0) {
+      *stop = 1;
+      atomicExch(P.err, 3);
+    }
+    return ok;
+  };
+  for (uint32_t it = 0;; it++) {
+    const int s = (int)(it % NS);
+    if (!__all_sync(kAll, mbar_wait_or_stop(&full[s], (it / NS) & 1u, kBulkWait, stop))) {
+      if (lane == 0) {
+        *stop = 1;
+        atomicExch(P.err, 3);
+      }
+      break;
+    }
+    const BulkEntry e = rec[s];
+    if (e.flags & 2) break;
+    const float2* st = reinterpret_cast<const float2*>(stages + (size_t)s * SB);
+    const float2* Fs = st + e.foff;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      const int i = tid + k * NC;
+      if (i < PP) {
+        float2 f[RB];
+#pragma unroll
+        for (int r = 0; r < RB; r++) f[r] = Fs[r * PP + i];
+#pragma unroll
+        for (int j = 0; j < G; j++)
+          if ((e.mask >> j) & 1) {
+            const float2 u = st[(FB + j * UB) / 8 + e.uoff[j] + i];
+#pragma unroll
+            for (int r = 0; r < RB; r++) cfma(acc[j][r][k], u, f[r]);
+          }
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);
+    seen |= e.mask;
+    if (!(e.flags & 1)) continue;
+    // inverse DFT of every (target, right-hand side) with an entry, the
+    // passes of m2l_f2l over NSPEC spectra at a time
+    bool ok = true;
+#pragma unroll
+    for (int q0 = 0; q0 < G * RB; q0 += NSPEC) {
+      bool live = false;
+#pragma unroll
+      for (int sp = 0; sp < NSPEC; sp++) {
+        const int j = (q0 + sp) / RB;
+        live |= j < e.nt && ((seen >> j) & 1);
+      }
+      if (!live || !ok) continue;
+      // this thread's output of the last pass (one per thread): its L entry
+      // is loaded now, so the load overlaps the first two passes
+      float2* l3 = nullptr;
+      float2 lold = czero<float2>();
+      if (tid < NSPEC * LL) {
+        const int sp = tid / LL, rem = tid - sp * LL;
+        const int q = q0 + sp, j = q / RB, r = q - j * RB;
+        if (j < e.nt && ((seen >> j) & 1)) {
+          l3 = Lx + ((e.tb + j) * R + e.r0 + r) * LL + rem;
+          lold = *l3;
+        }
+      }
+#pragma unroll
+      for (int sp = 0; sp < NSPEC; sp++)
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+          const int i = tid + k * NC;
+          if (i < PP) Js[sp * PP + i] = acc[(q0 + sp) / RB][(q0 + sp) % RB][k];
+        }
+      if (!(ok = cbarrier())) continue;
+      for (int o = tid; o < NSPEC * L * PD * PD; o += NC) {  // axis 0: (k1,k2) lines -> a
+        const int sp = o / (L * PD * PD), rem = o - sp * (L * PD * PD);
+        const int a = rem / (PD * PD), ln = rem - a * (PD * PD);
+        const float2* v = Js + sp * PP + ln;
+        float2 sum = v[0];
+#pragma unroll
+        for (int k0 = 1; k0 < PD; k0++) cfmac(sum, v[k0 * PD * PD], tw[(k0 * a) % PD]);
+        Cb[sp * L * PD * PD + a * PD * PD + ln] = sum;
+      }
+      if (!(ok = cbarrier())) continue;
+      for (int o = tid; o < NSPEC * L * L * PD; o += NC) {  // axis 1: (a,k2) lines -> b
+        const int sp = o / (L * L * PD), rem = o - sp * (L * L * PD);
+        const int a = rem / (L * PD), rem2 = rem - a * (L * PD);
+        const int b = rem2 / PD, k2 = rem2 - b * PD;
+        const float2* v = Cb + sp * L * PD * PD + a * PD * PD + k2;
+        float2 sum = v[0];
+#pragma unroll
+        for (int k1 = 1; k1 < PD; k1++) cfmac(sum, v[k1 * PD], tw[(k1 * b) % PD]);
+        D[sp * L * L * PD + (a * L + b) * PD + k2] = sum;
+      }
+      if (!(ok = cbarrier())) continue;
+      if (l3) {  // axis 2: (a,b) lines -> c, added into L
+        const int sp = tid / LL, rem = tid - sp * LL;
+        const int ln = rem / L, c = rem - ln * L;
+        const float2* v = D + sp * L * L * PD + ln * PD;
+        float2 sum = v[0];
+#pragma unroll
+        for (int k2 = 1; k2 < PD; k2++) cfmac(sum, v[k2], tw[(k2 * c) % PD]);
+        lold.x += sum.x * inv;
+        lold.y += sum.y * inv;
+        *l3 = lold;
+      }
+    }
+    if (!ok) break;
+#pragma unroll
+    for (int j = 0; j < G; j++)
+#pragma unroll
+      for (int r = 0; r < RB; r++)
+#pragma unroll
+        for (int k = 0; k < K; k++) acc[j][r][k] = czero<float2>();
+    seen = 0;
   }
 }
 
@@ -2044,7 +2408,8 @@ struct Launch {
                              (int)P2MCfg<T, L>::smem(kMaxRhsBlock));
     if (e != cudaSuccess) return e;
     if ((e = rhs_attr<1, 128>()) != cudaSuccess || (e = rhs_attr<2, 128>()) != cudaSuccess ||
-        (e = rhs_attr<4, 256>()) != cudaSuccess || (e = rhs_attr<8, 256>()) != cudaSuccess)
+        (e = rhs_attr<4, 256>()) != cudaSuccess || (e = rhs_attr<8, 256>()) != cudaSuccess ||
+        (e = bulk_attr()) != cudaSuccess)
       return e;
     return cudaSuccess;
   }
@@ -2066,13 +2431,36 @@ struct Launch {
     k_m2l_rhs<T, L, NT, RBE><<<grid, NT, smem_m2l(), s>>>(dp, t0, t1, f0, f1, R, (const C*)F, (const C*)ptab,
                                                           (C*)Lx, queue);
   }
+  // the shared-memory-staged kernel: FP32, orders 3-6
+  static constexpr bool kBulk = std::is_same<T, float>::value && L >= 3 && L <= 6;
+  static cudaError_t bulk_attr() {
+    if constexpr (kBulk)
+      return cudaFuncSetAttribute(k_m2l_bulk<L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)M2LBulk<L>::smem());
+    return cudaSuccess;
+  }
+  static bool m2l_bulk(const DevPlan& dp, int64_t t0, int64_t t1, int64_t f0, int64_t f1, int R, const void* F,
+                       const void* ptab, void* Lx, unsigned long long* queue, int nsm, int64_t lgroup,
+                       cudaStream_t s) {
+    if constexpr (kBulk) {
+      typedef M2LBulk<L> B;
+      if (lgroup <= 0 || lgroup > B::LCAP || R % B::RB) return false;
+      const int64_t nwork = (t1 - t0 + B::G - 1) / B::G * (R / B::RB);
+      const int grid = (int)std::min<int64_t>(nwork, (int64_t)nsm * B::CTAS);
+      k_m2l_bulk<L><<<grid, B::NT, B::smem(), s>>>(dp, t0, t1, f0, f1, R, (const float2*)F, (const float2*)ptab,
+                                                   (float2*)Lx, queue);
+      return true;
+    }
+    return false;
+  }
   // M2L for R right-hand sides in blocks of rb (1, 2, 4 or 8; a divisor of
-  // R, capped by the order's kMaxRB)
+  // R, capped by the order's kMaxRB), or staged through shared memory
   static void m2l_rhs(const DevPlan& dp, int64_t t0, int64_t t1, int64_t f0, int64_t f1, int R, int rb,
                       const void* F, const void* ptab, void* Lx, unsigned long long* queue, int nsm,
-                      cudaStream_t s) {
+                      int64_t lgroup, cudaStream_t s) {
     if (t1 <= t0) return;
     cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s);
+    if (m2l_bulk(dp, t0, t1, f0, f1, R, F, ptab, Lx, queue, nsm, lgroup, s)) return;
     if (rb > kMaxRB) rb = kMaxRB;
     while (rb > 1 && R % rb) rb >>= 1;
     if (rb >= 8)

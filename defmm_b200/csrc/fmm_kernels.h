@@ -8,6 +8,9 @@
 
 namespace dfb {
 
+// Consecutive target slots per CTA of the shared-memory-staged M2L.
+constexpr int kM2LGroup = 4;
+
 // Per-(precision, order) launchers of the expansion phases.  Complex arrays
 // are passed untyped; their element type is double2 (FP64) or float2.
 struct OpTable {
@@ -35,9 +38,14 @@ struct OpTable {
   void (*m2l)(const DevPlan&, int64_t t0, int64_t t1, int64_t f0, int64_t f1, const void* F, const void* ptab,
               void* Lx, unsigned long long* queue, int nsm, int nt, int pair, cudaStream_t);
   // The same for R right-hand sides (F: R spectra per source slot of the
-  // batch, Lx: base as above), rb of them per CTA sharing each spectrum load
+  // batch, Lx: base as above), rb of them per CTA sharing each spectrum load.
+  // lgroup > 0: the longest list total of kM2LGroup consecutive target
+  // slots; the FP32 path at orders 3-6 then stages spectra through shared
+  // memory with bulk copies, kM2LGroup target slots per CTA sharing each
+  // source's loads (bit-identical results); lgroup <= 0: one target slot per
+  // CTA.  F and ptab carry 16 bytes of slack after their last spectrum.
   void (*m2l_rhs)(const DevPlan&, int64_t t0, int64_t t1, int64_t f0, int64_t f1, int R, int rb, const void* F,
-                  const void* ptab, void* Lx, unsigned long long* queue, int nsm, cudaStream_t);
+                  const void* ptab, void* Lx, unsigned long long* queue, int nsm, int64_t lgroup, cudaStream_t);
   // L2P of the leaves' slots with a direction in [d0, d1) into pfar (R per
   // particle), written (accum = false) or added
   void (*l2p)(const DevPlan&, const int32_t* leaves, int n, const void* sig2, const void* Lx, double2* pfar, int R,

@@ -25,15 +25,12 @@
 #include "device_math.cuh"
 #include "fmm_kernels.h"
 #include "kernels.cuh"
+#include "ptx.cuh"
 
 namespace dfb {
 namespace {
 
 // ------------------------------------------------------------ PTX wrappers --
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-
 // Shared-memory matrix descriptor: K-major, no swizzle (canonical layout
 // ((8, n), 2) : ((1, SBO), LBO) in 16-byte units), Blackwell version field.
 __device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
@@ -62,28 +59,6 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t a, uint64_t b
 __device__ __forceinline__ void mma_commit(uint64_t* mbar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(mbar))
                : "memory");
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* m, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(m)), "r"(count) : "memory");
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-// Wait until the phase with the given parity has completed; false after
-// `limit` unsuccessful polls.
-__device__ __forceinline__ bool mbar_wait(uint64_t* m, uint32_t parity, uint32_t limit) {
-  for (uint32_t i = 0; i < limit; i++) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(done)
-        : "r"(smem_u32(m)), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
 }
 
 __device__ __forceinline__ void tmem_alloc(uint32_t* dst, uint32_t ncols) {  // one whole warp

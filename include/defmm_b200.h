@@ -121,6 +121,14 @@ int defmm_set_tensor_cores(defmm_handle* h, int on);
  * transfer-spectrum entry is read once for them.  Results are bit-identical
  * for every choice. */
 int defmm_set_rhs_per_cta(defmm_handle* h, int rb);
+/* No counterpart in the reference.  1: the grouped layout's mixed-precision
+ * M2L at orders 3-6 stages spectra through shared memory with bulk copies
+ * (cp.async.bulk), four consecutive target slots per CTA loading each
+ * source's spectra once for all of them (M2L.hpp:115-127 with the targets'
+ * lists merged); 0 (default, faster on the tested workloads): one target
+ * slot per CTA, rhs_per_cta right-hand sides.  Results are bit-identical
+ * either way. */
+int defmm_set_m2l_staging(defmm_handle* h, int on);
 
 /* No counterpart in the reference.  Independent operators (handles of
  * problems of any sizes, orders and wavenumbers) applied together: each
@@ -221,6 +229,8 @@ int defmm_probe_l2_read(int64_t bytes, int reps, double* gbs);
 #define DEFMM_INFO_TREE_DEVICE 35       /* 1 if prcmpt ordered the octrees' particles on the GPU */
 #define DEFMM_INFO_TREE_MS 36           /* prcmpt's octree build, ms */
 #define DEFMM_INFO_RHS_PER_CTA 37       /* right-hand sides per M2L CTA of the grouped layout */
+#define DEFMM_INFO_M2L_STAGING 38       /* 1: shared-memory-staged M2L with target groups enabled */
+#define DEFMM_INFO_M2L_GROUP_LIST 39    /* longest list total of four consecutive target slots */
 int defmm_info(const defmm_handle* h, int what, int64_t* value);
 
 /* Per-phase device times (ms) of the last gemv, in this order:

@@ -57,6 +57,10 @@ def test_argument_checks_without_device():
             A.set_rhs_per_cta(rb)
     A.set_rhs_per_cta(4)
     with pytest.raises(api.DefmmError):
+        A._check(api.lib().defmm_set_m2l_staging(A._h, 2))
+    A.set_m2l_staging(False)
+    A.set_m2l_staging(True)
+    with pytest.raises(api.DefmmError):
         A.autotune(reps=0)
     with pytest.raises(api.DefmmError):
         A.autotune(reps=1)  # before prcmpt

@@ -266,6 +266,37 @@ def test_rhs_blocks_do_not_change_any_right_hand_side(gpu):
         A.set_blocking(16, 0)
 
 
+@pytest.mark.parametrize("name", ["cube20k", "cube_lf", "blobs_sphere", "sphere_l6", "sphere_o3"])
+def test_staged_m2l_matches_one_target_per_cta(name, gpu):
+    # the mixed-precision M2L staged through shared memory by bulk copies
+    # (four target slots per CTA over their merged lists, orders 3-6) gives
+    # the bits of the one-target-slot kernel for every right-hand side, with
+    # right-hand-side counts that do and do not divide its block (8, 6), and
+    # with several direction groups; one right-hand side is checked against
+    # the oracle
+    if name == "sphere_o3":
+        w = W.sphere_surface(20000, seed=12, wavelengths=8)
+        src = trg = w.points
+        L, ncrit, kappa, lvmax = 3, 48, w.kappa, -1
+    else:
+        src, trg, _, L, ncrit, kappa, lvmax = case_inputs(name)
+    A = make(src, trg, L, ncrit, kappa, lvmax)
+    A.set_precision("mixed")
+    assert 0 < A.info("m2l_group_list") <= 2048
+    rng = np.random.default_rng(7)
+    for nrhs, groups in ((8, 0), (8, 3), (6, 0)):
+        Q = (rng.uniform(-1, 1, (nrhs, len(src))) + 1j * rng.uniform(-1, 1, (nrhs, len(src)))).astype(np.complex128)
+        A.set_blocking(nrhs, groups)
+        A.set_m2l_staging(False)
+        ref = A.matvec(Q)
+        A.set_m2l_staging(True)
+        assert A.info("m2l_staging") == 1
+        P = A.matvec(Q)
+        assert np.array_equal(P, ref), (nrhs, groups)
+    po = O.OracleFMM(src, trg, L, ncrit, kappa, lvmax).gemv(Q[0])
+    assert rel(P[0], po) <= MIXED_TOL
+
+
 def test_launch_choices_and_autotune_keep_results_bit_identical(gpu):
     # M2L threads per CTA, one or two target slots per M2L CTA and near-field
     # CTAs per SM change only the schedule: every combination gives the same
