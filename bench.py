@@ -629,6 +629,7 @@ def main():
     t0 = time.perf_counter()
     A.prcmpt(w.order, w.ncrit, w.kappa)
     setup_s = time.perf_counter() - t0
+    setup_steps = A.setup_times()
     if args.tensor_cores:
         A.set_tensor_cores(True)
     t0 = time.perf_counter()
@@ -800,7 +801,7 @@ def main():
             "setup_s": setup_s,
             "setup": {"prcmpt_s": setup_s, "level_walk_s": info["plan_walk_ms"] / 1e3,
                       "level_walk_on_gpu": bool(info["plan_walk_device"]), "upload_s": upload_s,
-                      "autotune_s": tune_s},
+                      "autotune_s": tune_s, "prcmpt_steps_s": setup_steps},
             "launch": tune,
             "plan": {k: info[k] for k in ["nlvl", "cpt", "slots_S", "slots_T", "far_hf", "far_lf", "near",
                                           "i_near", "tables", "permuted_spectra", "device_bytes"]},

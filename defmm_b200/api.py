@@ -90,6 +90,7 @@ def lib():
             "defmm_set_rhs_per_cta": (ctypes.c_int, [vp, ctypes.c_int]),
             "defmm_set_tensor_cores": (ctypes.c_int, [vp, ctypes.c_int]),
             "defmm_set_m2l_staging": (ctypes.c_int, [vp, ctypes.c_int]),
+            "defmm_setup_times": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.POINTER(i64)]),
             "defmm_batch_create": (vp, [i64, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.c_int]),
             "defmm_batch_launch": (ctypes.c_int, [vp, vp]),
             "defmm_batch_destroy": (None, [vp]),
@@ -213,6 +214,18 @@ class IBFMM_Mat:
     def set_tensor_cores(self, on=True):
         """Mixed precision: P2M on the tensor cores (tcgen05, split TF32)."""
         self._check(lib().defmm_set_tensor_cores(self._h, int(bool(on))))
+
+    def setup_times(self) -> dict:
+        """Seconds per step of the last prcmpt (defmm_setup_times)."""
+        n = ctypes.c_int64(0)
+        self._check(lib().defmm_setup_times(self._h, None, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(int(n.value))
+        self._check(lib().defmm_setup_times(self._h, buf, ctypes.byref(n)))
+        out = {}
+        for line in buf.value.decode().splitlines():
+            t, name = line.split("\t", 1)
+            out[name] = out.get(name, 0.0) + float(t)
+        return out
 
     def set_m2l_staging(self, on=True):
         """Grouped layout, mixed precision, orders 3-6: M2L staged through

@@ -1440,6 +1440,24 @@ int defmm_set_rhs_per_cta(defmm_handle* h, int rb) {
   return 0;
 }
 
+int defmm_setup_times(const defmm_handle* h, char* buf, int64_t* len) {
+  if (!h || !len) return DEFMM_ERR_ARG;
+  std::string txt;
+  char line[256];
+  for (const auto& st : h->plan.t_steps) {
+    std::snprintf(line, sizeof(line), "%.6f\t%s\n", st.second, st.first);
+    txt += line;
+  }
+  const int64_t cap = *len;
+  *len = (int64_t)txt.size() + 1;
+  if (buf && cap > 0) {
+    const size_t n = std::min<size_t>((size_t)cap - 1, txt.size());
+    std::memcpy(buf, txt.data(), n);
+    buf[n] = 0;
+  }
+  return 0;
+}
+
 int defmm_set_m2l_staging(defmm_handle* h, int on) {
   if (!h || (on != 0 && on != 1)) return DEFMM_ERR_ARG;
   h->m2l_staging = on != 0;

@@ -1092,6 +1092,7 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
   p.lvmax = lvmax;
   p.kappa = kappa;
   p.p2p_sym = ns == nt && (src == trg || std::memcmp(src, trg, sizeof(double) * 3 * (size_t)ns) == 0);
+  p.t_steps.clear();
   double t0 = now_s();
   // particles.hpp:79-100 (getBounds): one cube around targets and sources
   {
@@ -1121,12 +1122,15 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
   if (st) return st;
   p.tree_on_device = sorter != nullptr;
   p.t_tree = now_s() - t0;
+  p.t_steps.push_back({"octrees (bounds, particle ordering, cells)", p.t_tree});
   t0 = now_s();
+  double ts = t0;
   st = init_levels(p, err);
   if (st) return st;
   init_directions(p);
   init_small_tables(p);
   init_signatures(p);
+  p.step("levels, directions, small tables, signatures", ts);
   const Levels& v = p.lv;
   const int nlvl = v.nlvl;
 
@@ -1135,6 +1139,8 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
   st = (walker && !p.keep_lists) ? walker->walk(p, w, err) : walk_levels_host(p, w);
   if (st) return st;
   p.t_walk = now_s() - tw;
+  if (!walker || p.keep_lists) p.t_steps.push_back({"level walk (host)", p.t_walk});
+  ts = now_s();
   auto& near_pairs = w.near_pairs;
   auto& tab_nI = w.tab_nI;
 
@@ -1151,6 +1157,7 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
   };
   cell_csr(p.T, p.sT);
   cell_csr(p.S, p.sS);
+  p.step("slots per cell", ts);
 
   // M2L grouped by target slot, each slot's entries by increasing source
   // slot (so that consecutive target slots can be merged on their common
@@ -1204,6 +1211,7 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
     pfor((int64_t)p.m2l_tab.size(), 1 << 16, [&](int64_t e) { p.m2l_tab[e] = (uint32_t)pid[p.m2l_tab[e]]; });
   }
 
+  p.step("M2L entries by target slot, permuted spectra", ts);
   // CSR over slots from a per-slot visitor visit(k, emit), in slot order:
   // blocks of slots are visited in parallel once, each into its own buffer
   // (ptr holding block-local offsets), then shifted and copied into place
@@ -1272,6 +1280,7 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
         },
         p.l2l_ptr, p.l2l_parent);
   }
+  p.step("M2M and L2L transfer lists", ts);
   // leaves holding expansions (upwpass.hpp:39-47, dwnpass.hpp:39-47)
   for (int64_t c = 0; c < p.S.ncell; c++)
     if (p.S.leaf(c) && v.prec[p.S.lvl[c]]) p.p2m_leaf.push_back((int32_t)c);
@@ -1365,6 +1374,7 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
       }
     });
   }
+  p.step("near-field ranges and chunks", ts);
   if (p.p2p_sym) {
     build_symmetric_near(p);
     split_items(p, p.sym_ptr, p.sym_sfirst, p.sym_sn, &p.sym_soff, p.sym_item_chunk, p.sym_chunk_items,
@@ -1372,6 +1382,7 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
   }
   split_items(p, p.p2p_ptr, p.p2p_sfirst, p.p2p_sn, nullptr, p.p2p_item_chunk, p.p2p_chunk_items, p.p2p_order,
               false);
+  p.step("near-field symmetric blocks and work items", ts);
   p.t_lists = now_s() - t0;
 
   // transfer spectra, FP64 (circulant.hpp:133-144)
@@ -1384,6 +1395,7 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
     transfer_spectrum(p, rad, tab_nI[k].data(), &p.tables[k * (size_t)p.PP]);
   });
   p.t_tables = now_s() - t0;
+  p.step("transfer spectra (FP64)", ts);
   return 0;
 }
 

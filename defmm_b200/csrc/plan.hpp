@@ -9,6 +9,7 @@
 #pragma once
 
 #include <array>
+#include <chrono>
 #include <complex>
 #include <cstdint>
 #include <string>
@@ -16,6 +17,11 @@
 #include <vector>
 
 namespace dfb {
+
+// Seconds on a monotonic clock (setup step timing).
+inline double wall_seconds() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
 
 typedef std::complex<double> cplx;
 
@@ -145,6 +151,13 @@ struct Plan {
   bool keep_lists = false;
   std::vector<int32_t> rec_far_hf, rec_far_lf, rec_near;
   double t_tree = 0, t_lists = 0, t_tables = 0, t_walk = 0;  // t_walk: part of t_lists
+  // wall time of each setup step, in order (name, seconds)
+  std::vector<std::pair<const char*, double>> t_steps;
+  void step(const char* name, double& t0) {  // records now - t0 and resets t0
+    const double t = wall_seconds();
+    t_steps.push_back({name, t - t0});
+    t0 = t;
+  }
   bool tree_on_device = false;  // the octrees' particle ordering ran on the device
 };
 

@@ -364,9 +364,11 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
       return st;
     return 0;
   };
+  double tstep = wall_seconds();
   DTree T{}, S{};
   int st;
   if ((st = dtree(p.T, locT, T)) || (st = dtree(p.S, locS, S))) return st;
+  p.step("walk: cells per level, trees to the device", tstep);
 
   p.sT = Slots();
   p.sS = Slots();
@@ -624,6 +626,7 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
   p.sS.lvl_begin[nlvl] = p.sS.n;
   walk.near_pairs.resize(near_h.size());
   for (size_t i = 0; i < near_h.size(); i++) walk.near_pairs[i] = {near_h[i].x, near_h[i].y};
+  p.step("walk: levels (pairs, cones, effective directions, slots, far entries)", tstep);
 
   // M2L entries grouped by target slot: a stable radix sort of all levels'
   // entries (level order, then walk order) by target slot, as the host's
@@ -721,7 +724,9 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
   if (!pos) return fail_out(-5);
   if ((st = scan(cnt, pos, nslot + 1)) || (st = scan(used, pid, ntab + 1))) return fail_out(st);
   if (n) k_renumber<<<nblk(n), 256>>>(n, pid, (uint32_t*)key_out);
-  if (cudaDeviceSynchronize() != cudaSuccess) {
+  const cudaError_t esync = cudaDeviceSynchronize();
+  p.step("walk: far entries by target slot (radix sorts)", tstep);
+  if (esync != cudaSuccess) {
     cudaGetLastError();
     err = "device plan: M2L grouping failed";
     return fail_out(-4);
@@ -741,6 +746,7 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
   p.dev_m2l_tab = key_out;
   p.n_m2l = n;
   walk.m2l_done = true;
+  p.step("walk: M2L pointers and spectrum ids to the host", tstep);
   return 0;
 }
 

@@ -129,6 +129,12 @@ int defmm_set_rhs_per_cta(defmm_handle* h, int rb);
  * slot per CTA, rhs_per_cta right-hand sides.  Results are bit-identical
  * either way. */
 int defmm_set_m2l_staging(defmm_handle* h, int on);
+/* No counterpart in the reference.  Wall time of each step of the last
+ * prcmpt (octrees, levels and tables, the level walk's parts, slot lists,
+ * near-field lists, transfer spectra) as text lines "seconds<TAB>step".
+ * On entry *len is the capacity of buf (buf may be NULL); on return *len is
+ * the size needed including the terminating zero. */
+int defmm_setup_times(const defmm_handle* h, char* buf, int64_t* len);
 
 /* No counterpart in the reference.  Independent operators (handles of
  * problems of any sizes, orders and wavenumbers) applied together: each
