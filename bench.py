@@ -215,6 +215,11 @@ def phase_rooflines(info, L, phases, head, hn, peaks, l2_gbs, tune, rb_block=4):
                 tr = json.load(f).get(head, {})
             if tr.get("kernel") == kname and tr.get("bytes_per_pair") is not None:
                 head_rl["traffic"] = tr["bytes_per_pair"] * n_far
+            elif tr.get("kernel") == kname and tr.get("traffic_per_algorithmic_byte") is not None:
+                head_rl["traffic"] = tr["traffic_per_algorithmic_byte"] * m2l_hbm
+                head_rl["traffic_note"] = ("DRAM bytes per right-hand side: the ncu ratio of traffic to "
+                                           "algorithmic bytes on a smaller case (profiles/m2l_traffic.json) "
+                                           "times this run's algorithmic bytes")
         except (OSError, ValueError):
             pass
     return {"headline": head_rl, "phases": out}

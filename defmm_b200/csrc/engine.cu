@@ -108,6 +108,7 @@ struct defmm_handle {
   int rhs_block = 16;     // right-hand sides per pass of multi-RHS calls
   int rhs_block_m2l = 4;  // right-hand sides per M2L CTA (capped by the order)
   bool m2l_staging = false;  // grouped layout, FP32: shared-memory-staged M2L with target groups
+  int tune_level = -1;        // >= 0: timing runs of the autotuner (near field + M2L of this level only)
   int64_t m2l_lgroup = 0;   // longest list total of kM2LGroup consecutive target slots
   bool use_tc = false;    // mixed precision: P2M on the tensor cores (tcgen05)
   int groups_forced = 0;  // > 0: direction groups requested (also for one RHS)
@@ -659,12 +660,18 @@ int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) 
   const int nl = p.lv.nlvl;
   h->cur = s;
   int64_t nl_ = 0;
+  // autotuner timing run: only the phases its choices change (the near
+  // field, and M2L of the level with the most far pairs) on whatever the
+  // buffers hold; the next full matvec starts from fresh gathers and zeros
+  const bool tuning = h->tune_level >= 0 && h->events;
   rec(h, 2 * PH_TOTAL);
-  dfb::launch_gather(fp64, qin, d.S_perm, h->q.p, nS, 0, 0, 1, s);
-  nl_ += 1 + (p.p2m_leaf.empty() ? 0 : 1) + (p.l2p_leaf.empty() ? 0 : 1) + 1;
-  CK(cudaMemsetAsync(h->pfar.p, 0, 16 * nT, s));
+  if (!tuning) {
+    dfb::launch_gather(fp64, qin, d.S_perm, h->q.p, nS, 0, 0, 1, s);
+    nl_ += 1 + (p.p2m_leaf.empty() ? 0 : 1) + (p.l2p_leaf.empty() ? 0 : 1) + 1;
+    CK(cudaMemsetAsync(h->pfar.p, 0, 16 * nT, s));
+    CK(cudaMemsetAsync(h->Lx.p, 0, h->Lx.bytes, s));
+  }
   CK(cudaMemsetAsync(h->pnear.p, 0, 16 * nT, s));
-  CK(cudaMemsetAsync(h->Lx.p, 0, h->Lx.bytes, s));
   // near field on the second stream, overlapping the far field
   // (profiling runs it on the main stream so that phase times do not overlap)
   cudaStream_t sn = h->events ? s : h->st2;
@@ -694,6 +701,40 @@ int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) 
     nl_ += p.p2p_order.empty() ? 0 : 2;
   }
   if (h->events) cudaEventRecord(h->ev[2 * PH_P2P + 1], sn);
+  if (tuning) {
+    const int l = h->tune_level;
+    const auto& cS = p.sS.cone_begin[l];
+    const auto& cT = p.sT.cone_begin[l];
+    const int nc = (int)cS.size() - 1;
+    float tm2l = 0;
+    for (int c0 = 0; c0 < nc;) {
+      int c1 = c0 + 1;
+      while (c1 < nc && cS[c1 + 1] - cS[c0] <= h->f_cap) c1++;
+      const int64_t fs0 = cS[c0], fs1 = cS[c1], ts0 = cT[c0], ts1 = cT[c1];
+      if (ts1 > ts0 && fs1 > fs0) {
+        rec(h, 2 * PH_M2L);
+        ops->m2l(d, ts0, ts1, fs0, fs1, h->F.p, h->ptab.p, h->Lx.p, h->d_queue + 1, h->nsm, h->m2l_nt[fp64 ? 0 : 1],
+                 h->m2l_pair[fp64 ? 0 : 1], sf);
+        rec(h, 2 * PH_M2L + 1);
+        nl_++;
+        float a;
+        CK(cudaEventSynchronize(h->ev[2 * PH_M2L + 1]));
+        cudaEventElapsedTime(&a, h->ev[2 * PH_M2L], h->ev[2 * PH_M2L + 1]);
+        tm2l += a;
+      }
+      c0 = c1;
+    }
+    CK(cudaStreamSynchronize(sn));
+    CK(cudaStreamSynchronize(s));
+    for (int i = 0; i < PH_N; i++) h->phase_ms[i] = 0;
+    float a = 0;
+    cudaEventElapsedTime(&a, h->ev[2 * PH_P2P], h->ev[2 * PH_P2P + 1]);
+    h->phase_ms[PH_P2P] = a;
+    h->phase_ms[PH_M2L] = tm2l;
+    h->launches += nl_;
+    CK(cudaGetLastError());
+    return 0;
+  }
   // upward pass
   rec(h, 2 * PH_P2M);
   if (!fp64 && tc_on(h))
@@ -1273,10 +1314,21 @@ int defmm_autotune(defmm_handle* h, int reps, int32_t* choice) {
   const bool ev = h->events;
   h->events = true;  // phase timers, phases serialised
   drop_graph(h);     // the captured graph holds the old launch choices
-  // phases are serialised and timed separately in profiled matvecs, so one
-  // matvec times one M2L candidate and one near-field candidate together:
-  // four matvecs (the M2L candidates: one or two target slots per CTA at 128
-  // or 256 threads) cover the three near-field ones
+  {  // timing runs: the near field and M2L of the level with the most far pairs
+    const Plan& q = h->plan;
+    int64_t best = -1;
+    for (int l = q.lv.max_stage; l < q.lv.nlvl; l++) {
+      const int64_t e = q.m2l_ptr[q.sT.lvl_begin[l + 1]] - q.m2l_ptr[q.sT.lvl_begin[l]];
+      if (e > best) {
+        best = e;
+        h->tune_level = l;
+      }
+    }
+  }
+  // phases are serialised and timed separately in profiled runs, so one run
+  // times one M2L candidate and one near-field candidate together: four
+  // runs (the M2L candidates: one or two target slots per CTA at 128 or 256
+  // threads) cover the three near-field ones
   int m2l_best = 128, pair_best = 0, bps_best = 16;
   double tb_m2l = 1e300, tb_p2p = 1e300;
   const int m2l_cand[4][2] = {{0, 128}, {0, 256}, {1, 128}, {1, 256}};
@@ -1306,6 +1358,7 @@ int defmm_autotune(defmm_handle* h, int reps, int32_t* choice) {
   h->m2l_pair[pi] = pair_best;
   h->p2p_bps[pi] = bps_best;
   h->events = ev;
+  h->tune_level = -1;
   if (st) return st;
   {
     std::lock_guard<std::mutex> lock(g_tune_mu);
