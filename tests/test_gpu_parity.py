@@ -297,6 +297,48 @@ def test_staged_m2l_matches_one_target_per_cta(name, gpu):
     assert rel(P[0], po) <= MIXED_TOL
 
 
+def small_case(name):
+    if name == "sphere300":  # 3 levels, 48 far pairs
+        p = W.sphere_surface(300, seed=3, wavelengths=2).points
+        return p, p, 3, 32, 2 * np.pi
+    if name == "cube1000":  # order 4, leaf 16
+        p = W.cube_surface(1000, seed=4).points
+        return p, p, 4, 16, 2 * np.pi * 4 / np.sqrt(3)
+    if name == "near_only":  # a small target sphere inside source blobs: no far pair at all
+        src = W.gaussian_blobs(3000, seed=5, wavelengths=4).points
+        return src, W.sphere_surface(150, seed=6).points * 0.3, 4, 32, 2 * np.pi * 4 / np.sqrt(3)
+    raise KeyError(name)
+
+
+@pytest.mark.parametrize("name", ["sphere300", "cube1000", "near_only"])
+def test_small_and_degenerate_problems(name, gpu):
+    # the smallest valid trees (a few levels, tens of far pairs), and a
+    # problem whose interactions are all near field: FP64 against the oracle,
+    # mixed against FP64, several right-hand sides (one pass and forced
+    # direction groups) against single calls
+    src, trg, L, ncrit, kappa = small_case(name)
+    A = make(src, trg, L, ncrit, kappa)
+    rng = np.random.default_rng(11)
+    Q = (rng.uniform(-1, 1, (3, len(src))) + 1j * rng.uniform(-1, 1, (3, len(src)))).astype(np.complex128)
+    p = A.matvec(Q[0])
+    assert rel(p, O.OracleFMM(src, trg, L, ncrit, kappa, -1).gemv(Q[0])) <= FP64_TOL
+    if name == "near_only":
+        assert A.info("far_hf") + A.info("far_lf") == 0
+    single = np.stack([A.matvec(Q[r]) for r in range(3)])
+    for groups in (0, 2):
+        A.set_blocking(3, groups)
+        P = A.matvec(Q)
+        assert A.info("rhs_block") == 3
+        for r in range(3):
+            assert rel(P[r], single[r]) <= 1e-13
+    A.set_precision("mixed")
+    A.set_blocking(16, 0)
+    assert rel(A.matvec(Q[0]), p) <= MIXED_TOL
+    P = A.matvec(Q)
+    for r in range(3):
+        assert rel(P[r], single[r]) <= MIXED_TOL
+
+
 def test_launch_choices_and_autotune_keep_results_bit_identical(gpu):
     # M2L threads per CTA, one or two target slots per M2L CTA and near-field
     # CTAs per SM change only the schedule: every combination gives the same
