@@ -680,6 +680,7 @@ def main():
             A.autotune(reps=1)
             tune_s += time.perf_counter() - t0
         tune[prec] = {k: A.info(k) for k in ("m2l_threads", "m2l_pairing", "p2p_blocks_per_sm")}
+        tune[prec]["m2l_per_level"] = A.m2l_schedule()
         launches = [0]
 
         def one():

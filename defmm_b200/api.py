@@ -90,6 +90,7 @@ def lib():
             "defmm_set_rhs_per_cta": (ctypes.c_int, [vp, ctypes.c_int]),
             "defmm_set_tensor_cores": (ctypes.c_int, [vp, ctypes.c_int]),
             "defmm_set_m2l_staging": (ctypes.c_int, [vp, ctypes.c_int]),
+            "defmm_m2l_schedule": (ctypes.c_int, [vp, ip, ip, ctypes.c_int]),
             "defmm_setup_times": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.POINTER(i64)]),
             "defmm_batch_create": (vp, [i64, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.c_int]),
             "defmm_batch_launch": (ctypes.c_int, [vp, vp]),
@@ -214,6 +215,13 @@ class IBFMM_Mat:
     def set_tensor_cores(self, on=True):
         """Mixed precision: P2M on the tensor cores (tcgen05, split TF32)."""
         self._check(lib().defmm_set_tensor_cores(self._h, int(bool(on))))
+
+    def m2l_schedule(self) -> list:
+        """(threads, pairing) of the M2L launches per level, current precision."""
+        n = int(self.info("nlvl"))
+        t, p = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        self._check(lib().defmm_m2l_schedule(self._h, _ip(t), _ip(p), n))
+        return [(int(a), int(b)) for a, b in zip(t, p)]
 
     def setup_times(self) -> dict:
         """Seconds per step of the last prcmpt (defmm_setup_times)."""

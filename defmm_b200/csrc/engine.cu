@@ -98,6 +98,9 @@ struct defmm_handle {
   // slot (0: the order's default) and near-field CTAs per SM
   int m2l_nt[2] = {0, 0};
   int m2l_pair[2] = {0, 0};  // two target slots per M2L CTA
+  // per-level choices of the autotuner (per precision; < 0: the values above)
+  int16_t m2l_lvl_nt[2][32], m2l_lvl_pair[2][32];
+  double tune_lvl_ms[32];     // M2L time per level of the last timing run
   int p2p_bps[2] = {16, 16};
   int64_t nchunk = 0;
   size_t dev_bytes = 0;
@@ -158,6 +161,16 @@ void free_buf(DevBuf& b) {
   if (b.p) cudaFree(b.p);
   b.p = nullptr;
   b.bytes = 0;
+}
+
+// M2L launch choice of level l (the autotuner's per-level pick, else the
+// operator-wide one)
+void m2l_choice(const defmm_handle* h, int pi, int l, int* nt, int* pair) {
+  *nt = h->m2l_lvl_nt[pi][l] >= 0 ? h->m2l_lvl_nt[pi][l] : h->m2l_nt[pi];
+  *pair = h->m2l_lvl_pair[pi][l] >= 0 ? h->m2l_lvl_pair[pi][l] : h->m2l_pair[pi];
+}
+void m2l_levels_reset(defmm_handle* h, int pi) {
+  for (int l = 0; l < 32; l++) h->m2l_lvl_nt[pi][l] = h->m2l_lvl_pair[pi][l] = -1;
 }
 
 int ensure(defmm_handle* h, DevBuf& b, size_t bytes) {
@@ -702,27 +715,31 @@ int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) 
   }
   if (h->events) cudaEventRecord(h->ev[2 * PH_P2P + 1], sn);
   if (tuning) {
-    const int l = h->tune_level;
-    const auto& cS = p.sS.cone_begin[l];
-    const auto& cT = p.sT.cone_begin[l];
-    const int nc = (int)cS.size() - 1;
     float tm2l = 0;
-    for (int c0 = 0; c0 < nc;) {
-      int c1 = c0 + 1;
-      while (c1 < nc && cS[c1 + 1] - cS[c0] <= h->f_cap) c1++;
-      const int64_t fs0 = cS[c0], fs1 = cS[c1], ts0 = cT[c0], ts1 = cT[c1];
-      if (ts1 > ts0 && fs1 > fs0) {
-        rec(h, 2 * PH_M2L);
-        ops->m2l(d, ts0, ts1, fs0, fs1, h->F.p, h->ptab.p, h->Lx.p, h->d_queue + 1, h->nsm, h->m2l_nt[fp64 ? 0 : 1],
-                 h->m2l_pair[fp64 ? 0 : 1], sf);
-        rec(h, 2 * PH_M2L + 1);
-        nl_++;
-        float a;
-        CK(cudaEventSynchronize(h->ev[2 * PH_M2L + 1]));
-        cudaEventElapsedTime(&a, h->ev[2 * PH_M2L], h->ev[2 * PH_M2L + 1]);
-        tm2l += a;
+    for (int l = p.lv.max_stage; l < nl; l++) {
+      h->tune_lvl_ms[l] = 0;
+      const auto& cS = p.sS.cone_begin[l];
+      const auto& cT = p.sT.cone_begin[l];
+      const int nc = (int)cS.size() - 1;
+      int nt_l, pair_l;
+      m2l_choice(h, fp64 ? 0 : 1, l, &nt_l, &pair_l);
+      for (int c0 = 0; c0 < nc;) {
+        int c1 = c0 + 1;
+        while (c1 < nc && cS[c1 + 1] - cS[c0] <= h->f_cap) c1++;
+        const int64_t fs0 = cS[c0], fs1 = cS[c1], ts0 = cT[c0], ts1 = cT[c1];
+        if (ts1 > ts0 && fs1 > fs0) {
+          rec(h, 2 * PH_M2L);
+          ops->m2l(d, ts0, ts1, fs0, fs1, h->F.p, h->ptab.p, h->Lx.p, h->d_queue + 1, h->nsm, nt_l, pair_l, sf);
+          rec(h, 2 * PH_M2L + 1);
+          nl_++;
+          float a;
+          CK(cudaEventSynchronize(h->ev[2 * PH_M2L + 1]));
+          cudaEventElapsedTime(&a, h->ev[2 * PH_M2L], h->ev[2 * PH_M2L + 1]);
+          tm2l += a;
+          h->tune_lvl_ms[l] += a;
+        }
+        c0 = c1;
       }
-      c0 = c1;
     }
     CK(cudaStreamSynchronize(sn));
     CK(cudaStreamSynchronize(s));
@@ -767,8 +784,9 @@ int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) 
         nl_ += 2;
         rec(h, 2 * PH_M2F + 1);
         rec(h, 2 * PH_M2L);
-        ops->m2l(d, ts0, ts1, fs0, fs1, h->F.p, h->ptab.p, h->Lx.p, h->d_queue + 1, h->nsm, h->m2l_nt[fp64 ? 0 : 1],
-                 h->m2l_pair[fp64 ? 0 : 1], sf);
+        int nt_l, pair_l;
+        m2l_choice(h, fp64 ? 0 : 1, l, &nt_l, &pair_l);
+        ops->m2l(d, ts0, ts1, fs0, fs1, h->F.p, h->ptab.p, h->Lx.p, h->d_queue + 1, h->nsm, nt_l, pair_l, sf);
         rec(h, 2 * PH_M2L + 1);
         if (h->events) {
           float a;
@@ -933,10 +951,11 @@ int run_gemv_grouped(defmm_handle* h, const double2* qin, int64_t stride_in, dou
           ops->m2f((fs1 - fs0) * R, (const char*)Mbase + (size_t)fs0 * slot_b, g.F.p, s);
         });
         timed(PH_M2L, [&] {
-          if (R == 1)
-            ops->m2l(d, ts0, ts1, fs0, fs1, g.F.p, h->ptab.p, Lbase, h->d_queue + 1, h->nsm, h->m2l_nt[pi],
-                     h->m2l_pair[pi], s);
-          else
+          if (R == 1) {
+            int nt_l, pair_l;
+            m2l_choice(h, pi, l, &nt_l, &pair_l);
+            ops->m2l(d, ts0, ts1, fs0, fs1, g.F.p, h->ptab.p, Lbase, h->d_queue + 1, h->nsm, nt_l, pair_l, s);
+          } else
             ops->m2l_rhs(d, ts0, ts1, fs0, fs1, R, h->rhs_block_m2l, g.F.p, h->ptab.p, Lbase, h->d_queue + 1,
                          h->nsm, h->m2l_staging ? h->m2l_lgroup : 0, s);
         });
@@ -1169,7 +1188,11 @@ int ensure_device(defmm_handle* h) {
 // Launch choices of defmm_autotune per operator shape (order, precision,
 // levels, slots, far pairs, particle interactions, device) in this process.
 std::mutex g_tune_mu;
-std::map<std::array<int64_t, 9>, std::array<int, 3>> g_tune;
+struct TuneChoice {
+  int nt = 128, pair = 0, bps = 16;
+  int16_t lvl_nt[32], lvl_pair[32];  // per level; < 0: nt / pair
+};
+std::map<std::array<int64_t, 9>, TuneChoice> g_tune;
 
 uint64_t splitmix(uint64_t& s) {
   uint64_t z = (s += 0x9e3779b97f4a7c15ULL);
@@ -1192,7 +1215,12 @@ int defmm_device_count(void) {
   return n;
 }
 
-defmm_handle* defmm_create(void) { return new defmm_handle(); }
+defmm_handle* defmm_create(void) {
+  defmm_handle* h = new defmm_handle();
+  m2l_levels_reset(h, 0);
+  m2l_levels_reset(h, 1);
+  return h;
+}
 
 void defmm_destroy(defmm_handle* h) {
   if (!h) return;
@@ -1269,6 +1297,7 @@ int defmm_set_launch(defmm_handle* h, int m2l_threads, int p2p_blocks_per_sm) {
   const int pi = h->precision == DEFMM_PRECISION_FP64 ? 0 : 1;
   h->m2l_nt[pi] = m2l_threads;
   h->p2p_bps[pi] = p2p_blocks_per_sm ? p2p_blocks_per_sm : 16;
+  m2l_levels_reset(h, pi);
   if (h->device >= 0) drop_graph(h);
   return 0;
 }
@@ -1276,6 +1305,7 @@ int defmm_set_launch(defmm_handle* h, int m2l_threads, int p2p_blocks_per_sm) {
 int defmm_set_m2l_pairing(defmm_handle* h, int on) {
   if (!h || (on != 0 && on != 1)) return DEFMM_ERR_ARG;
   h->m2l_pair[h->precision == DEFMM_PRECISION_FP64 ? 0 : 1] = on;
+  m2l_levels_reset(h, h->precision == DEFMM_PRECISION_FP64 ? 0 : 1);
   if (h->device >= 0) drop_graph(h);
   return 0;
 }
@@ -1294,13 +1324,18 @@ int defmm_autotune(defmm_handle* h, int reps, int32_t* choice) {
     auto it = g_tune.find(key);
     if (it != g_tune.end()) {
       const int pi = h->precision == DEFMM_PRECISION_FP64 ? 0 : 1;
-      h->m2l_nt[pi] = it->second[0];
-      h->m2l_pair[pi] = it->second[1];
-      h->p2p_bps[pi] = it->second[2];
+      const TuneChoice& c = it->second;
+      h->m2l_nt[pi] = c.nt;
+      h->m2l_pair[pi] = c.pair;
+      h->p2p_bps[pi] = c.bps;
+      for (int l = 0; l < 32; l++) {
+        h->m2l_lvl_nt[pi][l] = c.lvl_nt[l];
+        h->m2l_lvl_pair[pi][l] = c.lvl_pair[l];
+      }
       drop_graph(h);
       if (choice) {
-        choice[0] = it->second[0];
-        choice[1] = it->second[2];
+        choice[0] = c.nt;
+        choice[1] = c.bps;
       }
       return 0;
     }
@@ -1314,23 +1349,32 @@ int defmm_autotune(defmm_handle* h, int reps, int32_t* choice) {
   const bool ev = h->events;
   h->events = true;  // phase timers, phases serialised
   drop_graph(h);     // the captured graph holds the old launch choices
-  {  // timing runs: the near field and M2L of the level with the most far pairs
-    const Plan& q = h->plan;
+  // timing runs: the near field and every level's M2L (run_gemv in tuning
+  // mode), M2L timed per level so each level gets its own launch choice
+  const Plan& q = h->plan;
+  int busiest = q.lv.max_stage;
+  {
     int64_t best = -1;
     for (int l = q.lv.max_stage; l < q.lv.nlvl; l++) {
       const int64_t e = q.m2l_ptr[q.sT.lvl_begin[l + 1]] - q.m2l_ptr[q.sT.lvl_begin[l]];
       if (e > best) {
         best = e;
-        h->tune_level = l;
+        busiest = l;
       }
     }
   }
-  // phases are serialised and timed separately in profiled runs, so one run
-  // times one M2L candidate and one near-field candidate together: four
-  // runs (the M2L candidates: one or two target slots per CTA at 128 or 256
-  // threads) cover the three near-field ones
-  int m2l_best = 128, pair_best = 0, bps_best = 16;
-  double tb_m2l = 1e300, tb_p2p = 1e300;
+  h->tune_level = busiest;
+  m2l_levels_reset(h, pi);
+  // one run times one M2L candidate (every level) and one near-field
+  // candidate together: four runs (the M2L candidates: one or two target
+  // slots per CTA at 128 or 256 threads) cover the three near-field ones
+  int bps_best = 16;
+  double tb_p2p = 1e300, tb_lvl[32];
+  int best_lvl[32];
+  for (int l = 0; l < 32; l++) {
+    tb_lvl[l] = 1e300;
+    best_lvl[l] = 0;
+  }
   const int m2l_cand[4][2] = {{0, 128}, {0, 256}, {1, 128}, {1, 256}};
   const int bps_cand[3] = {8, 16, 32};
   for (int i = 0; i < 4 && !st; i++) {
@@ -1338,35 +1382,63 @@ int defmm_autotune(defmm_handle* h, int reps, int32_t* choice) {
     h->m2l_nt[pi] = m2l_cand[i][1];
     const int b = bps_cand[i < 3 ? i : 2];
     h->p2p_bps[pi] = b;
-    double tm = 1e300, tp = 1e300;
+    double tp = 1e300, tl[32];
+    for (int l = 0; l < 32; l++) tl[l] = 1e300;
     for (int r = 0; r < reps && !st; r++) {
       st = run_gemv(h, (const double2*)h->rin.p, (double2*)h->rout.p, h->st);
-      tm = std::min(tm, h->phase_ms[PH_M2L]);
       tp = std::min(tp, h->phase_ms[PH_P2P]);
+      for (int l = q.lv.max_stage; l < q.lv.nlvl; l++) tl[l] = std::min(tl[l], h->tune_lvl_ms[l]);
     }
-    if (tm < tb_m2l) {
-      tb_m2l = tm;
-      pair_best = m2l_cand[i][0];
-      m2l_best = m2l_cand[i][1];
-    }
+    for (int l = q.lv.max_stage; l < q.lv.nlvl; l++)
+      if (tl[l] < tb_lvl[l]) {
+        tb_lvl[l] = tl[l];
+        best_lvl[l] = i;
+      }
     if (i < 3 && tp < tb_p2p) {
       tb_p2p = tp;
       bps_best = b;
     }
   }
-  h->m2l_nt[pi] = m2l_best;
-  h->m2l_pair[pi] = pair_best;
-  h->p2p_bps[pi] = bps_best;
+  // operator-wide choice: the busiest level's; per-level overrides elsewhere
+  TuneChoice c;
+  c.nt = m2l_cand[best_lvl[busiest]][1];
+  c.pair = m2l_cand[best_lvl[busiest]][0];
+  c.bps = bps_best;
+  for (int l = 0; l < 32; l++) c.lvl_nt[l] = c.lvl_pair[l] = -1;
+  for (int l = q.lv.max_stage; l < q.lv.nlvl; l++) {
+    c.lvl_nt[l] = (int16_t)m2l_cand[best_lvl[l]][1];
+    c.lvl_pair[l] = (int16_t)m2l_cand[best_lvl[l]][0];
+  }
+  h->m2l_nt[pi] = c.nt;
+  h->m2l_pair[pi] = c.pair;
+  h->p2p_bps[pi] = c.bps;
+  for (int l = 0; l < 32; l++) {
+    h->m2l_lvl_nt[pi][l] = c.lvl_nt[l];
+    h->m2l_lvl_pair[pi][l] = c.lvl_pair[l];
+  }
   h->events = ev;
   h->tune_level = -1;
   if (st) return st;
   {
     std::lock_guard<std::mutex> lock(g_tune_mu);
-    g_tune[key] = {m2l_best, pair_best, bps_best};
+    g_tune[key] = c;
   }
   if (choice) {
-    choice[0] = m2l_best;
-    choice[1] = bps_best;
+    choice[0] = c.nt;
+    choice[1] = c.bps;
+  }
+  return 0;
+}
+
+int defmm_m2l_schedule(const defmm_handle* h, int32_t* threads, int32_t* pairing, int n) {
+  if (!h || n < 0 || (n && (!threads || !pairing))) return DEFMM_ERR_ARG;
+  const int pi = h->precision == DEFMM_PRECISION_FP64 ? 0 : 1;
+  const int PP = h->built ? h->plan.PP : 0;
+  for (int l = 0; l < n; l++) {
+    int nt = 0, pair = 0;
+    if (l < 32) m2l_choice(h, pi, l, &nt, &pair);
+    threads[l] = nt ? nt : (PP > 1024 ? 256 : 128);
+    pairing[l] = pair;
   }
   return 0;
 }

@@ -265,15 +265,22 @@ int defmm_keep_lists(defmm_handle* h, int on);
 int defmm_set_plan_device(defmm_handle* h, int on);
 
 /* No counterpart in the reference.  Autotuner: on this operator and its
- * current precision, times `reps` profiled matvecs (zero charges, the
- * handle's own vectors) per candidate launch choice and keeps the fastest:
- * M2L threads per CTA (128 or 256) with one or two target slots per CTA
- * (timed on the M2L phase) and near-field CTAs per SM (8, 16 or 32, timed on
- * the near-field phase).  Every choice gives bit-identical results.  The
- * M2L threads and near-field CTAs per SM are written to choice[2] when not
- * NULL (also DEFMM_INFO_M2L_THREADS / DEFMM_INFO_P2P_BLOCKS_PER_SM; the
- * pairing: DEFMM_INFO_M2L_PAIRING); the next matvec captures a new graph. */
+ * current precision, times `reps` timing runs (the near field and every
+ * level's M2L on the handle's own buffers) per candidate launch choice and
+ * keeps the fastest: per level, M2L threads per CTA (128 or 256) with one or
+ * two target slots per CTA (timed on that level's M2L), and near-field CTAs
+ * per SM (8, 16 or 32, timed on the near-field phase).  Every choice gives
+ * bit-identical results.  The choice of the level with the most far pairs
+ * and the near-field CTAs per SM are written to choice[2] when not NULL
+ * (also DEFMM_INFO_M2L_THREADS / DEFMM_INFO_M2L_PAIRING /
+ * DEFMM_INFO_P2P_BLOCKS_PER_SM; every level's: defmm_m2l_schedule); the next
+ * matvec captures a new graph.  Choices are cached per operator shape in the
+ * process. */
 int defmm_autotune(defmm_handle* h, int reps, int32_t* choice);
+/* No counterpart in the reference.  The M2L launch choice of levels
+ * 0 .. n-1 for the current precision: threads[l] per CTA and pairing[l]
+ * (1: two target slots per CTA). */
+int defmm_m2l_schedule(const defmm_handle* h, int32_t* threads, int32_t* pairing, int n);
 /* No counterpart in the reference.  Sets the same launch choices by hand for
  * the current precision: m2l_threads 128 or 256 (0: the order's default),
  * p2p_blocks_per_sm 1..64 (0: 16). */

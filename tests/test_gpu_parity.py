@@ -360,7 +360,14 @@ def test_launch_choices_and_autotune_keep_results_bit_identical(gpu):
         assert c["m2l_threads"] in (128, 256) and c["p2p_blocks_per_sm"] in (8, 16, 32)
         assert c["m2l_pairing"] in (0, 1)
         assert A.info("m2l_threads") == c["m2l_threads"]
+        sched = A.m2l_schedule()  # the autotuner's choice per level
+        assert len(sched) == A.info("nlvl")
+        assert all(t in (128, 256) and pr in (0, 1) for t, pr in sched)
         assert np.array_equal(A.matvec(q), ref)
+        # the grouped layout runs the same per-level choices
+        A.set_blocking(16, 2)
+        assert np.array_equal(A.matvec(q), A.matvec(q))
+        A.set_blocking(16, 0)
 
 
 
