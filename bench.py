@@ -536,9 +536,10 @@ def run_orders(args, torch):
     """Error against FP64 direct sums (2,000 seeded targets) and time per
     matvec for orders 4-7, FP64 and mixed, on the spheroid at the 4M
     workload's points per square wavelength: N = 500,000, 90.5 wavelengths
-    along the long axis, leaf 96."""
+    along the long axis, leaf 96 (spheroid_orders4m: the 4M workload itself,
+    256 wavelengths)."""
     from defmm_b200 import IBFMM_Mat, workloads as W
-    n = 500_000
+    n = 4_000_000 if args.workload == "spheroid_orders4m" else 500_000
     rows = []
     for L in (4, 5, 6, 7):
         w = W.spheroid(n, seed=0, order=L, wavelengths=256.0 * math.sqrt(n / 4_000_000))
@@ -567,10 +568,11 @@ def run_orders(args, torch):
             row[prec] = {"ms": e0.elapsed_time(e1) / args.steps, "vs_direct": A.check_full(2000, seed=7)}
         row["mixed_vs_fp64_rel_l2"] = float(np.linalg.norm(out["mixed"] - out["fp64"]) / np.linalg.norm(out["fp64"]))
         rows.append(row)
-        del A
+        del A, dq, dp
+        torch.cuda.empty_cache()
     line = {"metric": "FMM error vs FP64 direct sums and ms per matvec by order, spheroid", "impl": "ours",
             "unit": "relative error", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "data": "synthetic",
-            "config": {"workload": "spheroid_orders", "n_points": n, "leaf_size": 96,
+            "config": {"workload": args.workload, "n_points": n, "leaf_size": 96,
                        "wavelengths_long_axis": 256.0 * math.sqrt(n / 4_000_000)},
             "orders": rows}
     print(json.dumps(line), flush=True)
@@ -615,6 +617,7 @@ def main():
             dist.barrier()
 
     extra = {"ragged48": run_ragged, "spheroid4m": run_spheroid, "spheroid_orders": run_orders,
+             "spheroid_orders4m": run_orders,
              "rhs64": run_rhs64, **{m: run_mixture for m in MIXTURES}}
     if args.workload in extra:
         if rank == 0:

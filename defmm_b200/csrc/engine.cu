@@ -111,7 +111,8 @@ struct defmm_handle {
   int rhs_block = 16;     // right-hand sides per pass of multi-RHS calls
   int rhs_block_m2l = 4;  // right-hand sides per M2L CTA (capped by the order)
   bool m2l_staging = false;  // grouped layout, FP32: shared-memory-staged M2L with target groups
-  int tune_level = -1;        // >= 0: timing runs of the autotuner (near field + M2L of this level only)
+  int tune_level = -1;        // >= 0: timing runs of the autotuner (near field + M2L of the tuned levels)
+  bool tune_lvl_on[32];       // levels whose M2L the timing runs execute
   int64_t m2l_lgroup = 0;   // longest list total of kM2LGroup consecutive target slots
   bool use_tc = false;    // mixed precision: P2M on the tensor cores (tcgen05)
   int groups_forced = 0;  // > 0: direction groups requested (also for one RHS)
@@ -718,6 +719,7 @@ int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) 
     float tm2l = 0;
     for (int l = p.lv.max_stage; l < nl; l++) {
       h->tune_lvl_ms[l] = 0;
+      if (!h->tune_lvl_on[l]) continue;
       const auto& cS = p.sS.cone_begin[l];
       const auto& cT = p.sT.cone_begin[l];
       const int nc = (int)cS.size() - 1;
@@ -1365,7 +1367,17 @@ int defmm_autotune(defmm_handle* h, int reps, int32_t* choice) {
   }
   h->tune_level = busiest;
   m2l_levels_reset(h, pi);
-  // one run times one M2L candidate (every level) and one near-field
+  // levels timed on their own: those with at least a tenth of the far pairs
+  // (the others take the busiest level's choice)
+  {
+    const int64_t tot = q.m2l_ptr.empty() ? 0 : q.m2l_ptr.back();
+    for (int l = 0; l < 32; l++) h->tune_lvl_on[l] = false;
+    for (int l = q.lv.max_stage; l < q.lv.nlvl; l++) {
+      const int64_t e = q.m2l_ptr[q.sT.lvl_begin[l + 1]] - q.m2l_ptr[q.sT.lvl_begin[l]];
+      h->tune_lvl_on[l] = l == busiest || 10 * e >= tot;
+    }
+  }
+  // one run times one M2L candidate (the tuned levels) and one near-field
   // candidate together: four runs (the M2L candidates: one or two target
   // slots per CTA at 128 or 256 threads) cover the three near-field ones
   int bps_best = 16;
@@ -1390,7 +1402,7 @@ int defmm_autotune(defmm_handle* h, int reps, int32_t* choice) {
       for (int l = q.lv.max_stage; l < q.lv.nlvl; l++) tl[l] = std::min(tl[l], h->tune_lvl_ms[l]);
     }
     for (int l = q.lv.max_stage; l < q.lv.nlvl; l++)
-      if (tl[l] < tb_lvl[l]) {
+      if (h->tune_lvl_on[l] && tl[l] < tb_lvl[l]) {
         tb_lvl[l] = tl[l];
         best_lvl[l] = i;
       }
@@ -1405,10 +1417,11 @@ int defmm_autotune(defmm_handle* h, int reps, int32_t* choice) {
   c.pair = m2l_cand[best_lvl[busiest]][0];
   c.bps = bps_best;
   for (int l = 0; l < 32; l++) c.lvl_nt[l] = c.lvl_pair[l] = -1;
-  for (int l = q.lv.max_stage; l < q.lv.nlvl; l++) {
-    c.lvl_nt[l] = (int16_t)m2l_cand[best_lvl[l]][1];
-    c.lvl_pair[l] = (int16_t)m2l_cand[best_lvl[l]][0];
-  }
+  for (int l = q.lv.max_stage; l < q.lv.nlvl; l++)
+    if (h->tune_lvl_on[l]) {
+      c.lvl_nt[l] = (int16_t)m2l_cand[best_lvl[l]][1];
+      c.lvl_pair[l] = (int16_t)m2l_cand[best_lvl[l]][0];
+    }
   h->m2l_nt[pi] = c.nt;
   h->m2l_pair[pi] = c.pair;
   h->p2p_bps[pi] = c.bps;

@@ -1920,11 +1920,23 @@ __global__ void __launch_bounds__(128) k_p2p_rhs(DevPlan P, int64_t nitem, const
             const double2 a = sa[j], bz = sb[j];
             const Q* qj = sq + j * RB;
             const float2 g = green32(x0 - a.x, x1 - a.y, x2 - bz.x, P.kappa);
+            if constexpr (RB % 2 == 0) {  // two right-hand sides per 16-byte load
+              const float4* q4 = reinterpret_cast<const float4*>(qj);
 #pragma unroll
-            for (int b = 0; b < RB; b++) {
-              const float2 qq = qj[b];
-              fs[b].x = fmaf(g.x, qq.x, fmaf(-g.y, qq.y, fs[b].x));
-              fs[b].y = fmaf(g.x, qq.y, fmaf(g.y, qq.x, fs[b].y));
+              for (int b = 0; b < RB; b += 2) {
+                const float4 qq = q4[b / 2];
+                fs[b].x = fmaf(g.x, qq.x, fmaf(-g.y, qq.y, fs[b].x));
+                fs[b].y = fmaf(g.x, qq.y, fmaf(g.y, qq.x, fs[b].y));
+                fs[b + 1].x = fmaf(g.x, qq.z, fmaf(-g.y, qq.w, fs[b + 1].x));
+                fs[b + 1].y = fmaf(g.x, qq.w, fmaf(g.y, qq.z, fs[b + 1].y));
+              }
+            } else {
+#pragma unroll
+              for (int b = 0; b < RB; b++) {
+                const float2 qq = qj[b];
+                fs[b].x = fmaf(g.x, qq.x, fmaf(-g.y, qq.y, fs[b].x));
+                fs[b].y = fmaf(g.x, qq.y, fmaf(g.y, qq.x, fs[b].y));
+              }
             }
           }
 #pragma unroll

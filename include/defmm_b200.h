@@ -265,10 +265,12 @@ int defmm_keep_lists(defmm_handle* h, int on);
 int defmm_set_plan_device(defmm_handle* h, int on);
 
 /* No counterpart in the reference.  Autotuner: on this operator and its
- * current precision, times `reps` timing runs (the near field and every
- * level's M2L on the handle's own buffers) per candidate launch choice and
- * keeps the fastest: per level, M2L threads per CTA (128 or 256) with one or
- * two target slots per CTA (timed on that level's M2L), and near-field CTAs
+ * current precision, times `reps` timing runs (the near field and the M2L
+ * of every level holding at least a tenth of the far pairs, on the handle's
+ * own buffers) per candidate launch choice and keeps the fastest: per such
+ * level (the others take the busiest level's), M2L threads per CTA (128 or
+ * 256) with one or two target slots per CTA (timed on that level's M2L),
+ * and near-field CTAs
  * per SM (8, 16 or 32, timed on the near-field phase).  Every choice gives
  * bit-identical results.  The choice of the level with the most far pairs
  * and the near-field CTAs per SM are written to choice[2] when not NULL
