@@ -1367,14 +1367,14 @@ int defmm_autotune(defmm_handle* h, int reps, int32_t* choice) {
   }
   h->tune_level = busiest;
   m2l_levels_reset(h, pi);
-  // levels timed on their own: those with at least a tenth of the far pairs
-  // (the others take the busiest level's choice)
+  // levels timed on their own: those with at least a quarter of the far
+  // pairs (the others take the busiest level's choice)
   {
     const int64_t tot = q.m2l_ptr.empty() ? 0 : q.m2l_ptr.back();
     for (int l = 0; l < 32; l++) h->tune_lvl_on[l] = false;
     for (int l = q.lv.max_stage; l < q.lv.nlvl; l++) {
       const int64_t e = q.m2l_ptr[q.sT.lvl_begin[l + 1]] - q.m2l_ptr[q.sT.lvl_begin[l]];
-      h->tune_lvl_on[l] = l == busiest || 10 * e >= tot;
+      h->tune_lvl_on[l] = l == busiest || 4 * e >= tot;
     }
   }
   // one run times one M2L candidate (the tuned levels) and one near-field

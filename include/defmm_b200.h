@@ -266,7 +266,7 @@ int defmm_set_plan_device(defmm_handle* h, int on);
 
 /* No counterpart in the reference.  Autotuner: on this operator and its
  * current precision, times `reps` timing runs (the near field and the M2L
- * of every level holding at least a tenth of the far pairs, on the handle's
+ * of every level holding at least a quarter of the far pairs, on the handle's
  * own buffers) per candidate launch choice and keeps the fastest: per such
  * level (the others take the busiest level's), M2L threads per CTA (128 or
  * 256) with one or two target slots per CTA (timed on that level's M2L),
