@@ -21,7 +21,7 @@ CU = ["fmm_kernels.cu", "tc_interp.cu", "engine.cu", "noalloc.cu", "plan_device.
 # no FMA contraction there
 CU_FLAGS = {"plan_device.cu": ["--fmad=false"]}
 CPP = ["plan.cpp"]
-HEADERS = ["plan.hpp", "kernels.cuh", "device_math.cuh", "ptx.cuh", "fmm_kernels.h", "engine_internal.h", "plan_device.hpp"]
+HEADERS = ["plan.hpp", "kernels.cuh", "device_math.cuh", "ptx.cuh", "fp64_math.hpp", "fmm_kernels.h", "engine_internal.h", "plan_device.hpp"]
 
 
 def _newer(target, deps):

@@ -4,6 +4,8 @@
 
 #include <cuda_runtime.h>
 
+#include "fp64_math.hpp"
+
 namespace dfb {
 
 // ----------------------------------------------------------------- basics --
@@ -27,35 +29,9 @@ __device__ __forceinline__ void lagrange_all(T x, T rad, T* b) {
   }
 }
 
-// FP64 sin and cos of x: Cody-Waite reduction by pi/2 in two FMA steps
-// (pi/2 split into its double and the remainder), then the Taylor series of
-// sin to degree 15 and of cos to degree 16 on [-pi/4, pi/4] (truncation
-// below 7e-17 relative), quadrant by n mod 4.
-__device__ __forceinline__ void sincos_cw(double x, double& s, double& c) {
-  const double n = rint(x * 0.6366197723675814);
-  double r = fma(-n, 1.5707963267948966, x);
-  r = fma(-n, 6.123233995736766e-17, r);
-  const double r2 = r * r;
-  double ps = fma(r2, -7.647163731819816e-13, 1.6059043836821613e-10);
-  ps = fma(r2, ps, -2.505210838544172e-08);
-  ps = fma(r2, ps, 2.7557319223985893e-06);
-  ps = fma(r2, ps, -1.984126984126984e-04);
-  ps = fma(r2, ps, 8.333333333333333e-03);
-  ps = fma(r2, ps, -1.6666666666666666e-01);
-  const double sr = fma(r * r2, ps, r);
-  double pc = fma(r2, 4.779477332387385e-14, -1.1470745597729725e-11);
-  pc = fma(r2, pc, 2.08767569878681e-09);
-  pc = fma(r2, pc, -2.755731922398589e-07);
-  pc = fma(r2, pc, 2.48015873015873e-05);
-  pc = fma(r2, pc, -1.388888888888889e-03);
-  pc = fma(r2, pc, 4.1666666666666664e-02);
-  pc = fma(r2, pc, -0.5);
-  const double cr = fma(r2, pc, 1.0);
-  const int q = __double2int_rn(n) & 3;
-  const double ss = (q & 1) ? cr : sr, cc = (q & 1) ? sr : cr;
-  s = (q & 2) ? -ss : ss;
-  c = ((q + 1) & 2) ? -cc : cc;
-}
+// FP64 sin and cos of x (Cody-Waite reduction by pi/2, Taylor series; the
+// same function the host plan uses, fp64_math.hpp)
+__device__ __forceinline__ void sincos_cw(double x, double& s, double& c) { sincos_fp64(x, s, c); }
 
 // exp(i a) with a in FP64
 template <typename C>

@@ -442,17 +442,62 @@ int prepare_tables(defmm_handle* h) {
     }
     return 0;
   };
-  std::vector<dfb::cplx> s1, s2;
-  for (size_t e = 0; e < p.sig.size() && e < 32; e++) {
-    s1.insert(s1.end(), p.sig[e].begin(), p.sig[e].end());
-    s2.insert(s2.end(), p.sig2[e].begin(), p.sig2[e].end());
-  }
   int st;
-  if ((st = put(h->sig, s1.data(), s1.size())) || (st = put(h->sig2, s2.data(), s2.size()))) return st;
+  DevBuf base;  // transfer spectra, tables x PP, in the precision's complex type
+  if (p.tables_on_device) {
+    // spectra and signatures computed on the device in FP64 (bit-identical
+    // to the host's), then rounded to FP32 for the mixed path
+    size_t nsig = 0;
+    for (size_t e = 0; e < p.sig.size() && e < 32; e++) nsig += p.sig[e].size();
+    const size_t ntabv = p.tab_fund.size() * (size_t)p.PP;
+    DevBuf t64, a64, b64;
+    if ((st = ensure(h, t64, std::max<size_t>(1, ntabv) * 16)) || (st = ensure(h, a64, std::max<size_t>(1, nsig) * 16)) ||
+        (st = ensure(h, b64, std::max<size_t>(1, nsig) * 16))) {
+      free_buf(t64);
+      free_buf(a64);
+      free_buf(b64);
+      return st;
+    }
+    std::string e;
+    st = dfb::device_plan_tables(p, (double2*)t64.p, (double2*)a64.p, (double2*)b64.p, e);
+    if (st) {
+      free_buf(t64);
+      free_buf(a64);
+      free_buf(b64);
+      return h->fail(DEFMM_ERR_CUDA, e);
+    }
+    if (fp64) {
+      std::swap(h->sig, a64);
+      std::swap(h->sig2, b64);
+      std::swap(base, t64);
+    } else {
+      if ((st = ensure(h, h->sig, std::max<size_t>(1, nsig) * 8)) ||
+          (st = ensure(h, h->sig2, std::max<size_t>(1, nsig) * 8)) || (st = ensure(h, base, std::max<size_t>(1, ntabv) * 8))) {
+        free_buf(t64);
+        free_buf(a64);
+        free_buf(b64);
+        return st;
+      }
+      dfb::tables_to_float((const double2*)a64.p, (float2*)h->sig.p, (int64_t)nsig, h->st);
+      dfb::tables_to_float((const double2*)b64.p, (float2*)h->sig2.p, (int64_t)nsig, h->st);
+      dfb::tables_to_float((const double2*)t64.p, (float2*)base.p, (int64_t)ntabv, h->st);
+      CK(cudaStreamSynchronize(h->st));
+    }
+    free_buf(t64);
+    free_buf(a64);
+    free_buf(b64);
+  } else {
+    std::vector<dfb::cplx> s1, s2;
+    for (size_t e = 0; e < p.sig.size() && e < 32; e++) {
+      s1.insert(s1.end(), p.sig[e].begin(), p.sig[e].end());
+      s2.insert(s2.end(), p.sig2[e].begin(), p.sig2[e].end());
+    }
+    if ((st = put(h->sig, s1.data(), s1.size())) || (st = put(h->sig2, s2.data(), s2.size())) ||
+        (st = put(base, p.tables.data(), p.tables.size())))
+      return st;
+  }
   {
     // permuted spectra used by M2L, gathered once on the device
-    DevBuf base;
-    if ((st = put(base, p.tables.data(), p.tables.size()))) return st;
     const int64_t np = (int64_t)p.ptab_key.size();
     if ((st = ensure(h, h->ptab, std::max<int64_t>(1, np) * p.PP * cs + 16))) {  // + slack as for F
       free_buf(base);

@@ -5,6 +5,7 @@
 // floating-point operations are the reference's, in the reference's order, so
 // the outcome is bit-identical; this file is compiled with FMA contraction off.
 #include "plan.hpp"
+#include "fp64_math.hpp"
 
 #include <algorithm>
 #include <atomic>
@@ -16,6 +17,19 @@
 #include <tuple>
 
 namespace dfb {
+
+void dft_twiddles(int P, double* w) {
+  for (int m = 0; m < P; m++) {
+    const long double a = 2.0L * 3.14159265358979323846264338327950288L * m / P;
+    w[2 * m] = (double)cosl(a);
+    w[2 * m + 1] = -(double)sinl(a);
+  }
+}
+
+double node_coord(int i, int L, double alpha) {  // thetis_polynomials.hpp:126
+  return alpha * (-1. + 2. * ((double)i / (double)(L - 1)));
+}
+
 namespace {
 
 unsigned hw_threads() {
@@ -489,7 +503,8 @@ void init_small_tables(Plan& p) {
 
 // planewave.hpp:44-69: sig = exp(-i kappa d.x) on the grid of radius R/2^(l+1)
 // and its square (the grid of radius R/2^l)
-void init_signatures(Plan& p) {
+// values = false: the sizes only (the device fills the values)
+void init_signatures(Plan& p, bool values) {
   const Levels& v = p.lv;
   p.sig.assign(std::max(1, v.cpt + 1), {});
   p.sig2.assign(std::max(1, v.cpt + 1), {});
@@ -502,6 +517,7 @@ void init_signatures(Plan& p) {
     auto& s2 = p.sig2[h];
     s1.resize((size_t)nd * p.LL);
     s2.resize((size_t)nd * p.LL);
+    if (!values) continue;
     pfor(nd, 16, [&](int64_t d) {
       const double* dv = &p.dirs[h][3 * d];
       for (int k = 0; k < p.LL; k++) {
@@ -510,7 +526,9 @@ void init_signatures(Plan& p) {
         double dp = 0.;
         for (int a = 0; a < 3; a++) dp += dv[a] * node1d(I[a], p.L, .5 * locrad);
         const double ang = p.kappa * dp;
-        const cplx s(std::cos(ang), -std::sin(ang));
+        double sn, cs;
+        sincos_fp64(ang, sn, cs);
+        const cplx s(cs, -sn);
         s1[d * p.LL + k] = s;
         s2[d * p.LL + k] = s * s;
       }
@@ -521,10 +539,9 @@ void init_signatures(Plan& p) {
 // Unnormalised forward 3-D DFT of size P (row-major), FP64, by definition.
 void dft3(cplx* x, int P) {
   std::vector<cplx> w(P), line(P), res(P);
-  for (int m = 0; m < P; m++) {
-    const long double a = 2.0L * 3.14159265358979323846264338327950288L * m / P;
-    w[m] = cplx((double)cosl(a), -(double)sinl(a));
-  }
+  std::vector<double> wt(2 * P);
+  dft_twiddles(P, wt.data());
+  for (int m = 0; m < P; m++) w[m] = cplx(wt[2 * m], wt[2 * m + 1]);
   int inner = 1;
   for (int d = 2; d >= 0; d--) {
     const int outer = P * P / inner;
@@ -553,7 +570,9 @@ void transfer_spectrum(const Plan& p, double rad, const int* nI, cplx* out) {
     for (int k = 0; k < 3; k++) z[k] = v[k] + p.tabZ[3 * i + k] * rad;
     const double R = norm3(z);
     const double a = R * p.kappa;
-    out[i] = cplx(std::cos(a), std::sin(a)) / (4. * M_PI * R);
+    double sn, cs;
+    sincos_fp64(a, sn, cs);
+    out[i] = cplx(cs, sn) / (4. * M_PI * R);
   }
   dft3(out, p.P);
 }
@@ -1129,7 +1148,9 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
   if (st) return st;
   init_directions(p);
   init_small_tables(p);
-  init_signatures(p);
+  const bool dev_tables = walker && !p.keep_lists;
+  p.tables_on_device = dev_tables;
+  init_signatures(p, !dev_tables);
   p.step("levels, directions, small tables, signatures", ts);
   const Levels& v = p.lv;
   const int nlvl = v.nlvl;
@@ -1385,17 +1406,24 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
   p.step("near-field symmetric blocks and work items", ts);
   p.t_lists = now_s() - t0;
 
-  // transfer spectra, FP64 (circulant.hpp:133-144)
+  // transfer spectra, FP64 (circulant.hpp:133-144); with a device plan the
+  // device computes them (and the signatures) when the operator uploads
   t0 = now_s();
   const int64_t ntab = (int64_t)tab_nI.size();
-  p.tables.assign(ntab * (size_t)p.PP, cplx(0., 0.));
-  pfor(ntab, 8, [&](int64_t k) {
-    const int l = p.tab_lvl[k];
-    const double rad = p.box_rad / (double)(1 << l);
-    transfer_spectrum(p, rad, tab_nI[k].data(), &p.tables[k * (size_t)p.PP]);
-  });
+  p.tables.clear();
+  p.tab_fund.clear();
+  if (dev_tables) {
+    p.tab_fund = std::move(tab_nI);
+  } else {
+    p.tables.assign(ntab * (size_t)p.PP, cplx(0., 0.));
+    pfor(ntab, 8, [&](int64_t k) {
+      const int l = p.tab_lvl[k];
+      const double rad = p.box_rad / (double)(1 << l);
+      transfer_spectrum(p, rad, tab_nI[k].data(), &p.tables[k * (size_t)p.PP]);
+    });
+  }
   p.t_tables = now_s() - t0;
-  p.step("transfer spectra (FP64)", ts);
+  p.step(dev_tables ? "transfer spectra (left to the device)" : "transfer spectra (FP64)", ts);
   return 0;
 }
 

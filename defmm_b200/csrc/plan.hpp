@@ -18,6 +18,12 @@
 
 namespace dfb {
 
+// exp(-2 pi i m / P), m < P, as (re, im) pairs: the twiddles of the plan's
+// forward DFTs (computed in long double, rounded once).
+void dft_twiddles(int P, double* w);
+// Node i of the equispaced grid of order L on [-alpha, alpha].
+double node_coord(int i, int L, double alpha);
+
 // Seconds on a monotonic clock (setup step timing).
 inline double wall_seconds() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -159,6 +165,11 @@ struct Plan {
     t0 = t;
   }
   bool tree_on_device = false;  // the octrees' particle ordering ran on the device
+  // Transfer spectra and signatures left to the device (device_plan_tables):
+  // `tables` and the values of sig/sig2 stay empty (sig/sig2 keep their
+  // sizes), tab_fund holds each table's fundamental index.
+  bool tables_on_device = false;
+  std::vector<std::array<int32_t, 3>> tab_fund;
 };
 
 // Result of the level-by-level dual traversal (hrzpass.hpp:62-143 with the

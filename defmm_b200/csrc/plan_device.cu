@@ -13,6 +13,7 @@
 #include <memory>
 #include <cstring>
 
+#include "fp64_math.hpp"
 #include "plan.hpp"
 #include "plan_device.hpp"
 
@@ -919,5 +920,167 @@ LevelWalker* device_level_walker() {
 }
 
 std::unique_ptr<TreeSorter> make_device_tree_sorter() { return std::unique_ptr<TreeSorter>(new DeviceSorter()); }
+
+// ------------------------------------------ transfer spectra and signatures --
+// The host plan's FP64 tables computed on the device with the same IEEE
+// operations in the same order (this file is built without FMA contraction;
+// sin and cos are sincos_fp64 on both sides), so they are bit-identical to
+// the host's.
+//
+// Transfer spectrum of table k (circulant.hpp:133-144): the kernel
+// exp(i kappa R) / (4 pi R) at R = |2 nI r + r tabZ_i| on the P^3 circulant
+// grid (r: the level's cell radius), then the unnormalised forward 3-D DFT by
+// definition, last axis first; one CTA per table, one line per thread.
+constexpr int kMaxGrid = 15;  // P = 2L - 1 at the largest order (8)
+
+__global__ void k_spectra(int64_t ntab, int P, const int32_t* __restrict__ fund, const double* __restrict__ rad,
+                          const double* __restrict__ tabZ, double kappa, const double2* __restrict__ tw,
+                          double2* __restrict__ out) {
+  extern __shared__ double2 sx[];
+  const int PP = P * P * P;
+  for (int64_t k = blockIdx.x; k < ntab; k += gridDim.x) {
+    const double r = rad[k];
+    double v[3];
+    for (int a = 0; a < 3; a++) v[a] = __dmul_rn(__dmul_rn(2., (double)fund[3 * k + a]), r);
+    for (int i = threadIdx.x; i < PP; i += blockDim.x) {
+      double t = 0.;
+      for (int a = 0; a < 3; a++) {
+        const double z = __dadd_rn(v[a], __dmul_rn(tabZ[3 * i + a], r));
+        t = __dadd_rn(t, __dmul_rn(z, z));
+      }
+      const double R = __dsqrt_rn(t);
+      double sn, cs;
+      sincos_fp64(__dmul_rn(R, kappa), sn, cs);
+      const double den = __dmul_rn(__dmul_rn(4., M_PI), R);
+      sx[i] = make_double2(__ddiv_rn(cs, den), __ddiv_rn(sn, den));
+    }
+    __syncthreads();
+    int inner = 1;
+    for (int axis = 2; axis >= 0; axis--) {
+      for (int ln = threadIdx.x; ln < P * P; ln += blockDim.x) {
+        double2* b = sx + (int64_t)(ln / inner) * P * inner + ln % inner;
+        double2 line[kMaxGrid], res[kMaxGrid];
+        for (int j = 0; j < P; j++) line[j] = b[j * inner];
+        for (int q = 0; q < P; q++) {
+          double ar = 0., ai = 0.;
+          for (int j = 0, m = 0; j < P; j++, m = (m + q) % P) {
+            const double2 x = line[j], w = tw[m];
+            ar = __dadd_rn(ar, __dsub_rn(__dmul_rn(x.x, w.x), __dmul_rn(x.y, w.y)));
+            ai = __dadd_rn(ai, __dadd_rn(__dmul_rn(x.x, w.y), __dmul_rn(x.y, w.x)));
+          }
+          res[q] = make_double2(ar, ai);
+        }
+        for (int q = 0; q < P; q++) b[q * inner] = res[q];
+      }
+      __syncthreads();
+      inner *= P;
+    }
+    for (int i = threadIdx.x; i < PP; i += blockDim.x) out[k * PP + i] = sx[i];
+    __syncthreads();
+  }
+}
+
+// Signatures of one HF stage (planewave.hpp:44-69): entry (d, k) =
+// exp(-i kappa dir_d . x_k) on the stage's grid, and its square.
+__global__ void k_signatures(int64_t n, int LL, const double* __restrict__ dirs, const double* __restrict__ nodes,
+                             double kappa, double2* __restrict__ s1, double2* __restrict__ s2) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t d = e / LL;
+    const int k = (int)(e - d * LL);
+    double dp = 0.;
+    for (int a = 0; a < 3; a++) dp = __dadd_rn(dp, __dmul_rn(dirs[3 * d + a], nodes[3 * k + a]));
+    double sn, cs;
+    sincos_fp64(__dmul_rn(kappa, dp), sn, cs);
+    const double re = cs, im = -sn;
+    s1[e] = make_double2(re, im);
+    s2[e] = make_double2(__dsub_rn(__dmul_rn(re, re), __dmul_rn(im, im)),
+                         __dadd_rn(__dmul_rn(re, im), __dmul_rn(im, re)));
+  }
+}
+
+__global__ void k_to_float(int64_t n, const double2* __restrict__ in, float2* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = make_float2(__double2float_rn(in[i].x), __double2float_rn(in[i].y));
+}
+
+int device_plan_tables(const Plan& p, double2* tables, double2* sig, double2* sig2, std::string& err) {
+  auto fail = [&](const char* what, cudaError_t e) {
+    err = std::string("device tables: ") + what + ": " + cudaGetErrorString(e);
+    cudaGetLastError();
+    return -4;
+  };
+  std::vector<void*> tmp;
+  auto up = [&](const void* src, size_t bytes, void** dst) -> cudaError_t {
+    cudaError_t e = cudaMalloc(dst, std::max<size_t>(1, bytes));
+    if (e != cudaSuccess) return e;
+    tmp.push_back(*dst);
+    return bytes ? cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice) : cudaSuccess;
+  };
+  auto release = [&]() {
+    for (void* q : tmp) cudaFree(q);
+  };
+  cudaError_t e = cudaSuccess;
+  const int64_t ntab = (int64_t)p.tab_fund.size();
+  if (ntab) {
+    std::vector<int32_t> fund(3 * ntab);
+    std::vector<double> rad(ntab), tw(2 * p.P);
+    for (int64_t k = 0; k < ntab; k++) {
+      for (int a = 0; a < 3; a++) fund[3 * k + a] = p.tab_fund[k][a];
+      rad[k] = p.box_rad / (double)(1 << p.tab_lvl[k]);
+    }
+    dft_twiddles(p.P, tw.data());
+    void *dfund, *drad, *dz, *dtw;
+    if ((e = up(fund.data(), fund.size() * 4, &dfund)) != cudaSuccess ||
+        (e = up(rad.data(), rad.size() * 8, &drad)) != cudaSuccess ||
+        (e = up(p.tabZ.data(), p.tabZ.size() * 8, &dz)) != cudaSuccess ||
+        (e = up(tw.data(), tw.size() * 8, &dtw)) != cudaSuccess) {
+      release();
+      return fail("upload", e);
+    }
+    const size_t smem = sizeof(double2) * (size_t)p.PP;
+    if ((e = cudaFuncSetAttribute(k_spectra, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess) {
+      release();
+      return fail("attribute", e);
+    }
+    k_spectra<<<(unsigned)std::min<int64_t>(ntab, 65535), 256, smem>>>(
+        ntab, p.P, (const int32_t*)dfund, (const double*)drad, (const double*)dz, p.kappa, (const double2*)dtw, tables);
+  }
+  int64_t off = 0;
+  for (size_t h = 0; h < p.sig.size() && h < 32; h++) {
+    const int64_t n = (int64_t)p.sig[h].size();
+    if (!n) continue;
+    int lvl = -1;  // the level whose HF stage is h
+    for (int l = 2; l < p.lv.nlvl; l++)
+      if (p.lv.prec[l] && p.lv.isHF[l] && p.lv.HFStage[l] == (int)h) lvl = l;
+    if (lvl < 0 || n != (int64_t)(p.dirs[h].size() / 3) * p.LL) {
+      release();
+      err = "device tables: signature layout";
+      return -4;
+    }
+    const double alpha = .5 * (p.box_rad / (double)(1 << lvl));
+    std::vector<double> nodes(3 * (size_t)p.LL);
+    for (int k = 0; k < p.LL; k++) {
+      const int I[3] = {k / (p.L * p.L), (k / p.L) % p.L, k % p.L};
+      for (int a = 0; a < 3; a++) nodes[3 * k + a] = node_coord(I[a], p.L, alpha);
+    }
+    void *dd, *dn;
+    if ((e = up(p.dirs[h].data(), p.dirs[h].size() * 8, &dd)) != cudaSuccess ||
+        (e = up(nodes.data(), nodes.size() * 8, &dn)) != cudaSuccess) {
+      release();
+      return fail("upload", e);
+    }
+    k_signatures<<<(unsigned)std::min<int64_t>((n + 255) / 256, 65535), 256>>>(
+        n, p.LL, (const double*)dd, (const double*)dn, p.kappa, sig + off, sig2 + off);
+    off += n;
+  }
+  e = cudaDeviceSynchronize();
+  release();
+  if (e != cudaSuccess) return fail("kernels", e);
+  return 0;
+}
+
+void tables_to_float(const double2* in, float2* out, int64_t n, cudaStream_t s) {
+  if (n) k_to_float<<<(unsigned)std::min<int64_t>((n + 255) / 256, 65535), 256, 0, s>>>(n, in, out);
+}
 
 }  // namespace dfb

@@ -2,6 +2,9 @@
 #pragma once
 
 #include <memory>
+#include <string>
+
+#include <cuda_runtime.h>
 
 #include "plan.hpp"
 
@@ -13,5 +16,11 @@ LevelWalker* device_level_walker();
 // The octree build's particle ordering on the current CUDA device; the same
 // cells and order as the host build, bit for bit.  One per prcmpt.
 std::unique_ptr<TreeSorter> make_device_tree_sorter();
+// The plan's FP64 transfer spectra (tables: tab_fund.size() x PP) and
+// signatures (sig, sig2: the host layout, stages after each other) computed
+// on the current device, bit-identical to the host's; 0 or -4 with err set.
+int device_plan_tables(const Plan& p, double2* tables, double2* sig, double2* sig2, std::string& err);
+// FP64 -> FP32 complex, rounded to nearest.
+void tables_to_float(const double2* in, float2* out, int64_t n, cudaStream_t s);
 
 }  // namespace dfb
