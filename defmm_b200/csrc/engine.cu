@@ -100,7 +100,7 @@ struct defmm_handle {
   int m2l_pair[2] = {0, 0};  // two target slots per M2L CTA
   // per-level choices of the autotuner (per precision; < 0: the values above)
   int16_t m2l_lvl_nt[2][32], m2l_lvl_pair[2][32];
-  double tune_lvl_ms[32];     // M2L time per level of the last timing run
+
   int p2p_bps[2] = {16, 16};
   int64_t nchunk = 0;
   size_t dev_bytes = 0;
@@ -111,8 +111,10 @@ struct defmm_handle {
   int rhs_block = 16;     // right-hand sides per pass of multi-RHS calls
   int rhs_block_m2l = 4;  // right-hand sides per M2L CTA (capped by the order)
   bool m2l_staging = false;  // grouped layout, FP32: shared-memory-staged M2L with target groups
-  int tune_level = -1;        // >= 0: timing runs of the autotuner (near field + M2L of the tuned levels)
+  int tune_level = -1;        // >= 0: timing runs of the autotuner (see run_gemv)
+  int tune_m2l = 0;           // 1: the timing run also times the M2L candidates
   bool tune_lvl_on[32];       // levels whose M2L the timing runs execute
+  double tune_ms[32][4], tune_pairs[32][4];  // per (level, M2L candidate): time, far pairs
   int64_t m2l_lgroup = 0;   // longest list total of kM2LGroup consecutive target slots
   bool use_tc = false;    // mixed precision: P2M on the tensor cores (tcgen05)
   int groups_forced = 0;  // > 0: direction groups requested (also for one RHS)
@@ -163,6 +165,9 @@ void free_buf(DevBuf& b) {
   b.p = nullptr;
   b.bytes = 0;
 }
+
+// The autotuner's M2L candidates: (two target slots per CTA, threads per CTA)
+constexpr int kM2LCand[4][2] = {{0, 128}, {0, 256}, {1, 128}, {1, 256}};
 
 // M2L launch choice of level l (the autotuner's per-level pick, else the
 // operator-wide one)
@@ -761,29 +766,36 @@ int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) 
   }
   if (h->events) cudaEventRecord(h->ev[2 * PH_P2P + 1], sn);
   if (tuning) {
+    // M2L candidates on interleaved slices of each tuned level's target
+    // slots (slice i runs candidate i mod 4), timed per slice and counted in
+    // far pairs, so one run compares every candidate on every tuned level
     float tm2l = 0;
-    for (int l = p.lv.max_stage; l < nl; l++) {
-      h->tune_lvl_ms[l] = 0;
+    for (int l = p.lv.max_stage; l < nl && h->tune_m2l; l++) {
+      for (int c = 0; c < 4; c++) h->tune_ms[l][c] = h->tune_pairs[l][c] = 0;
       if (!h->tune_lvl_on[l]) continue;
       const auto& cS = p.sS.cone_begin[l];
       const auto& cT = p.sT.cone_begin[l];
       const int nc = (int)cS.size() - 1;
-      int nt_l, pair_l;
-      m2l_choice(h, fp64 ? 0 : 1, l, &nt_l, &pair_l);
       for (int c0 = 0; c0 < nc;) {
         int c1 = c0 + 1;
         while (c1 < nc && cS[c1 + 1] - cS[c0] <= h->f_cap) c1++;
         const int64_t fs0 = cS[c0], fs1 = cS[c1], ts0 = cT[c0], ts1 = cT[c1];
-        if (ts1 > ts0 && fs1 > fs0) {
+        constexpr int kSlices = 16;
+        for (int i = 0; i < kSlices && ts1 > ts0 && fs1 > fs0; i++) {
+          const int64_t a0 = ts0 + (ts1 - ts0) * i / kSlices, a1 = ts0 + (ts1 - ts0) * (i + 1) / kSlices;
+          if (a1 <= a0) continue;
+          const int c = i % 4;
           rec(h, 2 * PH_M2L);
-          ops->m2l(d, ts0, ts1, fs0, fs1, h->F.p, h->ptab.p, h->Lx.p, h->d_queue + 1, h->nsm, nt_l, pair_l, sf);
+          ops->m2l(d, a0, a1, fs0, fs1, h->F.p, h->ptab.p, h->Lx.p, h->d_queue + 1, h->nsm, kM2LCand[c][1],
+                   kM2LCand[c][0], sf);
           rec(h, 2 * PH_M2L + 1);
           nl_++;
           float a;
           CK(cudaEventSynchronize(h->ev[2 * PH_M2L + 1]));
           cudaEventElapsedTime(&a, h->ev[2 * PH_M2L], h->ev[2 * PH_M2L + 1]);
           tm2l += a;
-          h->tune_lvl_ms[l] += a;
+          h->tune_ms[l][c] += a;
+          h->tune_pairs[l][c] += (double)(p.m2l_ptr[a1] - p.m2l_ptr[a0]);
         }
         c0 = c1;
       }
@@ -1396,8 +1408,8 @@ int defmm_autotune(defmm_handle* h, int reps, int32_t* choice) {
   const bool ev = h->events;
   h->events = true;  // phase timers, phases serialised
   drop_graph(h);     // the captured graph holds the old launch choices
-  // timing runs: the near field and every level's M2L (run_gemv in tuning
-  // mode), M2L timed per level so each level gets its own launch choice
+  // timing runs (run_gemv in tuning mode): the near field, and once the M2L
+  // of the tuned levels, so each level gets its own launch choice
   const Plan& q = h->plan;
   int busiest = q.lv.max_stage;
   {
@@ -1412,19 +1424,19 @@ int defmm_autotune(defmm_handle* h, int reps, int32_t* choice) {
   }
   h->tune_level = busiest;
   m2l_levels_reset(h, pi);
-  // levels timed on their own: those with at least a quarter of the far
-  // pairs (the others take the busiest level's choice)
+  // levels timed on their own: those with at least 2% of the far pairs (the
+  // others take the busiest level's choice)
   {
     const int64_t tot = q.m2l_ptr.empty() ? 0 : q.m2l_ptr.back();
     for (int l = 0; l < 32; l++) h->tune_lvl_on[l] = false;
     for (int l = q.lv.max_stage; l < q.lv.nlvl; l++) {
       const int64_t e = q.m2l_ptr[q.sT.lvl_begin[l + 1]] - q.m2l_ptr[q.sT.lvl_begin[l]];
-      h->tune_lvl_on[l] = l == busiest || 4 * e >= tot;
+      h->tune_lvl_on[l] = l == busiest || 50 * e >= tot;
     }
   }
-  // one run times one M2L candidate (the tuned levels) and one near-field
-  // candidate together: four runs (the M2L candidates: one or two target
-  // slots per CTA at 128 or 256 threads) cover the three near-field ones
+  // three timing runs, one per near-field candidate; the first also times
+  // the four M2L candidates (one or two target slots per CTA at 128 or 256
+  // threads) on interleaved slices of every tuned level
   int bps_best = 16;
   double tb_p2p = 1e300, tb_lvl[32];
   int best_lvl[32];
@@ -1432,30 +1444,30 @@ int defmm_autotune(defmm_handle* h, int reps, int32_t* choice) {
     tb_lvl[l] = 1e300;
     best_lvl[l] = 0;
   }
-  const int m2l_cand[4][2] = {{0, 128}, {0, 256}, {1, 128}, {1, 256}};
   const int bps_cand[3] = {8, 16, 32};
-  for (int i = 0; i < 4 && !st; i++) {
-    h->m2l_pair[pi] = m2l_cand[i][0];
-    h->m2l_nt[pi] = m2l_cand[i][1];
-    const int b = bps_cand[i < 3 ? i : 2];
-    h->p2p_bps[pi] = b;
-    double tp = 1e300, tl[32];
-    for (int l = 0; l < 32; l++) tl[l] = 1e300;
-    for (int r = 0; r < reps && !st; r++) {
+  for (int r = 0; r < reps && !st; r++)
+    for (int i = 0; i < 3 && !st; i++) {
+      h->p2p_bps[pi] = bps_cand[i];
+      h->tune_m2l = i == 0;
       st = run_gemv(h, (const double2*)h->rin.p, (double2*)h->rout.p, h->st);
-      tp = std::min(tp, h->phase_ms[PH_P2P]);
-      for (int l = q.lv.max_stage; l < q.lv.nlvl; l++) tl[l] = std::min(tl[l], h->tune_lvl_ms[l]);
-    }
-    for (int l = q.lv.max_stage; l < q.lv.nlvl; l++)
-      if (h->tune_lvl_on[l] && tl[l] < tb_lvl[l]) {
-        tb_lvl[l] = tl[l];
-        best_lvl[l] = i;
+      if (st) break;
+      if (h->phase_ms[PH_P2P] < tb_p2p) {
+        tb_p2p = h->phase_ms[PH_P2P];
+        bps_best = bps_cand[i];
       }
-    if (i < 3 && tp < tb_p2p) {
-      tb_p2p = tp;
-      bps_best = b;
+      if (i == 0)
+        for (int l = q.lv.max_stage; l < q.lv.nlvl; l++)
+          for (int c = 0; c < 4; c++)
+            if (h->tune_lvl_on[l] && h->tune_pairs[l][c] > 0) {
+              const double t = h->tune_ms[l][c] / h->tune_pairs[l][c];
+              if (t < tb_lvl[l]) {
+                tb_lvl[l] = t;
+                best_lvl[l] = c;
+              }
+            }
     }
-  }
+  h->tune_m2l = 0;
+  const int (&m2l_cand)[4][2] = kM2LCand;
   // operator-wide choice: the busiest level's; per-level overrides elsewhere
   TuneChoice c;
   c.nt = m2l_cand[best_lvl[busiest]][1];

@@ -265,16 +265,16 @@ int defmm_keep_lists(defmm_handle* h, int on);
 int defmm_set_plan_device(defmm_handle* h, int on);
 
 /* No counterpart in the reference.  Autotuner: on this operator and its
- * current precision, times `reps` timing runs (the near field and the M2L
- * of every level holding at least a quarter of the far pairs, on the handle's
- * own buffers) per candidate launch choice and keeps the fastest: per such
- * level (the others take the busiest level's), M2L threads per CTA (128 or
- * 256) with one or two target slots per CTA (timed on that level's M2L),
- * and near-field CTAs
- * per SM (8, 16 or 32, timed on the near-field phase).  Every choice gives
- * bit-identical results.  The choice of the level with the most far pairs
- * and the near-field CTAs per SM are written to choice[2] when not NULL
- * (also DEFMM_INFO_M2L_THREADS / DEFMM_INFO_M2L_PAIRING /
+ * current precision, `reps` times three timing runs on the handle's own
+ * buffers, one per near-field candidate (8, 16 or 32 CTAs per SM, timed on
+ * the near-field phase); the first also runs the M2L of every level holding
+ * at least 2% of the far pairs in 16 interleaved slices of its target slots,
+ * slice i with candidate i mod 4 (128 or 256 threads per CTA, one or two
+ * target slots per CTA), and each level keeps the candidate with the least
+ * time per far pair (the other levels take the busiest level's).  Every
+ * choice gives bit-identical results.  The choice of the level with the
+ * most far pairs and the near-field CTAs per SM are written to choice[2]
+ * when not NULL (also DEFMM_INFO_M2L_THREADS / DEFMM_INFO_M2L_PAIRING /
  * DEFMM_INFO_P2P_BLOCKS_PER_SM; every level's: defmm_m2l_schedule); the next
  * matvec captures a new graph.  Choices are cached per operator shape in the
  * process. */
