@@ -1260,7 +1260,7 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
     });
   };
   // M2M: children slots of each source slot (P2M/M2M operators, M2M.hpp:35-124)
-  {
+  if (!w.transfers_done) {
     const Slots& s = p.sS;
     slot_csr(
         s.n,
@@ -1278,7 +1278,7 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
         p.m2m_ptr, p.m2m_child);
   }
   // L2L: parent slots feeding each target slot (L2L.hpp:35-127)
-  {
+  if (!w.transfers_done) {
     const Slots& s = p.sT;
     slot_csr(
         s.n,

@@ -186,6 +186,9 @@ struct LevelWalk {
   // (the M2L CSR with permuted-spectrum ids): it fills Plan::m2l_ptr and
   // ptab_key and leaves the entries in Plan::dev_m2l_src / dev_m2l_tab.
   bool m2l_done = false;
+  // Set by a walker that also built Plan::m2m_ptr / m2m_child and
+  // l2l_ptr / l2l_parent.
+  bool transfers_done = false;
 };
 
 // Another implementation of the level walk (the device one); it must produce

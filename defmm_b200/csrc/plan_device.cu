@@ -220,6 +220,73 @@ __global__ void k_slots_hf(int64_t nc, int nd, const uint8_t* __restrict__ eff, 
   sdir[r] = d;
 }
 
+// M2M children of the source slots of one level (upwpass.hpp:49-60, the
+// host's m2m lists): parent slot r (cell pc, direction d) meets each son of
+// pc holding the slot of direction d / 4 (parent at an HF stage > 0) or its
+// LF slot (otherwise), in son order.  cdense maps the child level's (cell,
+// direction) to its slot (HF: loc * ndc + d; LF: loc), -1 where none.
+// out == nullptr: count into cnt; else write from off[r].
+__global__ void k_m2m_list(int64_t np, const int32_t* __restrict__ pcell, const int32_t* __restrict__ pdir, DTree S,
+                           int stage_pos, int chf, int ndc, const int32_t* __restrict__ cdense,
+                           int32_t* __restrict__ cnt, const int64_t* __restrict__ off, int32_t* __restrict__ out) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= np) return;
+  const int pc = pcell[r];
+  const int d = pdir ? pdir[r] : -1;
+  const int cd = stage_pos ? d / 4 : -1;
+  int n = 0;
+  const int64_t o = out ? off[r] : 0;
+  for (int64_t a = S.son_ptr[pc]; a < S.son_ptr[pc + 1]; a++) {
+    const int64_t loc = S.loc[S.sons[a]];
+    int32_t cs = -1;
+    if (chf) {
+      if (cd >= 0) cs = cdense[loc * ndc + cd];
+    } else if (cd < 0) {
+      cs = cdense[loc];
+    }
+    if (cs >= 0) {
+      if (out) out[o + n] = cs;
+      n++;
+    }
+  }
+  if (!out) cnt[r] = n;
+}
+
+// L2L parents of the target slots of one level (dwnpass.hpp:49-58, the
+// host's l2l lists): child slot r (cell c, direction dt) meets the slots of
+// its parent with directions 4 dt .. 4 dt + 3 (parent at an HF stage > 0),
+// all of its slots (HF stage 0), or its LF slot, in direction order.
+__global__ void k_l2l_list(int64_t nc, const int32_t* __restrict__ ccell, const int32_t* __restrict__ cdir, DTree T,
+                           int stage_pos, int phf, int ndp, const int32_t* __restrict__ pdense,
+                           int32_t* __restrict__ cnt, const int64_t* __restrict__ off, int32_t* __restrict__ out) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= nc) return;
+  const int pc = T.parent[ccell[r]];
+  const int dt = cdir ? cdir[r] : -1;
+  int n = 0;
+  const int64_t o = out ? off[r] : 0;
+  if (pc >= 0) {
+    const int64_t loc = T.loc[pc];
+    auto emit = [&](int32_t ps) {
+      if (ps >= 0) {
+        if (out) out[o + n] = ps;
+        n++;
+      }
+    };
+    if (stage_pos) {
+      for (int j = 0; j < 4; j++) {
+        const int d = 4 * dt + j;
+        if (d >= 0 && d < ndp) emit(pdense[loc * ndp + d]);
+      }
+    } else if (phf) {
+      for (int j = 0; j < ndp; j++) emit(pdense[loc * ndp + j]);
+    } else {
+      emit(pdense[loc]);
+    }
+  }
+  if (!out) cnt[r] = n;
+}
+
 __global__ void k_tabflags(int64_t nf, const int2* __restrict__ P, DTree T, DTree S, int m, int32_t* __restrict__ used) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= nf) return;
@@ -308,6 +375,25 @@ struct Arena {
       all.erase(it);
     }
   }
+};
+
+// One level's slots on the device during the walk: slot r has cell cell[r]
+// and direction dir[r] (dir == nullptr: LF, -1); dense maps (level-local
+// cell, direction) -> slot (HF: loc * nd + d; LF: loc), -1 where none.
+struct LvlSlots {
+  int64_t n = 0;
+  const int32_t* cell = nullptr;
+  const int32_t* dir = nullptr;
+  const int32_t* dense = nullptr;
+  int nd = 0;
+  bool prec = false, hf = false, stage_pos = false;  // stage_pos: HF with HF stage > 0
+  std::vector<void*> own;                            // device buffers to free with the level
+};
+
+// Transfer lists gathered on the host in slot order: per slot its count,
+// the entries after each other.
+struct TransferHost {
+  std::vector<int32_t> cnt, ent;
 };
 
 struct DeviceWalker final : LevelWalker {
@@ -417,6 +503,55 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
 
   std::vector<int2> near_h;
   int64_t table_count = 0;
+  // M2M / L2L transfer lists, level by level
+  LvlSlots prevSl, prevTl;
+  TransferHost m2m_h, l2l_h;
+  auto release_lvl = [&](LvlSlots& x) {
+    for (void* q : x.own)
+      if (q) A.drop(q);
+    x = LvlSlots();
+  };
+  // the lists of slots a (M2M: parents, L2L: children) against level b
+  auto transfer_lists = [&](const LvlSlots& a, const LvlSlots& b, const DTree& tr, bool m2m,
+                            TransferHost& th) -> int {
+    const int64_t n = a.n;
+    if (n == 0) return 0;
+    const size_t o = th.cnt.size();
+    th.cnt.resize(o + n, 0);
+    if (!b.dense || !b.prec || b.n == 0) return 0;
+    int32_t *cnt, *out;
+    int64_t* off;
+    DW_ALLOC(cnt, int32_t, n + 1);
+    DW_ALLOC(off, int64_t, n + 1);
+    if (m2m)
+      k_m2m_list<<<nblk(n), 256>>>(n, a.cell, a.dir, tr, a.stage_pos ? 1 : 0, b.hf ? 1 : 0, b.nd, b.dense, cnt,
+                                   nullptr, nullptr);
+    else
+      k_l2l_list<<<nblk(n), 256>>>(n, a.cell, a.dir, tr, b.stage_pos ? 1 : 0, b.hf ? 1 : 0, b.nd, b.dense, cnt,
+                                   nullptr, nullptr);
+    DW_CK(cudaGetLastError());
+    DW_CK(cudaMemset(cnt + n, 0, sizeof(int32_t)));
+    int s2 = scan(cnt, off, n + 1);
+    if (s2) return s2;
+    int64_t tot = 0;
+    if ((s2 = last(off, n, tot))) return s2;
+    DW_ALLOC(out, int32_t, tot);
+    if (m2m)
+      k_m2m_list<<<nblk(n), 256>>>(n, a.cell, a.dir, tr, a.stage_pos ? 1 : 0, b.hf ? 1 : 0, b.nd, b.dense, cnt, off,
+                                   out);
+    else
+      k_l2l_list<<<nblk(n), 256>>>(n, a.cell, a.dir, tr, b.stage_pos ? 1 : 0, b.hf ? 1 : 0, b.nd, b.dense, cnt, off,
+                                   out);
+    DW_CK(cudaGetLastError());
+    DW_CK(cudaMemcpy(th.cnt.data() + o, cnt, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    const size_t e0 = th.ent.size();
+    th.ent.resize(e0 + tot);
+    if (tot) DW_CK(cudaMemcpy(th.ent.data() + e0, out, (size_t)tot * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    A.drop(cnt);
+    A.drop(off);
+    A.drop(out);
+    return 0;
+  };
   std::vector<int32_t*> lv_ts, lv_ss;  // far entries per level, on the device
   std::vector<uint32_t*> lv_tab;
   std::vector<int64_t> lv_n;
@@ -519,8 +654,13 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
 
     // 4. slots of this level (cone-major, cells in DFS order)
     int32_t *denseT = nullptr, *denseS = nullptr;
+    LvlSlots curT, curS;  // this level's slots on the device (kept for the transfer lists)
     auto slots = [&](Slots& sl, const std::vector<int32_t>& cells, const int32_t* dcells, int64_t nc,
-                     const uint8_t* eff, int32_t*& dense) -> int {
+                     const uint8_t* eff, int32_t*& dense, LvlSlots& cur) -> int {
+      cur.prec = v.prec[l];
+      cur.hf = v.isHF[l];
+      cur.stage_pos = v.isHF[l] && v.HFStage[l] > 0;
+      cur.nd = nd;
       sl.lvl_begin[l] = sl.n;
       if (!v.prec[l]) {
         sl.cone_begin[l].assign(2, sl.n);
@@ -538,6 +678,9 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
         int s2 = upload_vec(A, dh, &dd, err);
         if (s2) return s2;
         dense = const_cast<int32_t*>(dd);
+        cur.n = nc;
+        cur.cell = dcells;  // the level's cell list, in slot order
+        cur.dir = nullptr;  // -1
         sl.n += nc;
         return 0;
       }
@@ -569,12 +712,21 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
       DW_CK(cudaMemcpy(sl.dir.data() + o, sdir, (size_t)cnt * sizeof(int32_t), cudaMemcpyDeviceToHost));
       A.drop(fl);
       A.drop(pos);
-      A.drop(scell);
-      A.drop(sdir);
+      cur.n = cnt;
+      cur.cell = scell;
+      cur.dir = sdir;
+      cur.own = {scell, sdir};
       sl.n += cnt;
       return 0;
     };
-    if ((st = slots(p.sT, lcT[l], cellsT, ncT, effT, denseT)) || (st = slots(p.sS, lcS[l], cellsS, ncS, effS, denseS)))
+    if ((st = slots(p.sT, lcT[l], cellsT, ncT, effT, denseT, curT)) ||
+        (st = slots(p.sS, lcS[l], cellsS, ncS, effS, denseS, curS)))
+      return st;
+    curT.dense = denseT;
+    curS.dense = denseS;
+    // M2M lists of the previous level's source slots (children here) and
+    // L2L lists of this level's target slots (parents there)
+    if ((st = transfer_lists(prevSl, curS, S, true, m2m_h)) || (st = transfer_lists(curT, prevTl, T, false, l2l_h)))
       return st;
 
     // 5. transfer-spectrum ids per fundamental index and the far entries
@@ -614,15 +766,39 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
     }
     if (cone) A.drop(cone);
     A.drop(fp);
-    if (denseT) A.drop(denseT);
-    if (denseS) A.drop(denseS);
-    A.drop(const_cast<int32_t*>(cellsT));
-    A.drop(const_cast<int32_t*>(cellsS));
+    // this level's slots, dense maps and cell lists become the previous level's
+    release_lvl(prevSl);
+    release_lvl(prevTl);
+    curS.own.push_back(denseS);
+    curS.own.push_back(const_cast<int32_t*>(cellsS));
+    curT.own.push_back(denseT);
+    curT.own.push_back(const_cast<int32_t*>(cellsT));
+    prevSl = curS;
+    prevTl = curT;
     if (prevT) A.drop(prevT);
     if (prevS) A.drop(prevS);
     prevT = effT;
     prevS = effS;
   }
+  {  // the deepest level's source slots have no children
+    LvlSlots none;
+    if ((st = transfer_lists(prevSl, none, S, true, m2m_h))) return st;
+  }
+  release_lvl(prevSl);
+  release_lvl(prevTl);
+  auto finish = [](const Slots& sl, TransferHost& t, std::vector<int64_t>& ptr, std::vector<int32_t>& ent) {
+    ptr.assign(sl.n + 1, 0);
+    int64_t run = 0;
+    for (int64_t k = 0; k < sl.n; k++) {
+      ptr[k] = run;
+      run += k < (int64_t)t.cnt.size() ? t.cnt[k] : 0;
+    }
+    ptr[sl.n] = run;
+    ent.swap(t.ent);
+  };
+  finish(p.sS, m2m_h, p.m2m_ptr, p.m2m_child);
+  finish(p.sT, l2l_h, p.l2l_ptr, p.l2l_parent);
+  walk.transfers_done = true;
   p.sT.lvl_begin[nlvl] = p.sT.n;
   p.sS.lvl_begin[nlvl] = p.sS.n;
   walk.near_pairs.resize(near_h.size());
