@@ -296,10 +296,18 @@ int upload_plan(defmm_handle* h) {
   UP(p.sS.cell_dirs, d.S_cdir);
   UP(to_i32(p.sT.cell_slots), d.T_cslot);
   UP(p.sT.cell_dirs, d.T_cdir);
-  UP(p.m2m_ptr, d.m2m_ptr);
-  UP(p.m2m_child, d.m2m_child);
-  UP(p.l2l_ptr, d.l2l_ptr);
-  UP(p.l2l_parent, d.l2l_parent);
+  if (p.dev_m2m_ptr) {  // built on the device by prcmpt
+    d.m2m_ptr = static_cast<const int64_t*>(p.dev_m2m_ptr);
+    d.m2m_child = static_cast<const int32_t*>(p.dev_m2m_child);
+    d.l2l_ptr = static_cast<const int64_t*>(p.dev_l2l_ptr);
+    d.l2l_parent = static_cast<const int32_t*>(p.dev_l2l_parent);
+    h->dev_bytes += (size_t)(p.sS.n + p.sT.n + 2) * 8 + (size_t)(p.n_m2m + p.n_l2l) * 4;
+  } else {
+    UP(p.m2m_ptr, d.m2m_ptr);
+    UP(p.m2m_child, d.m2m_child);
+    UP(p.l2l_ptr, d.l2l_ptr);
+    UP(p.l2l_parent, d.l2l_parent);
+  }
   UP(p.m2l_ptr, d.m2l_ptr);
   if (p.dev_m2l_src) {  // built on the device by prcmpt
     d.m2l_src = static_cast<const int32_t*>(p.dev_m2l_src);
@@ -1555,11 +1563,13 @@ int defmm_prcmpt(defmm_handle* h, int L, int Ncrit, double kappa, int lvMAX) {
   }
   int st = dfb::build_plan(h->plan, h->src.data(), (int64_t)h->src.size() / 3, h->trg.data(),
                            (int64_t)h->trg.size() / 3, L, Ncrit, kappa, lvMAX, e, walker, sorter.get());
+  // arrays the walk left on the device belong to this handle's plan (also
+  // when the build failed part way)
+  for (void* q : {h->plan.dev_m2l_src, h->plan.dev_m2l_tab, h->plan.dev_m2m_ptr, h->plan.dev_m2m_child,
+                  h->plan.dev_l2l_ptr, h->plan.dev_l2l_parent})
+    if (q) h->plan_allocs.push_back(q);
   if (st) return h->fail(st == -4 ? DEFMM_ERR_CUDA : st == -5 ? DEFMM_ERR_MEMORY : st, e);
   h->walked_on_device = walker != nullptr;
-  // M2L entries the walk left on the device belong to this handle's plan
-  if (h->plan.dev_m2l_src) h->plan_allocs.push_back(h->plan.dev_m2l_src);
-  if (h->plan.dev_m2l_tab) h->plan_allocs.push_back(h->plan.dev_m2l_tab);
   if (h->plan.lv.nlvl > 32) return h->fail(DEFMM_ERR_DEPTH, "more than 32 tree levels");
   {
     const std::vector<int64_t>& ptr = h->plan.m2l_ptr;
@@ -1904,8 +1914,8 @@ int defmm_info(const defmm_handle* h, int what, int64_t* v) {
       *v = n;
       break;
     }
-    case DEFMM_INFO_M2M_ENTRIES: *v = p.m2m_ptr.empty() ? 0 : p.m2m_ptr.back(); break;
-    case DEFMM_INFO_L2L_ENTRIES: *v = p.l2l_ptr.empty() ? 0 : p.l2l_ptr.back(); break;
+    case DEFMM_INFO_M2M_ENTRIES: *v = p.m2m_ptr.empty() ? p.n_m2m : p.m2m_ptr.back(); break;
+    case DEFMM_INFO_L2L_ENTRIES: *v = p.l2l_ptr.empty() ? p.n_l2l : p.l2l_ptr.back(); break;
     case DEFMM_INFO_P2M_POINT_SLOTS: {
       int64_t n = 0;
       for (int32_t c : p.p2m_leaf) n += (int64_t)p.S.nprt[c] * (p.sS.cell_ptr[c + 1] - p.sS.cell_ptr[c]);

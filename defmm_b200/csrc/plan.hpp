@@ -110,6 +110,11 @@ struct Plan {
   void* dev_m2l_src = nullptr;
   void* dev_m2l_tab = nullptr;
   int64_t n_m2l = 0;
+  // M2M / L2L transfer lists built by the device walk and left there: int64
+  // pointers over the source / target slots (n + 1) and int32 entries
+  // (n_m2m / n_l2l); m2m_ptr, m2m_child, l2l_ptr, l2l_parent stay empty.
+  void *dev_m2m_ptr = nullptr, *dev_m2m_child = nullptr, *dev_l2l_ptr = nullptr, *dev_l2l_parent = nullptr;
+  int64_t n_m2m = 0, n_l2l = 0;
   // M2M children of each source slot, L2L parents of each target slot
   std::vector<int64_t> m2m_ptr;            // sS.n + 1
   std::vector<int32_t> m2m_child;          // child slot
@@ -186,8 +191,8 @@ struct LevelWalk {
   // (the M2L CSR with permuted-spectrum ids): it fills Plan::m2l_ptr and
   // ptab_key and leaves the entries in Plan::dev_m2l_src / dev_m2l_tab.
   bool m2l_done = false;
-  // Set by a walker that also built Plan::m2m_ptr / m2m_child and
-  // l2l_ptr / l2l_parent.
+  // Set by a walker that also built the M2M / L2L transfer lists (on the
+  // device: Plan::dev_m2m_ptr etc.).
   bool transfers_done = false;
 };
 

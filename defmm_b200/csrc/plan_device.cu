@@ -390,12 +390,6 @@ struct LvlSlots {
   std::vector<void*> own;                            // device buffers to free with the level
 };
 
-// Transfer lists gathered on the host in slot order: per slot its count,
-// the entries after each other.
-struct TransferHost {
-  std::vector<int32_t> cnt, ent;
-};
-
 struct DeviceWalker final : LevelWalker {
   int walk(Plan& p, LevelWalk& w, std::string& err) override;
 };
@@ -503,54 +497,14 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
 
   std::vector<int2> near_h;
   int64_t table_count = 0;
-  // M2M / L2L transfer lists, level by level
-  LvlSlots prevSl, prevTl;
-  TransferHost m2m_h, l2l_h;
+  // every level's slots stay on the device until the M2M / L2L transfer
+  // lists are built after the walk
+  std::vector<LvlSlots> lvS(nlvl), lvT(nlvl);
+  double t_transfers = 0;  // wall time of the transfer lists
   auto release_lvl = [&](LvlSlots& x) {
     for (void* q : x.own)
       if (q) A.drop(q);
     x = LvlSlots();
-  };
-  // the lists of slots a (M2M: parents, L2L: children) against level b
-  auto transfer_lists = [&](const LvlSlots& a, const LvlSlots& b, const DTree& tr, bool m2m,
-                            TransferHost& th) -> int {
-    const int64_t n = a.n;
-    if (n == 0) return 0;
-    const size_t o = th.cnt.size();
-    th.cnt.resize(o + n, 0);
-    if (!b.dense || !b.prec || b.n == 0) return 0;
-    int32_t *cnt, *out;
-    int64_t* off;
-    DW_ALLOC(cnt, int32_t, n + 1);
-    DW_ALLOC(off, int64_t, n + 1);
-    if (m2m)
-      k_m2m_list<<<nblk(n), 256>>>(n, a.cell, a.dir, tr, a.stage_pos ? 1 : 0, b.hf ? 1 : 0, b.nd, b.dense, cnt,
-                                   nullptr, nullptr);
-    else
-      k_l2l_list<<<nblk(n), 256>>>(n, a.cell, a.dir, tr, b.stage_pos ? 1 : 0, b.hf ? 1 : 0, b.nd, b.dense, cnt,
-                                   nullptr, nullptr);
-    DW_CK(cudaGetLastError());
-    DW_CK(cudaMemset(cnt + n, 0, sizeof(int32_t)));
-    int s2 = scan(cnt, off, n + 1);
-    if (s2) return s2;
-    int64_t tot = 0;
-    if ((s2 = last(off, n, tot))) return s2;
-    DW_ALLOC(out, int32_t, tot);
-    if (m2m)
-      k_m2m_list<<<nblk(n), 256>>>(n, a.cell, a.dir, tr, a.stage_pos ? 1 : 0, b.hf ? 1 : 0, b.nd, b.dense, cnt, off,
-                                   out);
-    else
-      k_l2l_list<<<nblk(n), 256>>>(n, a.cell, a.dir, tr, b.stage_pos ? 1 : 0, b.hf ? 1 : 0, b.nd, b.dense, cnt, off,
-                                   out);
-    DW_CK(cudaGetLastError());
-    DW_CK(cudaMemcpy(th.cnt.data() + o, cnt, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost));
-    const size_t e0 = th.ent.size();
-    th.ent.resize(e0 + tot);
-    if (tot) DW_CK(cudaMemcpy(th.ent.data() + e0, out, (size_t)tot * sizeof(int32_t), cudaMemcpyDeviceToHost));
-    A.drop(cnt);
-    A.drop(off);
-    A.drop(out);
-    return 0;
   };
   std::vector<int32_t*> lv_ts, lv_ss;  // far entries per level, on the device
   std::vector<uint32_t*> lv_tab;
@@ -724,10 +678,6 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
       return st;
     curT.dense = denseT;
     curS.dense = denseS;
-    // M2M lists of the previous level's source slots (children here) and
-    // L2L lists of this level's target slots (parents there)
-    if ((st = transfer_lists(prevSl, curS, S, true, m2m_h)) || (st = transfer_lists(curT, prevTl, T, false, l2l_h)))
-      return st;
 
     // 5. transfer-spectrum ids per fundamental index and the far entries
     if (nf) {
@@ -766,44 +716,87 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
     }
     if (cone) A.drop(cone);
     A.drop(fp);
-    // this level's slots, dense maps and cell lists become the previous level's
-    release_lvl(prevSl);
-    release_lvl(prevTl);
+    // this level's slots, dense maps and cell lists: kept for the transfer lists
     curS.own.push_back(denseS);
     curS.own.push_back(const_cast<int32_t*>(cellsS));
     curT.own.push_back(denseT);
     curT.own.push_back(const_cast<int32_t*>(cellsT));
-    prevSl = curS;
-    prevTl = curT;
+    lvS[l] = curS;
+    lvT[l] = curT;
     if (prevT) A.drop(prevT);
     if (prevS) A.drop(prevS);
     prevT = effT;
     prevS = effS;
   }
-  {  // the deepest level's source slots have no children
-    LvlSlots none;
-    if ((st = transfer_lists(prevSl, none, S, true, m2m_h))) return st;
-  }
-  release_lvl(prevSl);
-  release_lvl(prevTl);
-  auto finish = [](const Slots& sl, TransferHost& t, std::vector<int64_t>& ptr, std::vector<int32_t>& ent) {
-    ptr.assign(sl.n + 1, 0);
-    int64_t run = 0;
-    for (int64_t k = 0; k < sl.n; k++) {
-      ptr[k] = run;
-      run += k < (int64_t)t.cnt.size() ? t.cnt[k] : 0;
+  // M2M lists of every source slot (children: the next level) and L2L lists
+  // of every target slot (parents: the previous level), counted per level
+  // into one array over all slots, one scan, then filled; left on the device
+  const double t_tr = wall_seconds();
+  auto transfers = [&](const Slots& sl, const std::vector<LvlSlots>& lv, const DTree& tr, bool m2m,
+                       void** ptr_out, void** ent_out, int64_t* n_out) -> int {
+    const int64_t n = sl.n;
+    int32_t* cnt;
+    DW_ALLOC(cnt, int32_t, n + 1);
+    DW_CK(cudaMemset(cnt, 0, (n + 1) * sizeof(int32_t)));
+    int64_t* ptr = nullptr;
+    if (cudaMalloc(&ptr, (n + 1) * sizeof(int64_t)) != cudaSuccess) {
+      cudaGetLastError();
+      err = "device plan: out of device memory";
+      return -5;
     }
-    ptr[sl.n] = run;
-    ent.swap(t.ent);
+    *ptr_out = ptr;  // handed to the plan's owner (also on error: freed there)
+    for (int pass = 0; pass < 2; pass++) {
+      if (pass == 1) {
+        int s2 = scan(cnt, ptr, n + 1);
+        if (s2) return s2;
+        if ((s2 = last(ptr, n, *n_out))) return s2;
+        if (cudaMalloc(ent_out, std::max<int64_t>(1, *n_out) * sizeof(int32_t)) != cudaSuccess) {
+          cudaGetLastError();
+          err = "device plan: out of device memory";
+          return -5;
+        }
+      }
+      for (int l = 0; l < nlvl; l++) {
+        const LvlSlots& a = lv[l];  // the slots whose lists are built
+        const int lb = m2m ? l + 1 : l - 1;
+        if (a.n == 0 || lb < 0 || lb >= nlvl) continue;
+        const LvlSlots& b = lv[lb];
+        if (!b.dense || !b.prec || b.n == 0) continue;
+        const int64_t base = sl.lvl_begin[l];
+        int32_t* out = pass ? static_cast<int32_t*>(*ent_out) : nullptr;
+        const int64_t* off = pass ? ptr + base : nullptr;
+        if (m2m)
+          k_m2m_list<<<nblk(a.n), 256>>>(a.n, a.cell, a.dir, tr, a.stage_pos ? 1 : 0, b.hf ? 1 : 0, b.nd, b.dense,
+                                         cnt + base, off, out);
+        else
+          k_l2l_list<<<nblk(a.n), 256>>>(a.n, a.cell, a.dir, tr, b.stage_pos ? 1 : 0, b.hf ? 1 : 0, b.nd, b.dense,
+                                         cnt + base, off, out);
+        DW_CK(cudaGetLastError());
+      }
+    }
+    A.drop(cnt);
+    return 0;
   };
-  finish(p.sS, m2m_h, p.m2m_ptr, p.m2m_child);
-  finish(p.sT, l2l_h, p.l2l_ptr, p.l2l_parent);
+  if ((st = transfers(p.sS, lvS, S, true, &p.dev_m2m_ptr, &p.dev_m2m_child, &p.n_m2m)) ||
+      (st = transfers(p.sT, lvT, T, false, &p.dev_l2l_ptr, &p.dev_l2l_parent, &p.n_l2l)))
+    return st;
+  for (int l = 0; l < nlvl; l++) {
+    release_lvl(lvS[l]);
+    release_lvl(lvT[l]);
+  }
+  p.m2m_ptr.clear();
+  p.m2m_child.clear();
+  p.l2l_ptr.clear();
+  p.l2l_parent.clear();
+  t_transfers = wall_seconds() - t_tr;
   walk.transfers_done = true;
   p.sT.lvl_begin[nlvl] = p.sT.n;
   p.sS.lvl_begin[nlvl] = p.sS.n;
   walk.near_pairs.resize(near_h.size());
   for (size_t i = 0; i < near_h.size(); i++) walk.near_pairs[i] = {near_h[i].x, near_h[i].y};
   p.step("walk: levels (pairs, cones, effective directions, slots, far entries)", tstep);
+  p.t_steps.back().second -= t_transfers;
+  p.t_steps.push_back({"walk: M2M and L2L transfer lists", t_transfers});
 
   // M2L entries grouped by target slot: a stable radix sort of all levels'
   // entries (level order, then walk order) by target slot, as the host's

@@ -1,11 +1,12 @@
 """The plan's octree build and level walk on the GPU (plan_device.cu: the
 particles ordered level by level with octant codes, counts and a stable
-radix sort; the dual traversal) against the host build and walk
-(plan.cpp, itself pinned to the reference's trees, cones and lists by
-tests/test_plan.py): same statistics, same effective directions per cell
-(the cell-array dump, which carries the slots' directions), and a
-bit-identical FP64 matvec, which needs identical slots and far entries in
-identical order.
+radix sort; the dual traversal with the M2M/L2L transfer lists; the transfer
+spectra and signatures) against the host build and walk (plan.cpp, itself
+pinned to the reference's trees, cones and lists by tests/test_plan.py):
+same statistics, same effective directions per cell (the cell-array dump,
+which carries the slots' directions), and a bit-identical FP64 matvec, which
+needs identical slots, far entries, transfer lists and tables in identical
+order.
 """
 import numpy as np
 import pytest
@@ -16,7 +17,7 @@ from tests.golden.cases import CASES, case_inputs
 pytestmark = pytest.mark.gpu
 
 STATS = ["nlvl", "cpt", "slots_S", "slots_T", "far_hf", "far_lf", "near", "i_near", "tables",
-         "permuted_spectra", "m2l_targets", "leaf_slots_S"]
+         "permuted_spectra", "m2l_targets", "leaf_slots_S", "m2m_entries", "l2l_entries"]
 
 
 def build(src, trg, L, ncrit, kappa, lvmax, device):
