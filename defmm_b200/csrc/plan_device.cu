@@ -203,6 +203,11 @@ __global__ void k_transpose(int64_t nc, int nd, const uint8_t* __restrict__ eff,
   fl[w] = eff[c * nd + d];
 }
 
+__global__ void k_cone_starts(int nd, int64_t nc, const int32_t* __restrict__ pos, int32_t* __restrict__ out) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d < nd) out[d] = pos[(int64_t)d * nc];
+}
+
 __global__ void k_slots_hf(int64_t nc, int nd, const uint8_t* __restrict__ eff, const int32_t* __restrict__ pos,
                            const int32_t* __restrict__ cells, int64_t base, int32_t* __restrict__ dense,
                            int32_t* __restrict__ scell, int32_t* __restrict__ sdir) {
@@ -501,6 +506,7 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
   // lists are built after the walk
   std::vector<LvlSlots> lvS(nlvl), lvT(nlvl);
   double t_transfers = 0;  // wall time of the transfer lists
+  double t_sub[4] = {0, 0, 0, 0};  // per sub-step of the level loop
   auto release_lvl = [&](LvlSlots& x) {
     for (void* q : x.own)
       if (q) A.drop(q);
@@ -518,6 +524,13 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
   uint8_t *prevT = nullptr, *prevS = nullptr;  // flags of the previous level
   for (int l = 0; l < nlvl; l++) {
     const bool prec = v.prec[l], hf = l > 0 && v.isHF[l];
+    double tsub = wall_seconds();
+    auto sub = [&](int k) {  // accumulate the wall time of sub-step k of the level
+      cudaDeviceSynchronize();
+      const double t = wall_seconds();
+      t_sub[k] += t - tsub;
+      tsub = t;
+    };
     // 1. classify and compact: far pairs, near pairs, next frontier
     int32_t *isfar, *isnear, *pfar, *pnear;
     int64_t *nch, *pch;
@@ -555,6 +568,7 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
     nfr = nx;
     if (hf) p.n_far_hf += nf; else p.n_far_lf += nf;
 
+    sub(0);
     // 2. fundamental index bound and (HF) the cone of each far pair
     int m = 0;
     int16_t* cone = nullptr;
@@ -586,6 +600,7 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
       A.drop(kc);
     }
 
+    sub(1);
     // 3. effective directions of this level (+ propagation from the parent level)
     const bool hfprec = v.prec[l] && v.isHF[l];
     const int64_t ncT = (int64_t)lcT[l].size(), ncS = (int64_t)lcS[l].size();
@@ -653,11 +668,17 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
       DW_ALLOC(sdir, int32_t, cnt);
       if (tot) k_slots_hf<<<nblk(tot), 256>>>(nc, nd, eff, pos, dcells, sl.n, dense, scell, sdir);
       DW_CK(cudaGetLastError());
-      // cone starts: pos at (d, 0)
-      std::vector<int32_t> ph(tot + 1);
-      DW_CK(cudaMemcpy(ph.data(), pos, (tot + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost));
+      // cone starts: pos at (d, 0), gathered on the device (nd values of the
+      // nc x nd positions)
+      int32_t* cs;
+      DW_ALLOC(cs, int32_t, nd);
+      k_cone_starts<<<nblk(nd), 256>>>(nd, nc, pos, cs);
+      DW_CK(cudaGetLastError());
+      std::vector<int32_t> ph(nd);
+      DW_CK(cudaMemcpy(ph.data(), cs, (size_t)nd * sizeof(int32_t), cudaMemcpyDeviceToHost));
+      A.drop(cs);
       sl.cone_begin[l].assign(nd + 1, 0);
-      for (int d = 0; d < nd; d++) sl.cone_begin[l][d] = sl.n + ph[(int64_t)d * nc];
+      for (int d = 0; d < nd; d++) sl.cone_begin[l][d] = sl.n + ph[d];
       sl.cone_begin[l][nd] = sl.n + cnt;
       const size_t o = sl.cell.size();
       sl.cell.resize(o + cnt);
@@ -679,6 +700,7 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
     curT.dense = denseT;
     curS.dense = denseS;
 
+    sub(2);
     // 5. transfer-spectrum ids per fundamental index and the far entries
     if (nf) {
       const int64_t nkey = (int64_t)(m + 1) * (m + 1) * (m + 1);
@@ -716,6 +738,7 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
     }
     if (cone) A.drop(cone);
     A.drop(fp);
+    sub(3);
     // this level's slots, dense maps and cell lists: kept for the transfer lists
     curS.own.push_back(denseS);
     curS.own.push_back(const_cast<int32_t*>(cellsS));
@@ -794,8 +817,12 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
   p.sS.lvl_begin[nlvl] = p.sS.n;
   walk.near_pairs.resize(near_h.size());
   for (size_t i = 0; i < near_h.size(); i++) walk.near_pairs[i] = {near_h[i].x, near_h[i].y};
-  p.step("walk: levels (pairs, cones, effective directions, slots, far entries)", tstep);
-  p.t_steps.back().second -= t_transfers;
+  p.step("walk: levels, other (allocations, copies)", tstep);
+  p.t_steps.back().second -= t_transfers + t_sub[0] + t_sub[1] + t_sub[2] + t_sub[3];
+  p.t_steps.push_back({"walk: levels, pair classification and near pairs", t_sub[0]});
+  p.t_steps.push_back({"walk: levels, cones of the far pairs", t_sub[1]});
+  p.t_steps.push_back({"walk: levels, effective directions and slots", t_sub[2]});
+  p.t_steps.push_back({"walk: levels, far entries", t_sub[3]});
   p.t_steps.push_back({"walk: M2M and L2L transfer lists", t_transfers});
 
   // M2L entries grouped by target slot: a stable radix sort of all levels'
