@@ -666,6 +666,26 @@ void level_slots(const Plan& p, int l, const LevelFlags& F, Slots& s,
 // for one tree holding both sources and targets.  Source ranges are unions
 // of whole leaves, and a leaf's own range is always present (its self pair).
 // Scratch is chunk-major: a chunk's symmetric ranges take consecutive slots.
+// Indices 0..n-1 ordered by decreasing key, ties in index order (the order
+// of a stable sort by key > key): a counting sort when the keys are small,
+// else a stable sort.
+std::vector<int32_t> order_by_decreasing(const std::vector<int64_t>& key) {
+  const int64_t n = (int64_t)key.size();
+  std::vector<int32_t> order(n);
+  int64_t kmax = 0;
+  for (int64_t k : key) kmax = std::max(kmax, k);
+  if (kmax >= 0 && kmax <= std::max<int64_t>(1 << 20, 4 * n)) {
+    std::vector<int64_t> start(kmax + 2, 0);
+    for (int64_t k : key) start[kmax - std::max<int64_t>(k, 0) + 1]++;  // bucket of key k: kmax - k
+    for (int64_t b = 0; b <= kmax; b++) start[b + 1] += start[b];
+    for (int64_t i = 0; i < n; i++) order[start[kmax - std::max<int64_t>(key[i], 0)]++] = (int32_t)i;
+    return order;
+  }
+  for (int64_t i = 0; i < n; i++) order[i] = (int32_t)i;
+  std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return key[a] > key[b]; });
+  return order;
+}
+
 void build_symmetric_near(Plan& p) {
   const Tree& T = p.T;
   const int64_t nch = (int64_t)p.p2p_tfirst.size();
@@ -763,9 +783,8 @@ void build_symmetric_near(Plan& p) {
     for (int64_t r = p.self_ptr[ch]; r < p.self_ptr[ch + 1]; r++) ws[ch] += p.self_sn[r];
   });
   p.self_order.clear();
-  for (int64_t ch = 0; ch < nch; ch++)
-    if (ws[ch]) p.self_order.push_back((int32_t)ch);
-  std::stable_sort(p.self_order.begin(), p.self_order.end(), [&](int32_t a, int32_t b) { return ws[a] > ws[b]; });
+  for (int32_t ch : order_by_decreasing(ws))
+    if (ws[ch]) p.self_order.push_back(ch);
 }
 
 // Cut every chunk's source ranges (CSR `ptr` over chunks) into items of at
@@ -842,9 +861,7 @@ void split_items(const Plan& p, std::vector<int64_t>& ptr, std::vector<int32_t>&
   sf.swap(nsf);
   sn.swap(nsn);
   if (soff) soff->swap(nso);
-  order.resize(chunk.size());
-  for (size_t k = 0; k < order.size(); k++) order[k] = (int32_t)k;
-  std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return work[a] > work[b]; });
+  order = order_by_decreasing(work);
 }
 
 }  // namespace
