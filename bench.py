@@ -587,7 +587,7 @@ def main():
     ap.add_argument("--workload", default="sphere2m")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--rhs-block", type=int, default=16)
+    ap.add_argument("--rhs-block", type=int, default=8, help="right-hand sides per pass of the rhs64 workload")
     ap.add_argument("--nrhs", type=int, default=8, help="right-hand sides of the block form")
     ap.add_argument("--groups", type=int, default=0,
                     help="direction groups of the block form's grouped layout (0: as memory needs)")
