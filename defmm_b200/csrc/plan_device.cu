@@ -233,7 +233,7 @@ __global__ void k_slots_hf(int64_t nc, int nd, const uint8_t* __restrict__ eff, 
 // out == nullptr: count into cnt; else write from off[r].
 __global__ void k_m2m_list(int64_t np, const int32_t* __restrict__ pcell, const int32_t* __restrict__ pdir, DTree S,
                            int stage_pos, int chf, int ndc, const int32_t* __restrict__ cdense,
-                           int32_t* __restrict__ cnt, const int64_t* __restrict__ off, int32_t* __restrict__ out) {
+                           int64_t* __restrict__ cnt, const int64_t* __restrict__ off, int32_t* __restrict__ out) {
   const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (r >= np) return;
   const int pc = pcell[r];
@@ -263,7 +263,7 @@ __global__ void k_m2m_list(int64_t np, const int32_t* __restrict__ pcell, const 
 // all of its slots (HF stage 0), or its LF slot, in direction order.
 __global__ void k_l2l_list(int64_t nc, const int32_t* __restrict__ ccell, const int32_t* __restrict__ cdir, DTree T,
                            int stage_pos, int phf, int ndp, const int32_t* __restrict__ pdense,
-                           int32_t* __restrict__ cnt, const int64_t* __restrict__ off, int32_t* __restrict__ out) {
+                           int64_t* __restrict__ cnt, const int64_t* __restrict__ off, int32_t* __restrict__ out) {
   const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (r >= nc) return;
   const int pc = T.parent[ccell[r]];
@@ -758,9 +758,9 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
   auto transfers = [&](const Slots& sl, const std::vector<LvlSlots>& lv, const DTree& tr, bool m2m,
                        void** ptr_out, void** ent_out, int64_t* n_out) -> int {
     const int64_t n = sl.n;
-    int32_t* cnt;
-    DW_ALLOC(cnt, int32_t, n + 1);
-    DW_CK(cudaMemset(cnt, 0, (n + 1) * sizeof(int32_t)));
+    int64_t* cnt;  // 64-bit, so that the scan's sums cannot overflow
+    DW_ALLOC(cnt, int64_t, n + 1);
+    DW_CK(cudaMemset(cnt, 0, (n + 1) * sizeof(int64_t)));
     int64_t* ptr = nullptr;
     if (cudaMalloc(&ptr, (n + 1) * sizeof(int64_t)) != cudaSuccess) {
       cudaGetLastError();
