@@ -1096,7 +1096,7 @@ __global__ void __launch_bounds__(M2LBulk<L>::NT, M2LBulk<L>::CTAS) k_m2l_bulk(
   static_assert((G * RB) % NSPEC == 0, "whole inverse-DFT rounds");
   static_assert(NSPEC * LL <= NC, "one output of the last inverse-DFT pass per thread");
   static_assert(NS * 16 + 8 + NS * sizeof(BulkEntry) + PD * 8 + 8 <= B::HDR, "header");
-  extern __shared__ __align__(128) unsigned char smem_raw[];
+  extern __shared__ __align__(16) unsigned char smem_raw[];  // stage offsets are multiples of 16 bytes
   unsigned char* stages = smem_raw;
   float2* Js = reinterpret_cast<float2*>(smem_raw + NS * SB);
   float2* Cb = Js + NSPEC * PP;
@@ -2064,8 +2064,6 @@ __device__ __forceinline__ void sym_steps(int ls, int tp_rt, double yx, double y
                                           typename std::conditional<MIXED, float2, double2>::type& accD,
                                           typename std::conditional<MIXED, float2, double2>::type& accT) {
   const int tp = TP ? TP : tp_rt;
-  constexpr int UNR = MIXED ? 4 : 1;
-#pragma unroll UNR
   const double2* txy = trxy + ls;
   const double2* tzw = trzw + ls;
   const double2* tql = tq + ls;
