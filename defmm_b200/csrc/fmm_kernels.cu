@@ -1916,7 +1916,7 @@ __global__ void __launch_bounds__(128) k_p2p_rhs(DevPlan P, int64_t nitem, const
           float2 fs[RB];
 #pragma unroll
           for (int b = 0; b < RB; b++) fs[b] = make_float2(0.f, 0.f);
-#pragma unroll 4
+#pragma unroll 8
           for (int j = j0; j < j1; j += GS) {
             const double2 a = sa[j], bz = sb[j];
             const Q* qj = sq + j * RB;
