@@ -2069,7 +2069,7 @@ __device__ __forceinline__ void sym_steps(int ls, int tp_rt, double yx, double y
   const double2* txy = trxy + ls;
   const double2* tzw = trzw + ls;
   const double2* tql = tq + ls;
-#pragma unroll 4
+#pragma unroll 8
   for (int st = 0; st < tp; st++) {
     const double2 a = txy[st], b = tzw[st];
     if constexpr (MIXED) {
