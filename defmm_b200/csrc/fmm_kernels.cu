@@ -404,8 +404,10 @@ struct Sep {
 // A lane reads its (b, c) lines (along axis 0) of each child's expansion
 // straight into registers, lanes at unit stride (the next child's are
 // prefetched during the current transfer); the transfer runs axis 0 first.
-// With R right-hand sides a warp takes one (parent slot, right-hand side);
-// the parent's expansions live at Mp + (slot R + r) LL, the children's at
+// Lane e holds child e's slot, octant and plane-wave phase, computed once
+// per parent slot.  With R right-hand sides a warp takes one parent slot and
+// runs its transfers for every right-hand side in turn; the parent's
+// expansions live at Mp + (slot R + r) LL, the children's at
 // Mc0 + (slot R + r) LL (both bases may be the same array).
 constexpr int kXferWarps = 4;  // warps (transfers in flight) per CTA
 
@@ -420,24 +422,32 @@ __global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 4 ? 6 
   constexpr int LL = L * L * L, NW = kXferWarps, NLN = S::NLN;
   __shared__ C sbuf[NW][LL];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t nw = (s1 - s0) * R;
-  for (int64_t w = blockIdx.x * NW + warp; w < nw; w += (int64_t)gridDim.x * NW) {
-    const int64_t ps = s0 + w / R;
-    const int rr = (int)(w % R);
+  for (int64_t ps = s0 + blockIdx.x * NW + warp; ps < s1; ps += (int64_t)gridDim.x * NW) {
     const int64_t eb = P.m2m_ptr[ps], ee = P.m2m_ptr[ps + 1];
     if (eb == ee) continue;  // leaf slot: written by P2M
     const int pc = P.sS_cell[ps], d = P.sS_dir[ps];
     const int lv = P.S_lvl[pc];
     const bool hf = P.ishf[lv] != 0;
     const int h = P.hfstage[lv];
-    const double4 pct = P.S_ctr[pc];
     const C* sg = sig + P.sig_off[h] + (int64_t)(hf ? d : 0) * LL;
     const C* sg2 = sig2 + P.sig_off[h] + (int64_t)(hf ? d : 0) * LL;
-    double dv[3] = {0., 0., 0.};
-    if (hf)
-      for (int k = 0; k < 3; k++) dv[k] = P.dirs[3 * (P.dir_off[h] + d) + k];
+    // child e (<= 8) on lane e: its slot, the octant of its centre (bit k
+    // set when v_k >= 0) and its phase exp(-i k d.v)
+    const int nch = (int)(ee - eb);
+    int my_cs = 0, my_oct = 0;
+    C my_ph = czero<C>();
+    if (lane < nch) {
+      my_cs = P.m2m_child[eb + lane];
+      const double4 pct = P.S_ctr[pc], ct = P.S_ctr[P.sS_cell[my_cs]];
+      const double v0 = ct.x - pct.x, v1 = ct.y - pct.y, v2 = ct.z - pct.z;
+      my_oct = (v0 < 0. ? 0 : 1) | (v1 < 0. ? 0 : 2) | (v2 < 0. ? 0 : 4);
+      if (hf) {
+        const double* dv = P.dirs + 3 * (P.dir_off[h] + d);
+        my_ph = expi<C>(-P.kappa * (dv[0] * v0 + dv[1] * v1 + dv[2] * v2));
+      }
+    }
     // with one line per lane (L <= 5) the parent's signature line and the
-    // next child's lines stay in registers; larger orders reload them
+    // next transfer's lines stay in registers; larger orders reload them
     constexpr bool REG = NLN == 1;
     C acc[NLN][L], sgr[REG ? NLN : 1][L];
 #pragma unroll
@@ -449,30 +459,25 @@ __global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 4 ? 6 
         if (REG) sgr[0][k] = (hf && ln < L * L) ? sg[k * L * L + ln] : czero<C>();
       }
     }
-    // children metadata fetched by lane (<= 8 children), broadcast below
-    const int nch = (int)(ee - eb);
-    int my_cs = 0;
-    double4 my_ct = make_double4(0., 0., 0., 0.);
-    if (lane < nch) {
-      my_cs = P.m2m_child[eb + lane];
-      my_ct = P.S_ctr[P.sS_cell[my_cs]];
-    }
-    C nxt[REG ? NLN : 1][L];  // next child's (a, b) lines, prefetched
+    C nxt[REG ? NLN : 1][L];  // next transfer's (a, b) lines, prefetched
     if (REG) {
-      const C* Mc = Mc0 + ((int64_t)__shfl_sync(0xffffffffu, my_cs, 0) * R + rr) * LL;
+      const C* Mc = Mc0 + (int64_t)__shfl_sync(0xffffffffu, my_cs, 0) * R * LL;
 #pragma unroll
       for (int k = 0; k < L; k++) nxt[0][k] = lane < L * L ? Mc[k * L * L + lane] : czero<C>();
     }
-    for (int e = 0; e < nch; e++) {
-      const double cx = __shfl_sync(0xffffffffu, my_ct.x, e), cy = __shfl_sync(0xffffffffu, my_ct.y, e),
-                   cz = __shfl_sync(0xffffffffu, my_ct.z, e);
-      const double v[3] = {cx - pct.x, cy - pct.y, cz - pct.z};
+    // transfers in (right-hand side, child) order
+    const int nit = nch * R;
+    int e = 0, rr = 0;
+    for (int it = 0; it < nit; it++) {
+      const int oct = __shfl_sync(0xffffffffu, my_oct, e);
       C in[NLN][L];
       if (REG) {
 #pragma unroll
         for (int k = 0; k < L; k++) in[0][k] = hf ? cmul(sgr[0][k], nxt[0][k]) : nxt[0][k];
-        if (e + 1 < nch) {
-          const C* Mc = Mc0 + ((int64_t)__shfl_sync(0xffffffffu, my_cs, e + 1) * R + rr) * LL;
+        const int e1 = e + 1 < nch ? e + 1 : 0, r1 = e + 1 < nch ? rr : rr + 1;
+        const int cs1 = __shfl_sync(0xffffffffu, my_cs, e1);
+        if (it + 1 < nit) {
+          const C* Mc = Mc0 + ((int64_t)cs1 * R + r1) * LL;
 #pragma unroll
           for (int k = 0; k < L; k++)
             if (lane < L * L) nxt[0][k] = Mc[k * L * L + lane];
@@ -490,9 +495,11 @@ __global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 4 ? 6 
         }
       }
       C res[NLN][L];
-      S::run_a0(v[0] < 0. ? 0 : 1, v[1] < 0. ? 0 : 1, v[2] < 0. ? 0 : 1, in, sbuf[warp], res, lane);
+      S::run_a0(oct & 1, (oct >> 1) & 1, (oct >> 2) & 1, in, sbuf[warp], res, lane);
       if (hf) {
-        const C ph = expi<C>(-P.kappa * (dv[0] * v[0] + dv[1] * v[1] + dv[2] * v[2]));
+        C ph;
+        ph.x = __shfl_sync(0xffffffffu, my_ph.x, e);
+        ph.y = __shfl_sync(0xffffffffu, my_ph.y, e);
 #pragma unroll
         for (int q = 0; q < NLN; q++)
 #pragma unroll
@@ -506,16 +513,22 @@ __global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 4 ? 6 
             acc[q][k].y += res[q][k].y;
           }
       }
-    }
+      if (++e == nch) {  // the last child of right-hand side rr
 #pragma unroll
-    for (int q = 0; q < NLN; q++) {
-      const int ln = lane + 32 * q;
-      if (ln < L * L)
+        for (int q = 0; q < NLN; q++) {
+          const int ln = lane + 32 * q;
 #pragma unroll
-        for (int k = 0; k < L; k++) {
-          const int l = ln * L + k;
-          Mp[(ps * R + rr) * LL + l] = hf ? cmulc(sg2[l], acc[q][k]) : acc[q][k];
+          for (int k = 0; k < L; k++) {
+            if (ln < L * L) {
+              const int l = ln * L + k;
+              Mp[(ps * R + rr) * LL + l] = hf ? cmulc(sg2[l], acc[q][k]) : acc[q][k];
+            }
+            acc[q][k] = czero<C>();
+          }
         }
+        e = 0;
+        rr++;
+      }
     }
   }
 }
@@ -525,8 +538,10 @@ __global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 4 ? 6 
 //   HF parent direction d (hfL2Lblock L2L.hpp:78-108 / hf2lfL2L :111-127):
 //     L_c += sum_d exp(i k v.d) conj(sig_d) o B_v(sig2_d o L_d)
 //   LF parent (lfL2L :35-41): L_c += B_v(L_p);   v = ctr_child - ctr_parent
-// With R right-hand sides a warp takes one (child slot, right-hand side);
-// children at Lc + (slot R + r) LL, parents at Lp0 + (slot R + r) LL.  Only
+// Lane e holds parent e's slot, direction and phase, computed once per child
+// slot.  With R right-hand sides a warp takes one child slot and runs its
+// transfers for every right-hand side in turn; children at
+// Lc + (slot R + r) LL, parents at Lp0 + (slot R + r) LL.  Only
 // parent slots in [p0, p1) contribute (a pass over part of the directions).
 template <typename T, int L>
 __global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 5 ? 6 : 3) : (L <= 5 ? 3 : 1)) k_l2l(DevPlan P, int64_t s0, int64_t s1,
@@ -540,10 +555,7 @@ __global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 5 ? 6 
   constexpr int LL = L * L * L, NW = kXferWarps, NLN = S::NLN;
   __shared__ C sbuf[NW][LL];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t nw = (s1 - s0) * R;
-  for (int64_t w = blockIdx.x * NW + warp; w < nw; w += (int64_t)gridDim.x * NW) {
-    const int64_t cs = s0 + w / R;
-    const int rr = (int)(w % R);
+  for (int64_t cs = s0 + blockIdx.x * NW + warp; cs < s1; cs += (int64_t)gridDim.x * NW) {
     const int64_t eb = P.l2l_ptr[cs], ee = P.l2l_ptr[cs + 1];
     if (eb == ee) continue;
     const int cc = P.sT_cell[cs];
@@ -580,16 +592,25 @@ __global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 5 ? 6 
       }
     }
     if (npa == 0) continue;
-    // with one line per lane (L <= 5) the next parent's lines are
+    // parent e on lane e: its phase exp(i k v.d_e)
+    C my_ph = czero<C>();
+    if (hf && lane < npa) {
+      const double* dv = P.dirs + 3 * (P.dir_off[h] + my_d);
+      my_ph = expi<C>(P.kappa * (v[0] * dv[0] + v[1] * dv[1] + v[2] * dv[2]));
+    }
+    // with one line per lane (L <= 5) the next transfer's lines are
     // prefetched into registers; larger orders load them when used
     constexpr bool REG = NLN == 1;
     C nxt[REG ? NLN : 1][L];
     if (REG) {
-      const C* Lp = Lp0 + ((int64_t)__shfl_sync(0xffffffffu, my_ps, 0) * R + rr) * LL;
+      const C* Lp = Lp0 + (int64_t)__shfl_sync(0xffffffffu, my_ps, 0) * R * LL;
 #pragma unroll
       for (int k = 0; k < L; k++) nxt[0][k] = lane < L * L ? Lp[lane * L + k] : czero<C>();
     }
-    for (int e = 0; e < npa; e++) {
+    // transfers in (right-hand side, parent) order
+    const int nit = npa * R;
+    int e = 0, rr = 0;
+    for (int it = 0; it < nit; it++) {
       const int d = __shfl_sync(0xffffffffu, my_d, e);
       const C* sg = sig + P.sig_off[h] + (int64_t)(hf ? d : 0) * LL;
       const C* sgq = sig2 + P.sig_off[h] + (int64_t)(hf ? d : 0) * LL;
@@ -597,8 +618,10 @@ __global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 5 ? 6 
       if (REG) {
 #pragma unroll
         for (int k = 0; k < L; k++) in[0][k] = (hf && lane < L * L) ? cmul(sgq[lane * L + k], nxt[0][k]) : nxt[0][k];
-        if (e + 1 < npa) {
-          const C* Lp = Lp0 + ((int64_t)__shfl_sync(0xffffffffu, my_ps, e + 1) * R + rr) * LL;
+        const int e1 = e + 1 < npa ? e + 1 : 0, r1 = e + 1 < npa ? rr : rr + 1;
+        const int ps1 = __shfl_sync(0xffffffffu, my_ps, e1);
+        if (it + 1 < nit) {
+          const C* Lp = Lp0 + ((int64_t)ps1 * R + r1) * LL;
 #pragma unroll
           for (int k = 0; k < L; k++)
             if (lane < L * L) nxt[0][k] = Lp[lane * L + k];
@@ -618,8 +641,9 @@ __global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 5 ? 6 
       C res[NLN][L];
       S::run(sg0, sg1, sg2i, in, sbuf[warp], res, lane);
       if (hf) {
-        const double* dv = P.dirs + 3 * (P.dir_off[h] + d);
-        const C ph = expi<C>(P.kappa * (v[0] * dv[0] + v[1] * dv[1] + v[2] * dv[2]));
+        C ph;
+        ph.x = __shfl_sync(0xffffffffu, my_ph.x, e);
+        ph.y = __shfl_sync(0xffffffffu, my_ph.y, e);
 #pragma unroll
         for (int q = 0; q < NLN; q++) {
           const int ln = lane + 32 * q;
@@ -636,19 +660,25 @@ __global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 5 ? 6 
             acc[q][k].y += res[q][k].y;
           }
       }
-    }
+      if (++e == npa) {  // the last parent of right-hand side rr
 #pragma unroll
-    for (int q = 0; q < NLN; q++) {
-      const int ln = lane + 32 * q;
-      if (ln < L * L)
+        for (int q = 0; q < NLN; q++) {
+          const int ln = lane + 32 * q;
 #pragma unroll
-        for (int k = 0; k < L; k++) {
-          const int64_t l = (cs * R + rr) * LL + k * L * L + ln;
-          C o = Lc[l];
-          o.x += acc[q][k].x;
-          o.y += acc[q][k].y;
-          Lc[l] = o;
+          for (int k = 0; k < L; k++) {
+            if (ln < L * L) {
+              const int64_t l = (cs * R + rr) * LL + k * L * L + ln;
+              C o = Lc[l];
+              o.x += acc[q][k].x;
+              o.y += acc[q][k].y;
+              Lc[l] = o;
+            }
+            acc[q][k] = czero<C>();
+          }
         }
+        e = 0;
+        rr++;
+      }
     }
   }
 }
@@ -2495,14 +2525,14 @@ struct Launch {
                   const void* Mc, int R, cudaStream_t s) {
     constexpr int NW = kXferWarps;
     if (s1 > s0)
-      k_m2m<T, L><<<grid_for((s1 - s0) * R, NW), 32 * NW, 0, s>>>(dp, s0, s1, (const C*)sig, (const C*)sig2, (C*)Mp,
+      k_m2m<T, L><<<grid_for(s1 - s0, NW), 32 * NW, 0, s>>>(dp, s0, s1, (const C*)sig, (const C*)sig2, (C*)Mp,
                                                                   (const C*)Mc, R);
   }
   static void l2l(const DevPlan& dp, int64_t s0, int64_t s1, const void* sig, const void* sig2, void* Lc,
                   const void* Lp, int R, int64_t p0, int64_t p1, cudaStream_t s) {
     constexpr int NW = kXferWarps;
     if (s1 > s0)
-      k_l2l<T, L><<<grid_for((s1 - s0) * R, NW), 32 * NW, 0, s>>>(dp, s0, s1, (const C*)sig, (const C*)sig2, (C*)Lc,
+      k_l2l<T, L><<<grid_for(s1 - s0, NW), 32 * NW, 0, s>>>(dp, s0, s1, (const C*)sig, (const C*)sig2, (C*)Lc,
                                                                   (const C*)Lp, R, p0, p1);
   }
   static void m2f(int64_t n, const void* M, void* F, cudaStream_t s) {
