@@ -86,6 +86,7 @@ def lib():
             "defmm_set_m2l_pairing": (ctypes.c_int, [vp, ctypes.c_int]),
             "defmm_set_blocking": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
             "defmm_dump_m2l": (ctypes.c_int, [vp, vp, vp, vp, ctypes.POINTER(i64)]),
+            "defmm_near_digest": (ctypes.c_int, [vp, vp]),
             "defmm_probe_l2_read": (ctypes.c_int, [i64, ctypes.c_int, dp]),
             "defmm_set_rhs_per_cta": (ctypes.c_int, [vp, ctypes.c_int]),
             "defmm_set_tensor_cores": (ctypes.c_int, [vp, ctypes.c_int]),
@@ -328,6 +329,13 @@ class IBFMM_Mat:
         tab = np.zeros(n[1], np.uint32)
         self._check(lib().defmm_dump_m2l(self._h, ptr.ctypes.data, src.ctypes.data, tab.ctypes.data, n))
         return ptr, src, tab
+
+    def near_digest(self):
+        """26 fingerprints of the near-field work lists as the matvec runs
+        them (defmm_near_digest)."""
+        d = np.zeros(26, np.uint64)
+        self._check(lib().defmm_near_digest(self._h, d.ctypes.data))
+        return d
 
 
 class MultiFreqMat:

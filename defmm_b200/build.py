@@ -16,7 +16,8 @@ LIB = os.path.join(HERE, "libdefmm_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU = ["fmm_kernels.cu", "tc_interp.cu", "engine.cu", "noalloc.cu", "plan_device.cu", "mlp.cu", "measure.cu"]
+CU = ["fmm_kernels.cu", "tc_interp.cu", "engine.cu", "noalloc.cu", "plan_device.cu", "near_device.cu", "mlp.cu",
+      "measure.cu"]
 # the device level walk reproduces the host plan's floating-point decisions:
 # no FMA contraction there
 CU_FLAGS = {"plan_device.cu": ["--fmad=false"]}

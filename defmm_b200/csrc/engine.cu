@@ -357,32 +357,61 @@ int upload_plan(defmm_handle* h) {
     bylvl(p.T.lvl, p.l2p_leaf, tmp, h->l2p_lvl_off);
     UP(tmp, h->d_l2p_bylvl);
   }
-  UP(p.p2p_tfirst, h->d_tfirst);
-  UP(p.p2p_tn, h->d_tn);
-  UP(p.p2p_ptr, h->d_p2p_ptr);
-  UP(p.p2p_sfirst, h->d_sfirst);
-  UP(p.p2p_sn, h->d_sn);
-  UP(p.p2p_order, h->d_p2p_order);
-  UP(p.p2p_item_chunk, h->d_p2p_item_chunk);
-  UP(p.p2p_chunk_items, h->d_p2p_chunk_items);
-  if (p.p2p_sym) {
-    UP(p.sym_item_chunk, h->d_sym_item_chunk);
-    UP(p.sym_chunk_items, h->d_sym_chunk_items);
-    UP(p.self_ptr, h->d_self_ptr);
-    UP(p.self_sfirst, h->d_self_sfirst);
-    UP(p.self_sn, h->d_self_sn);
-    UP(p.self_order, h->d_self_order);
-    UP(p.sym_ptr, h->d_sym_ptr);
-    UP(p.sym_sfirst, h->d_sym_sfirst);
-    UP(p.sym_sn, h->d_sym_sn);
-    UP(p.sym_soff, h->d_sym_soff);
-    UP(p.sym_order, h->d_sym_order);
-    UP(p.red_first, h->d_red_first);
-    UP(p.red_n, h->d_red_n);
-    UP(p.red_ptr, h->d_red_ptr);
-    UP(p.red_off, h->d_red_off);
+  if (p.nd.on) {  // built on the device by prcmpt
+    const Plan::NearOnDevice& n = p.nd;
+    h->d_tfirst = n.tfirst;
+    h->d_tn = n.tn;
+    h->d_p2p_ptr = n.p2p_ptr;
+    h->d_sfirst = n.p2p_sfirst;
+    h->d_sn = n.p2p_sn;
+    h->d_p2p_order = n.p2p_order;
+    h->d_p2p_item_chunk = n.p2p_item_chunk;
+    h->d_p2p_chunk_items = n.p2p_chunk_items;
+    if (p.p2p_sym) {
+      h->d_sym_item_chunk = n.sym_item_chunk;
+      h->d_sym_chunk_items = n.sym_chunk_items;
+      h->d_self_ptr = n.self_ptr;
+      h->d_self_sfirst = n.self_sfirst;
+      h->d_self_sn = n.self_sn;
+      h->d_self_order = n.self_order;
+      h->d_sym_ptr = n.sym_ptr;
+      h->d_sym_sfirst = n.sym_sfirst;
+      h->d_sym_sn = n.sym_sn;
+      h->d_sym_soff = n.sym_soff;
+      h->d_sym_order = n.sym_order;
+      h->d_red_first = n.red_first;
+      h->d_red_n = n.red_n;
+      h->d_red_ptr = n.red_ptr;
+      h->d_red_off = n.red_off;
+    }
+  } else {
+    UP(p.p2p_tfirst, h->d_tfirst);
+    UP(p.p2p_tn, h->d_tn);
+    UP(p.p2p_ptr, h->d_p2p_ptr);
+    UP(p.p2p_sfirst, h->d_sfirst);
+    UP(p.p2p_sn, h->d_sn);
+    UP(p.p2p_order, h->d_p2p_order);
+    UP(p.p2p_item_chunk, h->d_p2p_item_chunk);
+    UP(p.p2p_chunk_items, h->d_p2p_chunk_items);
+    if (p.p2p_sym) {
+      UP(p.sym_item_chunk, h->d_sym_item_chunk);
+      UP(p.sym_chunk_items, h->d_sym_chunk_items);
+      UP(p.self_ptr, h->d_self_ptr);
+      UP(p.self_sfirst, h->d_self_sfirst);
+      UP(p.self_sn, h->d_self_sn);
+      UP(p.self_order, h->d_self_order);
+      UP(p.sym_ptr, h->d_sym_ptr);
+      UP(p.sym_sfirst, h->d_sym_sfirst);
+      UP(p.sym_sn, h->d_sym_sn);
+      UP(p.sym_soff, h->d_sym_soff);
+      UP(p.sym_order, h->d_sym_order);
+      UP(p.red_first, h->d_red_first);
+      UP(p.red_n, h->d_red_n);
+      UP(p.red_ptr, h->d_red_ptr);
+      UP(p.red_off, h->d_red_off);
+    }
   }
-  h->nchunk = (int64_t)p.p2p_tfirst.size();
+  h->nchunk = p.near_chunks();
 #undef UP
   {
     void* e = nullptr;
@@ -390,7 +419,7 @@ int upload_plan(defmm_handle* h) {
     h->plan_allocs.push_back(e);
     CK(cudaMemset(e, 0, sizeof(int)));
     d.err = static_cast<int*>(e);
-    const size_t nitem = std::max<size_t>(1, std::max(p.p2p_item_chunk.size(), p.sym_item_chunk.size()));
+    const size_t nitem = (size_t)std::max<int64_t>(1, std::max(p.near_items(), p.near_sym_items()));
     void* tp = nullptr;
     CK(cudaMalloc(&tp, nitem * 32 * sizeof(double2)));
     h->plan_allocs.push_back(tp);
@@ -650,7 +679,7 @@ int prepare_grouped(defmm_handle* h, int R) {
   g.lfT1 = p.sT.n;
   const int64_t nS = (int64_t)p.S.perm.size(), nT = (int64_t)p.T.perm.size();
   const size_t slot_b = (size_t)R * p.LL * cs;
-  const size_t nitem = std::max<size_t>(1, p.p2p_item_chunk.size());
+  const size_t nitem = (size_t)std::max<int64_t>(1, p.near_items());
   int st;
   if ((st = ensure(h, g.q, (size_t)nS * R * cs)) || (st = ensure(h, g.pnear, (size_t)nT * R * 16)) ||
       (st = ensure(h, g.pfar, (size_t)nT * R * 16)) || (st = ensure(h, g.tpart, nitem * 32 * R * 16)) ||
@@ -753,24 +782,24 @@ int run_gemv(defmm_handle* h, const double2* qin, double2* out, cudaStream_t s) 
   CK(cudaStreamWaitEvent(sn, ready, 0));
   if (h->events) cudaEventRecord(h->ev[2 * PH_P2P], sn);
   if (h->use_sym) {  // own leaves, then symmetric blocks, then the mirrored partial sums
-    dfb::launch_p2p(fp64, d, (int64_t)p.self_order.size(), h->d_self_order, nullptr, h->d_tfirst, h->d_tn,
+    dfb::launch_p2p(fp64, d, p.near_self_items(), h->d_self_order, nullptr, h->d_tfirst, h->d_tn,
                     h->d_self_ptr, h->d_self_sfirst, h->d_self_sn, h->q.p, (double2*)h->pnear.p, nullptr,
                     h->d_queue, h->nsm, sn);
-    dfb::launch_p2p_sym(fp64, d, (int64_t)p.sym_order.size(), h->d_sym_order, h->d_sym_item_chunk, h->d_tfirst,
+    dfb::launch_p2p_sym(fp64, d, p.near_sym_items(), h->d_sym_order, h->d_sym_item_chunk, h->d_tfirst,
                         h->d_tn, h->d_sym_ptr, h->d_sym_sfirst, h->d_sym_sn, h->d_sym_soff, h->q.p, h->d_tpart,
                         h->pscr.p, h->d_queue, h->nsm, h->p2p_bps[fp64 ? 0 : 1], sn);
     dfb::launch_p2p_items(h->nchunk, h->d_tfirst, h->d_tn, h->d_sym_chunk_items, h->d_tpart, (double2*)h->pnear.p,
                           h->nsm, sn);
-    dfb::launch_p2p_reduce(fp64, (int64_t)p.red_first.size(), h->d_red_first, h->d_red_n, h->d_red_ptr,
+    dfb::launch_p2p_reduce(fp64, p.near_red_leaves(), h->d_red_first, h->d_red_n, h->d_red_ptr,
                            h->d_red_off, h->pscr.p, (double2*)h->pnear.p, h->nsm, sn);
-    nl_ += (p.self_order.empty() ? 0 : 1) + (p.sym_order.empty() ? 0 : 2) + (p.red_first.empty() ? 0 : 1);
+    nl_ += (p.near_self_items() ? 1 : 0) + (p.near_sym_items() ? 2 : 0) + (p.near_red_leaves() ? 1 : 0);
   } else {  // every interaction from the target side, in items
-    dfb::launch_p2p(fp64, d, (int64_t)p.p2p_order.size(), h->d_p2p_order, h->d_p2p_item_chunk, h->d_tfirst, h->d_tn,
+    dfb::launch_p2p(fp64, d, p.near_items(), h->d_p2p_order, h->d_p2p_item_chunk, h->d_tfirst, h->d_tn,
                     h->d_p2p_ptr, h->d_sfirst, h->d_sn, h->q.p, (double2*)h->pnear.p, h->d_tpart, h->d_queue,
                     h->nsm, sn);
     dfb::launch_p2p_items(h->nchunk, h->d_tfirst, h->d_tn, h->d_p2p_chunk_items, h->d_tpart, (double2*)h->pnear.p,
                           h->nsm, sn);
-    nl_ += p.p2p_order.empty() ? 0 : 2;
+    nl_ += p.near_items() ? 2 : 0;
   }
   if (h->events) cudaEventRecord(h->ev[2 * PH_P2P + 1], sn);
   if (tuning) {
@@ -974,12 +1003,12 @@ int run_gemv_grouped(defmm_handle* h, const double2* qin, int64_t stride_in, dou
   {
     float a = 0;
     if (h->events) CK(cudaEventRecord(e0, sn));
-    dfb::launch_p2p_rhs(fp64, d, (int64_t)p.p2p_order.size(), h->d_p2p_order, h->d_p2p_item_chunk, h->d_tfirst,
+    dfb::launch_p2p_rhs(fp64, d, p.near_items(), h->d_p2p_order, h->d_p2p_item_chunk, h->d_tfirst,
                         h->d_tn, h->d_p2p_ptr, h->d_sfirst, h->d_sn, g.q.p, R, (double2*)g.pnear.p,
                         (double2*)g.tpart.p, h->d_queue, h->nsm, h->p2p_bps[pi], sn);
     dfb::launch_p2p_items_rhs(h->nchunk, h->d_tfirst, h->d_tn, h->d_p2p_chunk_items, (const double2*)g.tpart.p, R,
                               (double2*)g.pnear.p, h->nsm, sn);
-    nk += p.p2p_order.empty() ? 0 : (R + 7) / 8 + 1;
+    nk += p.near_items() ? (R + 7) / 8 + 1 : 0;
     if (h->events) {
       CK(cudaEventRecord(e1, sn));
       CK(cudaEventSynchronize(e1));
@@ -1568,6 +1597,8 @@ int defmm_prcmpt(defmm_handle* h, int L, int Ncrit, double kappa, int lvMAX) {
   for (void* q : {h->plan.dev_m2l_src, h->plan.dev_m2l_tab, h->plan.dev_m2m_ptr, h->plan.dev_m2m_child,
                   h->plan.dev_l2l_ptr, h->plan.dev_l2l_parent})
     if (q) h->plan_allocs.push_back(q);
+  h->plan_allocs.insert(h->plan_allocs.end(), h->plan.dev_near_allocs.begin(), h->plan.dev_near_allocs.end());
+  h->plan.dev_near_allocs.clear();
   if (st) return h->fail(st == -4 ? DEFMM_ERR_CUDA : st == -5 ? DEFMM_ERR_MEMORY : st, e);
   h->walked_on_device = walker != nullptr;
   if (h->plan.lv.nlvl > 32) return h->fail(DEFMM_ERR_DEPTH, "more than 32 tree levels");
@@ -2018,6 +2049,77 @@ int defmm_dump_m2l(const defmm_handle* h, int64_t* ptr, int32_t* src, uint32_t* 
   if (tab)  // ids -> (table << 6) | hash keys
     for (int64_t i = 0; i < n[1]; i++) tab[i] = p.ptab_key[tab[i]];
   return 0;
+}
+
+int defmm_near_digest(const defmm_handle* h, uint64_t* digest) {
+  if (!h || !h->built || !digest) return DEFMM_ERR_ARG;
+  const Plan& p = h->plan;
+  const Plan::NearOnDevice& d = p.nd;
+  if (d.on && h->device >= 0 && cudaSetDevice(h->device) != cudaSuccess) return DEFMM_ERR_CUDA;
+  int k = 0;
+  bool ok = true;
+  // FNV-1a over the element count and the bytes of one array, wherever it lives
+  auto hash = [&](const void* host, const void* dev, int64_t n, size_t es) {
+    std::vector<unsigned char> buf;
+    const unsigned char* b = static_cast<const unsigned char*>(host);
+    if (d.on) {
+      buf.resize((size_t)n * es);
+      if (n && cudaMemcpy(buf.data(), dev, (size_t)n * es, cudaMemcpyDeviceToHost) != cudaSuccess) {
+        cudaGetLastError();
+        ok = false;
+      }
+      b = buf.data();
+    }
+    uint64_t x = 1469598103934665603ull;
+    for (int s = 0; s < 64; s += 8) x = (x ^ (((uint64_t)n >> s) & 0xff)) * 1099511628211ull;
+    for (size_t i = 0; i < (size_t)n * es; i++) x = (x ^ b[i]) * 1099511628211ull;
+    digest[k++] = x;
+  };
+  auto at = [&](const std::vector<int64_t>& v, const int64_t* dv, int64_t i) -> int64_t {
+    if (!d.on) return v.empty() ? 0 : v[i];
+    int64_t x = 0;
+    if (dv && cudaMemcpy(&x, dv + i, 8, cudaMemcpyDeviceToHost) != cudaSuccess) {
+      cudaGetLastError();
+      ok = false;
+    }
+    return x;
+  };
+#define NEAR_ARRAY(vec, dptr, n) hash((vec).data(), (dptr), d.on ? (int64_t)(n) : (int64_t)(vec).size(), sizeof((vec)[0]))
+  const bool sym = p.p2p_sym;
+  const int64_t nch = p.near_chunks(), nit = p.near_items(), nsy = sym ? p.near_sym_items() : 0;
+  const int64_t nred = sym ? p.near_red_leaves() : 0;
+  const int64_t npc = at(p.p2p_ptr, d.p2p_ptr, nit);
+  NEAR_ARRAY(p.p2p_tfirst, d.tfirst, nch);
+  NEAR_ARRAY(p.p2p_tn, d.tn, nch);
+  NEAR_ARRAY(p.p2p_ptr, d.p2p_ptr, nit + 1);
+  NEAR_ARRAY(p.p2p_sfirst, d.p2p_sfirst, npc);
+  NEAR_ARRAY(p.p2p_sn, d.p2p_sn, npc);
+  NEAR_ARRAY(p.p2p_item_chunk, d.p2p_item_chunk, nit);
+  NEAR_ARRAY(p.p2p_chunk_items, d.p2p_chunk_items, nch + 1);
+  NEAR_ARRAY(p.p2p_order, d.p2p_order, nit);
+  const int64_t nself = sym ? at(p.self_ptr, d.self_ptr, nch) : 0;
+  const int64_t nys = sym ? at(p.sym_ptr, d.sym_ptr, nsy) : 0;
+  const int64_t nro = sym ? at(p.red_ptr, d.red_ptr, nred) : 0;
+  NEAR_ARRAY(p.self_ptr, d.self_ptr, sym ? nch + 1 : 0);
+  NEAR_ARRAY(p.self_sfirst, d.self_sfirst, nself);
+  NEAR_ARRAY(p.self_sn, d.self_sn, nself);
+  NEAR_ARRAY(p.self_order, d.self_order, sym ? p.near_self_items() : 0);
+  NEAR_ARRAY(p.sym_ptr, d.sym_ptr, sym ? nsy + 1 : 0);
+  NEAR_ARRAY(p.sym_sfirst, d.sym_sfirst, nys);
+  NEAR_ARRAY(p.sym_sn, d.sym_sn, nys);
+  NEAR_ARRAY(p.sym_soff, d.sym_soff, nys);
+  NEAR_ARRAY(p.sym_item_chunk, d.sym_item_chunk, nsy);
+  NEAR_ARRAY(p.sym_chunk_items, d.sym_chunk_items, sym ? nch + 1 : 0);
+  NEAR_ARRAY(p.sym_order, d.sym_order, nsy);
+  NEAR_ARRAY(p.red_first, d.red_first, nred);
+  NEAR_ARRAY(p.red_n, d.red_n, nred);
+  NEAR_ARRAY(p.red_ptr, d.red_ptr, sym ? nred + 1 : 0);
+  NEAR_ARRAY(p.red_off, d.red_off, nro);
+#undef NEAR_ARRAY
+  digest[k++] = (uint64_t)p.sym_scratch;
+  digest[k++] = (uint64_t)p.i_near;
+  digest[k++] = (uint64_t)p.n_near;
+  return ok ? 0 : DEFMM_ERR_CUDA;
 }
 
 }  // extern "C"

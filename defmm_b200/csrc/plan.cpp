@@ -1326,8 +1326,9 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
     if (p.T.leaf(c) && v.prec[p.T.lvl[c]]) p.l2p_leaf.push_back((int32_t)c);
 
   // near field per target leaf: a near pair (t, s) sends the particles of s
-  // to every particle below t (P2P.hpp:43-79 on whole subtrees)
-  {
+  // to every particle below t (P2P.hpp:43-79 on whole subtrees); the device
+  // walk may have built these lists already (Plan::nd)
+  if (!w.near_done) {
     p.n_near = (int64_t)near_pairs.size();
     if (p.keep_lists)
       for (auto& pr : near_pairs) {
@@ -1411,16 +1412,16 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
         p.p2p_ptr[q + 1] = r;
       }
     });
+    p.step("near-field ranges and chunks", ts);
+    if (p.p2p_sym) {
+      build_symmetric_near(p);
+      split_items(p, p.sym_ptr, p.sym_sfirst, p.sym_sn, &p.sym_soff, p.sym_item_chunk, p.sym_chunk_items,
+                  p.sym_order, true);
+    }
+    split_items(p, p.p2p_ptr, p.p2p_sfirst, p.p2p_sn, nullptr, p.p2p_item_chunk, p.p2p_chunk_items, p.p2p_order,
+                false);
+    p.step("near-field symmetric blocks and work items", ts);
   }
-  p.step("near-field ranges and chunks", ts);
-  if (p.p2p_sym) {
-    build_symmetric_near(p);
-    split_items(p, p.sym_ptr, p.sym_sfirst, p.sym_sn, &p.sym_soff, p.sym_item_chunk, p.sym_chunk_items,
-                p.sym_order, true);
-  }
-  split_items(p, p.p2p_ptr, p.p2p_sfirst, p.p2p_sn, nullptr, p.p2p_item_chunk, p.p2p_chunk_items, p.p2p_order,
-              false);
-  p.step("near-field symmetric blocks and work items", ts);
   p.t_lists = now_s() - t0;
 
   // transfer spectra, FP64 (circulant.hpp:133-144); with a device plan the

@@ -155,6 +155,30 @@ struct Plan {
   std::vector<int32_t> red_first, red_n;
   std::vector<int64_t> red_ptr, red_off;     // leaves + 1 into red_off (chunk order)
   int64_t sym_scratch = 0;                   // scratch slots (one complex each)
+  // The same near-field lists built on the device by the device walk (the
+  // host vectors p2p_*, self_*, sym_*, red_* above then stay empty): device
+  // arrays with the host build's contents, and their sizes.  The operator
+  // that owns the plan releases them (dev_near_allocs).
+  struct NearOnDevice {
+    bool on = false;
+    int64_t nchunk = 0, p2p_items = 0, n_self_order = 0, sym_items = 0, n_red = 0;
+    const int32_t *tfirst = nullptr, *tn = nullptr;
+    const int64_t *p2p_ptr = nullptr, *p2p_chunk_items = nullptr;
+    const int32_t *p2p_sfirst = nullptr, *p2p_sn = nullptr, *p2p_item_chunk = nullptr, *p2p_order = nullptr;
+    const int64_t *self_ptr = nullptr;
+    const int32_t *self_sfirst = nullptr, *self_sn = nullptr, *self_order = nullptr;
+    const int64_t *sym_ptr = nullptr, *sym_soff = nullptr, *sym_chunk_items = nullptr;
+    const int32_t *sym_sfirst = nullptr, *sym_sn = nullptr, *sym_item_chunk = nullptr, *sym_order = nullptr;
+    const int32_t *red_first = nullptr, *red_n = nullptr;
+    const int64_t *red_ptr = nullptr, *red_off = nullptr;
+  } nd;
+  std::vector<void*> dev_near_allocs;
+  // sizes of the near-field lists wherever they were built
+  int64_t near_chunks() const { return nd.on ? nd.nchunk : (int64_t)p2p_tfirst.size(); }
+  int64_t near_items() const { return nd.on ? nd.p2p_items : (int64_t)p2p_order.size(); }
+  int64_t near_self_items() const { return nd.on ? nd.n_self_order : (int64_t)self_order.size(); }
+  int64_t near_sym_items() const { return nd.on ? nd.sym_items : (int64_t)sym_order.size(); }
+  int64_t near_red_leaves() const { return nd.on ? nd.n_red : (int64_t)red_first.size(); }
   // statistics
   int64_t n_far_hf = 0, n_far_lf = 0, n_near = 0, i_near = 0;
   // Optional record of the lists for parity checks: far (t, s, lvl, cone,
@@ -194,6 +218,9 @@ struct LevelWalk {
   // Set by a walker that also built the M2M / L2L transfer lists (on the
   // device: Plan::dev_m2m_ptr etc.).
   bool transfers_done = false;
+  // Set by a walker that also built the near-field lists (on the device:
+  // Plan::nd, with Plan::n_near and i_near); near_pairs then stays empty.
+  bool near_done = false;
 };
 
 // Another implementation of the level walk (the device one); it must produce

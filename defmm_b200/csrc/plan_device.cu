@@ -500,7 +500,8 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
   const double* d_dirs = nullptr;
   if ((st = upload_vec(A, alld, &d_dirs, err))) return st;
 
-  std::vector<int2> near_h;
+  // near pairs per level, kept on the device for the near-field lists
+  std::vector<std::pair<int2*, int64_t>> lv_near;
   int64_t table_count = 0;
   // every level's slots stay on the device until the M2M / L2L transfer
   // lists are built after the walk
@@ -557,12 +558,11 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
     if (nfr)
       k_scatter<<<nblk(nfr), 256>>>(nfr, F, T, S, isfar, pfar, isnear, pnear, nch, pch, fp, np_, next);
     DW_CK(cudaGetLastError());
-    if (nn) {
-      const size_t o = near_h.size();
-      near_h.resize(o + nn);
-      DW_CK(cudaMemcpy(near_h.data() + o, np_, (size_t)nn * sizeof(int2), cudaMemcpyDeviceToHost));
-    }
-    for (void* q : {(void*)isfar, (void*)isnear, (void*)pfar, (void*)pnear, (void*)nch, (void*)pch, (void*)np_, (void*)F})
+    if (nn)
+      lv_near.push_back({np_, nn});
+    else
+      A.drop(np_);
+    for (void* q : {(void*)isfar, (void*)isnear, (void*)pfar, (void*)pnear, (void*)nch, (void*)pch, (void*)F})
       A.drop(q);
     F = next;
     nfr = nx;
@@ -815,8 +815,6 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
   walk.transfers_done = true;
   p.sT.lvl_begin[nlvl] = p.sT.n;
   p.sS.lvl_begin[nlvl] = p.sS.n;
-  walk.near_pairs.resize(near_h.size());
-  for (size_t i = 0; i < near_h.size(); i++) walk.near_pairs[i] = {near_h[i].x, near_h[i].y};
   p.step("walk: levels, other (allocations, copies)", tstep);
   p.t_steps.back().second -= t_transfers + t_sub[0] + t_sub[1] + t_sub[2] + t_sub[3];
   p.t_steps.push_back({"walk: levels, pair classification and near pairs", t_sub[0]});
@@ -824,6 +822,28 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
   p.t_steps.push_back({"walk: levels, effective directions and slots", t_sub[2]});
   p.t_steps.push_back({"walk: levels, far entries", t_sub[3]});
   p.t_steps.push_back({"walk: M2M and L2L transfer lists", t_transfers});
+
+  // the near-field work lists from all levels' near pairs (walk order),
+  // built and kept on the device
+  {
+    double tn0 = wall_seconds();
+    int64_t nn = 0;
+    for (auto& x : lv_near) nn += x.second;
+    int2* all_near;
+    DW_ALLOC(all_near, int2, nn);
+    int64_t o = 0;
+    for (auto& x : lv_near) {
+      DW_CK(cudaMemcpy(all_near + o, x.first, x.second * sizeof(int2), cudaMemcpyDeviceToDevice));
+      A.drop(x.first);
+      o += x.second;
+    }
+    lv_near.clear();
+    p.n_near = nn;
+    if ((st = device_near_lists(p, all_near, nn, err))) return st;
+    A.drop(all_near);
+    walk.near_done = true;
+    p.step("walk: near-field lists (ranges, chunks, symmetric blocks, work items)", tn0);
+  }
 
   // M2L entries grouped by target slot: a stable radix sort of all levels'
   // entries (level order, then walk order) by target slot, as the host's

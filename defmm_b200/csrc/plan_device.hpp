@@ -20,6 +20,11 @@ std::unique_ptr<TreeSorter> make_device_tree_sorter();
 // signatures (sig, sig2: the host layout, stages after each other) computed
 // on the current device, bit-identical to the host's; 0 or -4 with err set.
 int device_plan_tables(const Plan& p, double2* tables, double2* sig, double2* sig2, std::string& err);
+// The near-field lists (Plan::nd) from the level walk's near pairs on the
+// device (npair (target cell, source cell) pairs in walk order), with the
+// host build's contents and order; also sets i_near and sym_scratch.
+// 0, -4 (CUDA error) or -5 (out of memory) with err set.
+int device_near_lists(Plan& p, const int2* d_near, int64_t npair, std::string& err);
 // FP64 -> FP32 complex, rounded to nearest.
 void tables_to_float(const double2* in, float2* out, int64_t n, cudaStream_t s);
 

@@ -320,6 +320,16 @@ int defmm_dump_lists(const defmm_handle* h, int32_t* far_hf, int32_t* far_lf,
 int defmm_dump_m2l(const defmm_handle* h, int64_t* ptr, int32_t* src,
                    uint32_t* tab, int64_t n[2]);
 
+/* No counterpart in the reference (its near field walks the P2P lists of
+ * each target leaf, P2P.hpp:43-79).  Fingerprints of the near-field work
+ * lists as the matvec runs them, for parity checks of the device plan
+ * against the host plan: digest[0..22] are 64-bit FNV-1a hashes of the
+ * chunk, work-item, symmetric-block and reduction arrays (count and bytes),
+ * digest[23..25] the scratch size, the particle interactions and the near
+ * pairs.  Identical whether prcmpt built the lists on the GPU or on the
+ * host. */
+int defmm_near_digest(const defmm_handle* h, uint64_t digest[26]);
+
 /* No counterpart in the reference.  Order-selection network (learned.py):
  * a perceptron DEFMM_MLP_IN -> DEFMM_MLP_HIDDEN -> DEFMM_MLP_HIDDEN ->
  * DEFMM_MLP_OUT (ReLU, ReLU, logits over interpolation orders 3..8) that

@@ -1,10 +1,12 @@
 """The plan's octree build and level walk on the GPU (plan_device.cu: the
 particles ordered level by level with octant codes, counts and a stable
-radix sort; the dual traversal with the M2M/L2L transfer lists; the transfer
-spectra and signatures) against the host build and walk (plan.cpp, itself
+radix sort; the dual traversal with the M2M/L2L transfer lists; the
+near-field chunks, symmetric blocks and work items; the transfer spectra and
+signatures) against the host build and walk (plan.cpp, itself
 pinned to the reference's trees, cones and lists by tests/test_plan.py):
 same statistics, same effective directions per cell (the cell-array dump,
-which carries the slots' directions), and a bit-identical FP64 matvec, which
+which carries the slots' directions), fingerprints of every near-field work
+list, and a bit-identical FP64 matvec, which
 needs identical slots, far entries, transfer lists and tables in identical
 order.
 """
@@ -36,6 +38,8 @@ def compare(src, trg, q, L, ncrit, kappa, lvmax):
     assert H.info("tree_device") == 0 and D.info("tree_device") == 1
     for k in STATS:
         assert H.info(k) == D.info(k), k
+    # near-field lists built on the device, element for element the host's
+    assert np.array_equal(H.near_digest(), D.near_digest())
     for which in ("T", "S"):
         for a, b in zip(H.tree(which), D.tree(which)):
             assert np.array_equal(a, b)

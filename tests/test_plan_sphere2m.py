@@ -69,9 +69,12 @@ def test_sphere2m_device_walk_is_bit_exact(gpu):
     for tag in "TS":
         assert digest(*D.tree(tag)) == m[f"tree_{tag}"], tag
     dptr, dsrc, dtab = D.m2l_entries()
+    dnear = D.near_digest()
     del D
     H = build(False, False)
     assert H.info("plan_walk_device") == 0
+    # near-field chunks, symmetric blocks, reduction rows and work items
+    assert np.array_equal(dnear, H.near_digest())
     hptr, hsrc, htab = H.m2l_entries()
     assert np.array_equal(dptr, hptr)
     assert np.array_equal(dsrc, hsrc)
