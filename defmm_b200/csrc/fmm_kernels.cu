@@ -857,6 +857,80 @@ __device__ __forceinline__ void m2l_f2l(const typename cpx_t<T>::type* acc, type
   }
 }
 
+// The same for the RB spectra of one target slot at once (acc[k RB + b]: the
+// K values of right-hand side b), their local expansions at Lt + b LL: each
+// axis pass runs over the lines of all RB spectra, so the CTA's threads stay
+// busy and the transform takes three barriers instead of 3 RB.  Every
+// output is computed by the operations of m2l_f2l for its spectrum.
+template <typename T, int L, int NT, int RB>
+__device__ __forceinline__ void m2l_f2l_rhs(const typename cpx_t<T>::type* acc, typename cpx_t<T>::type* Js,
+                                            typename cpx_t<T>::type* Cb, typename cpx_t<T>::type* D,
+                                            typename cpx_t<T>::type* __restrict__ Lt) {
+  typedef typename cpx_t<T>::type C;
+  constexpr int PD = 2 * L - 1, PP = PD * PD * PD, K = (PP + NT - 1) / NT, LL = L * L * L;
+  constexpr int NB = L * PD * PD, ND = L * L * PD;  // per spectrum: Cb, D elements
+  const T inv = T(1) / T(PP);
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    const int i = threadIdx.x + k * NT;
+    if (i < PP)
+#pragma unroll
+      for (int b = 0; b < RB; b++) Js[b * PP + i] = acc[k * RB + b];
+  }
+  __syncthreads();
+  for (int x = threadIdx.x; x < RB * PD * PD; x += NT) {  // axis 0: (k1,k2) lines -> a
+    const int b = x / (PD * PD), ln = x % (PD * PD);
+    const C* J = Js + b * PP;
+    C* Cq = Cb + b * NB;
+    C v[PD];
+#pragma unroll
+    for (int k0 = 0; k0 < PD; k0++) v[k0] = J[k0 * PD * PD + ln];
+#pragma unroll
+    for (int a = 0; a < L; a++) {
+      C s = v[0];
+#pragma unroll
+      for (int k0 = 1; k0 < PD; k0++) cfmac(s, v[k0], ctw<T, L>((k0 * a) % PD));
+      Cq[a * PD * PD + ln] = s;
+    }
+  }
+  __syncthreads();
+  for (int x = threadIdx.x; x < RB * L * PD; x += NT) {  // axis 1: (a,k2) lines -> b
+    const int r = x / (L * PD), ln = x % (L * PD);
+    const int a = ln / PD, k2 = ln % PD;
+    const C* Cq = Cb + r * NB;
+    C* Dq = D + r * ND;
+    C v[PD];
+#pragma unroll
+    for (int k1 = 0; k1 < PD; k1++) v[k1] = Cq[(a * PD + k1) * PD + k2];
+#pragma unroll
+    for (int b = 0; b < L; b++) {
+      C s = v[0];
+#pragma unroll
+      for (int k1 = 1; k1 < PD; k1++) cfmac(s, v[k1], ctw<T, L>((k1 * b) % PD));
+      Dq[(a * L + b) * PD + k2] = s;
+    }
+  }
+  __syncthreads();
+  for (int x = threadIdx.x; x < RB * L * L; x += NT) {  // axis 2: (a,b) lines -> c
+    const int r = x / (L * L), ln = x % (L * L);
+    const C* Dq = D + r * ND;
+    C* Lq = Lt + r * LL;
+    C v[PD];
+#pragma unroll
+    for (int k2 = 0; k2 < PD; k2++) v[k2] = Dq[ln * PD + k2];
+#pragma unroll
+    for (int c = 0; c < L; c++) {
+      C s = v[0];
+#pragma unroll
+      for (int k2 = 1; k2 < PD; k2++) cfmac(s, v[k2], ctw<T, L>((k2 * c) % PD));
+      C o = Lq[ln * L + c];
+      o.x += s.x * inv;
+      o.y += s.y * inv;
+      Lq[ln * L + c] = o;
+    }
+  }
+}
+
 // One CTA per target slot of a cone batch (M2L.hpp:115-157 target-stationary,
 // then the inverse DFT above):
 //   J[i] = sum_{(s, k) in list(t)} U_k[i] F_s[i]          (registers)
@@ -994,6 +1068,14 @@ template <typename T, int NT, int RB>
 constexpr int m2l_rhs_ctas() {
   return (sizeof(T) == 8 ? (RB >= 8 ? 512 : (RB >= 2 ? 768 : 1024)) : (RB >= 8 ? 768 : 1024)) / NT;
 }
+// FP32, orders <= 5, up to 4 right-hand sides per CTA: the inverse DFTs of
+// a target slot's RB spectra run together (m2l_f2l_rhs, RB workspaces in
+// shared memory, 43.5 KB at order 5, so 4 CTAs per SM still fit);
+// otherwise one after another
+template <typename T, int L, int RB>
+__host__ __device__ constexpr bool m2l_rhs_joint() {
+  return sizeof(T) == 4 && L <= 5 && RB > 1 && RB <= 4;
+}
 
 template <typename T, int L, int NT, int RB>
 __global__ void __launch_bounds__(NT, m2l_rhs_ctas<T, NT, RB>()) k_m2l_rhs(DevPlan P, int64_t t0, int64_t t1, int64_t f0, int64_t f1, int R,
@@ -1003,10 +1085,12 @@ __global__ void __launch_bounds__(NT, m2l_rhs_ctas<T, NT, RB>()) k_m2l_rhs(DevPl
                                                              unsigned long long* __restrict__ queue) {
   typedef typename cpx_t<T>::type C;
   constexpr int PD = 2 * L - 1, LL = L * L * L, PP = PD * PD * PD, K = (PP + NT - 1) / NT;
+  constexpr bool JOINT = m2l_rhs_joint<T, L, RB>();
+  constexpr int MS = JOINT ? RB : 1;  // inverse-DFT workspaces
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* Js = reinterpret_cast<C*>(smem_raw);
-  C* Cb = Js + PP;
-  C* D = Cb + L * PD * PD;
+  C* Cb = Js + MS * PP;
+  C* D = Cb + MS * L * PD * PD;
   __shared__ int64_t cur;
   const int nb = R / RB;
   const int64_t nwork = (t1 - t0) * nb;
@@ -1042,12 +1126,16 @@ __global__ void __launch_bounds__(NT, m2l_rhs_ctas<T, NT, RB>()) k_m2l_rhs(DevPl
         }
       }
     }
+    if constexpr (JOINT) {
+      m2l_f2l_rhs<T, L, NT, RB>(&acc[0][0], Js, Cb, D, Lx + (t * R + r0) * LL);
+    } else {
 #pragma unroll
-    for (int b = 0; b < RB; b++) {
-      C a[K];
+      for (int b = 0; b < RB; b++) {
+        C a[K];
 #pragma unroll
-      for (int k = 0; k < K; k++) a[k] = acc[k][b];
-      m2l_f2l<T, L, NT>(a, Js, Cb, D, Lx + (t * R + r0 + b) * LL);
+        for (int k = 0; k < K; k++) a[k] = acc[k][b];
+        m2l_f2l<T, L, NT>(a, Js, Cb, D, Lx + (t * R + r0 + b) * LL);
+      }
     }
   }
 }
@@ -2434,6 +2522,8 @@ struct Launch {
   static constexpr int NT = PP > 1024 ? 256 : 128;
   static size_t smem_m2f() { return sizeof(C) * M2FCfg<T, L>::PER_WARP * M2FCfg<T, L>::NW; }
   static size_t smem_m2l() { return sizeof(C) * (PP + L * P * P + L * L * P); }
+  template <int RB>
+  static size_t smem_m2l_rhs() { return (m2l_rhs_joint<T, L, RB>() ? RB : 1) * smem_m2l(); }
   static cudaError_t setup(const double* mats) {
     cudaError_t e0 = upload_tables(L, mats);
     if (e0 != cudaSuccess) return e0;
@@ -2463,7 +2553,8 @@ struct Launch {
   static cudaError_t rhs_attr() {
     if (RB > kMaxRB) return cudaSuccess;
     return cudaFuncSetAttribute(k_m2l_rhs<T, L, NT, (RB <= kMaxRB ? RB : 1)>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_m2l());
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem_m2l_rhs<(RB <= kMaxRB ? RB : 1)>());
   }
   template <int RB, int NT>
   static void m2l_rhs_go(const DevPlan& dp, int64_t t0, int64_t t1, int64_t f0, int64_t f1, int R, const void* F,
@@ -2471,7 +2562,7 @@ struct Launch {
     constexpr int RBE = RB <= kMaxRB ? RB : 1;
     const int64_t nwork = (t1 - t0) * (R / RBE);
     const int grid = (int)std::min<int64_t>(nwork, (int64_t)nsm * m2l_rhs_ctas<T, NT, RBE>());
-    k_m2l_rhs<T, L, NT, RBE><<<grid, NT, smem_m2l(), s>>>(dp, t0, t1, f0, f1, R, (const C*)F, (const C*)ptab,
+    k_m2l_rhs<T, L, NT, RBE><<<grid, NT, smem_m2l_rhs<RBE>(), s>>>(dp, t0, t1, f0, f1, R, (const C*)F, (const C*)ptab,
                                                           (C*)Lx, queue);
   }
   // the shared-memory-staged kernel: FP32, orders 3-6
