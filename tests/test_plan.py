@@ -54,6 +54,26 @@ def test_plan_matches_oracle_random(seed, wl, L, ncrit):
         assert np.array_equal(sort_rows(a), sort_rows(b))
 
 
+@pytest.mark.parametrize("same", [True, False])
+def test_near_digest_counts_and_determinism(same):
+    # the fingerprints of the near-field work lists (defmm_near_digest, the
+    # host build here): its counts are the plan's, and a rebuild repeats
+    # every array; distinct targets have no symmetric blocks (empty arrays)
+    pts = W.sphere_surface(8000, seed=5, wavelengths=6).points
+    trg = pts if same else W.sphere_surface(7000, seed=6, wavelengths=6).points * 0.9
+    kappa = 2 * np.pi * 3
+    A = plan(pts, trg, 4, 32, kappa, lists=False)
+    B = plan(pts, trg, 4, 32, kappa, lists=False)
+    da, db = A.near_digest(), B.near_digest()
+    assert np.array_equal(da, db)
+    assert int(da[25]) == A.info("near") and int(da[24]) == A.info("i_near")
+    empty = 1469598103934665603  # FNV-1a of a zero count (8 zero bytes) and no elements
+    for _ in range(8):
+        empty = (empty * 1099511628211) % (1 << 64)
+    for k in range(8, 23):  # own-leaf, symmetric and reduction arrays
+        assert (int(da[k]) == empty) == (not same), k
+
+
 def test_cones_use_first_pair_in_depth_first_order():
     # a lattice: many pairs share a translation; cones must be the ones of
     # the first pair in the reference's traversal (M2L.hpp:189-197)
