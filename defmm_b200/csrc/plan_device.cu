@@ -839,9 +839,23 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
     }
     lv_near.clear();
     p.n_near = nn;
-    if ((st = device_near_lists(p, all_near, nn, err))) return st;
+    st = device_near_lists(p, all_near, nn, err);
+    if (st == -5) {  // beyond device memory or 32-bit sort sizes: the host builds the lists
+      std::vector<int2> near_h((size_t)nn);
+      DW_CK(cudaMemcpy(near_h.data(), all_near, (size_t)nn * sizeof(int2), cudaMemcpyDeviceToHost));
+      walk.near_pairs.resize(near_h.size());
+      for (size_t i = 0; i < near_h.size(); i++) walk.near_pairs[i] = {near_h[i].x, near_h[i].y};
+      p.nd = Plan::NearOnDevice();
+      p.i_near = 0;
+      p.sym_scratch = 0;
+      err.clear();
+      st = 0;
+    } else if (st) {
+      return st;
+    } else {
+      walk.near_done = true;
+    }
     A.drop(all_near);
-    walk.near_done = true;
     p.step("walk: near-field lists (ranges, chunks, symmetric blocks, work items)", tn0);
   }
 

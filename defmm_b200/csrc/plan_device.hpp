@@ -23,7 +23,9 @@ int device_plan_tables(const Plan& p, double2* tables, double2* sig, double2* si
 // The near-field lists (Plan::nd) from the level walk's near pairs on the
 // device (npair (target cell, source cell) pairs in walk order), with the
 // host build's contents and order; also sets i_near and sym_scratch.
-// 0, -4 (CUDA error) or -5 (out of memory) with err set.
+// 0, -4 (CUDA error) or -5 (out of device memory, or more than 2^31 ranges
+// or scratch rows for the 32-bit sorts: the device walk then leaves the
+// lists to the host build) with err set.
 int device_near_lists(Plan& p, const int2* d_near, int64_t npair, std::string& err);
 // FP64 -> FP32 complex, rounded to nearest.
 void tables_to_float(const double2* in, float2* out, int64_t n, cudaStream_t s);
