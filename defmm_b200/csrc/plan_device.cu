@@ -502,6 +502,15 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
 
   // near pairs per level, kept on the device for the near-field lists
   std::vector<std::pair<int2*, int64_t>> lv_near;
+  // each level's slots (cell, direction; no direction array: LF, -1) on the
+  // device, copied to the host slot arrays once all levels are known
+  struct SlotSeg {
+    Slots* sl;
+    int64_t off, n;
+    const int32_t* cell;
+    const int32_t* dir;
+  };
+  std::vector<SlotSeg> slot_segs;
   int64_t table_count = 0;
   // every level's slots stay on the device until the M2M / L2L transfer
   // lists are built after the walk
@@ -638,11 +647,8 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
       if (!v.isHF[l]) {  // one LF expansion per cell
         sl.cone_begin[l] = {sl.n, sl.n + nc};
         std::vector<int32_t> dh(nc);
-        for (int64_t i = 0; i < nc; i++) {
-          sl.cell.push_back(cells[i]);
-          sl.dir.push_back(-1);
-          dh[i] = (int32_t)(sl.n + i);
-        }
+        for (int64_t i = 0; i < nc; i++) dh[i] = (int32_t)(sl.n + i);
+        slot_segs.push_back({&sl, sl.n, nc, dcells, nullptr});  // cells in slot order, direction -1
         const int32_t* dd = nullptr;
         int s2 = upload_vec(A, dh, &dd, err);
         if (s2) return s2;
@@ -680,11 +686,7 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
       sl.cone_begin[l].assign(nd + 1, 0);
       for (int d = 0; d < nd; d++) sl.cone_begin[l][d] = sl.n + ph[d];
       sl.cone_begin[l][nd] = sl.n + cnt;
-      const size_t o = sl.cell.size();
-      sl.cell.resize(o + cnt);
-      sl.dir.resize(o + cnt);
-      DW_CK(cudaMemcpy(sl.cell.data() + o, scell, (size_t)cnt * sizeof(int32_t), cudaMemcpyDeviceToHost));
-      DW_CK(cudaMemcpy(sl.dir.data() + o, sdir, (size_t)cnt * sizeof(int32_t), cudaMemcpyDeviceToHost));
+      slot_segs.push_back({&sl, sl.n, (int64_t)cnt, scell, sdir});
       A.drop(fl);
       A.drop(pos);
       cur.n = cnt;
@@ -750,6 +752,22 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
     if (prevS) A.drop(prevS);
     prevT = effT;
     prevS = effS;
+  }
+  {  // the slots' cells and directions to the host: arrays sized once, one copy per level
+    const double tc = wall_seconds();
+    for (Slots* sl : {&p.sT, &p.sS}) {
+      sl->cell.resize(sl->n);
+      sl->dir.resize(sl->n);
+    }
+    for (const SlotSeg& g : slot_segs) {
+      if (g.n == 0) continue;
+      DW_CK(cudaMemcpy(g.sl->cell.data() + g.off, g.cell, (size_t)g.n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+      if (g.dir)
+        DW_CK(cudaMemcpy(g.sl->dir.data() + g.off, g.dir, (size_t)g.n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+      else
+        std::fill(g.sl->dir.begin() + g.off, g.sl->dir.begin() + g.off + g.n, -1);
+    }
+    t_sub[2] += wall_seconds() - tc;
   }
   // M2M lists of every source slot (children: the next level) and L2L lists
   // of every target slot (parents: the previous level), counted per level
