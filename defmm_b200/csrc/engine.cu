@@ -292,10 +292,18 @@ int upload_plan(defmm_handle* h) {
   UP(p.sT.dir, d.sT_dir);
   UP(p.sS.cell_ptr, d.S_cptr);
   UP(p.sT.cell_ptr, d.T_cptr);
-  UP(to_i32(p.sS.cell_slots), d.S_cslot);
-  UP(p.sS.cell_dirs, d.S_cdir);
-  UP(to_i32(p.sT.cell_slots), d.T_cslot);
-  UP(p.sT.cell_dirs, d.T_cdir);
+  if (p.dev_cslot_S) {  // built on the device by prcmpt
+    d.S_cslot = static_cast<const int32_t*>(p.dev_cslot_S);
+    d.S_cdir = static_cast<const int32_t*>(p.dev_cdir_S);
+    d.T_cslot = static_cast<const int32_t*>(p.dev_cslot_T);
+    d.T_cdir = static_cast<const int32_t*>(p.dev_cdir_T);
+    h->dev_bytes += (size_t)(p.sS.n + p.sT.n) * 8;
+  } else {
+    UP(to_i32(p.sS.cell_slots), d.S_cslot);
+    UP(p.sS.cell_dirs, d.S_cdir);
+    UP(to_i32(p.sT.cell_slots), d.T_cslot);
+    UP(p.sT.cell_dirs, d.T_cdir);
+  }
   if (p.dev_m2m_ptr) {  // built on the device by prcmpt
     d.m2m_ptr = static_cast<const int64_t*>(p.dev_m2m_ptr);
     d.m2m_child = static_cast<const int32_t*>(p.dev_m2m_child);
@@ -1595,7 +1603,8 @@ int defmm_prcmpt(defmm_handle* h, int L, int Ncrit, double kappa, int lvMAX) {
   // arrays the walk left on the device belong to this handle's plan (also
   // when the build failed part way)
   for (void* q : {h->plan.dev_m2l_src, h->plan.dev_m2l_tab, h->plan.dev_m2m_ptr, h->plan.dev_m2m_child,
-                  h->plan.dev_l2l_ptr, h->plan.dev_l2l_parent})
+                  h->plan.dev_l2l_ptr, h->plan.dev_l2l_parent, h->plan.dev_cslot_T, h->plan.dev_cdir_T,
+                  h->plan.dev_cslot_S, h->plan.dev_cdir_S})
     if (q) h->plan_allocs.push_back(q);
   h->plan_allocs.insert(h->plan_allocs.end(), h->plan.dev_near_allocs.begin(), h->plan.dev_near_allocs.end());
   h->plan.dev_near_allocs.clear();

@@ -1193,9 +1193,11 @@ int build_plan(Plan& p, const double* src, int64_t ns, const double* trg,
                   s.cell_slots[pos] = k;
                 });
   };
-  cell_csr(p.T, p.sT);
-  cell_csr(p.S, p.sS);
-  p.step("slots per cell", ts);
+  if (!w.cells_done) {
+    cell_csr(p.T, p.sT);
+    cell_csr(p.S, p.sS);
+    p.step("slots per cell", ts);
+  }
 
   // M2L grouped by target slot, each slot's entries by increasing source
   // slot (so that consecutive target slots can be merged on their common

@@ -115,6 +115,10 @@ struct Plan {
   // (n_m2m / n_l2l); m2m_ptr, m2m_child, l2l_ptr, l2l_parent stay empty.
   void *dev_m2m_ptr = nullptr, *dev_m2m_child = nullptr, *dev_l2l_ptr = nullptr, *dev_l2l_parent = nullptr;
   int64_t n_m2m = 0, n_l2l = 0;
+  // Per-cell slot lists built by the device walk: int32 slot ids and
+  // directions in Slots::cell_ptr order, left on the device (sT / sS keep
+  // cell_ptr and cell_dirs on the host, cell_slots stays empty)
+  void *dev_cslot_T = nullptr, *dev_cdir_T = nullptr, *dev_cslot_S = nullptr, *dev_cdir_S = nullptr;
   // M2M children of each source slot, L2L parents of each target slot
   std::vector<int64_t> m2m_ptr;            // sS.n + 1
   std::vector<int32_t> m2m_child;          // child slot
@@ -218,6 +222,9 @@ struct LevelWalk {
   // Set by a walker that also built the M2M / L2L transfer lists (on the
   // device: Plan::dev_m2m_ptr etc.).
   bool transfers_done = false;
+  // Set by a walker that also built the per-cell slot lists (cell_ptr and
+  // cell_dirs on the host, slot ids on the device: Plan::dev_cslot_T etc.).
+  bool cells_done = false;
   // Set by a walker that also built the near-field lists (on the device:
   // Plan::nd, with Plan::n_near and i_near); near_pairs then stays empty.
   bool near_done = false;

@@ -516,6 +516,7 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
   // lists are built after the walk
   std::vector<LvlSlots> lvS(nlvl), lvT(nlvl);
   double t_transfers = 0;  // wall time of the transfer lists
+  double t_cells = 0;      // wall time of the per-cell slot lists
   double t_sub[4] = {0, 0, 0, 0};  // per sub-step of the level loop
   auto release_lvl = [&](LvlSlots& x) {
     for (void* q : x.own)
@@ -769,6 +770,72 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
     }
     t_sub[2] += wall_seconds() - tc;
   }
+  // per-cell slot lists (each cell's slots in slot order, so its directions
+  // increase): a stable radix sort of all slots by cell.  The slot ids and
+  // directions stay on the device; the pointers and directions also go to
+  // the host (cell_slots stays empty there)
+  if (p.sT.n < ((int64_t)1 << 31) - 1 && p.sS.n < ((int64_t)1 << 31) - 1) {
+    const double tc = wall_seconds();
+    auto csr = [&](Slots& sl, const Tree& tr, void** dslot, void** ddir) -> int {
+      const int64_t n = sl.n, nc = tr.ncell;
+      int32_t *cell, *dir, *idx, *keys, *cnt;
+      int64_t* ptr;
+      DW_ALLOC(cell, int32_t, n);
+      DW_ALLOC(dir, int32_t, n);
+      DW_ALLOC(idx, int32_t, n);
+      DW_ALLOC(keys, int32_t, n);
+      DW_ALLOC(cnt, int32_t, nc + 1);
+      DW_ALLOC(ptr, int64_t, nc + 1);
+      for (void** q : {dslot, ddir})
+        if (cudaMalloc(q, std::max<int64_t>(1, n) * sizeof(int32_t)) != cudaSuccess) {  // handed to the plan's owner
+          cudaGetLastError();
+          *q = nullptr;
+          err = "device plan: out of device memory";
+          return -5;
+        }
+      int32_t* cslot = static_cast<int32_t*>(*dslot);
+      int32_t* cdir = static_cast<int32_t*>(*ddir);
+      for (const SlotSeg& g : slot_segs) {
+        if (g.sl != &sl || g.n == 0) continue;
+        DW_CK(cudaMemcpy(cell + g.off, g.cell, (size_t)g.n * sizeof(int32_t), cudaMemcpyDeviceToDevice));
+        if (g.dir)
+          DW_CK(cudaMemcpy(dir + g.off, g.dir, (size_t)g.n * sizeof(int32_t), cudaMemcpyDeviceToDevice));
+        else
+          DW_CK(cudaMemset(dir + g.off, 0xff, (size_t)g.n * sizeof(int32_t)));  // -1
+      }
+      DW_CK(cudaMemset(cnt, 0, (nc + 1) * sizeof(int32_t)));
+      if (n) {
+        k_iota<<<nblk(n), 256>>>(n, idx);
+        k_count<<<nblk(n), 256>>>(n, cell, cnt);
+        int bits = 1;
+        while (bits < 31 && ((int64_t)1 << bits) <= nc) bits++;
+        size_t need = 0;
+        DW_CK(cub::DeviceRadixSort::SortPairs(nullptr, need, cell, keys, idx, cslot, (int)n, 0, bits));
+        char* t2 = A.get<char>(need);
+        if (!t2) {
+          err = "device plan: out of device memory";
+          return -5;
+        }
+        DW_CK(cub::DeviceRadixSort::SortPairs(t2, need, cell, keys, idx, cslot, (int)n, 0, bits));
+        A.drop(t2);
+        k_gather_i32<<<nblk(n), 256>>>(n, cslot, dir, cdir);
+        DW_CK(cudaGetLastError());
+      }
+      int st2 = scan(cnt, ptr, nc + 1);
+      if (st2) return st2;
+      sl.cell_ptr.resize(nc + 1);
+      sl.cell_dirs.resize(n);
+      sl.cell_slots.clear();
+      DW_CK(cudaMemcpy(sl.cell_ptr.data(), ptr, (nc + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost));
+      DW_CK(cudaMemcpy(sl.cell_dirs.data(), cdir, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+      for (void* q : {(void*)cell, (void*)dir, (void*)idx, (void*)keys, (void*)cnt, (void*)ptr}) A.drop(q);
+      return 0;
+    };
+    if ((st = csr(p.sT, p.T, &p.dev_cslot_T, &p.dev_cdir_T)) || (st = csr(p.sS, p.S, &p.dev_cslot_S, &p.dev_cdir_S)))
+      return st;
+    walk.cells_done = true;
+    t_cells = wall_seconds() - tc;
+  }
   // M2M lists of every source slot (children: the next level) and L2L lists
   // of every target slot (parents: the previous level), counted per level
   // into one array over all slots, one scan, then filled; left on the device
@@ -834,12 +901,13 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
   p.sT.lvl_begin[nlvl] = p.sT.n;
   p.sS.lvl_begin[nlvl] = p.sS.n;
   p.step("walk: levels, other (allocations, copies)", tstep);
-  p.t_steps.back().second -= t_transfers + t_sub[0] + t_sub[1] + t_sub[2] + t_sub[3];
+  p.t_steps.back().second -= t_transfers + t_cells + t_sub[0] + t_sub[1] + t_sub[2] + t_sub[3];
   p.t_steps.push_back({"walk: levels, pair classification and near pairs", t_sub[0]});
   p.t_steps.push_back({"walk: levels, cones of the far pairs", t_sub[1]});
   p.t_steps.push_back({"walk: levels, effective directions and slots", t_sub[2]});
   p.t_steps.push_back({"walk: levels, far entries", t_sub[3]});
   p.t_steps.push_back({"walk: M2M and L2L transfer lists", t_transfers});
+  if (walk.cells_done) p.t_steps.push_back({"walk: slots per cell (radix sort by cell)", t_cells});
 
   // the near-field work lists from all levels' near pairs (walk order),
   // built and kept on the device
