@@ -286,10 +286,18 @@ int upload_plan(defmm_handle* h) {
   UP(p.T.pos, d.T_pos);
   UP(p.S.perm, d.S_perm);
   UP(p.T.perm, d.T_perm);
-  UP(p.sS.cell, d.sS_cell);
-  UP(p.sS.dir, d.sS_dir);
-  UP(p.sT.cell, d.sT_cell);
-  UP(p.sT.dir, d.sT_dir);
+  if (p.dev_scell_S) {  // built on the device by prcmpt
+    d.sS_cell = static_cast<const int32_t*>(p.dev_scell_S);
+    d.sS_dir = static_cast<const int32_t*>(p.dev_sdir_S);
+    d.sT_cell = static_cast<const int32_t*>(p.dev_scell_T);
+    d.sT_dir = static_cast<const int32_t*>(p.dev_sdir_T);
+    h->dev_bytes += (size_t)(p.sS.n + p.sT.n) * 8;
+  } else {
+    UP(p.sS.cell, d.sS_cell);
+    UP(p.sS.dir, d.sS_dir);
+    UP(p.sT.cell, d.sT_cell);
+    UP(p.sT.dir, d.sT_dir);
+  }
   UP(p.sS.cell_ptr, d.S_cptr);
   UP(p.sT.cell_ptr, d.T_cptr);
   if (p.dev_cslot_S) {  // built on the device by prcmpt
@@ -1604,7 +1612,8 @@ int defmm_prcmpt(defmm_handle* h, int L, int Ncrit, double kappa, int lvMAX) {
   // when the build failed part way)
   for (void* q : {h->plan.dev_m2l_src, h->plan.dev_m2l_tab, h->plan.dev_m2m_ptr, h->plan.dev_m2m_child,
                   h->plan.dev_l2l_ptr, h->plan.dev_l2l_parent, h->plan.dev_cslot_T, h->plan.dev_cdir_T,
-                  h->plan.dev_cslot_S, h->plan.dev_cdir_S})
+                  h->plan.dev_cslot_S, h->plan.dev_cdir_S, h->plan.dev_scell_T, h->plan.dev_sdir_T,
+                  h->plan.dev_scell_S, h->plan.dev_sdir_S})
     if (q) h->plan_allocs.push_back(q);
   h->plan_allocs.insert(h->plan_allocs.end(), h->plan.dev_near_allocs.begin(), h->plan.dev_near_allocs.end());
   h->plan.dev_near_allocs.clear();

@@ -117,8 +117,10 @@ struct Plan {
   int64_t n_m2m = 0, n_l2l = 0;
   // Per-cell slot lists built by the device walk: int32 slot ids and
   // directions in Slots::cell_ptr order, left on the device (sT / sS keep
-  // cell_ptr and cell_dirs on the host, cell_slots stays empty)
+  // cell_ptr and cell_dirs on the host, cell_slots stays empty); with them
+  // the slots' own cells and directions (Slots::cell, dir), also on the host
   void *dev_cslot_T = nullptr, *dev_cdir_T = nullptr, *dev_cslot_S = nullptr, *dev_cdir_S = nullptr;
+  void *dev_scell_T = nullptr, *dev_sdir_T = nullptr, *dev_scell_S = nullptr, *dev_sdir_S = nullptr;
   // M2M children of each source slot, L2L parents of each target slot
   std::vector<int64_t> m2m_ptr;            // sS.n + 1
   std::vector<int32_t> m2m_child;          // child slot

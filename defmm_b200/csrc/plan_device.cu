@@ -771,29 +771,30 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
     t_sub[2] += wall_seconds() - tc;
   }
   // per-cell slot lists (each cell's slots in slot order, so its directions
-  // increase): a stable radix sort of all slots by cell.  The slot ids and
-  // directions stay on the device; the pointers and directions also go to
-  // the host (cell_slots stays empty there)
+  // increase): a stable radix sort of all slots by cell.  The slots' cells
+  // and directions and the per-cell slot ids and directions stay on the
+  // device; the pointers and directions also go to the host (cell_slots
+  // stays empty there)
   if (p.sT.n < ((int64_t)1 << 31) - 1 && p.sS.n < ((int64_t)1 << 31) - 1) {
     const double tc = wall_seconds();
-    auto csr = [&](Slots& sl, const Tree& tr, void** dslot, void** ddir) -> int {
+    auto csr = [&](Slots& sl, const Tree& tr, void** dcell, void** ddirs, void** dslot, void** ddir) -> int {
       const int64_t n = sl.n, nc = tr.ncell;
-      int32_t *cell, *dir, *idx, *keys, *cnt;
+      int32_t *idx, *keys, *cnt;
       int64_t* ptr;
-      DW_ALLOC(cell, int32_t, n);
-      DW_ALLOC(dir, int32_t, n);
       DW_ALLOC(idx, int32_t, n);
       DW_ALLOC(keys, int32_t, n);
       DW_ALLOC(cnt, int32_t, nc + 1);
       DW_ALLOC(ptr, int64_t, nc + 1);
-      for (void** q : {dslot, ddir})
+      for (void** q : {dcell, ddirs, dslot, ddir})
         if (cudaMalloc(q, std::max<int64_t>(1, n) * sizeof(int32_t)) != cudaSuccess) {  // handed to the plan's owner
           cudaGetLastError();
           *q = nullptr;
           err = "device plan: out of device memory";
           return -5;
         }
-      int32_t* cslot = static_cast<int32_t*>(*dslot);
+      int32_t* cell = static_cast<int32_t*>(*dcell);  // per slot: cell, direction
+      int32_t* dir = static_cast<int32_t*>(*ddirs);
+      int32_t* cslot = static_cast<int32_t*>(*dslot);  // per cell: slots, directions
       int32_t* cdir = static_cast<int32_t*>(*ddir);
       for (const SlotSeg& g : slot_segs) {
         if (g.sl != &sl || g.n == 0) continue;
@@ -828,10 +829,11 @@ int DeviceWalker::walk(Plan& p, LevelWalk& walk, std::string& err) {
       sl.cell_slots.clear();
       DW_CK(cudaMemcpy(sl.cell_ptr.data(), ptr, (nc + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost));
       DW_CK(cudaMemcpy(sl.cell_dirs.data(), cdir, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost));
-      for (void* q : {(void*)cell, (void*)dir, (void*)idx, (void*)keys, (void*)cnt, (void*)ptr}) A.drop(q);
+      for (void* q : {(void*)idx, (void*)keys, (void*)cnt, (void*)ptr}) A.drop(q);
       return 0;
     };
-    if ((st = csr(p.sT, p.T, &p.dev_cslot_T, &p.dev_cdir_T)) || (st = csr(p.sS, p.S, &p.dev_cslot_S, &p.dev_cdir_S)))
+    if ((st = csr(p.sT, p.T, &p.dev_scell_T, &p.dev_sdir_T, &p.dev_cslot_T, &p.dev_cdir_T)) ||
+        (st = csr(p.sS, p.S, &p.dev_scell_S, &p.dev_sdir_S, &p.dev_cslot_S, &p.dev_cdir_S)))
       return st;
     walk.cells_done = true;
     t_cells = wall_seconds() - tc;
