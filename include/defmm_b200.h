@@ -68,10 +68,11 @@ int defmm_load_inp(defmm_handle* h, const char* path, int64_t nparts, int which)
  * particles, or fixed depth lvMAX when lvMAX >= 0), the frequency regime,
  * cones, interaction lists, expansion slots and transfer spectra.  With a
  * GPU present (defmm_set_plan_device) the octrees' particle ordering (octant
- * codes, counts and a stable radix sort per level) and the level walk (dual
- * traversal, cones, effective directions, slots, far entries) run there, the
- * rest on the host (multi-threaded); the results are the host build's, bit
- * for bit.  2 <= L <= 8. */
+ * codes, counts and a stable radix sort per level), the level walk (dual
+ * traversal, cones, effective directions, slots, far entries), the M2M/L2L
+ * transfer lists, the per-cell slot lists and the near-field work lists run
+ * there (and the transfer spectra and signatures at upload), the cells on the
+ * host; the results are the host build's, bit for bit.  2 <= L <= 8. */
 int defmm_prcmpt(defmm_handle* h, int L, int Ncrit, double kappa, int lvMAX);
 
 /* Copy the plan to the current CUDA device (done by the first gemv when not
@@ -259,8 +260,9 @@ int defmm_keep_lists(defmm_handle* h, int on);
 
 /* No counterpart in the reference (its precomputation is host-only).  on != 0
  * (the default): prcmpt runs the level walk of the plan — dual traversal,
- * cones, effective directions, slots, far-field entries — on the GPU when one
- * is present, with results identical to the host walk; on == 0: always on
+ * cones, effective directions, slots, far-field entries — and the lists built
+ * from it (transfer, per-cell slot and near-field lists) on the GPU when one
+ * is present, with results identical to the host build; on == 0: always on
  * the host.  List records (defmm_keep_lists) always come from the host walk. */
 int defmm_set_plan_device(defmm_handle* h, int on);
 
