@@ -239,13 +239,15 @@ def test_grouped_layout_matches_oracle(name, gpu):
         assert rel(A.matvec(q), p) <= MIXED_TOL
 
 
-def test_rhs_blocks_do_not_change_any_right_hand_side(gpu):
+@pytest.mark.parametrize("name", ["sphere_l6", "cube20k"])
+def test_rhs_blocks_do_not_change_any_right_hand_side(name, gpu):
     # with the same direction groups, every right-hand side gets the same
     # bits whatever the block size of the pass (1, 2 or 4 of 5 vectors; the
-    # last block partly filled) and however many share an M2L CTA; the
-    # near-field, M2L and transfer arithmetic of one right-hand side does not
-    # depend on its neighbours
-    src, trg, q, L, ncrit, kappa, lvmax = case_inputs("sphere_l6")
+    # last block partly filled) and however many share an M2L CTA (at order
+    # 5 the inverse DFTs of a CTA's right-hand sides run as one transform);
+    # the near-field, M2L and transfer arithmetic of one right-hand side does
+    # not depend on its neighbours
+    src, trg, q, L, ncrit, kappa, lvmax = case_inputs(name)
     A = make(src, trg, L, ncrit, kappa, lvmax)
     rng = np.random.default_rng(5)
     Q = (rng.uniform(-1, 1, (5, len(src))) + 1j * rng.uniform(-1, 1, (5, len(src)))).astype(np.complex128)
@@ -253,7 +255,7 @@ def test_rhs_blocks_do_not_change_any_right_hand_side(gpu):
         A.set_precision(prec)
         A.set_blocking(1, 4)
         ref = np.stack([A.matvec(Q[r]) for r in range(5)])
-        assert A.info("groups") >= 3
+        assert A.info("groups") >= (3 if name == "sphere_l6" else 1)
         for rb in (2, 4):
             for per_cta in (1, 2, 4, 8):
                 A.set_blocking(rb, 4)
