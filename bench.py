@@ -416,7 +416,7 @@ def run_mixture(args, torch):
     the interpolation order (falling back to the fixed order 6 when it is not
     confident below order 8); the mixed-precision matvec at that order runs
     on whichever layout fits (the grouped layout when every expansion does
-    not), and FP64 direct sums at 2,000 seeded targets judge every result.
+    not), and FP64 direct sums at 2,000 seeded targets check every result.
     The plain FP64 path at the fixed order 6 is timed beside it."""
     from defmm_b200 import DefmmError, IBFMM_Mat, workloads as W
     from defmm_b200.learned import OrderModel

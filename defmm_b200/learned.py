@@ -13,7 +13,7 @@ the GPU with the library's own kernels (``defmm_mlp_*``: FP32 forward,
 backward and Adam); ``OrderModel.choose`` runs the BF16 inference kernel and
 falls back to the fixed order whenever the predicted probability of meeting
 the tolerance is below ``confidence`` at every order below 8.  Every matvec
-run at a chosen order can be judged by ``defmm_check_full``.
+run at a chosen order can be checked by ``defmm_check_full``.
 
     python -m defmm_b200.learned generate --out sweep.npz --problems 300
     python -m defmm_b200.learned train --data sweep.npz --out order_mlp.npz

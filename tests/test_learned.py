@@ -2,7 +2,7 @@
 forward, backward, Adam and BF16 inference kernels against the numpy oracle
 (oracle/mlp_ref.py); the oracle's gradient against finite differences; the
 committed network on the held-out problems of the committed order sweep,
-and one matvec at a chosen order judged by FP64 direct sums."""
+and one matvec at a chosen order checked by FP64 direct sums."""
 import ctypes
 import math
 import os
@@ -214,7 +214,7 @@ def test_committed_network_beats_the_fixed_order_at_tight_tolerances(gpu):
 
 
 @pytest.mark.gpu
-def test_chosen_order_is_judged_by_direct_sums(gpu):
+def test_chosen_order_is_checked_by_direct_sums(gpu):
     """One fresh problem (not in the sweep): the network's order for 1e-3,
     run and checked against FP64 direct sums at 2,000 targets."""
     from defmm_b200 import IBFMM_Mat, workloads as W
