@@ -412,7 +412,7 @@ struct Sep {
 constexpr int kXferWarps = 4;  // warps (transfers in flight) per CTA
 
 template <typename T, int L>
-__global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 4 ? 6 : (L == 5 ? 5 : 3)) : (L <= 5 ? 3 : 1)) k_m2m(DevPlan P, int64_t s0, int64_t s1,
+__global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 5 ? 6 : 3) : (L <= 5 ? 3 : 1)) k_m2m(DevPlan P, int64_t s0, int64_t s1,
                                                          const typename cpx_t<T>::type* __restrict__ sig,
                                                          const typename cpx_t<T>::type* __restrict__ sig2,
                                                          typename cpx_t<T>::type* __restrict__ Mp,
