@@ -544,7 +544,7 @@ __global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 5 ? 6 
 // Lc + (slot R + r) LL, parents at Lp0 + (slot R + r) LL.  Only
 // parent slots in [p0, p1) contribute (a pass over part of the directions).
 template <typename T, int L>
-__global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 5 ? 6 : 3) : (L <= 5 ? 3 : 1)) k_l2l(DevPlan P, int64_t s0, int64_t s1,
+__global__ void __launch_bounds__(32 * kXferWarps, sizeof(T) == 4 ? (L <= 5 ? 6 : 3) : (L <= 5 ? 4 : 1)) k_l2l(DevPlan P, int64_t s0, int64_t s1,
                                                          const typename cpx_t<T>::type* __restrict__ sig,
                                                          const typename cpx_t<T>::type* __restrict__ sig2,
                                                          typename cpx_t<T>::type* __restrict__ Lc,
